@@ -1,0 +1,190 @@
+/*
+ * ttrsvd.h - C ABI of the B200 (sm_100a) TT-SVD / TR-SVD library (libttrsvd.so).
+ *
+ * All matrices are column-major FP32 unless stated otherwise; tensors are column-major
+ * with mode 1 fastest, X(i1..id) at i1 + n1*(i2 + n2*(...)), exactly as the reference's
+ * GPU programs store them.  Every entry point returns a tt_status code; the message of
+ * the last failure on the calling thread is available from tt_last_error().
+ *
+ * Reference interfaces each entry point replaces are cited as file:line relative to the
+ * reference repository (YangletLiu/Tensor_Train_Ring_Decompositions_HPC_GPU).
+ */
+#ifndef TTRSVD_H
+#define TTRSVD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define TTRSVD_ABI_VERSION 1
+#define TT_MAX_ORDER 16
+#define TT_MAX_SMALL 128 /* largest Gram / Jacobi size handled on chip */
+
+/* Status codes.  The reference aborts through assert() on every library status
+ * (e.g. ttdecomposition/high_order_GPUs/ttdec6_singleGPU.cu:826-831); here every failure
+ * is a return code. */
+typedef enum tt_status {
+  TT_OK = 0,
+  TT_ERR_ARG = 1,        /* null pointer, bad flag or option */
+  TT_ERR_SHAPE = 2,      /* order, mode sizes or leading dimensions invalid */
+  TT_ERR_RANK = 3,       /* ranks invalid (r0 != rd for a ring, rank < 1, ...) */
+  TT_ERR_NONFINITE = 4,  /* NaN or Inf found in the input (TT_FLAG_CHECK_FINITE) */
+  TT_ERR_NOMEM = 5,      /* device or pinned allocation failed */
+  TT_ERR_NOCONV = 6,     /* Jacobi eigen-solver did not converge within max_sweeps */
+  TT_ERR_TIMEOUT = 7,    /* a bounded device-side wait ran out */
+  TT_ERR_CUDA = 8,       /* CUDA runtime error */
+  TT_ERR_UNSUPPORTED = 9 /* shape/rank combination outside the implemented range */
+} tt_status;
+
+/* GEMM engine for the two bulk GEMMs (sketch Y = A*W and projection B^T = A^T*Q). */
+enum {
+  TT_GEMM_AUTO = 0, /* tensor cores where the shape allows it */
+  TT_GEMM_TC = 1,   /* tcgen05 TF32 tensor-core tiles fed by TMA, FP32 accumulation in TMEM */
+  TT_GEMM_FP32 = 2  /* plain FP32 FMA (CUDA cores): the "plain FP32" form */
+};
+
+/* Per-unfolding factorisation. */
+enum {
+  TT_METHOD_EDRSVD = 0, /* randomized range finder + small eigen-SVD (basicRandSVD_LU) */
+  TT_METHOD_EXACT = 1   /* exact Gram-eigen step (longMatrixSVD_Eign_once_device); min(m,n) <= TT_MAX_SMALL */
+};
+
+/* Option flags. */
+enum {
+  TT_FLAG_HOST_IO = 1,        /* x and the cores are host pointers (copied in/out inside the call) */
+  TT_FLAG_CHECK_FINITE = 2,   /* scan x for NaN/Inf first and fail with TT_ERR_NONFINITE */
+  TT_FLAG_NO_FOLD = 4,        /* materialise full-rank steps instead of folding their rotation */
+  TT_FLAG_IDENTITY_GAUGE = 8, /* full-rank steps keep the identity basis (no Gram pass) */
+  TT_FLAG_KEEP_SIGMA = 16,    /* fill tt_stats.sigma */
+  TT_FLAG_PROFILE = 32        /* time the bulk passes over the largest unfolding (tt_stats.top_*) */
+};
+
+typedef struct tt_opts {
+  int method;            /* TT_METHOD_* */
+  int gemm;              /* TT_GEMM_* */
+  int oversample;        /* s: sketch width is r + s (reference: s = 8, ablation edrsvd_GPU:347) */
+  int power_iters;       /* p (reference: p = 1) */
+  unsigned long long seed;
+  double eps;            /* relative tolerance; 0 = fixed ranks (the reference accepts eps but ignores it) */
+  int flags;             /* TT_FLAG_* */
+  int max_sweeps;        /* Jacobi sweep limit (0 = default 40) */
+} tt_opts;
+
+#define TT_STATS_MAX_SIGMA 64
+typedef struct tt_stats {
+  double ms;                                   /* device time of the call (CUDA events) */
+  int nsteps;                                  /* unfoldings factorised */
+  int ranks[TT_MAX_ORDER + 1];                 /* ranks used (after clamping / adaptation) */
+  int nsigma[TT_MAX_ORDER];                    /* singular values stored per unfolding */
+  float sigma[TT_MAX_ORDER][TT_STATS_MAX_SIGMA];
+  int jacobi_sweeps;                           /* largest sweep count of any eigen-solve */
+  int kernels;                                 /* kernels launched by the call */
+  double est_rel_err;                          /* reserved (adaptive-rank error estimate) */
+  double flops;                                /* algorithmic FLOPs of the bulk GEMM passes executed */
+  double bytes;                                /* algorithmic HBM bytes of those passes (operands once) */
+  /* TT_FLAG_PROFILE: per pass kind (TT_PASS_*), summed device time (CUDA events on the
+   * context stream around each launch), algorithmic bytes moved and launch count. */
+  double pass_ms[4];
+  double pass_bytes[4];
+  int pass_launches[4];
+} tt_stats;
+
+/* Bulk pass kinds reported in tt_stats.pass_*. */
+enum { TT_PASS_GRAM = 0, TT_PASS_SKETCH = 1, TT_PASS_PROJECT = 2, TT_PASS_OTHER = 3 };
+
+typedef struct tt_ctx tt_ctx;
+
+/* Context: one device, one stream, a growing device workspace.  Not thread-safe per
+ * context; use one context per host thread.  Replaces the per-call cublasCreate /
+ * cusolverDnCreate of the reference (ttdec6_singleGPU.cu:808-815). */
+int tt_ctx_create(tt_ctx** out, int device, void* stream);
+int tt_ctx_destroy(tt_ctx* ctx);
+int tt_ctx_set_stream(tt_ctx* ctx, void* stream);
+int tt_ctx_reserve(tt_ctx* ctx, size_t bytes);
+const char* tt_last_error(void);
+void tt_default_opts(tt_opts* o);
+int tt_abi_version(void);
+
+/* Order-d TT-SVD with fixed ranks r[0..d] (r[0] = r[d] = 1).  cores[k] receives the
+ * column-major (r[k], n[k], r[k+1]) core.  Ranks larger than an unfolding can carry are
+ * zero-padded.  Replaces ttdec_half_lu_device_6 (ttdecomposition/high_order_GPUs/
+ * ttdec6_singleGPU.cu:799) and the order-3 ttdec_gpu_float (ttdecomposition/
+ * third_order_GPUs/opt/ttdec_gpu_float_rsvd_lu_half.cu:778), which discard their cores. */
+int tt_svd(tt_ctx* ctx, const float* x, int d, const int* n, const int* r, const tt_opts* opts,
+           float* const* cores, tt_stats* stats);
+
+/* Order-d TR-SVD with bond ranks r[0..d], r[0] = r[d].  Step 1 factorises unfolding 1 at
+ * rank r0*r1 (zero-padded beyond n1) and permutes (r0, r1, N) -> (r1, N, r0).  cores[k]
+ * receives the column-major (r[k], n[k], r[k+1]) ring core.  Replaces the TR
+ * ttdec_half_lu_device_6 (trdecomposition/high_order_GPUs/trdec6_singleGPU.cu:827) and
+ * trdec_gpu_float (trdecomposition/third_order_GPU/opt_GPU/trdec_gpu_float_rsvd_lu_half.cu:734). */
+int tr_svd(tt_ctx* ctx, const float* x, int d, const int* n, const int* r, const tt_opts* opts,
+           float* const* cores, tt_stats* stats);
+
+/* Relative reconstruction error ||X - TT(cores)||_F / ||X||_F computed on the device with
+ * FP64 accumulation; ring = 1 for TR cores.  Replaces calMSE / norm2HH
+ * (ttdecomposition/high_order_GPUs/ttdec6_singleGPU.cu:122-182), a serial host loop that
+ * also overwrote the input. */
+int tt_rel_error(tt_ctx* ctx, const float* x, int d, const int* n, const int* r, int ring,
+                 const float* const* cores, double* rel_err);
+
+/* ---- building blocks (device pointers, stream-ordered on the context's stream) ---- */
+
+/* Gaussian N(0,1) column-major (rows x cols, leading dim ld) matrix from Philox4x32-10.
+ * Replaces curandGenerateNormal (ttdec_gpu_float_rsvd_lu_half.cu:585-587). */
+int tt_k_gaussian(tt_ctx* ctx, float* out, long long rows, int cols, long long ld,
+                  unsigned long long seed, unsigned stream_id);
+
+/* Sketch Y = A * W: A (m x n, lda = m), W (n x N, ldw), Y (m x N, FP64, ldy = m).
+ * Replaces GemmEx Y = A*Omega / Y = A*Q (ttdec_gpu_float_rsvd_lu_half.cu:601-619,657-675). */
+int tt_k_sketch(tt_ctx* ctx, const float* a, long long m, long long n, const float* w, int N,
+                long long ldw, double* y, int gemm);
+
+/* Projection out = A^T * Q: A (m x n, lda = m), Q (m x N, ldq), out row-major n x N with
+ * row stride ldo (i.e. the column-major N x n matrix Q^T A).  Replaces GemmEx B = Q^T A
+ * and Z = A^T Q (ttdec_gpu_float_rsvd_lu_half.cu:631-649,690-708; ttdec6_singleGPU.cu:424-488). */
+int tt_k_project(tt_ctx* ctx, const float* a, long long m, long long n, const float* q, int N,
+                 long long ldq, float* out, long long ldo, int gemm);
+
+/* Gram of the rows W = A * A^T (m x m, FP64), A (m x n, lda = m), m <= TT_MAX_SMALL.
+ * Replaces largeMatrixSelfMulti_once_device (ttdec6_singleGPU.cu:388-401). */
+int tt_k_gram_rows(tt_ctx* ctx, const float* a, long long m, long long n, double* w);
+
+/* Gram of a tall matrix W = Z^T Z (N x N, FP64): Z is n x N with element (j, c) at
+ * z[j*rs + c*cs] (column-major: rs = 1, cs = ld; row-major: rs = ld, cs = 1). */
+int tt_k_gram_tall(tt_ctx* ctx, const float* z, long long n, int N, long long rs, long long cs,
+                   double* w);
+
+/* CholeskyQR2 in place on a tall FP32 matrix Y (n x N, column-major, ld): Y <- Q, R (N x N,
+ * FP64, upper) optional.  Columns that are numerically dependent are zeroed.  Replaces
+ * basicQR = geqrf + orgqr (ttdec_gpu_float_rsvd_lu_half.cu:85-159). */
+int tt_k_cholqr2(tt_ctx* ctx, float* y, long long n, int N, long long ld, double* r);
+
+/* Symmetric eigen-decomposition of W (N x N, FP64, column-major) by parallel cyclic
+ * Jacobi in shared memory; eigenvalues descending, eigenvectors as columns.  Replaces
+ * cusolverDnSsyevd + matrixInvertColumn (ttdec6_singleGPU.cu:274-290,334-385). */
+int tt_k_syev(tt_ctx* ctx, const double* w, int N, double* evals, double* evecs, int* sweeps);
+
+/* TR bond permute (r0, r1, N) -> (r1, N, r0), column-major.  Replaces tensorToMode231
+ * (trdecomposition/high_order_GPUs/trdec6_singleGPU.cu:49-58). */
+int tt_k_permute231(tt_ctx* ctx, const float* in, float* out, int r0, int r1, long long n);
+
+/* Reference-compatible entry points with pointer arguments (the C++ overloads with the
+ * reference's exact signatures are declared in ttrsvd_ref.h).  Return elapsed seconds
+ * (negative on failure), like the reference. */
+float tt_ref_ttdec_gpu_float(float* h_tensor, int* h_n_array, int* h_r_array, double* eps,
+                             float* single_error, float* single_com_ratio);
+float tt_ref_trdec_gpu_float(float* h_tensor, int* h_n_array, int* h_r_array, double* eps,
+                             float* single_error, float* single_com_ratio);
+float tt_ref_ttdec_half_lu_device_6(float* h_a, const int* tt_ranks, const int* tt_demns,
+                                    int calculate_times, int p, int cal_error);
+float tt_ref_trdec_half_lu_device_6(float* h_a, const int* tt_ranks, const int* tt_demns,
+                                    int calculate_times, int p, int cal_error);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* TTRSVD_H */

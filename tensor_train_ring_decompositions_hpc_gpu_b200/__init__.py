@@ -1,0 +1,341 @@
+"""B200-native TT-SVD / TR-SVD (EDrSVD per unfolding) over the C ABI of libttrsvd.so.
+
+Tensors follow the reference's storage convention: column-major, mode 1 fastest.  Device
+tensors are torch CUDA tensors (torch supplies device memory and the current stream);
+host tensors are NumPy arrays.  Every decomposition runs in the hand-written sm_100a
+kernels of libttrsvd.so; when the library is missing, importing the compute functions
+raises instead of falling back to anything else.
+
+Reference-compatible entry points (same names, argument meaning and return value):
+``ttdec_gpu_float``, ``trdec_gpu_float`` (order 3) and ``ttdec_half_lu_device_6``,
+``trdec_half_lu_device_6`` (order 6).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib
+from ._lib import (TT_FLAG_CHECK_FINITE, TT_FLAG_HOST_IO, TT_FLAG_IDENTITY_GAUGE, TT_FLAG_KEEP_SIGMA,
+                   TT_FLAG_NO_FOLD, TT_GEMM_AUTO, TT_GEMM_FP32, TT_GEMM_TC, TT_METHOD_EDRSVD,
+                   TT_METHOD_EXACT, TTError, check)
+
+__all__ = [
+    "tt_svd", "tr_svd", "rel_error", "Result", "gaussian", "sketch", "project", "gram_rows",
+    "gram_tall", "cholqr2", "syev", "permute231", "ttdec_gpu_float", "trdec_gpu_float",
+    "ttdec_half_lu_device_6", "trdec_half_lu_device_6", "TTError", "lib", "GEMM", "METHOD",
+]
+
+GEMM = {"auto": TT_GEMM_AUTO, "tc": TT_GEMM_TC, "fp32": TT_GEMM_FP32}
+METHOD = {"edrsvd": TT_METHOD_EDRSVD, "exact": TT_METHOD_EXACT}
+
+
+def lib():
+    return _lib.load()
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class _Ctx:
+    def __init__(self, device: int):
+        self.device = device
+        self.ptr = C.c_void_p()
+        check(lib().tt_ctx_create(C.byref(self.ptr), device, None))
+
+    def bind(self, stream_handle):
+        check(lib().tt_ctx_set_stream(self.ptr, C.c_void_p(stream_handle)))
+        return self.ptr
+
+    def __del__(self):
+        try:
+            if self.ptr:
+                lib().tt_ctx_destroy(self.ptr)
+        except Exception:
+            pass
+
+
+_CTX: dict = {}
+
+
+def _ctx_for(device: int | None = None, stream=None):
+    torch = _torch()
+    if device is None:
+        device = torch.cuda.current_device()
+    if device not in _CTX:
+        _CTX[device] = _Ctx(device)
+    ctx = _CTX[device]
+    if stream is None:
+        stream = torch.cuda.current_stream(device)
+    return ctx.bind(stream.cuda_stream)
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _fortran_buffer(x):
+    """Column-major flat device buffer of a torch tensor given in logical index order."""
+    torch = _torch()
+    d = x.dim()
+    buf = x.permute(*reversed(range(d))).contiguous() if d > 1 else x.contiguous()
+    if buf.dtype != torch.float32:
+        buf = buf.float()
+    return buf
+
+
+def _core_view(flat, r0, n, r1):
+    """Logical (r0, n, r1) view of a column-major core buffer."""
+    return flat.view(r1, n, r0).permute(2, 1, 0)
+
+
+@dataclass
+class Result:
+    cores: list
+    ms: float = 0.0
+    sigmas: list = field(default_factory=list)
+    ranks: list = field(default_factory=list)
+    kernels: int = 0
+    jacobi_sweeps: int = 0
+
+
+def _opts(gemm, method, oversample, power_iters, seed, flags, max_sweeps):
+    o = _lib.TTOpts()
+    lib().tt_default_opts(C.byref(o))
+    o.gemm = GEMM[gemm] if isinstance(gemm, str) else int(gemm)
+    o.method = METHOD[method] if isinstance(method, str) else int(method)
+    o.oversample = int(oversample)
+    o.power_iters = int(power_iters)
+    o.seed = int(seed)
+    o.flags = int(flags) | TT_FLAG_KEEP_SIGMA
+    o.max_sweeps = int(max_sweeps)
+    return o
+
+
+def _run(ring: bool, x, ranks, gemm="auto", method="edrsvd", oversample=8, power_iters=0,
+         seed=1234, flags=0, max_sweeps=40, shape=None):
+    ranks = [int(r) for r in ranks]
+    host = isinstance(x, np.ndarray)
+    if host:
+        xa = np.asfortranarray(x, dtype=np.float32)
+        shape = list(xa.shape)
+        d = len(shape)
+        cores_np = [np.zeros((ranks[k], shape[k], ranks[k + 1]), dtype=np.float32, order="F")
+                    for k in range(d)]
+        ptrs = (C.c_void_p * d)(*[c.ctypes.data for c in cores_np])
+        o = _opts(gemm, method, oversample, power_iters, seed, flags | TT_FLAG_HOST_IO, max_sweeps)
+        torch = _torch()
+        ctx = _ctx_for()
+        st = _lib.TTStats()
+        fn = lib().tr_svd if ring else lib().tt_svd
+        check(fn(ctx, C.c_void_p(xa.ctypes.data), d, _lib.int_array(shape), _lib.int_array(ranks),
+                 C.byref(o), ptrs, C.byref(st)))
+        cores = cores_np
+    else:
+        torch = _torch()
+        if shape is None:
+            shape = list(x.shape)
+            buf = _fortran_buffer(x)
+        else:
+            buf = x.reshape(-1)
+        d = len(shape)
+        flat = [torch.empty(ranks[k] * shape[k] * ranks[k + 1], device=buf.device, dtype=torch.float32)
+                for k in range(d)]
+        ptrs = (C.c_void_p * d)(*[t.data_ptr() for t in flat])
+        o = _opts(gemm, method, oversample, power_iters, seed, flags, max_sweeps)
+        ctx = _ctx_for(buf.device.index)
+        st = _lib.TTStats()
+        fn = lib().tr_svd if ring else lib().tt_svd
+        check(fn(ctx, _ptr(buf), d, _lib.int_array(shape), _lib.int_array(ranks), C.byref(o), ptrs,
+                 C.byref(st)))
+        cores = [_core_view(flat[k], ranks[k], shape[k], ranks[k + 1]) for k in range(d)]
+    sig = [np.array(st.sigma[k][: st.nsigma[k]], dtype=np.float64) for k in range(st.nsteps)]
+    return Result(cores=cores, ms=st.ms, sigmas=sig, ranks=list(st.ranks[: len(ranks)]),
+                  kernels=st.kernels, jacobi_sweeps=st.jacobi_sweeps)
+
+
+def tt_svd(x, ranks, **kw) -> Result:
+    """TT-SVD of ``x`` (torch CUDA tensor or NumPy array, logical shape (n1..nd)) at fixed
+    ranks ``[1, r1, ..., r_{d-1}, 1]``.  Keyword options: gemm ('auto' | 'tc' | 'fp32'),
+    method ('edrsvd' | 'exact'), oversample, power_iters, seed, flags, max_sweeps."""
+    return _run(False, x, ranks, **kw)
+
+
+def tr_svd(x, ranks, **kw) -> Result:
+    """TR-SVD of ``x`` with bond ranks ``[r0, r1, ..., r_{d-1}, r0]``."""
+    return _run(True, x, ranks, **kw)
+
+
+def rel_error(x, cores, ring: bool = False) -> float:
+    """||X - TT(cores)||_F / ||X||_F on the device (FP64 accumulation)."""
+    torch = _torch()
+    buf = _fortran_buffer(x)
+    d = x.dim()
+    shape = list(x.shape)
+    ranks = [cores[0].shape[0]] + [c.shape[2] for c in cores]
+    flat = []
+    for c in cores:
+        f = c.permute(2, 1, 0).contiguous().reshape(-1)
+        flat.append(f.float())
+    ptrs = (C.c_void_p * d)(*[t.data_ptr() for t in flat])
+    out = C.c_double()
+    check(lib().tt_rel_error(_ctx_for(buf.device.index), _ptr(buf), d, _lib.int_array(shape),
+                             _lib.int_array(ranks), 1 if ring else 0, ptrs, C.byref(out)))
+    return float(out.value)
+
+
+# ---- building blocks (torch CUDA tensors, column-major matrices as (rows, cols) tensors
+#      whose memory is column-major, i.e. the transpose of a contiguous (cols, rows) tensor) ----
+def _colmajor(rows, cols, dtype, device):
+    torch = _torch()
+    return torch.empty((cols, rows), dtype=dtype, device=device).t()
+
+
+def gaussian(rows: int, cols: int, seed: int, stream_id: int = 0, device=None):
+    """Column-major (rows x cols) N(0,1) matrix from the device Philox generator."""
+    torch = _torch()
+    out = _colmajor(rows, cols, torch.float32, device or torch.device("cuda"))
+    check(lib().tt_k_gaussian(_ctx_for(out.device.index), _ptr(out), rows, cols, rows, seed, stream_id))
+    return out
+
+
+def _as_colmajor(a):
+    """Column-major storage of a 2-D torch tensor (returns a (rows, cols) view with stride (1, rows))."""
+    return a.t().contiguous().t()
+
+
+def sketch(a, w, gemm="auto"):
+    """Y = A W (FP64 result) with A (m x n) and W (n x N) column-major FP32."""
+    torch = _torch()
+    a = _as_colmajor(a.float())
+    w = _as_colmajor(w.float())
+    m, n = a.shape
+    N = w.shape[1]
+    y = _colmajor(m, N, torch.float64, a.device)
+    check(lib().tt_k_sketch(_ctx_for(a.device.index), _ptr(a), m, n, _ptr(w), N, n, _ptr(y), GEMM[gemm]))
+    return y
+
+
+def project(a, q, gemm="auto"):
+    """Q^T A as an (N x n) column-major matrix (stored row-major n x N), A (m x n), Q (m x N)."""
+    torch = _torch()
+    a = _as_colmajor(a.float())
+    q = _as_colmajor(q.float())
+    m, n = a.shape
+    N = q.shape[1]
+    out = torch.empty((n, N), dtype=torch.float32, device=a.device)
+    check(lib().tt_k_project(_ctx_for(a.device.index), _ptr(a), m, n, _ptr(q), N, m, _ptr(out), N,
+                             GEMM[gemm]))
+    return out.t()
+
+
+def gram_rows(a):
+    torch = _torch()
+    a = _as_colmajor(a.float())
+    m, n = a.shape
+    w = _colmajor(m, m, torch.float64, a.device)
+    check(lib().tt_k_gram_rows(_ctx_for(a.device.index), _ptr(a), m, n, _ptr(w)))
+    return w
+
+
+def gram_tall(z):
+    """Z^T Z (FP64) of a column-major tall matrix Z (n x N)."""
+    torch = _torch()
+    z = _as_colmajor(z.float())
+    n, N = z.shape
+    w = _colmajor(N, N, torch.float64, z.device)
+    check(lib().tt_k_gram_tall(_ctx_for(z.device.index), _ptr(z), n, N, 1, n, _ptr(w)))
+    return w
+
+
+def cholqr2(y):
+    """CholeskyQR2 of a tall matrix; returns (Q, R)."""
+    torch = _torch()
+    q = y.float().t().contiguous().clone().t()  # private column-major copy
+    n, N = q.shape
+    r = _colmajor(N, N, torch.float64, q.device)
+    check(lib().tt_k_cholqr2(_ctx_for(q.device.index), _ptr(q), n, N, n, _ptr(r)))
+    return q, r
+
+
+def syev(w):
+    """Eigen-decomposition of a symmetric FP64 matrix (descending); returns (evals, evecs, sweeps)."""
+    torch = _torch()
+    w = _as_colmajor(w.double())
+    N = w.shape[0]
+    ev = torch.empty(N, dtype=torch.float64, device=w.device)
+    vec = _colmajor(N, N, torch.float64, w.device)
+    sw = C.c_int()
+    check(lib().tt_k_syev(_ctx_for(w.device.index), _ptr(w), N, _ptr(ev), _ptr(vec), C.byref(sw)))
+    return ev, vec, sw.value
+
+
+def permute231(x, r0: int, r1: int, n: int):
+    """(r0, r1, n) -> (r1, n, r0) on column-major flat buffers."""
+    torch = _torch()
+    x = x.reshape(-1).float().contiguous()
+    out = torch.empty_like(x)
+    check(lib().tt_k_permute231(_ctx_for(x.device.index), _ptr(x), _ptr(out), r0, r1, n))
+    return out
+
+
+# ---- reference-compatible entry points (host NumPy tensors, column-major) ----
+def _host_f32(h):
+    a = np.asarray(h)
+    if a.dtype != np.float32 or not (a.flags.f_contiguous or a.ndim == 1):
+        a = np.asfortranarray(a, dtype=np.float32)
+    return a
+
+
+def ttdec_gpu_float(h_tensor, h_n_array, h_r_array, eps=None, single_error=None, single_com_ratio=None):
+    """Order-3 TT-SVD; mirrors ttdec_gpu_float (ttdec_gpu_float_rsvd_lu_half.cu:778).
+    Returns elapsed seconds.  ``single_error``/``single_com_ratio``: optional 1-element float32
+    arrays that receive ||X-X^||/||X|| and the compression ratio."""
+    a = _host_f32(h_tensor)
+    e = np.zeros(1, np.float32) if single_error is None else single_error
+    cr = np.zeros(1, np.float32) if single_com_ratio is None else single_com_ratio
+    t = lib().tt_ref_ttdec_gpu_float(
+        C.c_void_p(a.ctypes.data), _lib.int_array(h_n_array), _lib.int_array(h_r_array), None,
+        e.ctypes.data_as(C.POINTER(C.c_float)) if single_error is not None else None,
+        cr.ctypes.data_as(C.POINTER(C.c_float)) if single_com_ratio is not None else None)
+    if t < 0:
+        raise TTError(int(-t), lib().tt_last_error().decode())
+    return float(t)
+
+
+def trdec_gpu_float(h_tensor, h_n_array, h_r_array, eps=None, single_error=None, single_com_ratio=None):
+    """Order-3 TR-SVD; mirrors trdec_gpu_float (trdec_gpu_float_rsvd_lu_half.cu:734)."""
+    a = _host_f32(h_tensor)
+    t = lib().tt_ref_trdec_gpu_float(
+        C.c_void_p(a.ctypes.data), _lib.int_array(h_n_array), _lib.int_array(h_r_array), None,
+        single_error.ctypes.data_as(C.POINTER(C.c_float)) if single_error is not None else None,
+        single_com_ratio.ctypes.data_as(C.POINTER(C.c_float)) if single_com_ratio is not None else None)
+    if t < 0:
+        raise TTError(int(-t), lib().tt_last_error().decode())
+    return float(t)
+
+
+def ttdec_half_lu_device_6(h_A, ttRanks, ttDemns, calculateTimes=1, p=64, calError=False):
+    """Order-6 TT-SVD; mirrors ttdec_half_lu_device_6 (ttdec6_singleGPU.cu:799)."""
+    a = _host_f32(h_A)
+    t = lib().tt_ref_ttdec_half_lu_device_6(C.c_void_p(a.ctypes.data), _lib.int_array(ttRanks),
+                                            _lib.int_array(ttDemns), int(calculateTimes), int(p),
+                                            1 if calError else 0)
+    if t < 0:
+        raise TTError(int(-t), lib().tt_last_error().decode())
+    return float(t)
+
+
+def trdec_half_lu_device_6(h_A, ttRanks, ttDemns, calculateTimes=1, p=64, calError=False):
+    """Order-6 TR-SVD; mirrors the TR ttdec_half_lu_device_6 (trdec6_singleGPU.cu:827)."""
+    a = _host_f32(h_A)
+    t = lib().tt_ref_trdec_half_lu_device_6(C.c_void_p(a.ctypes.data), _lib.int_array(ttRanks),
+                                            _lib.int_array(ttDemns), int(calculateTimes), int(p),
+                                            1 if calError else 0)
+    if t < 0:
+        raise TTError(int(-t), lib().tt_last_error().decode())
+    return float(t)

@@ -1,0 +1,61 @@
+// Shared helpers of the TT/TR-SVD kernels (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+
+#include "ttrsvd.h"
+
+namespace ttr {
+
+// Thread-local error message for tt_last_error().
+void set_error(int code, const char* fmt, ...);
+
+#define TT_TRY(expr)                  \
+  do {                                \
+    int st_ = (expr);                 \
+    if (st_ != TT_OK) return st_;     \
+  } while (0)
+
+#define TT_CUDA(expr)                                                                     \
+  do {                                                                                    \
+    cudaError_t e_ = (expr);                                                              \
+    if (e_ != cudaSuccess) {                                                              \
+      ::ttr::set_error(TT_ERR_CUDA, "%s:%d %s: %s", __FILE__, __LINE__, #expr,            \
+                       cudaGetErrorString(e_));                                           \
+      return TT_ERR_CUDA;                                                                 \
+    }                                                                                     \
+  } while (0)
+
+#define TT_LAUNCH_CHECK()                                                                 \
+  do {                                                                                    \
+    cudaError_t e_ = cudaGetLastError();                                                  \
+    if (e_ != cudaSuccess) {                                                              \
+      ::ttr::set_error(TT_ERR_CUDA, "%s:%d launch: %s", __FILE__, __LINE__,               \
+                       cudaGetErrorString(e_));                                           \
+      return TT_ERR_CUDA;                                                                 \
+    }                                                                                     \
+  } while (0)
+
+// Device status word written by kernels whose work can fail (non-convergence, timeouts).
+struct DevStatus {
+  int code;     // tt_status of the first failure, 0 if none
+  int detail;   // kernel-specific detail (sweeps used, stage index, ...)
+  int sweeps;   // largest Jacobi sweep count seen
+  int pad;
+};
+
+__device__ __forceinline__ void dev_fail(DevStatus* st, int code, int detail) {
+  if (st) {
+    if (atomicCAS(&st->code, 0, code) == 0) st->detail = detail;
+  }
+}
+
+inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
+inline long long ceil_div_ll(long long a, long long b) { return (a + b - 1) / b; }
+
+// Launch-count accounting (kernels launched by the current library call).
+extern thread_local int g_kernel_launches;
+inline void count_launch(int n = 1) { g_kernel_launches += n; }
+
+}  // namespace ttr

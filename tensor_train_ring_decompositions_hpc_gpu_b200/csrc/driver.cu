@@ -1,0 +1,870 @@
+// Host side of the TT-SVD / TR-SVD chain: context, workspace planning, the per-unfolding
+// factorisation (exact Gram-eigen or randomized EDrSVD) and the C ABI of ttrsvd.h.
+//
+// Chain (reference TT6:799-958 / TR6:827-1004): unfolding j is the column-major
+// (r_{j-1} n_j) x rest matrix; after step j the projected factor is re-read in place as the
+// next unfolding.  Steps whose target rank equals the row count (no truncation) are
+// carried as a pending orthogonal rotation P instead of being rewritten: the true data is
+// P^T times the raw data, every later quantity computed from the raw data is unchanged
+// except the next core, which gets the block rotation (I (x) P^T) folded in.
+#include <stdarg.h>
+#include <string.h>
+
+#include <algorithm>
+#include <string>
+#include <vector>
+
+#include "kernels.cuh"
+
+namespace ttr {
+
+static thread_local char g_err[512] = "";
+void set_error(int code, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  int n = snprintf(g_err, sizeof(g_err), "[%d] ", code);
+  if (n < 0) n = 0;
+  vsnprintf(g_err + n, sizeof(g_err) - n, fmt, ap);
+  va_end(ap);
+}
+
+}  // namespace ttr
+
+using namespace ttr;
+
+struct tt_ctx {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  char* arena = nullptr;
+  size_t cap = 0;
+  DevStatus* dstat = nullptr;
+  DevStatus* hstat = nullptr;
+  double* dsig = nullptr;  // TT_MAX_ORDER x TT_STATS_MAX_SIGMA
+  double* hsig = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+  std::vector<cudaEvent_t> pool;  // per-pass timing events (TT_FLAG_PROFILE)
+};
+
+extern "C" const char* tt_last_error(void) { return ttr::g_err; }
+extern "C" int tt_abi_version(void) { return TTRSVD_ABI_VERSION; }
+
+extern "C" void tt_default_opts(tt_opts* o) {
+  if (!o) return;
+  memset(o, 0, sizeof(*o));
+  o->method = TT_METHOD_EDRSVD;
+  o->gemm = TT_GEMM_AUTO;
+  o->oversample = 8;
+  o->power_iters = 0;
+  o->seed = 1234ULL;
+  o->eps = 0.0;
+  o->flags = TT_FLAG_KEEP_SIGMA;
+  o->max_sweeps = 40;
+}
+
+extern "C" int tt_ctx_create(tt_ctx** out, int device, void* stream) {
+  if (!out) {
+    set_error(TT_ERR_ARG, "null ctx pointer");
+    return TT_ERR_ARG;
+  }
+  *out = nullptr;
+  int ndev = 0;
+  TT_CUDA(cudaGetDeviceCount(&ndev));
+  if (device < 0 || device >= ndev) {
+    set_error(TT_ERR_ARG, "device %d out of range (%d devices)", device, ndev);
+    return TT_ERR_ARG;
+  }
+  TT_CUDA(cudaSetDevice(device));
+  int major = 0;
+  TT_CUDA(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+  if (major != 10) {
+    set_error(TT_ERR_UNSUPPORTED, "libttrsvd is built for sm_100a; device %d has compute capability %d.x",
+              device, major);
+    return TT_ERR_UNSUPPORTED;
+  }
+  tt_ctx* c = new tt_ctx();
+  c->device = device;
+  c->stream = reinterpret_cast<cudaStream_t>(stream);
+  if (cudaMalloc(&c->dstat, sizeof(DevStatus)) != cudaSuccess ||
+      cudaMallocHost(&c->hstat, sizeof(DevStatus)) != cudaSuccess ||
+      cudaMalloc(&c->dsig, sizeof(double) * TT_MAX_ORDER * TT_STATS_MAX_SIGMA) != cudaSuccess ||
+      cudaMallocHost(&c->hsig, sizeof(double) * TT_MAX_ORDER * TT_STATS_MAX_SIGMA) != cudaSuccess ||
+      cudaEventCreate(&c->ev0) != cudaSuccess || cudaEventCreate(&c->ev1) != cudaSuccess) {
+    set_error(TT_ERR_NOMEM, "context allocation failed");
+    tt_ctx_destroy(c);
+    return TT_ERR_NOMEM;
+  }
+  *out = c;
+  return TT_OK;
+}
+
+extern "C" int tt_ctx_destroy(tt_ctx* c) {
+  if (!c) return TT_OK;
+  cudaSetDevice(c->device);
+  if (c->stream) cudaStreamSynchronize(c->stream);
+  if (c->arena) cudaFree(c->arena);
+  if (c->dstat) cudaFree(c->dstat);
+  if (c->hstat) cudaFreeHost(c->hstat);
+  if (c->dsig) cudaFree(c->dsig);
+  if (c->hsig) cudaFreeHost(c->hsig);
+  if (c->ev0) cudaEventDestroy(c->ev0);
+  if (c->ev1) cudaEventDestroy(c->ev1);
+  for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
+  delete c;
+  return TT_OK;
+}
+
+extern "C" int tt_ctx_set_stream(tt_ctx* c, void* stream) {
+  if (!c) {
+    set_error(TT_ERR_ARG, "null ctx");
+    return TT_ERR_ARG;
+  }
+  c->stream = reinterpret_cast<cudaStream_t>(stream);
+  return TT_OK;
+}
+
+extern "C" int tt_ctx_reserve(tt_ctx* c, size_t bytes) {
+  if (!c) {
+    set_error(TT_ERR_ARG, "null ctx");
+    return TT_ERR_ARG;
+  }
+  if (bytes <= c->cap) return TT_OK;
+  TT_CUDA(cudaSetDevice(c->device));
+  if (c->arena) {
+    TT_CUDA(cudaStreamSynchronize(c->stream));
+    cudaFree(c->arena);
+    c->arena = nullptr;
+    c->cap = 0;
+  }
+  bytes = (bytes + (1u << 20) - 1) & ~size_t((1u << 20) - 1);
+  if (cudaMalloc(&c->arena, bytes) != cudaSuccess) {
+    cudaGetLastError();
+    set_error(TT_ERR_NOMEM, "workspace of %zu bytes", bytes);
+    return TT_ERR_NOMEM;
+  }
+  c->cap = bytes;
+  return TT_OK;
+}
+
+namespace {
+
+enum Path { PATH_EXACT_ROWS = 0, PATH_EXACT_COLS = 1, PATH_RAND = 2, PATH_IDENTITY = 3 };
+
+struct Step {
+  long long m = 0, cols = 0;
+  int r_req = 0, r_eff = 0, ks = 0;
+  int path = PATH_EXACT_ROWS;
+  bool fold = false;     // full-rank step carried as a pending rotation
+  bool perm231 = false;  // TR step 1
+  long long next_elems = 0;
+};
+
+struct Plan {
+  int d = 0;
+  bool ring = false;
+  std::vector<long long> n;
+  std::vector<int> r;
+  std::vector<Step> steps;
+  long long total = 0;
+  size_t max_data = 0, max_omega = 0, max_y = 0, max_bt = 0, max_core = 0, max_ws = 0;
+  int max_small = 0;
+};
+
+int engine_of(const tt_opts& o) {
+  if (o.gemm == TT_GEMM_FP32) return TT_GEMM_FP32;
+  return tc_available() ? TT_GEMM_TC : TT_GEMM_FP32;
+}
+
+int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Plan& P) {
+  if (d < 2 || d > TT_MAX_ORDER) {
+    set_error(TT_ERR_SHAPE, "order %d outside [2, %d]", d, TT_MAX_ORDER);
+    return TT_ERR_SHAPE;
+  }
+  if (!n || !r) {
+    set_error(TT_ERR_ARG, "null mode or rank array");
+    return TT_ERR_ARG;
+  }
+  P.d = d;
+  P.ring = ring;
+  P.n.assign(n, n + d);
+  P.r.assign(r, r + d + 1);
+  P.total = 1;
+  for (int k = 0; k < d; ++k) {
+    if (n[k] < 1) {
+      set_error(TT_ERR_SHAPE, "mode size n[%d] = %d", k, n[k]);
+      return TT_ERR_SHAPE;
+    }
+    P.total *= n[k];
+  }
+  for (int k = 0; k <= d; ++k)
+    if (r[k] < 1) {
+      set_error(TT_ERR_RANK, "rank r[%d] = %d", k, r[k]);
+      return TT_ERR_RANK;
+    }
+  if (!ring && (r[0] != 1 || r[d] != 1)) {
+    set_error(TT_ERR_RANK, "TT ranks need r[0] = r[d] = 1 (got %d, %d)", r[0], r[d]);
+    return TT_ERR_RANK;
+  }
+  if (ring && r[0] != r[d]) {
+    set_error(TT_ERR_RANK, "ring ranks need r[0] = r[d] (got %d, %d)", r[0], r[d]);
+    return TT_ERR_RANK;
+  }
+  const int s = std::max(0, o.oversample);
+  const bool nofold = (o.flags & TT_FLAG_NO_FOLD) != 0;
+  long long size = P.total;  // elements of the current (raw) data
+  long long rows_prev = 1;   // r_{k-1} of the true data
+  P.steps.clear();
+  for (int k = 0; k < d - 1; ++k) {
+    Step st;
+    const bool first_ring = ring && k == 0;
+    st.m = first_ring ? n[0] : rows_prev * n[k];
+    st.cols = size / st.m;
+    st.r_req = first_ring ? r[0] * r[1] : r[k + 1];
+    st.perm231 = first_ring && r[0] > 1;
+    const long long mn = std::min(st.m, st.cols);
+    st.r_eff = (int)std::min<long long>(st.r_req, mn);
+    if (o.method == TT_METHOD_EXACT || mn <= TT_MAX_SMALL) {
+      if (mn > TT_MAX_SMALL) {
+        set_error(TT_ERR_UNSUPPORTED, "exact step %d needs min(m, n) = %lld <= %d", k, mn, TT_MAX_SMALL);
+        return TT_ERR_UNSUPPORTED;
+      }
+      st.path = (st.m <= st.cols) ? PATH_EXACT_ROWS : PATH_EXACT_COLS;
+      st.ks = (int)mn;
+    } else {
+      st.path = PATH_RAND;
+      st.ks = (int)std::min<long long>({(long long)st.r_eff + s, mn, (long long)TT_MAX_SMALL});
+      if (st.ks < st.r_eff) {
+        set_error(TT_ERR_UNSUPPORTED, "step %d: rank %d above the sketch limit %d", k, st.r_eff, TT_MAX_SMALL);
+        return TT_ERR_UNSUPPORTED;
+      }
+    }
+    st.fold = !nofold && !st.perm231 && st.path == PATH_EXACT_ROWS && st.r_req == st.m &&
+              st.r_eff == st.m && !(ring && k == 0);
+    if (st.fold && (o.flags & TT_FLAG_IDENTITY_GAUGE)) st.path = PATH_IDENTITY;
+    st.next_elems = (long long)st.r_req * st.cols;
+    P.steps.push_back(st);
+    size = st.fold ? size : st.next_elems;
+    rows_prev = first_ring ? r[1] : st.r_req;
+    if (st.perm231 && st.path == PATH_EXACT_COLS)
+      P.max_bt = std::max<size_t>(P.max_bt, (size_t)st.next_elems);
+    if (!st.fold) P.max_data = std::max<size_t>(P.max_data, (size_t)st.next_elems);
+    P.max_core = std::max<size_t>(P.max_core, (size_t)st.m * std::max(st.r_req, st.ks));
+    P.max_small = std::max(P.max_small, std::max(st.ks, (int)std::min<long long>(mn, TT_MAX_SMALL)));
+    if (st.path == PATH_RAND) {
+      P.max_omega = std::max<size_t>(P.max_omega, (size_t)st.cols * st.ks);
+      P.max_y = std::max<size_t>(P.max_y, (size_t)st.m * st.ks);
+      P.max_bt = std::max<size_t>(P.max_bt, (size_t)st.cols * st.ks);
+      P.max_ws = std::max(P.max_ws, sketch_ws_bytes(st.m, st.cols, st.ks));
+      P.max_ws = std::max(P.max_ws, gram_ws_bytes(st.cols, st.ks));
+      P.max_ws = std::max(P.max_ws, gram_ws_bytes(st.m, st.ks));
+    } else {
+      P.max_ws = std::max(P.max_ws, gram_ws_bytes(std::max(st.m, st.cols), (int)mn));
+    }
+  }
+  P.max_ws += (size_t)TT_MAX_SMALL * TT_MAX_SMALL * sizeof(double) * 8;
+  return TT_OK;
+}
+
+size_t core_elems(const Plan& P, int k) { return (size_t)P.r[k] * P.n[k] * P.r[k + 1]; }
+
+struct Bufs {
+  float* x = nullptr;        // input on device
+  float* data[2] = {nullptr, nullptr};
+  float* omega = nullptr;
+  double* yd = nullptr;
+  float* yf = nullptr;
+  float* bt = nullptr;
+  float* corebuf = nullptr;
+  float* ef = nullptr;
+  double* w = nullptr;
+  double* evals = nullptr;
+  double* evecs = nullptr;
+  double* colscale = nullptr;
+  double* pend[2] = {nullptr, nullptr};
+  int* flag = nullptr;
+  std::vector<float*> cores;  // device cores
+};
+
+size_t plan_bytes(const Plan& P, bool host_io) {
+  const size_t S = TT_MAX_SMALL;
+  size_t b = 0;
+  auto add = [&](size_t bytes) { b += (bytes + 255) & ~size_t(255); };
+  if (host_io) add(P.total * sizeof(float));
+  add(P.max_data * sizeof(float));
+  add(P.max_data * sizeof(float));
+  add(P.max_omega * sizeof(float));
+  add(P.max_y * sizeof(double));
+  add(P.max_y * sizeof(float));
+  add(P.max_bt * sizeof(float));
+  add(P.max_core * sizeof(float));
+  add(S * S * sizeof(float));
+  add(S * S * sizeof(double) * 4);
+  add(S * sizeof(double) * 2);
+  add(S * S * sizeof(double) * 2);
+  add(256);
+  if (host_io)
+    for (int k = 0; k < P.d; ++k) add(core_elems(P, k) * sizeof(float));
+  add(P.max_ws);
+  return b + (1 << 20);
+}
+
+int carve(tt_ctx* c, const Plan& P, bool host_io, Bufs& B, Arena& ws) {
+  Arena a{c->arena, c->cap, 0};
+  const size_t S = TT_MAX_SMALL;
+  if (host_io) B.x = a.take<float>(P.total);
+  B.data[0] = a.take<float>(std::max<size_t>(P.max_data, 1));
+  B.data[1] = a.take<float>(std::max<size_t>(P.max_data, 1));
+  B.omega = a.take<float>(std::max<size_t>(P.max_omega, 1));
+  B.yd = a.take<double>(std::max<size_t>(P.max_y, 1));
+  B.yf = a.take<float>(std::max<size_t>(P.max_y, 1));
+  B.bt = a.take<float>(std::max<size_t>(P.max_bt, 1));
+  B.corebuf = a.take<float>(std::max<size_t>(P.max_core, 1));
+  B.ef = a.take<float>(S * S);
+  B.w = a.take<double>(S * S);
+  B.evecs = a.take<double>(S * S);
+  B.pend[0] = a.take<double>(S * S);
+  B.pend[1] = a.take<double>(S * S);
+  B.evals = a.take<double>(S);
+  B.colscale = a.take<double>(S);
+  B.flag = a.take<int>(64);
+  if (host_io) {
+    B.cores.resize(P.d);
+    for (int k = 0; k < P.d; ++k) B.cores[k] = a.take<float>(core_elems(P, k));
+  }
+  if (!B.data[1] || !B.flag || (host_io && !B.cores[P.d - 1])) {
+    set_error(TT_ERR_NOMEM, "workspace carve");
+    return TT_ERR_NOMEM;
+  }
+  ws = Arena{c->arena + a.off, c->cap - a.off, 0};
+  return TT_OK;
+}
+
+// Store sqrt(evals[0:cnt]) of step k for the stats (device-side copy; read back at the end).
+__global__ void k_store_sigma(const double* evals, int cnt, double* dst) {
+  const int i = threadIdx.x;
+  if (i < TT_STATS_MAX_SIGMA) dst[i] = (i < cnt) ? sqrt(fmax(evals[i], 0.0)) : -1.0;
+}
+
+int emit_core(const float* raw, float* out, const double* pend, int R, long long ni, int ncols,
+              cudaStream_t s) {
+  if (pend) return launch_fold_rows(raw, out, pend, R, ni, ncols, s);
+  TT_CUDA(cudaMemcpyAsync(out, raw, sizeof(float) * (size_t)R * ni * ncols, cudaMemcpyDeviceToDevice, s));
+  return TT_OK;
+}
+
+__global__ void k_eye(double* p, int m) {
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx < m * m) p[idx] = (idx % m == idx / m) ? 1.0 : 0.0;
+}
+
+// Accounting of the bulk passes: algorithmic FLOPs/bytes always, device time when profiling.
+struct PassRec {
+  int kind;
+  double bytes;
+  cudaEvent_t a, b;
+};
+struct Passes {
+  tt_ctx* c = nullptr;
+  cudaStream_t s = nullptr;
+  bool on = false;
+  size_t next = 0;
+  double flops = 0.0, bytes = 0.0;
+  std::vector<PassRec> recs;
+  template <typename F>
+  int run(int kind, double fl, double by, F&& fn) {
+    flops += fl;
+    bytes += by;
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (on) {
+      while (c->pool.size() < next + 2) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) break;
+        c->pool.push_back(e);
+      }
+      if (c->pool.size() >= next + 2) {
+        a = c->pool[next];
+        b = c->pool[next + 1];
+        next += 2;
+        cudaEventRecord(a, s);
+      }
+    }
+    const int st = fn();
+    if (a) {
+      cudaEventRecord(b, s);
+      recs.push_back({kind, by, a, b});
+    }
+    return st;
+  }
+};
+
+int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, float* const* cores_out,
+              tt_stats* stats) {
+  const bool host_io = (o.flags & TT_FLAG_HOST_IO) != 0;
+  TT_CUDA(cudaSetDevice(c->device));
+  TT_TRY(tt_ctx_reserve(c, plan_bytes(P, host_io)));
+  Bufs B;
+  Arena ws;
+  TT_TRY(carve(c, P, host_io, B, ws));
+  cudaStream_t s = c->stream;
+  const int engine = engine_of(o);
+  const int max_sweeps = o.max_sweeps > 0 ? o.max_sweeps : 40;
+  g_kernel_launches = 0;
+  Passes pass;
+  pass.c = c;
+  pass.s = s;
+  pass.on = (o.flags & TT_FLAG_PROFILE) != 0;
+
+  TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), s));
+  TT_CUDA(cudaEventRecord(c->ev0, s));
+  const float* x = x_in;
+  if (host_io) {
+    TT_CUDA(cudaMemcpyAsync(B.x, x_in, sizeof(float) * P.total, cudaMemcpyHostToDevice, s));
+    x = B.x;
+  }
+  std::vector<float*> cores(P.d);
+  for (int k = 0; k < P.d; ++k) cores[k] = host_io ? B.cores[k] : cores_out[k];
+
+  if (o.flags & TT_FLAG_CHECK_FINITE) {
+    TT_CUDA(cudaMemsetAsync(B.flag, 0, sizeof(int), s));
+    TT_TRY(launch_check_finite(x, P.total, B.flag, s));
+    int hflag = 0;
+    TT_CUDA(cudaMemcpyAsync(&hflag, B.flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    TT_CUDA(cudaStreamSynchronize(s));
+    if (hflag) {
+      set_error(TT_ERR_NONFINITE, "input holds NaN or Inf");
+      return TT_ERR_NONFINITE;
+    }
+  }
+
+  const float* cur = x;
+  int slot = 0;
+  const double* pend = nullptr;  // pending rotation (rows_prev x rows_prev), or null
+  int pend_slot = 0;
+  long long rows_prev = 1;
+  const int nsteps = (int)P.steps.size();
+  for (int k = 0; k < nsteps; ++k) {
+    const Step& st = P.steps[k];
+    const long long m = st.m, cols = st.cols;
+    const int rq = st.r_req, re = st.r_eff;
+    float* next = B.data[slot];
+    double* sigdst = c->dsig + (size_t)k * TT_STATS_MAX_SIGMA;
+    const bool ring1 = P.ring && k == 0;
+    float* core_dst = ring1 ? B.corebuf : cores[k];
+    // For the ring's first core the (n1 x q) basis is rearranged below.
+    const long long ni = P.n[k];
+
+    if (st.path == PATH_IDENTITY) {
+      // Core = (I (x) P^T) I_m as an (rows_prev n_k) x m matrix; no pending rotation afterwards.
+      k_eye<<<ceil_div(m * m, 256), 256, 0, s>>>(B.w, (int)m);
+      count_launch();
+      TT_LAUNCH_CHECK();
+      if (pend) {
+        TT_TRY(launch_f64_to_f32_cols(B.w, m, m, (int)m, B.corebuf, m, (int)m, s));
+        TT_TRY(launch_fold_rows(B.corebuf, core_dst, pend, (int)rows_prev, ni, (int)m, s));
+      } else {
+        TT_TRY(launch_f64_to_f32_cols(B.w, m, m, (int)m, core_dst, m, (int)m, s));
+      }
+      k_store_sigma<<<1, 64, 0, s>>>(B.evals, 0, sigdst);
+      count_launch();
+      pend = nullptr;
+      rows_prev = rq;
+      continue;  // data unchanged
+    }
+
+    if (st.path == PATH_EXACT_ROWS) {
+      TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols,
+                      [&] { return launch_gram(cur, cols, (int)m, m, 1, B.w, false, ws, s); }));
+      TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
+      k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
+      count_launch();
+      // basis (m x r_req, zero-padded beyond r_eff), FP32
+      TT_TRY(launch_f64_to_f32_cols(B.evecs, m, m, re, B.ef, m, rq, s));
+      if (ring1) {
+        TT_TRY(launch_ring_core1(B.ef, (int)m, P.r[0], P.r[1], cores[0], s));
+      } else {
+        TT_TRY(emit_core(B.ef, core_dst, pend, (int)rows_prev, ni, rq, s));
+      }
+      if (st.fold) {
+        // next data = raw data; pending rotation = eigenvectors of the raw Gram
+        double* pnew = B.pend[pend_slot ^ 1];
+        TT_CUDA(cudaMemcpyAsync(pnew, B.evecs, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, s));
+        pend = pnew;
+        pend_slot ^= 1;
+        rows_prev = rq;
+        continue;
+      }
+      TT_TRY(pass.run(TT_PASS_PROJECT, 2.0 * m * cols * rq, 4.0 * m * cols + 4.0 * rq * cols, [&] {
+        return launch_project(cur, m, cols, B.ef, rq, m, next, st.perm231 ? 0 : rq,
+                              st.perm231 ? OUT_PERM231 : OUT_ROWMAJOR, P.r[0], P.r[1],
+                              engine == TT_GEMM_TC && re < m ? TT_GEMM_TC : TT_GEMM_FP32, ws, s);
+      }));
+    } else if (st.path == PATH_EXACT_COLS) {
+      // W = A^T A over the rows of A (vectors = rows i, components = columns)
+      TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * cols * cols, 4.0 * m * cols,
+                      [&] { return launch_gram(cur, m, (int)cols, 1, m, B.w, true, ws, s); }));
+      TT_TRY(launch_syev(B.w, (int)cols, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
+      k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(cols, TT_STATS_MAX_SIGMA), sigdst);
+      count_launch();
+      TT_TRY(launch_inv_sigma(B.evals, re, B.colscale, 1e-30, s));
+      float* ubuf = B.corebuf;
+      TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * m * cols * rq, 4.0 * m * cols + 4.0 * m * rq, [&] {
+        return launch_small_nn(cur, m, (int)cols, m, B.evecs, rq, cols, B.colscale, re, ubuf, m, s);
+      }));
+      if (ring1) {
+        TT_TRY(launch_ring_core1(ubuf, (int)m, P.r[0], P.r[1], cores[0], s));
+      } else {
+        TT_TRY(emit_core(ubuf, core_dst, pend, (int)rows_prev, ni, rq, s));
+      }
+      if (st.perm231) {
+        float* tmp = B.bt;  // q x cols scratch (q <= 128, cols <= 128)
+        TT_TRY(launch_sigma_vt(B.evals, B.evecs, (int)cols, rq, re, tmp, s));
+        TT_TRY(launch_permute231(tmp, next, P.r[0], P.r[1], cols, s));
+      } else {
+        TT_TRY(launch_sigma_vt(B.evals, B.evecs, (int)cols, rq, re, next, s));
+      }
+    } else {  // PATH_RAND
+      const int ks = st.ks;
+      TT_TRY(launch_gaussian(B.omega, cols, ks, cols, o.seed, (unsigned)k, s));
+      const double fl_pass = 2.0 * m * cols * ks;
+      const double by_pass = 4.0 * m * cols + 4.0 * cols * ks;
+      TT_TRY(pass.run(TT_PASS_SKETCH, fl_pass, by_pass, [&] {
+        return launch_sketch(cur, m, cols, B.omega, ks, 1, cols, B.yd, engine, ws, s);
+      }));
+      TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, ks, B.yf, m, ks, s));
+      TT_TRY(launch_cholqr2(B.yf, m, ks, 1, m, nullptr, ws, c->dstat, s));
+      for (int it = 0; it < o.power_iters; ++it) {
+        TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
+          return launch_project(cur, m, cols, B.yf, ks, m, B.bt, ks, OUT_ROWMAJOR, 1, 1, engine, ws, s);
+        }));
+        TT_TRY(pass.run(TT_PASS_OTHER, 6.0 * cols * ks * ks, 24.0 * cols * ks, [&] {
+          return launch_cholqr2(B.bt, cols, ks, ks, 1, nullptr, ws, c->dstat, s);
+        }));
+        TT_TRY(pass.run(TT_PASS_SKETCH, fl_pass, by_pass, [&] {
+          return launch_sketch(cur, m, cols, B.bt, ks, ks, 1, B.yd, engine, ws, s);
+        }));
+        TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, ks, B.yf, m, ks, s));
+        TT_TRY(launch_cholqr2(B.yf, m, ks, 1, m, nullptr, ws, c->dstat, s));
+      }
+      // B^T = A^T Q (cols x ks, row-major) = B (ks x cols, column-major)
+      TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
+        return launch_project(cur, m, cols, B.yf, ks, m, B.bt, ks, OUT_ROWMAJOR, 1, 1, engine, ws, s);
+      }));
+      TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ks * ks, 4.0 * cols * ks,
+                      [&] { return launch_gram(B.bt, cols, ks, ks, 1, B.w, true, ws, s); }));
+      TT_TRY(launch_syev(B.w, ks, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
+      k_store_sigma<<<1, 64, 0, s>>>(B.evals, std::min(ks, TT_STATS_MAX_SIGMA), sigdst);
+      count_launch();
+      // next = E_r^T B  (rotation of the small factor; plain FP32 keeps it exact to FP32)
+      TT_TRY(launch_f64_to_f32_cols(B.evecs, ks, ks, re, B.ef, ks, rq, s));
+      TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * ks * cols * rq, 4.0 * ks * cols + 4.0 * rq * cols, [&] {
+        return launch_project(B.bt, ks, cols, B.ef, rq, ks, next, st.perm231 ? 0 : rq,
+                              st.perm231 ? OUT_PERM231 : OUT_ROWMAJOR, P.r[0], P.r[1], TT_GEMM_FP32,
+                              ws, s);
+      }));
+      // core = Q E_r
+      float* ubuf = B.corebuf;
+      TT_TRY(launch_small_nn(B.yf, m, ks, m, B.evecs, rq, ks, nullptr, re, ubuf, m, s));
+      if (ring1) {
+        TT_TRY(launch_ring_core1(ubuf, (int)m, P.r[0], P.r[1], cores[0], s));
+      } else {
+        TT_TRY(emit_core(ubuf, core_dst, pend, (int)rows_prev, ni, rq, s));
+      }
+    }
+    pend = nullptr;
+    cur = next;
+    slot ^= 1;
+    rows_prev = ring1 ? P.r[1] : rq;
+  }
+  // last core: (rows_prev, n_d, r_d) = current data, with a pending rotation folded in
+  {
+    const int k = P.d - 1;
+    const long long ni = P.n[k] * (long long)P.r[P.d];
+    TT_TRY(emit_core(cur, cores[k], pend, (int)rows_prev, ni, 1, s));
+  }
+  TT_CUDA(cudaEventRecord(c->ev1, s));
+  if (host_io) {
+    for (int k = 0; k < P.d; ++k)
+      TT_CUDA(cudaMemcpyAsync(cores_out[k], cores[k], sizeof(float) * core_elems(P, k),
+                              cudaMemcpyDeviceToHost, s));
+  }
+  TT_CUDA(cudaMemcpyAsync(c->hstat, c->dstat, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
+  TT_CUDA(cudaMemcpyAsync(c->hsig, c->dsig, sizeof(double) * TT_MAX_ORDER * TT_STATS_MAX_SIGMA,
+                          cudaMemcpyDeviceToHost, s));
+  TT_CUDA(cudaStreamSynchronize(s));
+  if (stats) {
+    memset(stats, 0, sizeof(*stats));
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, c->ev0, c->ev1);
+    stats->ms = ms;
+    stats->nsteps = nsteps;
+    for (int k = 0; k <= P.d; ++k) stats->ranks[k] = P.r[k];
+    for (int k = 0; k < nsteps; ++k) {
+      int cnt = 0;
+      for (int i = 0; i < TT_STATS_MAX_SIGMA; ++i) {
+        const double v = c->hsig[(size_t)k * TT_STATS_MAX_SIGMA + i];
+        if (v < 0) break;
+        stats->sigma[k][i] = (float)v;
+        ++cnt;
+      }
+      stats->nsigma[k] = cnt;
+    }
+    stats->jacobi_sweeps = c->hstat->sweeps;
+    stats->kernels = g_kernel_launches;
+    stats->flops = pass.flops;
+    stats->bytes = pass.bytes;
+    for (const PassRec& rec : pass.recs) {
+      float pm = 0.f;
+      cudaEventElapsedTime(&pm, rec.a, rec.b);
+      stats->pass_ms[rec.kind] += pm;
+      stats->pass_bytes[rec.kind] += rec.bytes;
+      stats->pass_launches[rec.kind] += 1;
+    }
+  }
+  if (c->hstat->code != 0) {
+    set_error(c->hstat->code, "device status %d (detail %d)", c->hstat->code, c->hstat->detail);
+    return c->hstat->code;
+  }
+  return TT_OK;
+}
+
+int run_entry(tt_ctx* c, const float* x, int d, const int* n, const int* r, const tt_opts* opts,
+              float* const* cores, tt_stats* stats, bool ring) {
+  if (!c || !x || !cores) {
+    set_error(TT_ERR_ARG, "null argument");
+    return TT_ERR_ARG;
+  }
+  tt_opts o;
+  if (opts)
+    o = *opts;
+  else
+    tt_default_opts(&o);
+  Plan P;
+  TT_TRY(make_plan(d, n, r, ring, o, P));
+  for (int k = 0; k < d; ++k)
+    if (!cores[k]) {
+      set_error(TT_ERR_ARG, "null core pointer %d", k);
+      return TT_ERR_ARG;
+    }
+  return run_chain(c, x, P, o, cores, stats);
+}
+
+}  // namespace
+
+extern "C" int tt_svd(tt_ctx* ctx, const float* x, int d, const int* n, const int* r,
+                      const tt_opts* opts, float* const* cores, tt_stats* stats) {
+  return run_entry(ctx, x, d, n, r, opts, cores, stats, false);
+}
+
+extern "C" int tr_svd(tt_ctx* ctx, const float* x, int d, const int* n, const int* r,
+                      const tt_opts* opts, float* const* cores, tt_stats* stats) {
+  return run_entry(ctx, x, d, n, r, opts, cores, stats, true);
+}
+
+extern "C" int tt_rel_error(tt_ctx* c, const float* x, int d, const int* n, const int* r, int ring,
+                            const float* const* cores, double* rel_err) {
+  if (!c || !x || !n || !r || !cores || !rel_err) {
+    set_error(TT_ERR_ARG, "null argument");
+    return TT_ERR_ARG;
+  }
+  if (d < 2 || d > TT_MAX_ORDER) {
+    set_error(TT_ERR_SHAPE, "order %d", d);
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  long long N = 1;
+  for (int k = 1; k < d; ++k) N *= n[k];
+  // merged right part M_k sizes: r_{k-1} * (n_k ... n_d) * r_d
+  long long maxm = 0;
+  {
+    long long rest = r[d];
+    for (int k = d - 1; k >= 1; --k) {
+      rest *= n[k];
+      maxm = std::max(maxm, (long long)r[k - 1] * rest);
+    }
+  }
+  TT_TRY(tt_ctx_reserve(c, sizeof(float) * (size_t)maxm * 2 + 4096 + (1 << 20)));
+  Arena a{c->arena, c->cap, 0};
+  float* buf[2] = {a.take<float>(maxm), a.take<float>(maxm)};
+  double* acc = a.take<double>(2);
+  if (!buf[1] || !acc) {
+    set_error(TT_ERR_NOMEM, "error workspace");
+    return TT_ERR_NOMEM;
+  }
+  cudaStream_t s = c->stream;
+  const float* mk = cores[d - 1];
+  long long cols = (long long)n[d - 1] * r[d];
+  int sl = 0;
+  for (int k = d - 2; k >= 1; --k) {
+    // M_k = G_k (r_{k-1} n_k x r_k) * M_{k+1} (r_k x cols)
+    TT_TRY(launch_gemm_nn(cores[k], (long long)r[k] * n[k], r[k + 1], mk, cols, buf[sl], s));
+    mk = buf[sl];
+    sl ^= 1;
+    cols *= n[k];
+  }
+  TT_CUDA(cudaMemsetAsync(acc, 0, 2 * sizeof(double), s));
+  TT_TRY(launch_recon_err(x, n[0], N, cores[0], ring ? r[0] : 1, r[1], mk, acc, s));
+  double h[2] = {0, 0};
+  TT_CUDA(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, s));
+  TT_CUDA(cudaStreamSynchronize(s));
+  *rel_err = h[1] > 0 ? sqrt(h[0] / h[1]) : 0.0;
+  return TT_OK;
+}
+
+// ---- building blocks ----
+namespace {
+int ws_for(tt_ctx* c, size_t bytes, Arena& ws) {
+  TT_TRY(tt_ctx_reserve(c, bytes + (1 << 20)));
+  ws = Arena{c->arena, c->cap, 0};
+  return TT_OK;
+}
+int check_status(tt_ctx* c) {
+  TT_CUDA(cudaMemcpyAsync(c->hstat, c->dstat, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
+  TT_CUDA(cudaStreamSynchronize(c->stream));
+  if (c->hstat->code) {
+    set_error(c->hstat->code, "device status %d (detail %d)", c->hstat->code, c->hstat->detail);
+    return c->hstat->code;
+  }
+  return TT_OK;
+}
+}  // namespace
+
+#define TT_NEED(p)                                \
+  do {                                            \
+    if (!(p)) {                                   \
+      set_error(TT_ERR_ARG, "null argument " #p); \
+      return TT_ERR_ARG;                          \
+    }                                             \
+  } while (0)
+
+extern "C" int tt_k_gaussian(tt_ctx* c, float* out, long long rows, int cols, long long ld,
+                             unsigned long long seed, unsigned stream_id) {
+  TT_NEED(c);
+  TT_NEED(out);
+  if (rows < 0 || cols < 0 || ld < rows) {
+    set_error(TT_ERR_SHAPE, "gaussian shape");
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  TT_TRY(launch_gaussian(out, rows, cols, ld, seed, stream_id, c->stream));
+  TT_CUDA(cudaStreamSynchronize(c->stream));
+  return TT_OK;
+}
+
+extern "C" int tt_k_sketch(tt_ctx* c, const float* a, long long m, long long n, const float* w,
+                           int N, long long ldw, double* y, int gemm) {
+  TT_NEED(c);
+  TT_NEED(a);
+  TT_NEED(w);
+  TT_NEED(y);
+  if (m < 1 || n < 1 || N < 1 || ldw < n) {
+    set_error(TT_ERR_SHAPE, "sketch shape");
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  Arena ws;
+  TT_TRY(ws_for(c, sketch_ws_bytes(m, n, N) * 2, ws));
+  const int eng = (gemm == TT_GEMM_FP32 || !tc_available()) ? TT_GEMM_FP32 : TT_GEMM_TC;
+  TT_TRY(launch_sketch(a, m, n, w, N, 1, ldw, y, eng, ws, c->stream));
+  TT_CUDA(cudaStreamSynchronize(c->stream));
+  return TT_OK;
+}
+
+extern "C" int tt_k_project(tt_ctx* c, const float* a, long long m, long long n, const float* q,
+                            int N, long long ldq, float* out, long long ldo, int gemm) {
+  TT_NEED(c);
+  TT_NEED(a);
+  TT_NEED(q);
+  TT_NEED(out);
+  if (m < 1 || n < 1 || N < 1 || ldq < m || ldo < N) {
+    set_error(TT_ERR_SHAPE, "project shape");
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  Arena ws;
+  TT_TRY(ws_for(c, 1 << 20, ws));
+  const int eng = (gemm == TT_GEMM_FP32 || !tc_available()) ? TT_GEMM_FP32 : TT_GEMM_TC;
+  TT_TRY(launch_project(a, m, n, q, N, ldq, out, ldo, OUT_ROWMAJOR, 1, 1, eng, ws, c->stream));
+  TT_CUDA(cudaStreamSynchronize(c->stream));
+  return TT_OK;
+}
+
+extern "C" int tt_k_gram_rows(tt_ctx* c, const float* a, long long m, long long n, double* w) {
+  TT_NEED(c);
+  TT_NEED(a);
+  TT_NEED(w);
+  if (m < 1 || n < 1 || m > TT_MAX_SMALL) {
+    set_error(TT_ERR_SHAPE, "gram_rows shape");
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  Arena ws;
+  TT_TRY(ws_for(c, gram_ws_bytes(n, (int)m), ws));
+  TT_TRY(launch_gram(a, n, (int)m, m, 1, w, false, ws, c->stream));
+  TT_CUDA(cudaStreamSynchronize(c->stream));
+  return TT_OK;
+}
+
+extern "C" int tt_k_gram_tall(tt_ctx* c, const float* z, long long n, int N, long long rs,
+                              long long cs, double* w) {
+  TT_NEED(c);
+  TT_NEED(z);
+  TT_NEED(w);
+  if (n < 1 || N < 1 || N > TT_MAX_SMALL) {
+    set_error(TT_ERR_SHAPE, "gram_tall shape");
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  Arena ws;
+  TT_TRY(ws_for(c, gram_ws_bytes(n, N), ws));
+  TT_TRY(launch_gram(z, n, N, rs, cs, w, true, ws, c->stream));
+  TT_CUDA(cudaStreamSynchronize(c->stream));
+  return TT_OK;
+}
+
+extern "C" int tt_k_cholqr2(tt_ctx* c, float* y, long long n, int N, long long ld, double* r) {
+  TT_NEED(c);
+  TT_NEED(y);
+  if (n < 1 || N < 1 || N > TT_MAX_SMALL || ld < n) {
+    set_error(TT_ERR_SHAPE, "cholqr2 shape");
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  Arena ws;
+  TT_TRY(ws_for(c, gram_ws_bytes(n, N) + 8 * TT_MAX_SMALL * TT_MAX_SMALL * sizeof(double), ws));
+  TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
+  TT_TRY(launch_cholqr2(y, n, N, 1, ld, r, ws, c->dstat, c->stream));
+  return check_status(c);
+}
+
+extern "C" int tt_k_syev(tt_ctx* c, const double* w, int N, double* evals, double* evecs,
+                         int* sweeps) {
+  TT_NEED(c);
+  TT_NEED(w);
+  TT_NEED(evals);
+  TT_NEED(evecs);
+  if (N < 1 || N > TT_MAX_SMALL) {
+    set_error(TT_ERR_SHAPE, "syev size %d", N);
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  Arena ws;
+  TT_TRY(ws_for(c, 2 * TT_MAX_SMALL * TT_MAX_SMALL * sizeof(double), ws));
+  TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
+  TT_TRY(launch_syev(w, N, evals, evecs, 40, ws, c->dstat, c->stream));
+  int st = check_status(c);
+  if (sweeps) *sweeps = c->hstat->sweeps;
+  return st;
+}
+
+extern "C" int tt_k_permute231(tt_ctx* c, const float* in, float* out, int r0, int r1, long long n) {
+  TT_NEED(c);
+  TT_NEED(in);
+  TT_NEED(out);
+  if (r0 < 1 || r1 < 1 || n < 1 || r0 * r1 > 8192) {
+    set_error(TT_ERR_SHAPE, "permute231 shape");
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  TT_TRY(launch_permute231(in, out, r0, r1, n, c->stream));
+  TT_CUDA(cudaStreamSynchronize(c->stream));
+  return TT_OK;
+}

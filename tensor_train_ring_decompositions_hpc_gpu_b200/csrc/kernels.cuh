@@ -1,0 +1,106 @@
+// Launchers of the TT/TR-SVD kernels.  All take device pointers and run on `stream`.
+#pragma once
+#include "common.cuh"
+
+namespace ttr {
+
+// Workspace bump allocator over one device arena.
+struct Arena {
+  char* base = nullptr;
+  size_t cap = 0;
+  size_t off = 0;
+  template <typename T>
+  T* take(size_t count) {
+    size_t bytes = (count * sizeof(T) + 255) & ~size_t(255);
+    if (off + bytes > cap) return nullptr;
+    T* p = reinterpret_cast<T*>(base + off);
+    off += bytes;
+    return p;
+  }
+  size_t mark() const { return off; }
+  void reset(size_t m) { off = m; }
+};
+
+// Bytes a launcher needs from the arena (callers reserve before launching).
+size_t sketch_ws_bytes(long long m, long long n, int N);
+size_t gram_ws_bytes(long long nvec, int M);
+
+// Philox Gaussian fill (column-major rows x cols, ld).
+int launch_gaussian(float* out, long long rows, int cols, long long ld, unsigned long long seed,
+                    unsigned stream_id, cudaStream_t s);
+
+// Y (m x N, FP64, ld = m) = A (m x n, lda = m) * W, W element (j, c) at w[j*wj + c*wc].
+// engine: TT_GEMM_FP32 or TT_GEMM_TC.
+int launch_sketch(const float* a, long long m, long long n, const float* w, int N, long long wj,
+                  long long wc, double* y, int engine, Arena& ws, cudaStream_t s);
+
+// Output modes of the projection.
+enum { OUT_ROWMAJOR = 0, OUT_PERM231 = 1 };
+
+// out = A^T Q: A (m x n, lda = m), Q (m x N, ldq).  OUT_ROWMAJOR: out[j*ldo + c];
+// OUT_PERM231: column c = a + r0*b of Q^T A goes to out[b + r1*(j + n*a)] (TR bond permute).
+int launch_project(const float* a, long long m, long long n, const float* q, int N, long long ldq,
+                   float* out, long long ldo, int mode, int r0, int r1, int engine, Arena& ws,
+                   cudaStream_t s);
+
+// W (M x M, FP64, ld = M) = sum_j x_j x_j^T with x_j[c] = x[j*vs + c*es], M <= 128.
+// acc64: FP64 products and accumulation; else FP32 products with FP64 flush every 1024 vectors.
+int launch_gram(const float* x, long long nvec, int M, long long vs, long long es, double* w,
+                bool acc64, Arena& ws, cudaStream_t s);
+
+// CholeskyQR2 on a tall FP32 matrix, element (j, c) at y[j*vs + c*es], n x N.
+// Writes R (N x N, FP64, upper) when r != nullptr.
+int launch_cholqr2(float* y, long long n, int N, long long vs, long long es, double* r,
+                   Arena& ws, DevStatus* st, cudaStream_t s);
+
+// Symmetric eigen-decomposition by parallel cyclic Jacobi (FP64, N <= 128).
+int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps,
+                Arena& ws, DevStatus* st, cudaStream_t s);
+
+// out (r0, r1, n) -> (r1, n, r0) column-major.
+int launch_permute231(const float* in, float* out, int r0, int r1, long long n, cudaStream_t s);
+
+// C (M x N, FP32, ldc) = A (M x K, FP32, lda) * B (K x N, FP64, ldb), optionally scaled
+// column-wise by colscale[c] (FP64) and with columns >= nvalid set to zero.
+int launch_small_nn(const float* a, long long M, int K, long long lda, const double* b, int N,
+                    long long ldb, const double* colscale, int nvalid, float* c, long long ldc,
+                    cudaStream_t s);
+
+// Fold a pending row rotation into a core: out[(a + R*i) + M*b] = sum_a' P[a' + R*a] *
+// in[(a' + R*i) + M*b] with M = R * ni.  In place is not allowed.
+int launch_fold_rows(const float* in, float* out, const double* p, int R, long long ni, int ncols,
+                     cudaStream_t s);
+
+// Copy the first `k` columns of an FP64 (rows x ?) matrix to FP32 (rows x ncols), zero-padding.
+int launch_f64_to_f32_cols(const double* in, long long rows, long long ldin, int k, float* out,
+                           long long ldout, int ncols, cudaStream_t s);
+
+// next (k x n) = diag(sqrt(evals[0:k])) * V[:, 0:k]^T, V (n x n, FP64), rows >= kvalid zeroed.
+int launch_sigma_vt(const double* evals, const double* v, int n, int k, int kvalid, float* out,
+                    cudaStream_t s);
+
+// Column scale helper for U = A V / sigma: colscale[a] = 1/sigma_a (0 when sigma tiny).
+int launch_inv_sigma(const double* evals, int k, double* colscale, double rel_floor, cudaStream_t s);
+
+// Ring core 1: core[a + r0*(i + n1*b)] = u[i + n1*(a + r0*b)].
+int launch_ring_core1(const float* u, int n1, int r0, int r1, float* core, cudaStream_t s);
+
+// NaN/Inf scan; *flag set to 1 when found.
+int launch_check_finite(const float* x, long long count, int* flag, cudaStream_t s);
+
+// Sum of squares (FP64) of (x - y) and of x, accumulated into acc[0], acc[1].
+int launch_diff_norm(const float* x, const float* y, long long count, double* acc, cudaStream_t s);
+
+// Dense C (M x N) = A (M x K) * B (K x N), all FP32 column-major, small K (core merging).
+int launch_gemm_nn(const float* a, long long M, int K, const float* b, long long N, float* c,
+                   cudaStream_t s);
+
+// Fused reconstruction check of a ring/train: acc += sum_J ||X[:, J] - sum_a G1[a] M[:, J, a]||^2
+// and ||X||^2, where G1 is (r0, n1, r1) and M is (r1, N, r0).
+int launch_recon_err(const float* x, int n1, long long N, const float* g1, int r0, int r1,
+                     const float* mrg, double* acc, cudaStream_t s);
+
+// Tensor-core engine availability (sm_100 device and kernels compiled in).
+bool tc_available();
+
+}  // namespace ttr

@@ -1,0 +1,140 @@
+"""Kernel-level checks of libttrsvd.so on the GPU against NumPy / the oracle."""
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+
+def _ttr():
+    import tensor_train_ring_decompositions_hpc_gpu_b200 as ttr
+    return ttr
+
+
+def _randn_cm(rows, cols, seed, dev):
+    import torch
+    g = torch.Generator(device="cpu").manual_seed(seed)
+    a = torch.randn((cols, rows), generator=g, dtype=torch.float32)
+    return a.to(dev).t()  # column-major (rows x cols)
+
+
+def _rel(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return np.linalg.norm((a - b).ravel()) / max(np.linalg.norm(b.ravel()), 1e-300)
+
+
+def test_gaussian_matches_oracle(gpu):
+    ttr = _ttr()
+    g = ttr.gaussian(1001, 7, seed=99, stream_id=3).cpu().numpy()
+    ref = oracle.gaussian_from_philox(1001, 7, 99, 3)
+    np.testing.assert_allclose(g, ref, rtol=1e-4, atol=2e-5)
+
+
+# TF32 tensor cores keep 10 mantissa bits: relative error of a product-sum is ~1e-3 worst case.
+TOL = {"fp32": 2e-6, "tc": 3e-3}
+
+
+@pytest.mark.parametrize("gemm", ["fp32", "tc"])
+@pytest.mark.parametrize("m,n,N", [(256, 4096, 24), (1024, 3000, 40), (300, 777, 17), (128, 65536, 48),
+                                   (32, 5000, 32), (4096, 256, 24)])
+def test_sketch(gpu, gemm, m, n, N):
+    ttr = _ttr()
+    a = _randn_cm(m, n, 1, gpu)
+    w = _randn_cm(n, N, 2, gpu)
+    y = ttr.sketch(a, w, gemm).cpu().numpy()
+    ref = a.double().cpu().numpy() @ w.double().cpu().numpy()
+    assert _rel(y, ref) < TOL[gemm]
+
+
+@pytest.mark.parametrize("gemm", ["fp32", "tc"])
+@pytest.mark.parametrize("m,n,N", [(256, 4096, 24), (1024, 3000, 40), (32, 100000, 32), (300, 777, 17),
+                                   (40, 65536, 32), (1024, 1024, 64)])
+def test_project(gpu, gemm, m, n, N):
+    ttr = _ttr()
+    a = _randn_cm(m, n, 3, gpu)
+    q = _randn_cm(m, N, 4, gpu)
+    out = ttr.project(a, q, gemm).cpu().numpy()  # (N x n)
+    ref = q.double().cpu().numpy().T @ a.double().cpu().numpy()
+    assert _rel(out, ref) < TOL[gemm]
+
+
+@pytest.mark.parametrize("m,n", [(32, 100000), (16, 5000), (48, 7777), (64, 4096), (128, 3000), (5, 999)])
+def test_gram_rows(gpu, m, n):
+    ttr = _ttr()
+    a = _randn_cm(m, n, 5, gpu)
+    w = ttr.gram_rows(a).cpu().numpy()
+    ad = a.double().cpu().numpy()
+    assert _rel(w, ad @ ad.T) < 1e-6
+
+
+@pytest.mark.parametrize("n,N", [(100000, 40), (5000, 16), (777, 48), (4096, 64), (3000, 128)])
+def test_gram_tall(gpu, n, N):
+    ttr = _ttr()
+    z = _randn_cm(n, N, 6, gpu)
+    w = ttr.gram_tall(z).cpu().numpy()
+    zd = z.double().cpu().numpy()
+    assert _rel(w, zd.T @ zd) < 1e-12
+
+
+@pytest.mark.parametrize("n,N", [(1024, 40), (100000, 24), (5000, 64), (300, 128)])
+def test_cholqr2(gpu, n, N):
+    ttr = _ttr()
+    y = _randn_cm(n, N, 7, gpu)
+    q, r = ttr.cholqr2(y)
+    qd = q.double().cpu().numpy()
+    rd = r.cpu().numpy()
+    orth = np.linalg.norm(qd.T @ qd - np.eye(N))
+    assert orth < 1e-5
+    assert _rel(qd @ rd, y.double().cpu().numpy()) < 1e-5
+
+
+def test_cholqr2_rank_deficient_zeroes_dependent_columns(gpu):
+    import torch
+    ttr = _ttr()
+    base = _randn_cm(2000, 6, 8, gpu)
+    y = torch.cat([base, base[:, :2] * 2.0], dim=1)
+    y = y.t().contiguous().t()
+    q, _ = ttr.cholqr2(y)
+    qd = q.double().cpu().numpy()
+    norms = np.linalg.norm(qd, axis=0)
+    assert np.all(norms[:6] > 0.99) and np.all(norms[6:] < 1e-3)
+
+
+@pytest.mark.parametrize("N", [5, 24, 32, 40, 64, 96, 128])
+def test_syev(gpu, N):
+    import torch
+    ttr = _ttr()
+    rng = np.random.default_rng(N)
+    b = rng.standard_normal((N, N + 7))
+    w = b @ b.T
+    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu))
+    ev = ev.cpu().numpy()
+    vec = vec.cpu().numpy()
+    ref = np.sort(np.linalg.eigvalsh(w))[::-1]
+    np.testing.assert_allclose(ev, ref, rtol=1e-11, atol=1e-11 * ref[0])
+    assert np.linalg.norm(w @ vec - vec * ev) < 1e-10 * ref[0] * N
+    assert np.linalg.norm(vec.T @ vec - np.eye(N)) < 1e-12 * N
+    assert 1 <= sweeps <= 40
+
+
+def test_syev_graded_spectrum_relative_accuracy(gpu):
+    import torch
+    ttr = _ttr()
+    rng = np.random.default_rng(1)
+    q, _ = np.linalg.qr(rng.standard_normal((40, 40)))
+    lam = np.logspace(0, -10, 40)
+    w = (q * lam) @ q.T
+    ev, _, _ = ttr.syev(torch.from_numpy(w).to(gpu))
+    np.testing.assert_allclose(ev.cpu().numpy()[:20], lam[:20], rtol=1e-8)
+
+
+@pytest.mark.parametrize("r0,r1,n", [(8, 8, 100000), (2, 4, 777), (1, 32, 5000), (3, 5, 12345)])
+def test_permute231_bit_exact(gpu, r0, r1, n):
+    import torch
+    ttr = _ttr()
+    x = torch.randn(r0 * r1 * n, device=gpu)
+    out = ttr.permute231(x, r0, r1, n).cpu().numpy()
+    ref = x.cpu().numpy().reshape(r0, r1, n, order="F").transpose(1, 2, 0).ravel(order="F")
+    assert np.array_equal(out, ref)

@@ -1,0 +1,217 @@
+"""End-to-end parity of the CUDA TT-SVD / TR-SVD chain against the FP64 oracle.
+
+Bar (from the project's correctness statement): reconstruction error within 1e-3 absolute
+of the oracle's exact truncated SVD chain at the same ranks, leading singular values of
+every unfolding within 1e-4 relative.
+"""
+import os
+
+import numpy as np
+import pytest
+
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+ERR_ABS = 1e-3
+SIG_REL = 1e-4
+GOLD = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _ttr():
+    import tensor_train_ring_decompositions_hpc_gpu_b200 as ttr
+    return ttr
+
+
+def _to_dev(x, dev):
+    import torch
+    return torch.from_numpy(np.asfortranarray(x, dtype=np.float32)).to(dev)
+
+
+def _cores_np(res):
+    return [c.detach().cpu().numpy().astype(np.float64) for c in res.cores]
+
+
+def _check(x, res, ref_cores, ref_sig, ring, nsig=4, err_abs=ERR_ABS, sig_rel=SIG_REL):
+    full = oracle.tr_full if ring else oracle.tt_full
+    err = oracle.rel_error(x, full(_cores_np(res), "gpu"))
+    err_ref = oracle.rel_error(x, full(ref_cores, "gpu"))
+    assert abs(err - err_ref) <= err_abs, (err, err_ref)
+    for k, s_ref in enumerate(ref_sig):
+        s = res.sigmas[k]
+        if len(s) == 0:
+            continue
+        kk = min(nsig, len(s), len(s_ref))
+        np.testing.assert_allclose(s[:kk], s_ref[:kk], rtol=sig_rel, err_msg=f"unfolding {k + 1}")
+    return err, err_ref
+
+
+TT_CASES = [
+    # (shape, ranks, noise, gemm, opts)
+    ((64, 64, 64), (1, 16, 16, 1), 1e-3, "fp32", {}),
+    ((64, 64, 64), (1, 16, 16, 1), 1e-3, "tc", {}),
+    ((256, 256, 256), (1, 16, 16, 1), 1e-3, "fp32", {"oversample": 8, "power_iters": 1}),
+    ((256, 256, 256), (1, 16, 16, 1), 1e-3, "tc", {"oversample": 8, "power_iters": 1}),
+    ((256, 256, 256), (1, 16, 16, 1), 1e-3, "tc", {"oversample": 8, "power_iters": 0}),
+    ((8, 8, 8, 8, 8, 8), (1, 4, 4, 4, 4, 4, 1), 1e-4, "fp32", {}),
+    ((8, 8, 8, 8, 8, 8), (1, 4, 4, 4, 4, 4, 1), 1e-4, "tc", {}),
+    ((12, 12, 12, 12, 12, 12), (1, 12, 20, 20, 12, 1, 1)[:7], 1e-4, "tc", {}),
+    ((7, 9, 5, 8, 6), (1, 5, 9, 7, 4, 1), 1e-3, "fp32", {}),
+    ((16, 16, 16, 16, 16), (1, 16, 40, 40, 16, 1), 1e-4, "tc", {}),
+]
+
+
+@pytest.mark.parametrize("shape,ranks,noise,gemm,opts", TT_CASES)
+def test_tt_parity(gpu, shape, ranks, noise, gemm, opts):
+    ttr = _ttr()
+    ranks = list(ranks)
+    ranks[-1] = 1
+    gen_ranks = [1] + [max(1, r) for r in ranks[1:-1]] + [1]
+    x = oracle.make_tt_tensor(list(shape), gen_ranks, noise, seed=11).astype(np.float64)
+    res = ttr.tt_svd(_to_dev(x, gpu), ranks, gemm=gemm, **opts)
+    ref_cores, ref_sig = oracle.tt_svd(x, ranks)
+    for k, c in enumerate(res.cores):
+        assert tuple(c.shape) == (ranks[k], shape[k], ranks[k + 1])
+    _check(x, res, ref_cores, ref_sig, ring=False)
+
+
+@pytest.mark.parametrize("gemm", ["fp32", "tc"])
+@pytest.mark.parametrize("shape,ranks", [
+    ((6, 6, 6, 6, 6, 6), (2, 3, 6, 6, 6, 3, 2)),
+    ((8, 8, 8, 8, 8, 8), (2, 4, 8, 8, 8, 8, 2)),
+    ((16, 16, 16, 16, 16, 16), (4, 4, 16, 16, 16, 16, 4)),
+    ((40, 30, 20), (2, 10, 12, 2)),
+])
+def test_tr_parity(gpu, gemm, shape, ranks):
+    ttr = _ttr()
+    x = oracle.make_tr_tensor(list(shape), 2, 1e-4, seed=13).astype(np.float64)
+    res = ttr.tr_svd(_to_dev(x, gpu), list(ranks), gemm=gemm)
+    ref_cores, ref_sig = oracle.tr_svd(x, list(ranks))
+    _check(x, res, ref_cores, ref_sig, ring=True)
+
+
+def test_tr_rank_above_first_mode_is_zero_padded(gpu):
+    # c3's first split: r0*r1 = 64 > n1 = 32 (scaled down: 4*4 = 16 > n1 = 8)
+    ttr = _ttr()
+    x = oracle.make_tr_tensor([8, 8, 8, 8, 8, 8], 4, 1e-4, seed=17).astype(np.float64)
+    ranks = [4, 4, 4, 4, 4, 4, 4]
+    res = ttr.tr_svd(_to_dev(x, gpu), ranks, gemm="tc")
+    ref_cores, ref_sig = oracle.tr_svd(x, ranks)
+    _check(x, res, ref_cores, ref_sig, ring=True)
+    g1 = res.cores[0].cpu().numpy()
+    # bond components 8..15 of (a + 4 b) are zero columns
+    flat = g1.transpose(1, 0, 2).reshape(8, 16, order="F")
+    assert np.abs(flat[:, 8:]).max() == 0.0
+
+
+@pytest.mark.parametrize("flags", ["none", "no_fold", "identity"])
+def test_fold_modes_same_error(gpu, flags):
+    ttr = _ttr()
+    shape, ranks = (8, 8, 8, 8, 8, 8), [1, 8, 20, 20, 8, 4, 1]
+    x = oracle.make_tt_tensor(list(shape), [1, 8, 8, 8, 8, 4, 1], 1e-4, seed=19).astype(np.float64)
+    fl = {"none": 0, "no_fold": ttr.TT_FLAG_NO_FOLD, "identity": ttr.TT_FLAG_IDENTITY_GAUGE}[flags]
+    res = ttr.tt_svd(_to_dev(x, gpu), ranks, gemm="tc", flags=fl)
+    ref_cores, ref_sig = oracle.tt_svd(x, ranks)
+    if flags == "identity":
+        ref_sig = ref_sig[1:]
+        res.sigmas = res.sigmas[1:]
+    _check(x, res, ref_cores, ref_sig, ring=False)
+    # left-orthonormal cores (all but the last)
+    for c in _cores_np(res)[:-1]:
+        u = c.reshape(-1, c.shape[2], order="F")
+        assert np.linalg.norm(u.T @ u - np.eye(u.shape[1])) < 1e-4
+
+
+def test_golden_python_reference_through_gpu(gpu):
+    """The reference's own Python TT-SVD results (golden vectors) reproduced by the CUDA chain."""
+    ttr = _ttr()
+    g = np.load(os.path.join(GOLD, "tt6_python_ref.npz"))
+    x = g["x"]
+    k = [int(v) for v in g["k"]]
+    res = ttr.tt_svd(_to_dev(x, gpu), k, gemm="tc")
+    err = oracle.rel_error(x, oracle.tt_full(_cores_np(res), "gpu"))
+    assert abs(err - float(g["err"])) < ERR_ABS
+    for j in range(5):
+        s_ref = g[f"sigma{j + 1}"]
+        kk = min(3, len(res.sigmas[j]))
+        np.testing.assert_allclose(res.sigmas[j][:kk], s_ref[:kk], rtol=SIG_REL)
+
+
+def test_golden_python_reference_tr_error(gpu):
+    ttr = _ttr()
+    g = np.load(os.path.join(GOLD, "tr6_python_ref_noisy.npz"))
+    x = g["x"]
+    k = [int(v) for v in g["k"]]
+    res = ttr.tr_svd(_to_dev(x, gpu), k, gemm="tc")
+    # step-1 singular values are convention independent
+    np.testing.assert_allclose(res.sigmas[0][:4], g["sigma1"][:4], rtol=SIG_REL)
+    err = oracle.rel_error(x, oracle.tr_full(_cores_np(res), "gpu"))
+    ref_cores, _ = oracle.tr_svd(x, k, convention="gpu")
+    assert abs(err - oracle.rel_error(x, oracle.tr_full(ref_cores, "gpu"))) < ERR_ABS
+
+
+def test_host_io_path_and_device_error(gpu):
+    ttr = _ttr()
+    x = oracle.make_tt_tensor([20, 30, 40], [1, 6, 6, 1], 1e-3, seed=23)
+    res = ttr.tt_svd(x, [1, 6, 6, 1])  # NumPy in, NumPy cores out
+    e_host = oracle.rel_error(x, oracle.tt_full([c.astype(np.float64) for c in res.cores], "gpu"))
+    import torch
+    xd = _to_dev(x, gpu)
+    cores = [torch.from_numpy(np.ascontiguousarray(c.transpose(2, 1, 0))).to(gpu).permute(2, 1, 0)
+             for c in res.cores]
+    e_dev = ttr.rel_error(xd, cores)
+    assert abs(e_host - e_dev) < 1e-6
+    assert e_dev < 5e-3
+
+
+def test_nonfinite_input_rejected(gpu):
+    ttr = _ttr()
+    x = oracle.make_tt_tensor([10, 10, 10], [1, 3, 3, 1], 0.0, seed=1)
+    x[3, 4, 5] = np.nan
+    with pytest.raises(ttr.TTError) as e:
+        ttr.tt_svd(_to_dev(x, gpu), [1, 3, 3, 1], flags=ttr.TT_FLAG_CHECK_FINITE)
+    assert e.value.code == 4
+
+
+@pytest.mark.parametrize("ranks", [[2, 3, 3, 1], [1, 0, 3, 1], [1, 3, 3, 2]])
+def test_bad_ranks_rejected(gpu, ranks):
+    ttr = _ttr()
+    x = oracle.make_tt_tensor([10, 10, 10], [1, 3, 3, 1], 0.0, seed=1)
+    with pytest.raises(ttr.TTError) as e:
+        ttr.tt_svd(_to_dev(x, gpu), ranks)
+    assert e.value.code == 3
+
+
+def test_reference_entry_points(gpu, capsys):
+    ttr = _ttr()
+    x = oracle.make_tt_tensor([64, 64, 64], [1, 8, 8, 1], 1e-4, seed=29)
+    err = np.zeros(1, np.float32)
+    cr = np.zeros(1, np.float32)
+    t = ttr.ttdec_gpu_float(x, [64, 64, 64], [1, 8, 8, 1], None, err, cr)
+    assert t > 0 and err[0] < 1e-3
+    x6 = oracle.make_tt_tensor([6] * 6, [1, 3, 3, 3, 3, 3, 1], 1e-4, seed=31)
+    t6 = ttr.ttdec_half_lu_device_6(x6, [1, 3, 3, 3, 3, 3, 1], [6] * 6, 2, 64, True)
+    assert t6 > 0
+    out = capsys.readouterr().out
+    assert "MSE:" in out
+    xr = oracle.make_tr_tensor([6] * 6, 2, 1e-4, seed=37)
+    tr = ttr.trdec_half_lu_device_6(xr, [2, 2, 4, 4, 4, 4, 2], [6] * 6, 1, 64, False)
+    assert tr > 0
+    e3 = np.zeros(1, np.float32)
+    xr3 = oracle.make_tr_tensor([30, 30, 30], 2, 1e-4, seed=41)
+    t3 = ttr.trdec_gpu_float(xr3, [30, 30, 30], [2, 2, 8, 2], None, e3, None)
+    assert t3 > 0 and np.isfinite(e3[0])
+
+
+def test_engines_agree_and_deterministic(gpu):
+    ttr = _ttr()
+    x = oracle.make_tt_tensor([32, 32, 32, 32], [1, 16, 16, 16, 1], 1e-4, seed=43)
+    xd = _to_dev(x, gpu)
+    a = ttr.tt_svd(xd, [1, 16, 16, 16, 1], gemm="tc", seed=5)
+    b = ttr.tt_svd(xd, [1, 16, 16, 16, 1], gemm="tc", seed=5)
+    for ca, cb in zip(a.cores, b.cores):
+        assert np.array_equal(ca.cpu().numpy(), cb.cpu().numpy())
+    c = ttr.tt_svd(xd, [1, 16, 16, 16, 1], gemm="fp32", seed=5)
+    ea = ttr.rel_error(xd, a.cores)
+    ec = ttr.rel_error(xd, c.cores)
+    assert abs(ea - ec) < 1e-4
