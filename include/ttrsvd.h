@@ -150,8 +150,10 @@ int tt_k_project(tt_ctx* ctx, const float* a, long long m, long long n, const fl
                  long long ldq, float* out, long long ldo, int gemm);
 
 /* Gram of the rows W = A * A^T (m x m, FP64), A (m x n, lda = m), m <= TT_MAX_SMALL.
+ * gemm = TT_GEMM_TC uses tcgen05 TF32 tiles (operands rounded to nearest by the TMA unit,
+ * FP32 accumulation, FP64 across blocks); TT_GEMM_FP32 the FP32 FMA kernel.
  * Replaces largeMatrixSelfMulti_once_device (ttdec6_singleGPU.cu:388-401). */
-int tt_k_gram_rows(tt_ctx* ctx, const float* a, long long m, long long n, double* w);
+int tt_k_gram_rows(tt_ctx* ctx, const float* a, long long m, long long n, double* w, int gemm);
 
 /* Gram of a tall matrix W = Z^T Z (N x N, FP64): Z is n x N with element (j, c) at
  * z[j*rs + c*cs] (column-major: rs = 1, cs = ld; row-major: rs = ld, cs = 1). */

@@ -26,7 +26,7 @@ from __future__ import annotations
 import numpy as np
 
 __all__ = [
-    "unfold", "truncated_svd", "gram_eig", "tt_svd", "tr_svd", "tt_full", "tr_full",
+    "unfold", "canon_signs", "truncated_svd", "gram_eig", "tt_svd", "tr_svd", "tt_full", "tr_full",
     "rel_error", "tt_random_cores", "tr_random_cores", "add_noise", "make_tt_tensor",
     "make_tr_tensor", "edrsvd_plain", "edrsvd_gram", "gram_eig_step", "ttdec6_gram",
     "trdec6_gram", "philox4x32_10", "gaussian_from_philox", "ref_uniform_tt_tensor",
@@ -40,6 +40,19 @@ __all__ = [
 def unfold(flat: np.ndarray, m: int, n: int) -> np.ndarray:
     """Column-major (m x n) view of a flat buffer (``TT6:817-818``)."""
     return flat.reshape(m, n, order="F")
+
+
+def canon_signs(u: np.ndarray, svt: np.ndarray, k: int):
+    """Sign convention of the CUDA chain: for each of the first k columns of the basis u, the
+    entry of largest magnitude (lowest row on ties) is made positive; the matching row of
+    svt is negated with it.  TR-SVD's later unfoldings depend on these signs."""
+    for a in range(min(k, u.shape[1])):
+        col = u[:, a]
+        i = int(np.argmax(np.abs(col)))
+        if col[i] < 0:
+            u[:, a] = -col
+            svt[a] = -svt[a]
+    return u, svt
 
 
 def truncated_svd(a: np.ndarray, r: int):
@@ -103,6 +116,7 @@ def tt_svd(x: np.ndarray, ranks, method: str = "svd", convention: str = "gpu", d
             r = u.shape[1]
         sigmas.append(s)
         if convention == "gpu":
+            u, svt = canon_signs(u.copy(), svt.copy(), min(r, a.shape[0], a.shape[1]))
             cores.append(u.reshape(r_prev, n[k], r, order="F"))
         else:
             cores.append(u.reshape(r_prev, n[k], r, order="C"))
@@ -146,6 +160,7 @@ def tr_svd(x: np.ndarray, ranks, method: str = "svd", convention: str = "gpu", d
         uq, s, svt = gram_eig(a, q)
     sigmas = [s]
     if convention == "gpu":
+        uq, svt = canon_signs(uq.copy(), svt.copy(), min(q, n[0], ncols))
         g1 = uq.reshape(n[0], r0, r1, order="F").transpose(1, 0, 2)  # (r0, n1, r1)
         t = svt.reshape(r0, r1, ncols, order="F").transpose(1, 2, 0)  # (r1, N, r0)
         flat = t.ravel(order="F")
@@ -167,6 +182,8 @@ def tr_svd(x: np.ndarray, ranks, method: str = "svd", convention: str = "gpu", d
             u, s, svt = gram_eig(a, ranks[k + 1])
             r = u.shape[1]
         sigmas.append(s)
+        if convention == "gpu":
+            u, svt = canon_signs(u.copy(), svt.copy(), min(r, a.shape[0], a.shape[1]))
         cores.append(u.reshape(r_prev, n[k], r, order=order))
         flat = svt.ravel(order=order)
         r_prev = r

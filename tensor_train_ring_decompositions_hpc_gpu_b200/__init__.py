@@ -233,12 +233,13 @@ def project(a, q, gemm="auto"):
     return out.t()
 
 
-def gram_rows(a):
+def gram_rows(a, gemm="fp32"):
+    """A A^T (FP64) of a column-major (m x n) matrix, m <= 128."""
     torch = _torch()
     a = _as_colmajor(a.float())
     m, n = a.shape
     w = _colmajor(m, m, torch.float64, a.device)
-    check(lib().tt_k_gram_rows(_ctx_for(a.device.index), _ptr(a), m, n, _ptr(w)))
+    check(lib().tt_k_gram_rows(_ctx_for(a.device.index), _ptr(a), m, n, _ptr(w), GEMM[gemm]))
     return w
 
 

@@ -85,7 +85,7 @@ def load():
         "tt_k_gaussian": (i, [vp, vp, ll, i, ll, ull, C.c_uint]),
         "tt_k_sketch": (i, [vp, vp, ll, ll, vp, i, ll, vp, i]),
         "tt_k_project": (i, [vp, vp, ll, ll, vp, i, ll, vp, ll, i]),
-        "tt_k_gram_rows": (i, [vp, vp, ll, ll, vp]),
+        "tt_k_gram_rows": (i, [vp, vp, ll, ll, vp, i]),
         "tt_k_gram_tall": (i, [vp, vp, ll, i, ll, ll, vp]),
         "tt_k_cholqr2": (i, [vp, vp, ll, i, ll, vp]),
         "tt_k_syev": (i, [vp, vp, i, vp, vp, P(i)]),

@@ -166,12 +166,23 @@ struct Plan {
   std::vector<Step> steps;
   long long total = 0;
   size_t max_data = 0, max_omega = 0, max_y = 0, max_bt = 0, max_core = 0, max_ws = 0;
+  size_t max_ef = (size_t)TT_MAX_SMALL * TT_MAX_SMALL;  // FP32 basis (m x r or ks x r)
   int max_small = 0;
 };
 
 int engine_of(const tt_opts& o) {
   if (o.gemm == TT_GEMM_FP32) return TT_GEMM_FP32;
   return tc_available() ? TT_GEMM_TC : TT_GEMM_FP32;
+}
+
+// Engine of a bulk pass over an m x cols unfolding.  TT_GEMM_AUTO keeps passes below 2^24
+// elements on the FP32 kernels (they are cheap there and carry full FP32 precision); the
+// tensor cores take the large unfoldings, where HBM bandwidth decides.
+int engine_for(const tt_opts& o, long long m, long long cols) {
+  const int e = engine_of(o);
+  if (e == TT_GEMM_TC && o.gemm == TT_GEMM_AUTO && (double)m * (double)cols < 16777216.0)
+    return TT_GEMM_FP32;
+  return e;
 }
 
 int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Plan& P) {
@@ -248,6 +259,7 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
       P.max_bt = std::max<size_t>(P.max_bt, (size_t)st.next_elems);
     if (!st.fold) P.max_data = std::max<size_t>(P.max_data, (size_t)st.next_elems);
     P.max_core = std::max<size_t>(P.max_core, (size_t)st.m * std::max(st.r_req, st.ks));
+    P.max_ef = std::max<size_t>(P.max_ef, (size_t)std::max<long long>(st.m, st.ks) * st.r_req);
     P.max_small = std::max(P.max_small, std::max(st.ks, (int)std::min<long long>(mn, TT_MAX_SMALL)));
     if (st.path == PATH_RAND) {
       P.max_omega = std::max<size_t>(P.max_omega, (size_t)st.cols * st.ks);
@@ -258,6 +270,7 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
       P.max_ws = std::max(P.max_ws, gram_ws_bytes(st.m, st.ks));
     } else {
       P.max_ws = std::max(P.max_ws, gram_ws_bytes(std::max(st.m, st.cols), (int)mn));
+      P.max_ws = std::max(P.max_ws, gram_tc_ws_bytes(st.m, st.cols));
     }
   }
   P.max_ws += (size_t)TT_MAX_SMALL * TT_MAX_SMALL * sizeof(double) * 8;
@@ -296,7 +309,7 @@ size_t plan_bytes(const Plan& P, bool host_io) {
   add(P.max_y * sizeof(float));
   add(P.max_bt * sizeof(float));
   add(P.max_core * sizeof(float));
-  add(S * S * sizeof(float));
+  add(P.max_ef * sizeof(float));
   add(S * S * sizeof(double) * 4);
   add(S * sizeof(double) * 2);
   add(S * S * sizeof(double) * 2);
@@ -318,7 +331,7 @@ int carve(tt_ctx* c, const Plan& P, bool host_io, Bufs& B, Arena& ws) {
   B.yf = a.take<float>(std::max<size_t>(P.max_y, 1));
   B.bt = a.take<float>(std::max<size_t>(P.max_bt, 1));
   B.corebuf = a.take<float>(std::max<size_t>(P.max_core, 1));
-  B.ef = a.take<float>(S * S);
+  B.ef = a.take<float>(P.max_ef);
   B.w = a.take<double>(S * S);
   B.evecs = a.take<double>(S * S);
   B.pend[0] = a.take<double>(S * S);
@@ -405,7 +418,6 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
   Arena ws;
   TT_TRY(carve(c, P, host_io, B, ws));
   cudaStream_t s = c->stream;
-  const int engine = engine_of(o);
   const int max_sweeps = o.max_sweeps > 0 ? o.max_sweeps : 40;
   g_kernel_launches = 0;
   Passes pass;
@@ -445,6 +457,7 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
     const Step& st = P.steps[k];
     const long long m = st.m, cols = st.cols;
     const int rq = st.r_req, re = st.r_eff;
+    const int engine = engine_for(o, m, cols);
     float* next = B.data[slot];
     double* sigdst = c->dsig + (size_t)k * TT_STATS_MAX_SIGMA;
     const bool ring1 = P.ring && k == 0;
@@ -471,13 +484,19 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
     }
 
     if (st.path == PATH_EXACT_ROWS) {
-      TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols,
-                      [&] { return launch_gram(cur, cols, (int)m, m, 1, B.w, false, ws, s); }));
+      TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols, [&] {
+        if (engine == TT_GEMM_TC) {
+          const int rc = launch_gram_tc(cur, m, cols, B.w, ws, c->dstat, s);
+          if (rc != TT_ERR_UNSUPPORTED) return rc;
+        }
+        return launch_gram(cur, cols, (int)m, m, 1, B.w, false, ws, s);
+      }));
       TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
-      // basis (m x r_req, zero-padded beyond r_eff), FP32
+      // basis (m x r_req, zero-padded beyond r_eff), FP32, canonical column signs
       TT_TRY(launch_f64_to_f32_cols(B.evecs, m, m, re, B.ef, m, rq, s));
+      TT_TRY(launch_canon_cols(B.ef, m, re, m, B.evecs, (int)m, m, s));
       if (ring1) {
         TT_TRY(launch_ring_core1(B.ef, (int)m, P.r[0], P.r[1], cores[0], s));
       } else {
@@ -495,7 +514,7 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
       TT_TRY(pass.run(TT_PASS_PROJECT, 2.0 * m * cols * rq, 4.0 * m * cols + 4.0 * rq * cols, [&] {
         return launch_project(cur, m, cols, B.ef, rq, m, next, st.perm231 ? 0 : rq,
                               st.perm231 ? OUT_PERM231 : OUT_ROWMAJOR, P.r[0], P.r[1],
-                              engine == TT_GEMM_TC && re < m ? TT_GEMM_TC : TT_GEMM_FP32, ws, s);
+                              engine == TT_GEMM_TC && re < m ? TT_GEMM_TC : TT_GEMM_FP32, ws, c->dstat, s);
       }));
     } else if (st.path == PATH_EXACT_COLS) {
       // W = A^T A over the rows of A (vectors = rows i, components = columns)
@@ -509,6 +528,7 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
       TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * m * cols * rq, 4.0 * m * cols + 4.0 * m * rq, [&] {
         return launch_small_nn(cur, m, (int)cols, m, B.evecs, rq, cols, B.colscale, re, ubuf, m, s);
       }));
+      TT_TRY(launch_canon_cols(ubuf, m, re, m, B.evecs, (int)cols, cols, s));
       if (ring1) {
         TT_TRY(launch_ring_core1(ubuf, (int)m, P.r[0], P.r[1], cores[0], s));
       } else {
@@ -527,42 +547,43 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
       const double fl_pass = 2.0 * m * cols * ks;
       const double by_pass = 4.0 * m * cols + 4.0 * cols * ks;
       TT_TRY(pass.run(TT_PASS_SKETCH, fl_pass, by_pass, [&] {
-        return launch_sketch(cur, m, cols, B.omega, ks, 1, cols, B.yd, engine, ws, s);
+        return launch_sketch(cur, m, cols, B.omega, ks, 1, cols, B.yd, engine, ws, c->dstat, s);
       }));
       TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, ks, B.yf, m, ks, s));
       TT_TRY(launch_cholqr2(B.yf, m, ks, 1, m, nullptr, ws, c->dstat, s));
       for (int it = 0; it < o.power_iters; ++it) {
         TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
-          return launch_project(cur, m, cols, B.yf, ks, m, B.bt, ks, OUT_ROWMAJOR, 1, 1, engine, ws, s);
+          return launch_project(cur, m, cols, B.yf, ks, m, B.bt, ks, OUT_ROWMAJOR, 1, 1, engine, ws, c->dstat, s);
         }));
         TT_TRY(pass.run(TT_PASS_OTHER, 6.0 * cols * ks * ks, 24.0 * cols * ks, [&] {
           return launch_cholqr2(B.bt, cols, ks, ks, 1, nullptr, ws, c->dstat, s);
         }));
         TT_TRY(pass.run(TT_PASS_SKETCH, fl_pass, by_pass, [&] {
-          return launch_sketch(cur, m, cols, B.bt, ks, ks, 1, B.yd, engine, ws, s);
+          return launch_sketch(cur, m, cols, B.bt, ks, ks, 1, B.yd, engine, ws, c->dstat, s);
         }));
         TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, ks, B.yf, m, ks, s));
         TT_TRY(launch_cholqr2(B.yf, m, ks, 1, m, nullptr, ws, c->dstat, s));
       }
       // B^T = A^T Q (cols x ks, row-major) = B (ks x cols, column-major)
       TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
-        return launch_project(cur, m, cols, B.yf, ks, m, B.bt, ks, OUT_ROWMAJOR, 1, 1, engine, ws, s);
+        return launch_project(cur, m, cols, B.yf, ks, m, B.bt, ks, OUT_ROWMAJOR, 1, 1, engine, ws, c->dstat, s);
       }));
       TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ks * ks, 4.0 * cols * ks,
                       [&] { return launch_gram(B.bt, cols, ks, ks, 1, B.w, true, ws, s); }));
       TT_TRY(launch_syev(B.w, ks, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, std::min(ks, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
+      // core = Q E_r with canonical column signs (E's columns follow)
+      float* ubuf = B.corebuf;
+      TT_TRY(launch_small_nn(B.yf, m, ks, m, B.evecs, rq, ks, nullptr, re, ubuf, m, s));
+      TT_TRY(launch_canon_cols(ubuf, m, re, m, B.evecs, ks, ks, s));
       // next = E_r^T B  (rotation of the small factor; plain FP32 keeps it exact to FP32)
       TT_TRY(launch_f64_to_f32_cols(B.evecs, ks, ks, re, B.ef, ks, rq, s));
       TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * ks * cols * rq, 4.0 * ks * cols + 4.0 * rq * cols, [&] {
         return launch_project(B.bt, ks, cols, B.ef, rq, ks, next, st.perm231 ? 0 : rq,
                               st.perm231 ? OUT_PERM231 : OUT_ROWMAJOR, P.r[0], P.r[1], TT_GEMM_FP32,
-                              ws, s);
+                              ws, c->dstat, s);
       }));
-      // core = Q E_r
-      float* ubuf = B.corebuf;
-      TT_TRY(launch_small_nn(B.yf, m, ks, m, B.evecs, rq, ks, nullptr, re, ubuf, m, s));
       if (ring1) {
         TT_TRY(launch_ring_core1(ubuf, (int)m, P.r[0], P.r[1], cores[0], s));
       } else {
@@ -673,12 +694,13 @@ extern "C" int tt_rel_error(tt_ctx* c, const float* x, int d, const int* n, cons
   long long N = 1;
   for (int k = 1; k < d; ++k) N *= n[k];
   // merged right part M_k sizes: r_{k-1} * (n_k ... n_d) * r_d
+  // M_k (cores k..d-1 merged) holds r[k] * n[k] * ... * n[d-1] * r[d] floats.
   long long maxm = 0;
   {
     long long rest = r[d];
     for (int k = d - 1; k >= 1; --k) {
       rest *= n[k];
-      maxm = std::max(maxm, (long long)r[k - 1] * rest);
+      maxm = std::max(maxm, (long long)r[k] * rest);
     }
   }
   TT_TRY(tt_ctx_reserve(c, sizeof(float) * (size_t)maxm * 2 + 4096 + (1 << 20)));
@@ -763,9 +785,9 @@ extern "C" int tt_k_sketch(tt_ctx* c, const float* a, long long m, long long n, 
   Arena ws;
   TT_TRY(ws_for(c, sketch_ws_bytes(m, n, N) * 2, ws));
   const int eng = (gemm == TT_GEMM_FP32 || !tc_available()) ? TT_GEMM_FP32 : TT_GEMM_TC;
-  TT_TRY(launch_sketch(a, m, n, w, N, 1, ldw, y, eng, ws, c->stream));
-  TT_CUDA(cudaStreamSynchronize(c->stream));
-  return TT_OK;
+  TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
+  TT_TRY(launch_sketch(a, m, n, w, N, 1, ldw, y, eng, ws, c->dstat, c->stream));
+  return check_status(c);
 }
 
 extern "C" int tt_k_project(tt_ctx* c, const float* a, long long m, long long n, const float* q,
@@ -782,12 +804,13 @@ extern "C" int tt_k_project(tt_ctx* c, const float* a, long long m, long long n,
   Arena ws;
   TT_TRY(ws_for(c, 1 << 20, ws));
   const int eng = (gemm == TT_GEMM_FP32 || !tc_available()) ? TT_GEMM_FP32 : TT_GEMM_TC;
-  TT_TRY(launch_project(a, m, n, q, N, ldq, out, ldo, OUT_ROWMAJOR, 1, 1, eng, ws, c->stream));
-  TT_CUDA(cudaStreamSynchronize(c->stream));
-  return TT_OK;
+  TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
+  TT_TRY(launch_project(a, m, n, q, N, ldq, out, ldo, OUT_ROWMAJOR, 1, 1, eng, ws, c->dstat, c->stream));
+  return check_status(c);
 }
 
-extern "C" int tt_k_gram_rows(tt_ctx* c, const float* a, long long m, long long n, double* w) {
+extern "C" int tt_k_gram_rows(tt_ctx* c, const float* a, long long m, long long n, double* w,
+                              int gemm) {
   TT_NEED(c);
   TT_NEED(a);
   TT_NEED(w);
@@ -797,10 +820,13 @@ extern "C" int tt_k_gram_rows(tt_ctx* c, const float* a, long long m, long long 
   }
   TT_CUDA(cudaSetDevice(c->device));
   Arena ws;
-  TT_TRY(ws_for(c, gram_ws_bytes(n, (int)m), ws));
-  TT_TRY(launch_gram(a, n, (int)m, m, 1, w, false, ws, c->stream));
-  TT_CUDA(cudaStreamSynchronize(c->stream));
-  return TT_OK;
+  TT_TRY(ws_for(c, std::max(gram_ws_bytes(n, (int)m), gram_tc_ws_bytes(m, n)), ws));
+  TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
+  int rc = TT_ERR_UNSUPPORTED;
+  if (gemm != TT_GEMM_FP32 && tc_available()) rc = launch_gram_tc(a, m, n, w, ws, c->dstat, c->stream);
+  if (rc == TT_ERR_UNSUPPORTED) rc = launch_gram(a, n, (int)m, m, 1, w, false, ws, c->stream);
+  TT_TRY(rc);
+  return check_status(c);
 }
 
 extern "C" int tt_k_gram_tall(tt_ctx* c, const float* z, long long n, int N, long long rs,

@@ -188,18 +188,24 @@ size_t sketch_ws_bytes(long long m, long long n, int N) {
   long long jchunk;
   int nsplit;
   sketch_split_plan(m, n, &jchunk, &nsplit);
-  return (size_t)nsplit * (size_t)N * (size_t)m * sizeof(double) + 4096;
+  const size_t simt = (size_t)nsplit * (size_t)N * (size_t)m * sizeof(double) + 4096;
+  return std::max(simt, sketch_tc_ws_bytes(m, n, N));
 }
 
-int launch_sketch_tc(const float* a, long long m, long long n, const float* w, int N, long long wj,
-                     long long wc, double* y, Arena& ws, cudaStream_t s);
+int launch_reduce_splits(const double* part, long long count, int nsplit, double* y, cudaStream_t s) {
+  if (count <= 0) return TT_OK;
+  k_reduce_splits<<<std::min(ceil_div(count, 256), 8 * num_sms()), 256, 0, s>>>(part, count, nsplit, y);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  return TT_OK;
+}
 
 int launch_sketch(const float* a, long long m, long long n, const float* w, int N, long long wj,
-                  long long wc, double* y, int engine, Arena& ws, cudaStream_t s) {
+                  long long wc, double* y, int engine, Arena& ws, DevStatus* st, cudaStream_t s) {
   if (m <= 0 || n <= 0 || N <= 0) return TT_OK;
   if (engine == TT_GEMM_TC) {
-    int st = launch_sketch_tc(a, m, n, w, N, wj, wc, y, ws, s);
-    if (st != TT_ERR_UNSUPPORTED) return st;
+    int rc = launch_sketch_tc(a, m, n, w, N, wj, wc, y, ws, st, s);
+    if (rc != TT_ERR_UNSUPPORTED) return rc;
   }
   long long jchunk;
   int nsplit;
@@ -221,11 +227,7 @@ int launch_sketch(const float* a, long long m, long long n, const float* w, int 
   }
   count_launch();
   TT_LAUNCH_CHECK();
-  const long long count = (long long)N * m;
-  k_reduce_splits<<<std::min(ceil_div(count, 256), 8 * num_sms()), 256, 0, s>>>(part, count,
-                                                                                 nsplit, y);
-  count_launch();
-  TT_LAUNCH_CHECK();
+  TT_TRY(launch_reduce_splits(part, (long long)N * m, nsplit, y, s));
   ws.reset(mk);
   return TT_OK;
 }
@@ -316,17 +318,13 @@ __global__ void __launch_bounds__(256) k_project_simt(const float* __restrict__ 
   }
 }
 
-int launch_project_tc(const float* a, long long m, long long n, const float* q, int N,
-                      long long ldq, float* out, long long ldo, int mode, int r0, int r1,
-                      Arena& ws, cudaStream_t s);
-
 int launch_project(const float* a, long long m, long long n, const float* q, int N, long long ldq,
                    float* out, long long ldo, int mode, int r0, int r1, int engine, Arena& ws,
-                   cudaStream_t s) {
+                   DevStatus* st, cudaStream_t s) {
   if (n <= 0 || N <= 0) return TT_OK;
   if (engine == TT_GEMM_TC) {
-    int st = launch_project_tc(a, m, n, q, N, ldq, out, ldo, mode, r0, r1, ws, s);
-    if (st != TT_ERR_UNSUPPORTED) return st;
+    int rc = launch_project_tc(a, m, n, q, N, ldq, out, ldo, mode, r0, r1, ws, st, s);
+    if (rc != TT_ERR_UNSUPPORTED) return rc;
   }
   const int NT = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : 64;
   dim3 grid(ceil_div(n, 256), ceil_div(N, NT));
@@ -660,7 +658,9 @@ __global__ void __launch_bounds__(128) k_apply_rinv(float* __restrict__ y, long 
     }
   }
   __syncthreads();
-  constexpr int CB = NP < 32 ? NP : 32;
+  // Output chunk width divides NP (NP is a multiple of 16), so cb + c < NP always.
+  constexpr int CB = (NP % 32 == 0) ? 32 : 16;
+  static_assert(NP % CB == 0, "chunk width must divide the padded width");
   for (int cb = 0; cb < NP; cb += CB) {
     float outv[CB];
 #pragma unroll
@@ -1073,6 +1073,57 @@ int launch_ring_core1(const float* u, int n1, int r0, int r1, float* core, cudaS
   const int total = n1 * r0 * r1;
   if (total <= 0) return TT_OK;
   k_ring_core1<<<ceil_div(total, 256), 256, 0, s>>>(u, n1, r0, r1, core);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  return TT_OK;
+}
+
+// Sign convention of every basis column: the entry of largest magnitude (lowest row on ties)
+// is made positive, and column a of the FP64 companion (the small factor that produced the
+// basis) is negated together with it.  TR-SVD's later unfoldings depend on these signs.
+__global__ void __launch_bounds__(256) k_canon_cols(float* __restrict__ u, long long m, int r,
+                                                    long long ldu, double* __restrict__ comp, int K,
+                                                    long long ldc) {
+  __shared__ float bv[256];
+  __shared__ long long bi[256];
+  __shared__ int flip;
+  const int a = blockIdx.x;
+  if (a >= r) return;
+  float best = -1.f;
+  long long besti = 0;
+  for (long long i = threadIdx.x; i < m; i += blockDim.x) {
+    const float v = fabsf(u[i + ldu * a]);
+    if (v > best) {
+      best = v;
+      besti = i;
+    }
+  }
+  bv[threadIdx.x] = best;
+  bi[threadIdx.x] = besti;
+  __syncthreads();
+  for (int o = blockDim.x / 2; o > 0; o >>= 1) {
+    if (threadIdx.x < o) {
+      const float v2 = bv[threadIdx.x + o];
+      const long long i2 = bi[threadIdx.x + o];
+      if (v2 > bv[threadIdx.x] || (v2 == bv[threadIdx.x] && i2 < bi[threadIdx.x])) {
+        bv[threadIdx.x] = v2;
+        bi[threadIdx.x] = i2;
+      }
+    }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) flip = (bv[0] > 0.f && u[bi[0] + ldu * a] < 0.f) ? 1 : 0;
+  __syncthreads();
+  if (!flip) return;
+  for (long long i = threadIdx.x; i < m; i += blockDim.x) u[i + ldu * a] = -u[i + ldu * a];
+  if (comp)
+    for (int k = threadIdx.x; k < K; k += blockDim.x) comp[k + ldc * a] = -comp[k + ldc * a];
+}
+
+int launch_canon_cols(float* u, long long m, int r, long long ldu, double* comp, int K,
+                      long long ldc, cudaStream_t s) {
+  if (r <= 0 || m <= 0) return TT_OK;
+  k_canon_cols<<<r, 256, 0, s>>>(u, m, r, ldu, comp, K, ldc);
   count_launch();
   TT_LAUNCH_CHECK();
   return TT_OK;

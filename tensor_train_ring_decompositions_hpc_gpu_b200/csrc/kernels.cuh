@@ -32,7 +32,10 @@ int launch_gaussian(float* out, long long rows, int cols, long long ld, unsigned
 // Y (m x N, FP64, ld = m) = A (m x n, lda = m) * W, W element (j, c) at w[j*wj + c*wc].
 // engine: TT_GEMM_FP32 or TT_GEMM_TC.
 int launch_sketch(const float* a, long long m, long long n, const float* w, int N, long long wj,
-                  long long wc, double* y, int engine, Arena& ws, cudaStream_t s);
+                  long long wc, double* y, int engine, Arena& ws, DevStatus* st, cudaStream_t s);
+
+// y[idx] = sum over splits of part[split * count + idx] (FP64, fixed order).
+int launch_reduce_splits(const double* part, long long count, int nsplit, double* y, cudaStream_t s);
 
 // Output modes of the projection.
 enum { OUT_ROWMAJOR = 0, OUT_PERM231 = 1 };
@@ -41,7 +44,7 @@ enum { OUT_ROWMAJOR = 0, OUT_PERM231 = 1 };
 // OUT_PERM231: column c = a + r0*b of Q^T A goes to out[b + r1*(j + n*a)] (TR bond permute).
 int launch_project(const float* a, long long m, long long n, const float* q, int N, long long ldq,
                    float* out, long long ldo, int mode, int r0, int r1, int engine, Arena& ws,
-                   cudaStream_t s);
+                   DevStatus* st, cudaStream_t s);
 
 // W (M x M, FP64, ld = M) = sum_j x_j x_j^T with x_j[c] = x[j*vs + c*es], M <= 128.
 // acc64: FP64 products and accumulation; else FP32 products with FP64 flush every 1024 vectors.
@@ -85,6 +88,11 @@ int launch_inv_sigma(const double* evals, int k, double* colscale, double rel_fl
 // Ring core 1: core[a + r0*(i + n1*b)] = u[i + n1*(a + r0*b)].
 int launch_ring_core1(const float* u, int n1, int r0, int r1, float* core, cudaStream_t s);
 
+// Column sign convention: largest-magnitude entry of each of the first r columns of U made
+// positive; the same columns of the FP64 companion (K rows, ldc) are negated alongside.
+int launch_canon_cols(float* u, long long m, int r, long long ldu, double* comp, int K,
+                      long long ldc, cudaStream_t s);
+
 // NaN/Inf scan; *flag set to 1 when found.
 int launch_check_finite(const float* x, long long count, int* flag, cudaStream_t s);
 
@@ -100,7 +108,17 @@ int launch_gemm_nn(const float* a, long long M, int K, const float* b, long long
 int launch_recon_err(const float* x, int n1, long long N, const float* g1, int r0, int r1,
                      const float* mrg, double* acc, cudaStream_t s);
 
-// Tensor-core engine availability (sm_100 device and kernels compiled in).
+// Tensor-core engine availability (sm_100 device, TMA encoder found, TTR_DISABLE_TC unset).
 bool tc_available();
+size_t sketch_tc_ws_bytes(long long m, long long n, int N);
+size_t gram_tc_ws_bytes(long long m, long long n);
+// W (m x m, FP64, ld = m) = A A^T on the tensor cores, A column-major m x n, m <= 128.
+int launch_gram_tc(const float* a, long long m, long long n, double* w, Arena& ws, DevStatus* st,
+                   cudaStream_t s);
+int launch_sketch_tc(const float* a, long long m, long long n, const float* w, int N, long long wj,
+                     long long wc, double* y, Arena& ws, DevStatus* st, cudaStream_t s);
+int launch_project_tc(const float* a, long long m, long long n, const float* q, int N,
+                      long long ldq, float* out, long long ldo, int mode, int r0, int r1,
+                      Arena& ws, DevStatus* st, cudaStream_t s);
 
 }  // namespace ttr

@@ -113,7 +113,10 @@ static float order6(float* h_a, const int* ranks, const int* dims, int times, bo
     if (t < 0) return (float)t;
     total += t;
     // Same report line as the reference (ttdec6_singleGPU.cu:782); the value is ||X-X^||/||X||.
-    if (cal_error) printf("\n*********************** MSE: %f ******************\n", err);
+    if (cal_error) {
+      printf("\n*********************** MSE: %f ******************\n", err);
+      fflush(stdout);
+    }
   }
   return (float)(total / times);
 }

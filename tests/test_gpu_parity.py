@@ -32,17 +32,34 @@ def _cores_np(res):
     return [c.detach().cpu().numpy().astype(np.float64) for c in res.cores]
 
 
-def _check(x, res, ref_cores, ref_sig, ring, nsig=4, err_abs=ERR_ABS, sig_rel=SIG_REL):
+def _targets(ranks, ring):
+    """Target rank of each unfolding: r0*r1 for a ring's first split, r_{k+1} otherwise."""
+    d = len(ranks) - 1
+    return [ranks[0] * ranks[1] if (ring and k == 0) else ranks[k + 1] for k in range(d - 1)]
+
+
+# Absolute floor of the singular-value comparison, relative to sigma_1 of the unfolding:
+# FP32 inputs resolve ~1e-6 of sigma_1; TF32 tensor-core operands (10-bit mantissa, rounded
+# to nearest) resolve ~2e-4 of sigma_1 on unfoldings with few rows.
+SIG_FLOOR = {"fp32": 2e-6, "auto": 2e-6, "tc": 2e-4}
+
+
+def _check(x, res, ref_cores, ref_sig, ring, ranks, nsig=4, err_abs=ERR_ABS, sig_rel=SIG_REL,
+           skip_first=False, gemm="auto"):
+    """Reconstruction error within err_abs of the oracle's; leading singular values (up to the
+    unfolding's target rank) within sig_rel plus the engine's floor SIG_FLOOR * sigma_1."""
     full = oracle.tr_full if ring else oracle.tt_full
     err = oracle.rel_error(x, full(_cores_np(res), "gpu"))
     err_ref = oracle.rel_error(x, full(ref_cores, "gpu"))
     assert abs(err - err_ref) <= err_abs, (err, err_ref)
+    tg = _targets(ranks, ring)
     for k, s_ref in enumerate(ref_sig):
-        s = res.sigmas[k]
-        if len(s) == 0:
+        if skip_first and k == 0:
             continue
-        kk = min(nsig, len(s), len(s_ref))
-        np.testing.assert_allclose(s[:kk], s_ref[:kk], rtol=sig_rel, err_msg=f"unfolding {k + 1}")
+        s = res.sigmas[k]
+        kk = min(nsig, len(s), len(s_ref), tg[k])
+        np.testing.assert_allclose(s[:kk], s_ref[:kk], rtol=sig_rel, atol=SIG_FLOOR[gemm] * s_ref[0],
+                                   err_msg=f"unfolding {k + 1}")
     return err, err_ref
 
 
@@ -72,10 +89,10 @@ def test_tt_parity(gpu, shape, ranks, noise, gemm, opts):
     ref_cores, ref_sig = oracle.tt_svd(x, ranks)
     for k, c in enumerate(res.cores):
         assert tuple(c.shape) == (ranks[k], shape[k], ranks[k + 1])
-    _check(x, res, ref_cores, ref_sig, ring=False)
+    _check(x, res, ref_cores, ref_sig, ring=False, ranks=ranks, gemm=gemm)
 
 
-@pytest.mark.parametrize("gemm", ["fp32", "tc"])
+@pytest.mark.parametrize("gemm", ["fp32", "tc", "auto"])
 @pytest.mark.parametrize("shape,ranks", [
     ((6, 6, 6, 6, 6, 6), (2, 3, 6, 6, 6, 3, 2)),
     ((8, 8, 8, 8, 8, 8), (2, 4, 8, 8, 8, 8, 2)),
@@ -87,7 +104,7 @@ def test_tr_parity(gpu, gemm, shape, ranks):
     x = oracle.make_tr_tensor(list(shape), 2, 1e-4, seed=13).astype(np.float64)
     res = ttr.tr_svd(_to_dev(x, gpu), list(ranks), gemm=gemm)
     ref_cores, ref_sig = oracle.tr_svd(x, list(ranks))
-    _check(x, res, ref_cores, ref_sig, ring=True)
+    _check(x, res, ref_cores, ref_sig, ring=True, ranks=list(ranks), gemm=gemm)
 
 
 def test_tr_rank_above_first_mode_is_zero_padded(gpu):
@@ -97,7 +114,7 @@ def test_tr_rank_above_first_mode_is_zero_padded(gpu):
     ranks = [4, 4, 4, 4, 4, 4, 4]
     res = ttr.tr_svd(_to_dev(x, gpu), ranks, gemm="tc")
     ref_cores, ref_sig = oracle.tr_svd(x, ranks)
-    _check(x, res, ref_cores, ref_sig, ring=True)
+    _check(x, res, ref_cores, ref_sig, ring=True, ranks=ranks, gemm="tc")
     g1 = res.cores[0].cpu().numpy()
     # bond components 8..15 of (a + 4 b) are zero columns
     flat = g1.transpose(1, 0, 2).reshape(8, 16, order="F")
@@ -112,10 +129,7 @@ def test_fold_modes_same_error(gpu, flags):
     fl = {"none": 0, "no_fold": ttr.TT_FLAG_NO_FOLD, "identity": ttr.TT_FLAG_IDENTITY_GAUGE}[flags]
     res = ttr.tt_svd(_to_dev(x, gpu), ranks, gemm="tc", flags=fl)
     ref_cores, ref_sig = oracle.tt_svd(x, ranks)
-    if flags == "identity":
-        ref_sig = ref_sig[1:]
-        res.sigmas = res.sigmas[1:]
-    _check(x, res, ref_cores, ref_sig, ring=False)
+    _check(x, res, ref_cores, ref_sig, ring=False, ranks=ranks, skip_first=(flags == "identity"), gemm="tc")
     # left-orthonormal cores (all but the last)
     for c in _cores_np(res)[:-1]:
         u = c.reshape(-1, c.shape[2], order="F")
@@ -128,13 +142,13 @@ def test_golden_python_reference_through_gpu(gpu):
     g = np.load(os.path.join(GOLD, "tt6_python_ref.npz"))
     x = g["x"]
     k = [int(v) for v in g["k"]]
-    res = ttr.tt_svd(_to_dev(x, gpu), k, gemm="tc")
+    res = ttr.tt_svd(_to_dev(x, gpu), k)
     err = oracle.rel_error(x, oracle.tt_full(_cores_np(res), "gpu"))
     assert abs(err - float(g["err"])) < ERR_ABS
     for j in range(5):
         s_ref = g[f"sigma{j + 1}"]
-        kk = min(3, len(res.sigmas[j]))
-        np.testing.assert_allclose(res.sigmas[j][:kk], s_ref[:kk], rtol=SIG_REL)
+        kk = min(3, len(res.sigmas[j]), k[j + 1])
+        np.testing.assert_allclose(res.sigmas[j][:kk], s_ref[:kk], rtol=SIG_REL, atol=2e-6 * s_ref[0])
 
 
 def test_golden_python_reference_tr_error(gpu):
@@ -182,7 +196,7 @@ def test_bad_ranks_rejected(gpu, ranks):
     assert e.value.code == 3
 
 
-def test_reference_entry_points(gpu, capsys):
+def test_reference_entry_points(gpu, capfd):
     ttr = _ttr()
     x = oracle.make_tt_tensor([64, 64, 64], [1, 8, 8, 1], 1e-4, seed=29)
     err = np.zeros(1, np.float32)
@@ -192,7 +206,7 @@ def test_reference_entry_points(gpu, capsys):
     x6 = oracle.make_tt_tensor([6] * 6, [1, 3, 3, 3, 3, 3, 1], 1e-4, seed=31)
     t6 = ttr.ttdec_half_lu_device_6(x6, [1, 3, 3, 3, 3, 3, 1], [6] * 6, 2, 64, True)
     assert t6 > 0
-    out = capsys.readouterr().out
+    out = capfd.readouterr().out
     assert "MSE:" in out
     xr = oracle.make_tr_tensor([6] * 6, 2, 1e-4, seed=37)
     tr = ttr.trdec_half_lu_device_6(xr, [2, 2, 4, 4, 4, 4, 2], [6] * 6, 1, 64, False)
@@ -214,4 +228,5 @@ def test_engines_agree_and_deterministic(gpu):
     c = ttr.tt_svd(xd, [1, 16, 16, 16, 1], gemm="fp32", seed=5)
     ea = ttr.rel_error(xd, a.cores)
     ec = ttr.rel_error(xd, c.cores)
-    assert abs(ea - ec) < 1e-4
+    # TF32 operands (round to nearest) add ~1e-4-level white error per projected step
+    assert ea < ERR_ABS and ec < ERR_ABS and abs(ea - ec) < 5e-4
