@@ -170,6 +170,19 @@ int tt_k_cholqr2(tt_ctx* ctx, float* y, long long n, int N, long long ld, double
  * cusolverDnSsyevd + matrixInvertColumn (ttdec6_singleGPU.cu:274-290,334-385). */
 int tt_k_syev(tt_ctx* ctx, const double* w, int N, double* evals, double* evecs, int* sweeps);
 
+/* Allocation-free sketch Y = A * W (same operands and result as tt_k_sketch), for callers
+ * that cannot call cudaMalloc: a process whose device memory belongs to another allocator or
+ * a pre-reserved arena, or a latency-critical loop that must not let cudaMalloc synchronise
+ * the device.  No context is needed; the call allocates nothing.  The kernel's split-K
+ * scratch is one static device array of 2^21 doubles (16 MiB, held by every GPU that loads
+ * the library until exit); m * N above 2^21 - 32 is rejected with TT_ERR_SHAPE.  All calls
+ * share that array: calls that overlap on the GPU race and must be serialised.  The first
+ * call on a device looks up the array's address (with that device current) and should come
+ * before any stream capture.  Runs on `stream` (NULL = legacy default stream) and returns
+ * after the result is complete.  This entry point has no counterpart in the reference. */
+int tt_k_sketch_noalloc(const float* a, long long m, long long n, const float* w, int N,
+                        long long ldw, double* y, int gemm, void* stream);
+
 /* TR bond permute (r0, r1, N) -> (r1, N, r0), column-major.  Replaces tensorToMode231
  * (trdecomposition/high_order_GPUs/trdec6_singleGPU.cu:49-58). */
 int tt_k_permute231(tt_ctx* ctx, const float* in, float* out, int r0, int r1, long long n);

@@ -28,7 +28,7 @@ EXPORTED = [
     "tt_ctx_create", "tt_ctx_destroy", "tt_ctx_set_stream", "tt_ctx_reserve", "tt_last_error",
     "tt_default_opts", "tt_abi_version", "tt_svd", "tr_svd", "tt_rel_error", "tt_k_gaussian",
     "tt_k_sketch", "tt_k_project", "tt_k_gram_rows", "tt_k_gram_tall", "tt_k_cholqr2",
-    "tt_k_syev", "tt_k_permute231", "tt_ref_ttdec_gpu_float", "tt_ref_trdec_gpu_float",
+    "tt_k_syev", "tt_k_sketch_noalloc", "tt_k_permute231", "tt_ref_ttdec_gpu_float", "tt_ref_trdec_gpu_float",
     "tt_ref_ttdec_half_lu_device_6", "tt_ref_trdec_half_lu_device_6",
 ]
 
@@ -90,6 +90,7 @@ def load():
         "tt_k_cholqr2": (i, [vp, vp, ll, i, ll, vp]),
         "tt_k_syev": (i, [vp, vp, i, vp, vp, P(i)]),
         "tt_k_permute231": (i, [vp, vp, vp, i, i, ll]),
+        "tt_k_sketch_noalloc": (i, [vp, ll, ll, vp, i, ll, vp, i, vp]),
         "tt_ref_ttdec_gpu_float": (C.c_float, [vp, P(i), P(i), P(d), P(C.c_float), P(C.c_float)]),
         "tt_ref_trdec_gpu_float": (C.c_float, [vp, P(i), P(i), P(d), P(C.c_float), P(C.c_float)]),
         "tt_ref_ttdec_half_lu_device_6": (C.c_float, [vp, P(i), P(i), i, i, i]),

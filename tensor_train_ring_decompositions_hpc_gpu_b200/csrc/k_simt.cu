@@ -232,6 +232,40 @@ int launch_sketch(const float* a, long long m, long long n, const float* w, int 
   return TT_OK;
 }
 
+// FP32 sketch with the split partials in caller-provided scratch (`part`, `part_cap` doubles);
+// the split count is lowered until the partials fit.  Allocates nothing.
+int launch_sketch_simt_static(const float* a, long long m, long long n, const float* w, int N,
+                              long long wj, long long wc, double* y, double* part, size_t part_cap,
+                              cudaStream_t s) {
+  if (m <= 0 || n <= 0 || N <= 0) return TT_OK;
+  long long jchunk;
+  int nsplit;
+  sketch_split_plan(m, n, &jchunk, &nsplit);
+  const long long max_ns = (long long)(part_cap / ((size_t)N * (size_t)m));
+  if (max_ns < 1) {
+    set_error(TT_ERR_SHAPE, "sketch partials of %lld x %d doubles exceed the scratch of %zu doubles", m, N,
+              part_cap);
+    return TT_ERR_SHAPE;
+  }
+  if (nsplit > max_ns) {
+    jchunk = (n + max_ns - 1) / max_ns;
+    jchunk = (jchunk + 31) / 32 * 32;
+    nsplit = (int)((n + jchunk - 1) / jchunk);
+  }
+  const int NT = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : 64;
+  const int cblk = ceil_div(N, NT);
+  dim3 grid(ceil_div(m, 256), nsplit, cblk);
+  switch (NT) {
+    case 16: k_sketch_simt<16><<<grid, 256, 0, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
+    case 32: k_sketch_simt<32><<<grid, 256, 0, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
+    case 48: k_sketch_simt<48><<<grid, 256, 0, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
+    default: k_sketch_simt<64><<<grid, 256, 0, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
+  }
+  count_launch();
+  TT_LAUNCH_CHECK();
+  return launch_reduce_splits(part, (long long)N * m, nsplit, y, s);
+}
+
 // ---------------------------------------------------------------------------------------
 // Plain-FP32 projection  out = A^T Q  (A column-major m x n, contraction over m)
 // ---------------------------------------------------------------------------------------

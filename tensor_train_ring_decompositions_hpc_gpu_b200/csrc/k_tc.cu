@@ -1072,4 +1072,65 @@ int launch_sketch_tc(const float* a, long long m, long long n, const float* w, i
   return TT_OK;
 }
 
+
+// Sketch with the split-K partials in caller-provided scratch (`part`, `part_cap` doubles): the
+// split count is lowered until the partials fit.  Allocates nothing.
+int launch_sketch_tc_static(const float* a, long long m, long long n, const float* w, int N,
+                            long long wj, long long wc, double* y, double* part, size_t part_cap,
+                            DevStatus* st, cudaStream_t s) {
+  if (!init_tc()) return TT_ERR_UNSUPPORTED;
+  if (wj != 1 || N > 128 || (m & 31) || (wc & 3) || (reinterpret_cast<uintptr_t>(a) & 15) ||
+      (reinterpret_cast<uintptr_t>(w) & 15) || n > (1LL << 31) - 256 || m > (1LL << 31))
+    return TT_ERR_UNSUPPORTED;
+  int MT, ng, ns;
+  long long kc;
+  const int BN = sketch_tc_plan(m, n, N, &MT, &ng, &ns, &kc);
+  const int BK = MT >= 8 ? 8 : MT == 4 ? 16 : 32;
+  const long long max_ns = (long long)(part_cap / ((size_t)N * (size_t)m));
+  if (max_ns < 1) {
+    set_error(TT_ERR_SHAPE, "sketch partials of %lld x %d doubles exceed the scratch of %zu doubles", m, N,
+              part_cap);
+    return TT_ERR_SHAPE;
+  }
+  if (ns > max_ns) {
+    kc = (n + max_ns - 1) / max_ns;
+    kc = (kc + BK - 1) / BK * BK;
+    ns = (int)((n + kc - 1) / kc);
+  }
+  CUtensorMap ma, mb;
+  TT_TRY(make_map(&ma, a, (unsigned long long)m, (unsigned long long)n, (unsigned long long)m * 4, 32,
+                  (unsigned)BK, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
+  const CUtensorMapSwizzle bsw = BK == 8 ? CU_TENSOR_MAP_SWIZZLE_32B
+                                 : BK == 16 ? CU_TENSOR_MAP_SWIZZLE_64B
+                                            : CU_TENSOR_MAP_SWIZZLE_128B;
+  TT_TRY(make_map(&mb, w, (unsigned long long)n, (unsigned long long)N, (unsigned long long)wc * 4,
+                  (unsigned)BK, (unsigned)BN, bsw, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
+  int rc;
+#define SK(BNV, MTV) rc = run_sketch<BNV, MTV>(ma, mb, m, n, N, kc, ns, ng, part, st, s)
+#define SK_MT(BNV)                   \
+  switch (MT) {                      \
+    case 8: SK(BNV, 8); break;       \
+    case 4: SK(BNV, 4); break;       \
+    case 2: SK(BNV, 2); break;       \
+    default: SK(BNV, 1); break;      \
+  }
+  switch (BN) {
+    case 16: SK_MT(16); break;
+    case 32: SK_MT(32); break;
+    case 48: SK_MT(48); break;
+    case 64: SK_MT(64); break;
+    default:
+      switch (MT) {
+        case 4: SK(128, 4); break;
+        case 2: SK(128, 2); break;
+        default: SK(128, 1); break;
+      }
+      break;
+  }
+#undef SK_MT
+#undef SK
+  if (rc != TT_OK) return rc;
+  return launch_reduce_splits(part, (long long)N * m, ns, y, s);
+}
+
 }  // namespace ttr

@@ -108,6 +108,14 @@ int launch_gemm_nn(const float* a, long long M, int K, const float* b, long long
 int launch_recon_err(const float* x, int n1, long long N, const float* g1, int r0, int r1,
                      const float* mrg, double* acc, cudaStream_t s);
 
+// Sketch variants that take their split-K scratch from the caller (no allocation).
+int launch_sketch_tc_static(const float* a, long long m, long long n, const float* w, int N,
+                            long long wj, long long wc, double* y, double* part, size_t part_cap,
+                            DevStatus* st, cudaStream_t s);
+int launch_sketch_simt_static(const float* a, long long m, long long n, const float* w, int N,
+                              long long wj, long long wc, double* y, double* part, size_t part_cap,
+                              cudaStream_t s);
+
 // Tensor-core engine availability (sm_100 device, TMA encoder found, TTR_DISABLE_TC unset).
 bool tc_available();
 size_t sketch_tc_ws_bytes(long long m, long long n, int N);
