@@ -438,6 +438,7 @@ def run_ours(args, wl):
                        "parallelism": f"replicas x{world}", "flops_per_step": fl,
                        "library_flops_per_step": lib_fl, "hbm_bytes_per_step": stats[-1].bytes},
             "rel_err": err.value,
+            "jacobi_sweeps_max": int(max(st.jacobi_sweeps for st in stats)),
             "roofline": roof,
             "cpu_baseline": cpu,
             "e2e": e2e,
@@ -465,8 +466,15 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--ref-frac", type=float, default=1.0 / 32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--shape", default=None, help="override the mode sizes, e.g. 32,32,32,32,24,24")
+    ap.add_argument("--ranks", default=None, help="override the ranks, e.g. 1,32,32,32,32,24,1")
     args = ap.parse_args()
-    wl = WORKLOADS[args.workload]
+    wl = dict(WORKLOADS[args.workload])
+    if args.shape:
+        wl["shape"] = [int(v) for v in args.shape.split(",")]
+        wl["ranks"] = [int(v) for v in args.ranks.split(",")]
+        wl["desc"] = f"{'TR' if wl['ring'] else 'TT'}-SVD of {'x'.join(map(str, wl['shape']))} " \
+                     f"ranks ({','.join(map(str, wl['ranks']))}), {wl['noise']:g} noise"
     if args.impl == "reference":
         return run_reference(args, wl)
     return run_ours(args, wl)

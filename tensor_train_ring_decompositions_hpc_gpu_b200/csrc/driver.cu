@@ -268,7 +268,11 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
       P.max_ws = std::max(P.max_ws, sketch_ws_bytes(st.m, st.cols, st.ks));
       P.max_ws = std::max(P.max_ws, gram_ws_bytes(st.cols, st.ks));
       P.max_ws = std::max(P.max_ws, gram_ws_bytes(st.m, st.ks));
+      P.max_ws = std::max(P.max_ws, gram_tc_ws_bytes(st.ks, st.cols));
+      P.max_ws = std::max(P.max_ws, project_ws_bytes(st.m, st.cols, st.ks));
+      P.max_ws = std::max(P.max_ws, project_ws_bytes(st.ks, st.cols, st.r_req));
     } else {
+      P.max_ws = std::max(P.max_ws, project_ws_bytes(st.m, st.cols, st.r_req));
       P.max_ws = std::max(P.max_ws, gram_ws_bytes(std::max(st.m, st.cols), (int)mn));
       P.max_ws = std::max(P.max_ws, gram_tc_ws_bytes(st.m, st.cols));
     }
@@ -568,8 +572,15 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
       TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
         return launch_project(cur, m, cols, B.yf, ks, m, B.bt, ks, OUT_ROWMAJOR, 1, 1, engine, ws, c->dstat, s);
       }));
-      TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ks * ks, 4.0 * cols * ks,
-                      [&] { return launch_gram(B.bt, cols, ks, ks, 1, B.w, true, ws, s); }));
+      // Gram of the small factor B (ks x cols, column-major = B^T row-major): the input of the
+      // eigen-based small SVD (TT3O:717), on the tensor cores for long B.
+      TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ks * ks, 4.0 * cols * ks, [&] {
+        if (engine == TT_GEMM_TC) {
+          const int rc = launch_gram_tc(B.bt, ks, cols, B.w, ws, c->dstat, s);
+          if (rc != TT_ERR_UNSUPPORTED) return rc;
+        }
+        return launch_gram(B.bt, cols, ks, ks, 1, B.w, true, ws, s);
+      }));
       TT_TRY(launch_syev(B.w, ks, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, std::min(ks, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
@@ -802,7 +813,7 @@ extern "C" int tt_k_project(tt_ctx* c, const float* a, long long m, long long n,
   }
   TT_CUDA(cudaSetDevice(c->device));
   Arena ws;
-  TT_TRY(ws_for(c, 1 << 20, ws));
+  TT_TRY(ws_for(c, std::max<size_t>(1 << 20, project_ws_bytes(m, n, N)), ws));
   const int eng = (gemm == TT_GEMM_FP32 || !tc_available()) ? TT_GEMM_FP32 : TT_GEMM_TC;
   TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
   TT_TRY(launch_project(a, m, n, q, N, ldq, out, ldo, OUT_ROWMAJOR, 1, 1, eng, ws, c->dstat, c->stream));

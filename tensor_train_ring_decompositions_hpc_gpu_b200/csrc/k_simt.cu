@@ -54,12 +54,15 @@ __global__ void k_gaussian(float* __restrict__ out, long long rows, long long to
     sincospif(2.0f * u1, &s0, &c0);
     sincospif(2.0f * u3, &s1, &c1);
     const float g[4] = {r0 * c0, r0 * s0, r1 * c1, r1 * s1};
+    // element e = row + rows * col; one 64-bit division per call, then step through rows
+    long long col = (4 * c) / rows;
+    long long row = 4 * c - col * rows;
 #pragma unroll
     for (int l = 0; l < 4; ++l) {
-      const long long e = 4 * c + l;
-      if (e < total) {
-        const long long row = e % rows, col = e / rows;
-        out[row + ld * col] = g[l];
+      if (4 * c + l < total) out[row + ld * col] = g[l];
+      if (++row == rows) {
+        row = 0;
+        ++col;
       }
     }
   }
@@ -163,13 +166,33 @@ __global__ void __launch_bounds__(256) k_sketch_simt(const float* __restrict__ a
   (void)cblk;
 }
 
-__global__ void k_reduce_splits(const double* __restrict__ part, long long count, int nsplit,
-                                double* __restrict__ y) {
-  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < count;
-       idx += (long long)gridDim.x * blockDim.x) {
-    double s = 0.0;
-    for (int k = 0; k < nsplit; ++k) s += part[(long long)k * count + idx];
-    y[idx] = s;
+// Sum of nsplit partial blocks: each 256-thread block owns 32 consecutive outputs, its 8 warps
+// read interleaved splits (coalesced 256-byte rows, several loads in flight per lane) and the
+// 8 warp sums are added in a fixed order, so the result does not depend on scheduling.
+__global__ void __launch_bounds__(256) k_reduce_splits(const double* __restrict__ part, long long count,
+                                                       int nsplit, double* __restrict__ y) {
+  __shared__ double red[8][33];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  for (long long base = (long long)blockIdx.x * 32; base < count; base += (long long)gridDim.x * 32) {
+    const long long idx = base + lane;
+    double s0 = 0.0, s1 = 0.0;
+    if (idx < count) {
+      int k = warp;
+      for (; k + 8 < nsplit; k += 16) {
+        s0 += part[(long long)k * count + idx];
+        s1 += part[(long long)(k + 8) * count + idx];
+      }
+      if (k < nsplit) s0 += part[(long long)k * count + idx];
+    }
+    red[warp][lane] = s0 + s1;
+    __syncthreads();
+    if (warp == 0 && idx < count) {
+      double t = 0.0;
+#pragma unroll
+      for (int w = 0; w < 8; ++w) t += red[w][lane];
+      y[idx] = t;
+    }
+    __syncthreads();
   }
 }
 
@@ -194,7 +217,8 @@ size_t sketch_ws_bytes(long long m, long long n, int N) {
 
 int launch_reduce_splits(const double* part, long long count, int nsplit, double* y, cudaStream_t s) {
   if (count <= 0) return TT_OK;
-  k_reduce_splits<<<std::min(ceil_div(count, 256), 8 * num_sms()), 256, 0, s>>>(part, count, nsplit, y);
+  k_reduce_splits<<<(int)std::min<long long>(ceil_div_ll(count, 32), 16LL * num_sms()), 256, 0, s>>>(
+      part, count, nsplit, y);
   count_launch();
   TT_LAUNCH_CHECK();
   return TT_OK;
@@ -275,7 +299,8 @@ template <int NT>
 __global__ void __launch_bounds__(256) k_project_simt(const float* __restrict__ a, long long m,
                                                       long long n, const float* __restrict__ q,
                                                       int N, long long ldq, float* __restrict__ out,
-                                                      long long ldo, int mode, int r0, int r1) {
+                                                      long long ldo, int mode, int r0, int r1,
+                                                      long long kchunk) {
   constexpr int TJ = 256, KC = 32, RJ = 8, RC = NT / 8;
   __shared__ __align__(16) float as[KC][TJ];
   __shared__ __align__(16) float qs[KC][NT];
@@ -289,7 +314,11 @@ __global__ void __launch_bounds__(256) k_project_simt(const float* __restrict__ 
 #pragma unroll
     for (int c = 0; c < RC; ++c) acc[e][c] = 0.f;
   const bool vec = ((m & 3) == 0) && ((((uintptr_t)a) & 15) == 0);
-  for (long long k0 = 0; k0 < m; k0 += KC) {
+  // K range of this split (blockIdx.z); the split's output block is out + z * n * ldo.
+  const long long kb = (long long)blockIdx.z * kchunk;
+  const long long ke = (kb + kchunk < m) ? kb + kchunk : m;
+  out += (long long)blockIdx.z * n * ldo;
+  for (long long k0 = kb; k0 < ke; k0 += KC) {
 #pragma unroll
     for (int qq = 0; qq < (TJ * KC / 4) / 256; ++qq) {
       const int f = tid + 256 * qq;
@@ -298,13 +327,13 @@ __global__ void __launch_bounds__(256) k_project_simt(const float* __restrict__ 
       float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
       if (j < n) {
         const float* p = a + j * m + k;
-        if (vec && k + 3 < m) {
+        if (vec && k + 3 < ke) {
           v = __ldg(reinterpret_cast<const float4*>(p));
         } else {
-          if (k < m) v.x = p[0];
-          if (k + 1 < m) v.y = p[1];
-          if (k + 2 < m) v.z = p[2];
-          if (k + 3 < m) v.w = p[3];
+          if (k < ke) v.x = p[0];
+          if (k + 1 < ke) v.y = p[1];
+          if (k + 2 < ke) v.z = p[2];
+          if (k + 3 < ke) v.w = p[3];
         }
       }
       const int kk = 4 * k4;
@@ -316,7 +345,7 @@ __global__ void __launch_bounds__(256) k_project_simt(const float* __restrict__ 
     for (int f = tid; f < KC * NT; f += 256) {
       const int kk = f % KC, c = f / KC;
       const long long k = k0 + kk;
-      qs[kk][c] = (k < m && c0 + c < N) ? q[k + ldq * (long long)(c0 + c)] : 0.f;
+      qs[kk][c] = (k < ke && c0 + c < N) ? q[k + ldq * (long long)(c0 + c)] : 0.f;
     }
     __syncthreads();
 #pragma unroll 4
@@ -352,6 +381,158 @@ __global__ void __launch_bounds__(256) k_project_simt(const float* __restrict__ 
   }
 }
 
+// Small-K projection out = Q^T A for K = m <= 64 (the rotation E_r^T B of a small factor, or
+// an m <= 64 unfolding): one column of A per thread.  A's columns are contiguous, so a tile of
+// 256 columns is one contiguous block: it is staged through shared memory with coalesced
+// float4 loads (odd row stride, conflict-free), Q sits in shared memory as float4 rows, and
+// row-major outputs leave through shared memory as one contiguous block.
+template <int NP>
+__global__ void __launch_bounds__(256) k_proj_smallk(const float* __restrict__ a, int m, long long n,
+                                                     const float* __restrict__ q, int N, long long ldq,
+                                                     float* __restrict__ out, long long ldo, int mode,
+                                                     int r0, int r1) {
+  constexpr int TJ = 256;
+  extern __shared__ __align__(16) float sm_pk[];
+  float* Es = sm_pk;            // m x NP: Es[k * NP + c] = Q[k + ldq c]
+  float* Xs = Es + 64 * NP;     // TJ x S input tile, then TJ x (NP + 1) output tile
+  const int S = (m & 1) ? m : m + 1;
+  constexpr int OS = NP + 1;
+  const int tid = threadIdx.x;
+  for (int idx = tid; idx < m * NP; idx += TJ) {
+    const int k = idx / NP, c = idx - (idx / NP) * NP;
+    Es[idx] = (c < N) ? q[k + ldq * (long long)c] : 0.f;
+  }
+  const bool vec = (m & 3) == 0 && ((reinterpret_cast<uintptr_t>(a) & 15) == 0);
+  // Row-major outputs with ldo == N form one contiguous block per tile; bond-permuted outputs
+  // (r0, r1, n) -> (r1, n, r0) form r0 contiguous runs of r1 * nj values per tile.
+  const bool staged_out = (mode == OUT_ROWMAJOR && ldo == N) || (mode == OUT_PERM231 && r0 * r1 == N);
+  for (long long tile = blockIdx.x; tile * TJ < n; tile += gridDim.x) {
+    const long long j0 = tile * TJ;
+    const int nj = (int)((n - j0 < TJ) ? n - j0 : TJ);
+    const float* src = a + j0 * m;
+    const int cnt = nj * m;
+    __syncthreads();
+    if (vec) {
+      for (int f4 = tid; f4 < (cnt >> 2); f4 += TJ) {
+        const float4 v = __ldg(reinterpret_cast<const float4*>(src) + f4);
+        const int e = 4 * f4, col = e / m, k = e - col * m;
+        float* d = Xs + col * S + k;
+        d[0] = v.x;
+        d[1] = v.y;
+        d[2] = v.z;
+        d[3] = v.w;
+      }
+    } else {
+      for (int f = tid; f < cnt; f += TJ) {
+        const int col = f / m, k = f - col * m;
+        Xs[col * S + k] = __ldg(src + f);
+      }
+    }
+    __syncthreads();
+    float acc[NP];
+#pragma unroll
+    for (int c = 0; c < NP; ++c) acc[c] = 0.f;
+    if (tid < nj) {
+      const float* xr = Xs + tid * S;
+      for (int k = 0; k < m; ++k) {
+        const float x = xr[k];
+        const float4* er = reinterpret_cast<const float4*>(Es + k * NP);
+#pragma unroll
+        for (int c4 = 0; c4 < NP / 4; ++c4) {
+          const float4 e = er[c4];
+          acc[4 * c4] = fmaf(x, e.x, acc[4 * c4]);
+          acc[4 * c4 + 1] = fmaf(x, e.y, acc[4 * c4 + 1]);
+          acc[4 * c4 + 2] = fmaf(x, e.z, acc[4 * c4 + 2]);
+          acc[4 * c4 + 3] = fmaf(x, e.w, acc[4 * c4 + 3]);
+        }
+      }
+    }
+    if (staged_out) {
+      __syncthreads();
+      if (tid < nj) {
+#pragma unroll
+        for (int c = 0; c < NP; ++c)
+          if (c < N) Xs[tid * OS + c] = acc[c];
+      }
+      __syncthreads();
+      if (mode == OUT_ROWMAJOR) {
+        float* dst = out + j0 * N;
+        for (int f = tid; f < nj * N; f += TJ) {
+          const int col = f / N, c = f - col * N;
+          dst[f] = Xs[col * OS + c];
+        }
+      } else {
+        const int run = r1 * nj;
+        for (int ai = 0; ai < r0; ++ai) {
+          float* dst = out + (long long)r1 * (j0 + n * (long long)ai);
+          for (int f = tid; f < run; f += TJ) {
+            const int col = f / r1, bi = f - col * r1;
+            dst[f] = Xs[col * OS + ai + r0 * bi];
+          }
+        }
+      }
+    } else if (tid < nj) {
+      const long long j = j0 + tid;
+#pragma unroll
+      for (int c = 0; c < NP; ++c) {
+        if (c >= N) continue;
+        if (mode == OUT_ROWMAJOR) {
+          out[j * ldo + c] = acc[c];
+        } else {
+          const int ai = c % r0, bi = c / r0;
+          out[(long long)bi + (long long)r1 * (j + n * (long long)ai)] = acc[c];
+        }
+      }
+    }
+  }
+}
+
+// Sum of the K-split partial projections (row-major n x N blocks) into the requested layout.
+__global__ void k_project_reduce(const float* __restrict__ part, long long n, int N, int nsplit,
+                                 float* __restrict__ out, long long ldo, int mode, int r0, int r1) {
+  const long long total = n * N;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    float v = 0.f;
+    for (int z = 0; z < nsplit; ++z) v += part[(long long)z * total + idx];
+    const long long j = idx / N;
+    const int c = (int)(idx - j * N);
+    if (mode == OUT_ROWMAJOR) {
+      out[j * ldo + c] = v;
+    } else {
+      const int ai = c % r0, bi = c / r0;
+      out[(long long)bi + (long long)r1 * (j + n * (long long)ai)] = v;
+    }
+  }
+}
+
+namespace {
+constexpr size_t kProjectSplitCap = 16u << 20;  // bytes of K-split partials
+
+// K splits for projections whose column tiles alone cannot fill the GPU.
+int project_ksplit(long long m, long long n, int N, long long* kchunk) {
+  const int NT = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : 64;
+  const long long blocks = ceil_div_ll(n, 256) * ceil_div_ll(N, NT);
+  int ks = 1;
+  if (m >= 256 && blocks < 2LL * num_sms()) {
+    ks = (int)std::min<long long>(ceil_div_ll(2LL * num_sms(), blocks), m / 64);
+    const long long cap = (long long)(kProjectSplitCap / (sizeof(float) * (size_t)n * N));
+    ks = (int)std::max<long long>(1, std::min<long long>(ks, cap));
+  }
+  long long kc = ceil_div_ll(m, ks);
+  kc = ceil_div_ll(kc, 32) * 32;
+  *kchunk = kc;
+  return (int)ceil_div_ll(m, kc);
+}
+}  // namespace
+
+size_t project_ws_bytes(long long m, long long n, int N) {
+  long long kc;
+  const int ks = project_ksplit(m, n, N, &kc);
+  const size_t split = ks > 1 ? (size_t)ks * n * N * sizeof(float) : 0;
+  return split + 2 * (size_t)m * N * sizeof(float) + 4096;
+}
+
 int launch_project(const float* a, long long m, long long n, const float* q, int N, long long ldq,
                    float* out, long long ldo, int mode, int r0, int r1, int engine, Arena& ws,
                    DevStatus* st, cudaStream_t s) {
@@ -361,15 +542,61 @@ int launch_project(const float* a, long long m, long long n, const float* q, int
     if (rc != TT_ERR_UNSUPPORTED) return rc;
   }
   const int NT = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : 64;
-  dim3 grid(ceil_div(n, 256), ceil_div(N, NT));
+  if (m <= 64 && N <= 64) {
+    const size_t shm = (64 * (size_t)NT + 256 * (size_t)std::max<long long>(m + 1, NT + 1)) * sizeof(float);
+    static bool attr = false;
+    if (!attr) {
+      cudaFuncSetAttribute(k_proj_smallk<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+      cudaFuncSetAttribute(k_proj_smallk<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+      cudaFuncSetAttribute(k_proj_smallk<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+      cudaFuncSetAttribute(k_proj_smallk<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+      attr = true;
+    }
+    const int grid = (int)std::min<long long>(ceil_div_ll(n, 256), 4LL * num_sms());
+    const int mi = (int)m;
+    switch (NT) {
+      case 16: k_proj_smallk<16><<<grid, 256, shm, s>>>(a, mi, n, q, N, ldq, out, ldo, mode, r0, r1); break;
+      case 32: k_proj_smallk<32><<<grid, 256, shm, s>>>(a, mi, n, q, N, ldq, out, ldo, mode, r0, r1); break;
+      case 48: k_proj_smallk<48><<<grid, 256, shm, s>>>(a, mi, n, q, N, ldq, out, ldo, mode, r0, r1); break;
+      default: k_proj_smallk<64><<<grid, 256, shm, s>>>(a, mi, n, q, N, ldq, out, ldo, mode, r0, r1); break;
+    }
+    count_launch();
+    TT_LAUNCH_CHECK();
+    return TT_OK;
+  }
+  long long kc;
+  int ks = project_ksplit(m, n, N, &kc);
+  float* part = nullptr;
+  const size_t mk = ws.mark();
+  if (ks > 1) {
+    part = ws.take<float>((size_t)ks * n * N);
+    if (!part) {
+      ks = 1;
+      kc = m;
+    }
+  } else {
+    kc = m;
+  }
+  dim3 grid(ceil_div(n, 256), ceil_div(N, NT), ks);
+  float* dst = ks > 1 ? part : out;
+  const long long ldd = ks > 1 ? N : ldo;
+  const int md = ks > 1 ? OUT_ROWMAJOR : mode;
   switch (NT) {
-    case 16: k_project_simt<16><<<grid, 256, 0, s>>>(a, m, n, q, N, ldq, out, ldo, mode, r0, r1); break;
-    case 32: k_project_simt<32><<<grid, 256, 0, s>>>(a, m, n, q, N, ldq, out, ldo, mode, r0, r1); break;
-    case 48: k_project_simt<48><<<grid, 256, 0, s>>>(a, m, n, q, N, ldq, out, ldo, mode, r0, r1); break;
-    default: k_project_simt<64><<<grid, 256, 0, s>>>(a, m, n, q, N, ldq, out, ldo, mode, r0, r1); break;
+    case 16: k_project_simt<16><<<grid, 256, 0, s>>>(a, m, n, q, N, ldq, dst, ldd, md, r0, r1, kc); break;
+    case 32: k_project_simt<32><<<grid, 256, 0, s>>>(a, m, n, q, N, ldq, dst, ldd, md, r0, r1, kc); break;
+    case 48: k_project_simt<48><<<grid, 256, 0, s>>>(a, m, n, q, N, ldq, dst, ldd, md, r0, r1, kc); break;
+    default: k_project_simt<64><<<grid, 256, 0, s>>>(a, m, n, q, N, ldq, dst, ldd, md, r0, r1, kc); break;
   }
   count_launch();
   TT_LAUNCH_CHECK();
+  if (ks > 1) {
+    const long long total = n * N;
+    k_project_reduce<<<(int)std::min<long long>(ceil_div_ll(total, 256), 8LL * num_sms()), 256, 0, s>>>(
+        part, n, N, ks, out, ldo, mode, r0, r1);
+    count_launch();
+    TT_LAUNCH_CHECK();
+  }
+  ws.reset(mk);
   return TT_OK;
 }
 
@@ -585,10 +812,11 @@ int launch_gram(const float* x, long long nvec, int M, long long vs, long long e
 __global__ void __launch_bounds__(256) k_chol_inv(const double* __restrict__ w, int N,
                                                   double* __restrict__ r_out,
                                                   double* __restrict__ rinv, double rel_tol,
-                                                  DevStatus* st) {
+                                                  int ri_smem, DevStatus* st) {
   extern __shared__ double sm[];
-  double* A = sm;                 // N x N (row-major), upper part becomes R
-  int* dead = reinterpret_cast<int*>(sm + N * N);
+  double* A = sm;                                // N x N (row-major), upper part becomes R
+  double* Ri = ri_smem ? sm + N * N : rinv;      // N x N (column-major) R^-1, on chip if it fits
+  int* dead = reinterpret_cast<int*>(sm + (ri_smem ? 2 : 1) * N * N);
   __shared__ double piv_s, dmax_s;
   const int tid = threadIdx.x;
   for (int idx = tid; idx < N * N; idx += blockDim.x) {
@@ -637,8 +865,8 @@ __global__ void __launch_bounds__(256) k_chol_inv(const double* __restrict__ w, 
       r_out[idx] = (j >= i) ? A[i * N + j] : 0.0;
     }
   }
-  // R^-1 column by column (column-major output in global memory).
-  for (int idx = tid; idx < N * N; idx += blockDim.x) rinv[idx] = 0.0;
+  // R^-1 column by column in shared memory, then one coalesced copy out.
+  for (int idx = tid; idx < N * N; idx += blockDim.x) Ri[idx] = 0.0;
   __syncthreads();
   for (int j = 0; j < N; ++j) {
     if (dead[j]) continue;  // uniform across the block
@@ -651,13 +879,15 @@ __global__ void __launch_bounds__(256) k_chol_inv(const double* __restrict__ w, 
         v = 0.0;
       } else {
         double acc = 0.0;
-        for (int k = i; k < j; ++k) acc += rinv[i + (long long)N * k] * A[k * N + j];
+        for (int k = i; k < j; ++k) acc += Ri[i + N * k] * A[k * N + j];
         v = -acc / rjj;
       }
-      rinv[i + (long long)N * j] = v;
+      Ri[i + N * j] = v;
     }
     __syncthreads();
   }
+  if (ri_smem)
+    for (int idx = tid; idx < N * N; idx += blockDim.x) rinv[idx] = Ri[idx];
   (void)st;
 }
 
@@ -734,12 +964,226 @@ __global__ void k_mul_upper(const double* __restrict__ r2, const double* __restr
   r[idx] = (j >= i) ? acc : 0.0;
 }
 
+// Single-CTA CholeskyQR2 for sketches that fit in shared memory (n rows x N <= 64 columns):
+// both passes in one launch.  Y is staged row-major with a padded stride S (S/4 odd, so the
+// float4 row accesses of neighbouring threads fall in distinct banks); per pass:
+//   Gram W = Y^T Y in FP64 (4x4 register tiles over the upper tile triangle, row groups
+//   reduced through W), right-looking Cholesky in FP64 (one barrier per column, dead pivots
+//   below rel_tol * max diag), then Q = Y R^-1 by forward substitution, one row per thread in
+//   FP32 registers against an FP32 copy of R (column-major, diagonal stored as 1/r_cc).
+// Optional R output (column-major) = R2 * R1.
+template <int NP>
+__global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, int n, int N, long long vs,
+                                                       long long es, int S, double* __restrict__ r,
+                                                       double rel_tol) {
+  constexpr int NT = 512;
+  extern __shared__ __align__(16) unsigned char sm_cq[];
+  float* Ys = reinterpret_cast<float*>(sm_cq);                       // n x S
+  double* W = reinterpret_cast<double*>(Ys + (size_t)n * S);         // N x N row-major
+  const int WN = (N * N + 1) & ~1;
+  float* Rf = reinterpret_cast<float*>(W + WN);                      // NP x NP, Rf[c*NP+k] = R[k][c]
+  float* invd = Rf + NP * NP;                                        // NP
+  double* R1 = reinterpret_cast<double*>(invd + NP);                 // N x N (only with r)
+  const int tid = threadIdx.x;
+  const int TTa = (N + 3) >> 2;
+  const int ngrp = S >> 2;
+  for (int f = tid; f < n * ngrp; f += NT) {
+    const int i = f % n, q4 = f / n;
+    float v[4];
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      const int c = 4 * q4 + e;
+      v[e] = (c < N) ? y[(long long)i * vs + (long long)c * es] : 0.f;
+    }
+    *reinterpret_cast<float4*>(&Ys[(size_t)i * S + 4 * q4]) = make_float4(v[0], v[1], v[2], v[3]);
+  }
+  // Tile assignment for the Gram: tile t of the TTa x TTa upper triangle, row group g.
+  const int nt = TTa * (TTa + 1) / 2;
+  const int groups = min(32, max(1, NT / nt));
+  const int t = tid % nt, g = tid / nt;
+  const bool act = g < groups;
+  int ta = 0, rem = act ? t : 0;
+  while (rem >= TTa - ta) {
+    rem -= TTa - ta;
+    ++ta;
+  }
+  const int tb = ta + rem;
+  for (int pass = 0; pass < 2; ++pass) {
+    __syncthreads();
+    double acc[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+    if (act) {
+      for (int v = g; v < n; v += groups) {
+        const float4 xa = *reinterpret_cast<const float4*>(&Ys[(size_t)v * S + 4 * ta]);
+        const float4 xb = *reinterpret_cast<const float4*>(&Ys[(size_t)v * S + 4 * tb]);
+        const double av[4] = {xa.x, xa.y, xa.z, xa.w};
+        const double bv[4] = {xb.x, xb.y, xb.z, xb.w};
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[p * 4 + q] = fma(av[p], bv[q], acc[p * 4 + q]);
+      }
+    }
+    for (int gg = 0; gg < groups; ++gg) {
+      if (act && g == gg) {
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) {
+            const int i = 4 * ta + p, j = 4 * tb + q;
+            if (i < N && j < N) W[i * N + j] = (gg == 0 ? 0.0 : W[i * N + j]) + acc[p * 4 + q];
+          }
+      }
+      __syncthreads();
+    }
+    double dmax = 0.0;
+    for (int k = 0; k < N; ++k) dmax = fmax(dmax, W[k * N + k]);
+    const double tol = rel_tol * dmax;
+    for (int k = 0; k < N; ++k) {
+      const double d = W[k * N + k];
+      if (d > tol && dmax > 0.0) {
+        const double inv = 1.0 / d;
+        const int rm = N - k - 1;
+        for (int idx = tid; idx < rm * rm; idx += NT) {
+          const int i = k + 1 + idx / rm, j = k + 1 + idx % rm;
+          if (j >= i) W[i * N + j] -= W[k * N + i] * W[k * N + j] * inv;
+        }
+      }
+      __syncthreads();
+    }
+    // R[k][c] = W[k][c] / sqrt(W[k][k]) on live rows (c >= k); dead rows are zero.
+    for (int idx = tid; idx < NP * NP; idx += NT) {
+      const int c = idx / NP, k = idx % NP;
+      float v = 0.f;
+      if (c < N && k < c) {
+        const double d = W[k * N + k];
+        if (d > tol && dmax > 0.0) v = (float)(W[k * N + c] / sqrt(d));
+      }
+      Rf[idx] = v;
+    }
+    for (int c = tid; c < NP; c += NT) {
+      float v = 0.f;
+      if (c < N) {
+        const double d = W[c * N + c];
+        if (d > tol && dmax > 0.0) v = (float)(1.0 / sqrt(d));
+      }
+      invd[c] = v;
+    }
+    if (r) {
+      for (int idx = tid; idx < N * N; idx += NT) {
+        const int k = idx % N, c = idx / N;  // column-major (k, c)
+        const double dk = W[k * N + k];
+        const bool live = dk > tol && dmax > 0.0;
+        if (pass == 0) {
+          R1[idx] = (live && c >= k) ? W[k * N + c] / sqrt(dk) : 0.0;
+        } else {
+          double a = 0.0;
+          if (live && c >= k) {
+            const double sk = 1.0 / sqrt(dk);
+            for (int j = k; j <= c; ++j) a += W[k * N + j] * sk * R1[j + N * c];
+          }
+          r[idx] = a;
+        }
+      }
+    }
+    __syncthreads();
+    // Forward substitution q R = y, one row per thread.
+    for (int i = tid; i < n; i += NT) {
+      float q[NP];
+#pragma unroll
+      for (int j4 = 0; j4 < NP / 4; ++j4) {
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (j4 < TTa) v = *reinterpret_cast<const float4*>(&Ys[(size_t)i * S + 4 * j4]);
+        q[4 * j4] = v.x;
+        q[4 * j4 + 1] = v.y;
+        q[4 * j4 + 2] = v.z;
+        q[4 * j4 + 3] = v.w;
+      }
+#pragma unroll
+      for (int c = 0; c < NP; ++c) {
+        float a = q[c];
+#pragma unroll
+        for (int k4 = 0; k4 < (c + 3) / 4; ++k4) {
+          const float4 rr = *reinterpret_cast<const float4*>(&Rf[c * NP + 4 * k4]);
+          a = fmaf(-q[4 * k4], rr.x, a);
+          a = fmaf(-q[4 * k4 + 1], rr.y, a);
+          a = fmaf(-q[4 * k4 + 2], rr.z, a);
+          a = fmaf(-q[4 * k4 + 3], rr.w, a);
+        }
+        q[c] = a * invd[c];
+      }
+      if (pass == 0) {
+#pragma unroll
+        for (int j4 = 0; j4 < NP / 4; ++j4)
+          if (j4 < TTa)
+            *reinterpret_cast<float4*>(&Ys[(size_t)i * S + 4 * j4]) =
+                make_float4(q[4 * j4], q[4 * j4 + 1], q[4 * j4 + 2], q[4 * j4 + 3]);
+      } else {
+#pragma unroll
+        for (int c = 0; c < NP; ++c)
+          if (c < N) y[(long long)i * vs + (long long)c * es] = q[c];
+      }
+    }
+  }
+}
+
+static int max_optin_smem() {
+  static int v = 0;
+  if (v == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    if (v <= 0) v = 48 * 1024;
+  }
+  return v;
+}
+
+// Shared-memory bytes of k_cholqr2_small, or 0 when the sketch does not fit.
+static size_t cholqr2_small_smem(long long n, int N, bool want_r, int* S_out) {
+  if (N < 1 || N > 64 || n < 1 || n > (1LL << 20)) return 0;
+  const int NP = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : 64;
+  int S = 4 * ((N + 3) / 4);
+  if (((S / 4) & 1) == 0) S += 4;
+  const size_t WN = ((size_t)N * N + 1) & ~(size_t)1;
+  const size_t bytes = (size_t)n * S * 4 + WN * 8 + (size_t)NP * NP * 4 + NP * 4 +
+                       (want_r ? (size_t)N * N * 8 : 0);
+  if (bytes > (size_t)max_optin_smem()) return 0;
+  *S_out = S;
+  return bytes;
+}
+
 int launch_cholqr2(float* y, long long n, int N, long long vs, long long es, double* r,
                    Arena& ws, DevStatus* st, cudaStream_t s) {
   if (N <= 0 || n <= 0) return TT_OK;
   if (N > TT_MAX_SMALL) {
     set_error(TT_ERR_UNSUPPORTED, "cholqr2 width %d > %d", N, TT_MAX_SMALL);
     return TT_ERR_UNSUPPORTED;
+  }
+  int S = 0;
+  const size_t sshm = cholqr2_small_smem(n, N, r != nullptr, &S);
+  if (sshm > 0) {
+    static bool attr_small = false;
+    if (!attr_small) {
+      const int mx = max_optin_smem();
+      cudaFuncSetAttribute(k_cholqr2_small<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+      cudaFuncSetAttribute(k_cholqr2_small<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+      cudaFuncSetAttribute(k_cholqr2_small<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+      cudaFuncSetAttribute(k_cholqr2_small<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+      attr_small = true;
+    }
+    const int nn = (int)n;
+    if (N <= 16)
+      k_cholqr2_small<16><<<1, 512, sshm, s>>>(y, nn, N, vs, es, S, r, 1e-12);
+    else if (N <= 32)
+      k_cholqr2_small<32><<<1, 512, sshm, s>>>(y, nn, N, vs, es, S, r, 1e-12);
+    else if (N <= 48)
+      k_cholqr2_small<48><<<1, 512, sshm, s>>>(y, nn, N, vs, es, S, r, 1e-12);
+    else
+      k_cholqr2_small<64><<<1, 512, sshm, s>>>(y, nn, N, vs, es, S, r, 1e-12);
+    count_launch();
+    TT_LAUNCH_CHECK();
+    return TT_OK;
   }
   const size_t mk = ws.mark();
   double* w = ws.take<double>((size_t)N * N);
@@ -751,7 +1195,8 @@ int launch_cholqr2(float* y, long long n, int N, long long vs, long long es, dou
     return TT_ERR_NOMEM;
   }
   const int NP = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : N <= 64 ? 64 : 128;
-  const size_t shm = (size_t)N * N * sizeof(double) + N * sizeof(int) + 16;
+  const int ri_smem = 2 * (size_t)N * N * sizeof(double) + N * sizeof(int) + 16 <= 200 * 1024;
+  const size_t shm = (size_t)(ri_smem ? 2 : 1) * N * N * sizeof(double) + N * sizeof(int) + 16;
   static bool attr_set = false;
   if (!attr_set) {
     cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
@@ -764,7 +1209,7 @@ int launch_cholqr2(float* y, long long n, int N, long long vs, long long es, dou
   }
   for (int pass = 0; pass < 2; ++pass) {
     TT_TRY(launch_gram(y, n, N, vs, es, w, true, ws, s));
-    k_chol_inv<<<1, 256, shm, s>>>(w, N, pass == 0 ? r1 : r2, rinv, 1e-12, st);
+    k_chol_inv<<<1, 256, shm, s>>>(w, N, pass == 0 ? r1 : r2, rinv, 1e-12, ri_smem, st);
     count_launch();
     TT_LAUNCH_CHECK();
     const int grid = ceil_div(n, 128);
@@ -808,11 +1253,18 @@ __global__ void __launch_bounds__(256) k_syev_jacobi(const double* __restrict__ 
   int* qq = pp + Np / 2;
   int* order = qq + Np / 2;
   __shared__ int nrot;
+  __shared__ double floor_abs;
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int idx = tid; idx < Np * Np; idx += nt) {
     const int i = idx / Np, j = idx % Np;
     W[idx] = (i < N && j < N) ? w_in[i + (long long)N * j] : 0.0;
     V[idx] = (i == j) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double dm = 0.0;
+    for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(W[i * Np + i]));
+    floor_abs = 1e-15 * dm;
   }
   __syncthreads();
   const double tol = 1e-14;
@@ -834,7 +1286,7 @@ __global__ void __launch_bounds__(256) k_syev_jacobi(const double* __restrict__ 
         double c = 1.0, s = 0.0;
         if (q < N) {
           const double apq = W[p * Np + q], app = W[p * Np + p], aqq = W[q * Np + q];
-          if (fabs(apq) > tol * sqrt(fabs(app * aqq)) && apq != 0.0) {
+          if (fabs(apq) > tol * sqrt(fabs(app * aqq)) && fabs(apq) > floor_abs) {
             const double theta = (aqq - app) / (2.0 * apq);
             const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(1.0 + theta * theta));
             c = 1.0 / sqrt(1.0 + t * t);
@@ -903,12 +1355,211 @@ __global__ void __launch_bounds__(256) k_syev_jacobi(const double* __restrict__ 
   for (int a = tid; a < N; a += nt) evals[a] = W[order[a] * Np + order[a]];
 }
 
+// Small-N variant (N <= 64), latency-oriented: one barrier per round.
+//  * W and V are double-buffered in shared memory; a round computes W' = J^T W J and V' = V J
+//    for all Np/2 rotations at once (each entry from at most four old entries), 31 warps
+//    covering the entries with their (row, column) fixed for the whole solve.
+//  * The round-robin pairing of every round (partner, pair slot, which side) is tabulated
+//    once at start-up.
+//  * The last warp computes the NEXT round's rotations while the others apply the current
+//    one: it evaluates the three entries of J^T W J it needs directly from the current W.
+//  * Rotation angle: t from an FP32 evaluation of theta on the matrix scaled by its largest
+//    diagonal entry, then c = 1/sqrt(1 + t^2), s = t c in FP64, so every applied J is
+//    orthogonal to FP64 precision (an inexact t only leaves a tiny a_pq for a later sweep).
+//  * Rotations are skipped when a_pq^2 <= 1e-28 |a_pp a_qq| (relative accuracy) or
+//    |a_pq| <= 1e-15 max|diag| (FP64 rounding floor); the solve ends after Np-1 consecutive
+//    rounds without a rotation.  Eigenvalues are ordered by a parallel rank count.
+__device__ __forceinline__ int rr_slot_index(int x, int r, int NR) {
+  if (x == 0) return 0;
+  int v = x - 1 + r;
+  if (v >= NR) v -= NR;
+  return 1 + v;
+}
+
+__global__ void __launch_bounds__(1024) k_syev_fast(const double* __restrict__ w_in, int N,
+                                                     double* __restrict__ evals,
+                                                     double* __restrict__ evecs, int max_sweeps,
+                                                     DevStatus* st) {
+  constexpr int PW = 31;            // warp that computes the next round's rotations
+  constexpr int NE = PW * 32;       // threads applying rotations
+  constexpr int MAXE = (64 * 64 + NE - 1) / NE;
+  extern __shared__ __align__(16) double sm_fast[];
+  const int Np = N + (N & 1);
+  const int NR = Np - 1;
+  const int NN = Np * Np;
+  double* W0 = sm_fast;
+  double* W1 = W0 + NN;
+  double* V0 = W1 + NN;
+  double* V1 = V0 + NN;
+  int* tab = reinterpret_cast<int*>(V1 + NN);  // NR x Np: partner | pair << 8 | (index < partner) << 16
+  __shared__ double csb[2][32], snb[2][32];
+  __shared__ int order[64];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  for (int idx = tid; idx < NN; idx += blockDim.x) {
+    const int i = idx / Np, j = idx - (idx / Np) * Np;
+    W0[idx] = (i < N && j < N) ? w_in[i + (long long)N * j] : 0.0;
+    V0[idx] = (i == j) ? 1.0 : 0.0;
+  }
+  for (int idx = tid; idx < NR * Np; idx += blockDim.x) {
+    const int r = idx / Np, x = idx - (idx / Np) * Np;
+    const int i = rr_slot_index(x, r, NR);
+    const int y = Np - 1 - x;
+    const int pi = rr_slot_index(y, r, NR);
+    const int k = x < y ? x : y;
+    tab[r * Np + i] = pi | (k << 8) | ((i < pi ? 1 : 0) << 16);
+  }
+  __syncthreads();
+  double dm = 0.0;
+  for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(W0[i * Np + i]));
+  const double inv_s = dm > 0.0 ? 1.0 / dm : 1.0;
+
+  // Rotation (c, s) annihilating a_pq; false when the pair is already below the thresholds.
+  auto rotation = [&](double app, double aqq, double apq, double& c, double& s) -> bool {
+    const double ps = app * inv_s, qs = aqq * inv_s, as = apq * inv_s;
+    c = 1.0;
+    s = 0.0;
+    if (!(fabs(as) > 1e-15 && as * as > 1e-28 * fabs(ps * qs))) return false;
+    const float th = (float)(qs - ps) / (2.0f * (float)as);
+    const float tf = copysignf(1.0f, th) / (fabsf(th) + sqrtf(fmaf(th, th, 1.0f)));
+    const double t = (double)tf;
+    c = rsqrt(fma(t, t, 1.0));
+    s = t * c;
+    return true;
+  };
+  // Entry (a, b) of J^T W J for the round whose pairing row is `tb` and rotations (cs, sn).
+  auto rotated_entry = [&](const double* W, const int* tb, const double* cs, const double* sn, int a,
+                           int b) -> double {
+    const int ta = tb[a], tbb = tb[b];
+    const int pa = ta & 255, ka = (ta >> 8) & 255, pb = tbb & 255, kb = (tbb >> 8) & 255;
+    const double jaa = cs[ka], jpa = (ta >> 16) ? -sn[ka] : sn[ka];
+    const double jbb = cs[kb], jpb = (tbb >> 16) ? -sn[kb] : sn[kb];
+    return jaa * (W[a * Np + b] * jbb + W[a * Np + pb] * jpb) +
+           jpa * (W[pa * Np + b] * jbb + W[pa * Np + pb] * jpb);
+  };
+
+  // Rotations of round 0.
+  if (warp == PW) {
+    for (int k = lane; k < Np / 2; k += 32) {
+      int p = rr_slot_index(k, 0, NR), q = rr_slot_index(Np - 1 - k, 0, NR);
+      if (p > q) {
+        const int t = p;
+        p = q;
+        q = t;
+      }
+      double c = 1.0, s = 0.0;
+      if (q < N) rotation(W0[p * Np + p], W0[q * Np + q], W0[p * Np + q], c, s);
+      csb[0][k] = c;
+      snb[0][k] = s;
+    }
+  }
+  int eij[MAXE];  // row | column << 8 of this thread's entries
+#pragma unroll
+  for (int u = 0; u < MAXE; ++u) {
+    const int e = tid + u * NE;
+    eij[u] = (e / Np) | ((e - (e / Np) * Np) << 8);
+  }
+  __syncthreads();
+
+  int cur = 0;
+  int R = 0;  // global round counter (parity selects the rotation buffer)
+  int sweep = 0;
+  bool converged = false;
+  for (; sweep < max_sweeps; ++sweep) {
+    int rotated = 0;
+    for (int rnd = 0; rnd < NR; ++rnd, ++R) {
+      const double* W = cur ? W1 : W0;
+      const double* V = cur ? V1 : V0;
+      double* Wn = cur ? W0 : W1;
+      double* Vn = cur ? V0 : V1;
+      const int pb = R & 1;
+      const double* cs = csb[pb];
+      const double* sn = snb[pb];
+      const int* tb = tab + rnd * Np;
+      if (warp != PW) {
+#pragma unroll
+        for (int u = 0; u < MAXE; ++u) {
+          const int e = tid + u * NE;
+          if (e < NN) {
+            const int i = eij[u] & 255, j = eij[u] >> 8;
+            Wn[e] = rotated_entry(W, tb, cs, sn, i, j);
+            const int tj = tb[j];
+            const int pj = tj & 255, kj = (tj >> 8) & 255;
+            const double jjj = cs[kj], jpj = (tj >> 16) ? -sn[kj] : sn[kj];
+            Vn[e] = V[i * Np + j] * jjj + V[i * Np + pj] * jpj;
+          }
+        }
+      } else {
+        const int rn = (rnd + 1 == NR) ? 0 : rnd + 1;
+        for (int k = lane; k < Np / 2; k += 32) {
+          int p = rr_slot_index(k, rn, NR), q = rr_slot_index(Np - 1 - k, rn, NR);
+          if (p > q) {
+            const int t = p;
+            p = q;
+            q = t;
+          }
+          double c = 1.0, s = 0.0;
+          if (q < N) {
+            const double app = rotated_entry(W, tb, cs, sn, p, p);
+            const double aqq = rotated_entry(W, tb, cs, sn, q, q);
+            const double apq = rotated_entry(W, tb, cs, sn, p, q);
+            if (rotation(app, aqq, apq, c, s)) rotated = 1;
+          }
+          csb[pb ^ 1][k] = c;
+          snb[pb ^ 1][k] = s;
+        }
+      }
+      cur ^= 1;
+      if (rnd + 1 < NR) __syncthreads();
+    }
+    if (!__syncthreads_or(rotated)) {
+      converged = true;
+      break;
+    }
+  }
+  const double* Wf = cur ? W1 : W0;
+  const double* Vf = cur ? V1 : V0;
+  if (tid < N) {
+    double la = Wf[tid * Np + tid];
+    if (la != la) la = -INFINITY;
+    int rank = 0;
+    for (int b = 0; b < N; ++b) {
+      double lb = Wf[b * Np + b];
+      if (lb != lb) lb = -INFINITY;
+      rank += (lb > la || (lb == la && b < tid)) ? 1 : 0;
+    }
+    order[rank] = tid;
+  }
+  if (tid == 0 && st) {
+    atomicMax(&st->sweeps, sweep + 1);
+    if (!converged) dev_fail(st, TT_ERR_NOCONV, sweep);
+  }
+  __syncthreads();
+  for (int idx = tid; idx < N * N; idx += blockDim.x) {
+    const int i = idx % N, a = idx / N;
+    evecs[i + (long long)N * a] = Vf[i * Np + order[a]];
+  }
+  for (int a = tid; a < N; a += blockDim.x) evals[a] = Wf[order[a] * Np + order[a]];
+}
+
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps, Arena& ws,
                 DevStatus* st, cudaStream_t s) {
   if (N <= 0) return TT_OK;
   if (N > TT_MAX_SMALL) {
     set_error(TT_ERR_UNSUPPORTED, "eigen-solver size %d > %d", N, TT_MAX_SMALL);
     return TT_ERR_UNSUPPORTED;
+  }
+  if (N <= 64) {
+    const int Nps = N + (N & 1);
+    const size_t shm_fast = 4 * (size_t)Nps * Nps * sizeof(double) + (size_t)(Nps - 1) * Nps * sizeof(int);
+    static bool attr_fast = false;
+    if (!attr_fast) {
+      cudaFuncSetAttribute(k_syev_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+      attr_fast = true;
+    }
+    k_syev_fast<<<1, 1024, shm_fast, s>>>(w, N, evals, evecs, max_sweeps, st);
+    count_launch();
+    TT_LAUNCH_CHECK();
+    return TT_OK;
   }
   const int Np = N + (N & 1);
   const bool vsm = Np <= 64;

@@ -84,6 +84,13 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
       "l"((unsigned long long)map), "r"(bar), "r"(c0), "r"(c1)
       : "memory");
 }
+__device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, uint32_t bar,
+                                            int c0, int c1, int c2) {
+  asm volatile(
+      "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4, %5}], [%2];" ::"r"(dst),
+      "l"((unsigned long long)map), "r"(bar), "r"(c0), "r"(c1), "r"(c2)
+      : "memory");
+}
 __device__ __forceinline__ void tmem_alloc(uint32_t dst_smem, uint32_t ncols) {
   asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(dst_smem),
                "r"(ncols)
@@ -383,7 +390,7 @@ template <int BN, int MT, int BK, int STAGES>
 __global__ void __launch_bounds__(192, 1)
     k_sketch_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                 long long m, long long n, int N, long long kchunk, int nsplit, int ngroups,
-                double* __restrict__ part, DevStatus* st) {
+                double* __restrict__ part, DevStatus* st, int a3d) {
   constexpr int BLK = MT * 4;                   // 32-row blocks per group
   constexpr uint32_t ABLK = BK * 128;           // one 32-row block, BK columns
   constexpr uint32_t A_BYTES = BLK * ABLK;
@@ -450,9 +457,14 @@ __global__ void __launch_bounds__(192, 1)
           mbar_expect_tx(bars.full(stage), A_BYTES + B_BYTES);
           const uint32_t sa = sbase + stage * STAGE_BYTES;
           const int jc = (int)(jb + (long long)kb * BK);
+          if (a3d) {
+            // all BLK 32-row blocks of the group in one copy: (row in block, column, block)
+            tma_load_3d(sa, &tmA, bars.full(stage), 0, jc, i0 / 32);
+          } else {
 #pragma unroll 1
-          for (int blk = 0; blk < BLK; ++blk)
-            tma_load_2d(sa + blk * ABLK, &tmA, bars.full(stage), i0 + blk * 32, jc);
+            for (int blk = 0; blk < BLK; ++blk)
+              tma_load_2d(sa + blk * ABLK, &tmA, bars.full(stage), i0 + blk * 32, jc);
+          }
           tma_load_2d(sa + A_BYTES, &tmB, bars.full(stage), jc, 0);
           ++nissued;
           if (++stage == STAGES) {
@@ -773,6 +785,21 @@ int make_map(CUtensorMap* map, const void* base, unsigned long long d0, unsigned
   return TT_OK;
 }
 
+// 3-D map over a column-major m x n FP32 matrix viewed as (32 rows of a block, column, block):
+// strides m*4 bytes (column) and 128 bytes (block), box (32, bk, nblk).  One copy then fills
+// nblk consecutive 32-row blocks of bk columns each, laid out block after block.
+int make_map_blocks(CUtensorMap* map, const float* base, unsigned long long m, unsigned long long n,
+                    unsigned bk, unsigned nblk, CUtensorMapSwizzle sw, CUtensorMapDataType dt) {
+  cuuint64_t dims[3] = {32, n, m / 32};
+  cuuint64_t strides[2] = {m * 4, 128};
+  cuuint32_t box[3] = {32, bk, nblk};
+  cuuint32_t es[3] = {1, 1, 1};
+  CUresult r = g_encode(map, dt, 3, const_cast<float*>(base), dims, strides, box, es,
+                        CU_TENSOR_MAP_INTERLEAVE_NONE, sw, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                        CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  return r == CUDA_SUCCESS ? TT_OK : TT_ERR_UNSUPPORTED;
+}
+
 template <typename K>
 int set_smem(K kernel, size_t bytes) {
   return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess
@@ -831,7 +858,8 @@ int run_project(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap&
 
 template <int BN, int MT>
 int run_sketch(const CUtensorMap& ma, const CUtensorMap& mb, long long m, long long n, int N,
-               long long kchunk, int nsplit, int ngroups, double* part, DevStatus* st, cudaStream_t s) {
+               long long kchunk, int nsplit, int ngroups, double* part, DevStatus* st, cudaStream_t s,
+               int a3d) {
   constexpr int BK = MT >= 8 ? 8 : MT == 4 ? 16 : 32;
   constexpr uint32_t STAGE = ((MT * 4) * BK * 128 + BN * BK * 4 + 1023) & ~1023u;
   constexpr int STAGES = (int)std::min<size_t>(8, kSmemBudget / STAGE);
@@ -847,7 +875,7 @@ int run_sketch(const CUtensorMap& ma, const CUtensorMap& mb, long long m, long l
   }
   const int units = ngroups * nsplit;
   const int grid = std::min(units, g_sms);
-  kern<<<grid, 192, smem, s>>>(ma, mb, m, n, N, kchunk, nsplit, ngroups, part, st);
+  kern<<<grid, 192, smem, s>>>(ma, mb, m, n, N, kchunk, nsplit, ngroups, part, st, a3d);
   count_launch();
   TT_LAUNCH_CHECK();
   return TT_OK;
@@ -1034,15 +1062,23 @@ int launch_sketch_tc(const float* a, long long m, long long n, const float* w, i
     return TT_ERR_NOMEM;
   }
   CUtensorMap ma, mb;
-  TT_TRY(make_map(&ma, a, (unsigned long long)m, (unsigned long long)n, (unsigned long long)m * 4, 32,
-                  (unsigned)BK, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
+  // One 3-D copy per stage when the driver accepts the block view (MT*4 blocks of 32 rows),
+  // otherwise one 2-D copy per 32-row block.
+  int a3d = 0;
+  if (!getenv("TTR_SKETCH_2D") &&
+      make_map_blocks(&ma, a, (unsigned long long)m, (unsigned long long)n, (unsigned)BK, (unsigned)(MT * 4),
+                      CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32) == TT_OK)
+    a3d = 1;
+  else
+    TT_TRY(make_map(&ma, a, (unsigned long long)m, (unsigned long long)n, (unsigned long long)m * 4, 32,
+                    (unsigned)BK, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
   const CUtensorMapSwizzle bsw = BK == 8 ? CU_TENSOR_MAP_SWIZZLE_32B
                                  : BK == 16 ? CU_TENSOR_MAP_SWIZZLE_64B
                                             : CU_TENSOR_MAP_SWIZZLE_128B;
   TT_TRY(make_map(&mb, w, (unsigned long long)n, (unsigned long long)N, (unsigned long long)wc * 4,
                   (unsigned)BK, (unsigned)BN, bsw, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
   int rc;
-#define SK(BNV, MTV) rc = run_sketch<BNV, MTV>(ma, mb, m, n, N, kc, ns, ng, part, st, s)
+#define SK(BNV, MTV) rc = run_sketch<BNV, MTV>(ma, mb, m, n, N, kc, ns, ng, part, st, s, a3d)
 #define SK_MT(BNV)                   \
   switch (MT) {                      \
     case 8: SK(BNV, 8); break;       \
@@ -1098,15 +1134,23 @@ int launch_sketch_tc_static(const float* a, long long m, long long n, const floa
     ns = (int)((n + kc - 1) / kc);
   }
   CUtensorMap ma, mb;
-  TT_TRY(make_map(&ma, a, (unsigned long long)m, (unsigned long long)n, (unsigned long long)m * 4, 32,
-                  (unsigned)BK, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
+  // One 3-D copy per stage when the driver accepts the block view (MT*4 blocks of 32 rows),
+  // otherwise one 2-D copy per 32-row block.
+  int a3d = 0;
+  if (!getenv("TTR_SKETCH_2D") &&
+      make_map_blocks(&ma, a, (unsigned long long)m, (unsigned long long)n, (unsigned)BK, (unsigned)(MT * 4),
+                      CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32) == TT_OK)
+    a3d = 1;
+  else
+    TT_TRY(make_map(&ma, a, (unsigned long long)m, (unsigned long long)n, (unsigned long long)m * 4, 32,
+                    (unsigned)BK, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
   const CUtensorMapSwizzle bsw = BK == 8 ? CU_TENSOR_MAP_SWIZZLE_32B
                                  : BK == 16 ? CU_TENSOR_MAP_SWIZZLE_64B
                                             : CU_TENSOR_MAP_SWIZZLE_128B;
   TT_TRY(make_map(&mb, w, (unsigned long long)n, (unsigned long long)N, (unsigned long long)wc * 4,
                   (unsigned)BK, (unsigned)BN, bsw, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
   int rc;
-#define SK(BNV, MTV) rc = run_sketch<BNV, MTV>(ma, mb, m, n, N, kc, ns, ng, part, st, s)
+#define SK(BNV, MTV) rc = run_sketch<BNV, MTV>(ma, mb, m, n, N, kc, ns, ng, part, st, s, a3d)
 #define SK_MT(BNV)                   \
   switch (MT) {                      \
     case 8: SK(BNV, 8); break;       \

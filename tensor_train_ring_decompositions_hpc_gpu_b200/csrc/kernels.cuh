@@ -24,6 +24,7 @@ struct Arena {
 // Bytes a launcher needs from the arena (callers reserve before launching).
 size_t sketch_ws_bytes(long long m, long long n, int N);
 size_t gram_ws_bytes(long long nvec, int M);
+size_t project_ws_bytes(long long m, long long n, int N);
 
 // Philox Gaussian fill (column-major rows x cols, ld).
 int launch_gaussian(float* out, long long rows, int cols, long long ld, unsigned long long seed,

@@ -52,8 +52,10 @@ def test_sketch(gpu, gemm, m, n, N):
 
 
 @pytest.mark.parametrize("gemm", ["fp32", "tc"])
+# m <= 64 takes the one-column-per-thread kernel; small n with m >= 256 splits K.
 @pytest.mark.parametrize("m,n,N", [(256, 4096, 24), (1024, 3000, 40), (32, 100000, 32), (300, 777, 17),
-                                   (40, 65536, 32), (1024, 1024, 64)])
+                                   (40, 65536, 32), (1024, 1024, 64), (37, 5000, 20), (6, 1001, 5),
+                                   (64, 3001, 64), (4096, 100, 8)])
 def test_project(gpu, gemm, m, n, N):
     ttr = _ttr()
     a = _randn_cm(m, n, 3, gpu)
@@ -99,7 +101,10 @@ def test_gram_tall(gpu, n, N):
     assert _rel(w, zd.T @ zd) < 1e-12
 
 
-@pytest.mark.parametrize("n,N", [(1024, 40), (100000, 24), (5000, 64), (300, 128)])
+# (1024, 40), (512, 64), (1000, 33), (64, 5), (7, 3), (2048, 16), (1024, 48) fit in one CTA's
+# shared memory (single-launch kernel); the others take the multi-kernel path.
+@pytest.mark.parametrize("n,N", [(1024, 40), (512, 64), (1000, 33), (64, 5), (7, 3), (2048, 16), (1024, 48),
+                                 (100000, 24), (5000, 64), (300, 128), (4096, 16)])
 def test_cholqr2(gpu, n, N):
     ttr = _ttr()
     y = _randn_cm(n, N, 7, gpu)
@@ -123,7 +128,7 @@ def test_cholqr2_rank_deficient_zeroes_dependent_columns(gpu):
     assert np.all(norms[:6] > 0.99) and np.all(norms[6:] < 1e-3)
 
 
-@pytest.mark.parametrize("N", [5, 24, 32, 40, 64, 96, 128])
+@pytest.mark.parametrize("N", [1, 2, 5, 24, 32, 33, 40, 63, 64, 65, 96, 128])
 def test_syev(gpu, N):
     import torch
     ttr = _ttr()
@@ -138,6 +143,25 @@ def test_syev(gpu, N):
     assert np.linalg.norm(w @ vec - vec * ev) < 1e-10 * ref[0] * N
     assert np.linalg.norm(vec.T @ vec - np.eye(N)) < 1e-12 * N
     assert 1 <= sweeps <= 40
+
+
+@pytest.mark.parametrize("N,rank", [(40, 12), (64, 1), (32, 0), (96, 30)])
+def test_syev_rank_deficient_terminates(gpu, N, rank):
+    """Gram matrices of rank-deficient sketches have eigenvalues at the FP64 rounding floor;
+    the sweep loop must still converge (rotations below that floor are skipped)."""
+    import torch
+    ttr = _ttr()
+    rng = np.random.default_rng(N + rank)
+    b = rng.standard_normal((N, rank))
+    w = b @ b.T
+    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu))
+    ev = ev.cpu().numpy()
+    vec = vec.cpu().numpy()
+    ref = np.sort(np.linalg.eigvalsh(w))[::-1]
+    scale = max(ref[0], 1.0)
+    np.testing.assert_allclose(ev, ref, atol=1e-12 * scale * N)
+    assert np.linalg.norm(vec.T @ vec - np.eye(N)) < 1e-12 * N
+    assert 1 <= sweeps < 40
 
 
 def test_syev_graded_spectrum_relative_accuracy(gpu):
