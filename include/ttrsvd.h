@@ -19,7 +19,7 @@
 extern "C" {
 #endif
 
-#define TTRSVD_ABI_VERSION 1
+#define TTRSVD_ABI_VERSION 2
 #define TT_MAX_ORDER 16
 #define TT_MAX_SMALL 128 /* largest Gram / Jacobi size handled on chip */
 
@@ -36,7 +36,8 @@ typedef enum tt_status {
   TT_ERR_NOCONV = 6,     /* Jacobi eigen-solver did not converge within max_sweeps */
   TT_ERR_TIMEOUT = 7,    /* a bounded device-side wait ran out */
   TT_ERR_CUDA = 8,       /* CUDA runtime error */
-  TT_ERR_UNSUPPORTED = 9 /* shape/rank combination outside the implemented range */
+  TT_ERR_UNSUPPORTED = 9, /* shape/rank combination outside the implemented range */
+  TT_ERR_IO = 10          /* core file missing, unreadable, truncated or not a core file */
 } tt_status;
 
 /* GEMM engine for the two bulk GEMMs (sketch Y = A*W and projection B^T = A^T*Q). */
@@ -90,6 +91,12 @@ typedef struct tt_stats {
   double pass_ms[4];
   double pass_bytes[4];
   int pass_launches[4];
+  /* TT_FLAG_PROFILE: the single longest bulk pass of the call (kind, unfolding index,
+   * device time, algorithmic bytes). */
+  int top_kind;
+  int top_step;
+  double top_ms;
+  double top_bytes;
 } tt_stats;
 
 /* Bulk pass kinds reported in tt_stats.pass_*. */
@@ -182,6 +189,20 @@ int tt_k_syev(tt_ctx* ctx, const double* w, int N, double* evals, double* evecs,
  * after the result is complete.  This entry point has no counterpart in the reference. */
 int tt_k_sketch_noalloc(const float* a, long long m, long long n, const float* w, int N,
                         long long ldw, double* y, int gemm, void* stream);
+
+/* Core files.  The reference frees its cores before returning (ttdec6_singleGPU.cu:947-952)
+ * and has no file format; this one stores a decomposition for later use.  Layout
+ * (little-endian): 8-byte magic "TTRCORE1", int32 kind (0 = TT, 1 = TR), int32 d,
+ * int32 dtype (0 = FP32), int32 reserved (0), int64 n[d], int64 r[d+1], then core k as
+ * r[k] * n[k] * r[k+1] FP32 values, column-major (r[k], n[k], r[k+1]).  `device` = 1 when
+ * the core pointers are device memory (copied through the host). */
+int tt_cores_save(const char* path, int d, const int* n, const int* r, int ring,
+                  const float* const* cores, int device);
+/* Reads the header: d, n[0..d-1], r[0..d] (arrays of TT_MAX_ORDER and TT_MAX_ORDER + 1 ints)
+ * and ring (0/1). */
+int tt_cores_header(const char* path, int* d, int* n, int* r, int* ring);
+/* Reads the cores into caller buffers sized from tt_cores_header. */
+int tt_cores_load(const char* path, float* const* cores, int device);
 
 /* TR bond permute (r0, r1, N) -> (r1, N, r0), column-major.  Replaces tensorToMode231
  * (trdecomposition/high_order_GPUs/trdec6_singleGPU.cu:49-58). */

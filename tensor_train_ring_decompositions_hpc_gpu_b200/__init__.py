@@ -13,6 +13,7 @@ Reference-compatible entry points (same names, argument meaning and return value
 from __future__ import annotations
 
 import ctypes as C
+import os
 from dataclasses import dataclass, field
 
 import numpy as np
@@ -282,6 +283,36 @@ def permute231(x, r0: int, r1: int, n: int):
     out = torch.empty_like(x)
     check(lib().tt_k_permute231(_ctx_for(x.device.index), _ptr(x), _ptr(out), r0, r1, n))
     return out
+
+
+# ---- core files ----
+def save_cores(path: str, cores, ring: bool = False) -> None:
+    """Write cores (logical (r_{k-1}, n_k, r_k) arrays, NumPy or torch, host or CUDA) to a
+    core file (format in include/ttrsvd.h)."""
+    d = len(cores)
+    n = [int(c.shape[1]) for c in cores]
+    r = [int(cores[0].shape[0])] + [int(c.shape[2]) for c in cores]
+    host = []
+    for c in cores:
+        if hasattr(c, "detach"):
+            c = c.detach().float().cpu().numpy()
+        host.append(np.asfortranarray(np.asarray(c, dtype=np.float32)))
+    ptrs = (C.c_void_p * d)(*[h.ctypes.data for h in host])
+    check(lib().tt_cores_save(os.fsencode(path), d, _lib.int_array(n), _lib.int_array(r), 1 if ring else 0,
+                              ptrs, 0))
+
+
+def load_cores(path: str):
+    """Read a core file; returns (cores as column-major NumPy arrays, ring)."""
+    d = C.c_int()
+    ring = C.c_int()
+    n = (C.c_int * _lib.TT_MAX_ORDER)()
+    r = (C.c_int * (_lib.TT_MAX_ORDER + 1))()
+    check(lib().tt_cores_header(os.fsencode(path), C.byref(d), n, r, C.byref(ring)))
+    cores = [np.empty((r[k], n[k], r[k + 1]), dtype=np.float32, order="F") for k in range(d.value)]
+    ptrs = (C.c_void_p * d.value)(*[c.ctypes.data for c in cores])
+    check(lib().tt_cores_load(os.fsencode(path), ptrs, 0))
+    return cores, bool(ring.value)
 
 
 # ---- reference-compatible entry points (host NumPy tensors, column-major) ----

@@ -11,7 +11,7 @@ TT_OK = 0
 STATUS_NAMES = {
     0: "TT_OK", 1: "TT_ERR_ARG", 2: "TT_ERR_SHAPE", 3: "TT_ERR_RANK", 4: "TT_ERR_NONFINITE",
     5: "TT_ERR_NOMEM", 6: "TT_ERR_NOCONV", 7: "TT_ERR_TIMEOUT", 8: "TT_ERR_CUDA",
-    9: "TT_ERR_UNSUPPORTED",
+    9: "TT_ERR_UNSUPPORTED", 10: "TT_ERR_IO",
 }
 TT_GEMM_AUTO, TT_GEMM_TC, TT_GEMM_FP32 = 0, 1, 2
 TT_METHOD_EDRSVD, TT_METHOD_EXACT = 0, 1
@@ -28,7 +28,8 @@ EXPORTED = [
     "tt_ctx_create", "tt_ctx_destroy", "tt_ctx_set_stream", "tt_ctx_reserve", "tt_last_error",
     "tt_default_opts", "tt_abi_version", "tt_svd", "tr_svd", "tt_rel_error", "tt_k_gaussian",
     "tt_k_sketch", "tt_k_project", "tt_k_gram_rows", "tt_k_gram_tall", "tt_k_cholqr2",
-    "tt_k_syev", "tt_k_sketch_noalloc", "tt_k_permute231", "tt_ref_ttdec_gpu_float", "tt_ref_trdec_gpu_float",
+    "tt_k_syev", "tt_k_sketch_noalloc", "tt_cores_save", "tt_cores_header", "tt_cores_load",
+    "tt_k_permute231", "tt_ref_ttdec_gpu_float", "tt_ref_trdec_gpu_float",
     "tt_ref_ttdec_half_lu_device_6", "tt_ref_trdec_half_lu_device_6",
 ]
 
@@ -48,6 +49,7 @@ class TTStats(C.Structure):
         ("jacobi_sweeps", C.c_int), ("kernels", C.c_int), ("est_rel_err", C.c_double),
         ("flops", C.c_double), ("bytes", C.c_double), ("pass_ms", C.c_double * 4),
         ("pass_bytes", C.c_double * 4), ("pass_launches", C.c_int * 4),
+        ("top_kind", C.c_int), ("top_step", C.c_int), ("top_ms", C.c_double), ("top_bytes", C.c_double),
     ]
 
 
@@ -91,6 +93,9 @@ def load():
         "tt_k_syev": (i, [vp, vp, i, vp, vp, P(i)]),
         "tt_k_permute231": (i, [vp, vp, vp, i, i, ll]),
         "tt_k_sketch_noalloc": (i, [vp, ll, ll, vp, i, ll, vp, i, vp]),
+        "tt_cores_save": (i, [C.c_char_p, i, P(i), P(i), i, P(vp), i]),
+        "tt_cores_header": (i, [C.c_char_p, P(i), P(i), P(i), P(i)]),
+        "tt_cores_load": (i, [C.c_char_p, P(vp), i]),
         "tt_ref_ttdec_gpu_float": (C.c_float, [vp, P(i), P(i), P(d), P(C.c_float), P(C.c_float)]),
         "tt_ref_trdec_gpu_float": (C.c_float, [vp, P(i), P(i), P(d), P(C.c_float), P(C.c_float)]),
         "tt_ref_ttdec_half_lu_device_6": (C.c_float, [vp, P(i), P(i), i, i, i]),

@@ -156,6 +156,12 @@ struct Step {
   bool fold = false;     // full-rank step carried as a pending rotation
   bool perm231 = false;  // TR step 1
   long long next_elems = 0;
+  // Row compaction: a basis zero-padded beyond r_eff produces zero rows in the next data, so
+  // only the first n_out rows are written and later unfoldings skip them; the cores get the
+  // zero rows back.  rows_in = rows of the stored data per mode index entering this step,
+  // core_rows = the core's first rank; n_out = rows written; r1_out = TR bond r1 actually
+  // carried after step 1 (n_out = r0 * r1_out).
+  int rows_in = 1, core_rows = 1, n_out = 0, r1_out = 0;
 };
 
 struct Plan {
@@ -168,6 +174,7 @@ struct Plan {
   size_t max_data = 0, max_omega = 0, max_y = 0, max_bt = 0, max_core = 0, max_ws = 0;
   size_t max_ef = (size_t)TT_MAX_SMALL * TT_MAX_SMALL;  // FP32 basis (m x r or ks x r)
   int max_small = 0;
+  int last_rows = 1;  // rows per mode index of the data left for the last core
 };
 
 int engine_of(const tt_opts& o) {
@@ -222,7 +229,7 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
   const int s = std::max(0, o.oversample);
   const bool nofold = (o.flags & TT_FLAG_NO_FOLD) != 0;
   long long size = P.total;  // elements of the current (raw) data
-  long long rows_prev = 1;   // r_{k-1} of the true data
+  long long rows_prev = 1;   // rows per mode index of the stored data (effective r_{k-1})
   P.steps.clear();
   for (int k = 0; k < d - 1; ++k) {
     Step st;
@@ -233,7 +240,11 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
     st.perm231 = first_ring && r[0] > 1;
     const long long mn = std::min(st.m, st.cols);
     st.r_eff = (int)std::min<long long>(st.r_req, mn);
-    if (o.method == TT_METHOD_EXACT || mn <= TT_MAX_SMALL) {
+    // Exact Gram-eigen step when the small side is tiny (<= 64: one-CTA eigen-solver), when
+    // a sketch would cover half of it anyway, or on request; otherwise EDrSVD.
+    const bool small_exact =
+        mn <= 64 || (mn <= TT_MAX_SMALL && 2LL * (st.r_eff + s) >= mn);
+    if (o.method == TT_METHOD_EXACT || small_exact) {
       if (mn > TT_MAX_SMALL) {
         set_error(TT_ERR_UNSUPPORTED, "exact step %d needs min(m, n) = %lld <= %d", k, mn, TT_MAX_SMALL);
         return TT_ERR_UNSUPPORTED;
@@ -249,12 +260,22 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
       }
     }
     st.fold = !nofold && !st.perm231 && st.path == PATH_EXACT_ROWS && st.r_req == st.m &&
-              st.r_eff == st.m && !(ring && k == 0);
+              st.r_eff == st.m && !(ring && k == 0) && rows_prev == r[k];
     if (st.fold && (o.flags & TT_FLAG_IDENTITY_GAUGE)) st.path = PATH_IDENTITY;
-    st.next_elems = (long long)st.r_req * st.cols;
+    st.rows_in = first_ring ? 1 : (int)rows_prev;
+    st.core_rows = first_ring ? 1 : r[k];
+    if (first_ring) {
+      st.r1_out = (st.r_eff + r[0] - 1) / r[0];
+      st.n_out = r[0] * st.r1_out;
+    } else {
+      st.r1_out = 0;
+      st.n_out = st.fold ? st.r_req : st.r_eff;
+    }
+    st.next_elems = (long long)st.n_out * st.cols;
     P.steps.push_back(st);
     size = st.fold ? size : st.next_elems;
-    rows_prev = first_ring ? r[1] : st.r_req;
+    rows_prev = first_ring ? st.r1_out : st.n_out;
+    P.last_rows = (int)rows_prev;
     if (st.perm231 && st.path == PATH_EXACT_COLS)
       P.max_bt = std::max<size_t>(P.max_bt, (size_t)st.next_elems);
     if (!st.fold) P.max_data = std::max<size_t>(P.max_data, (size_t)st.next_elems);
@@ -361,10 +382,13 @@ __global__ void k_store_sigma(const double* evals, int cnt, double* dst) {
   if (i < TT_STATS_MAX_SIGMA) dst[i] = (i < cnt) ? sqrt(fmax(evals[i], 0.0)) : -1.0;
 }
 
-int emit_core(const float* raw, float* out, const double* pend, int R, long long ni, int ncols,
+// Core (Rcore, ni, ncols) from the basis `raw` ((Rin ni) x ncols): a pending rotation is folded
+// in (then Rin == Rcore), compacted rows Rin < Rcore come back as zero rows.
+int emit_core(const float* raw, float* out, const double* pend, int Rin, int Rcore, long long ni, int ncols,
               cudaStream_t s) {
-  if (pend) return launch_fold_rows(raw, out, pend, R, ni, ncols, s);
-  TT_CUDA(cudaMemcpyAsync(out, raw, sizeof(float) * (size_t)R * ni * ncols, cudaMemcpyDeviceToDevice, s));
+  if (pend) return launch_fold_rows(raw, out, pend, Rin, ni, ncols, s);
+  if (Rin != Rcore) return launch_expand_rows(raw, Rin, out, Rcore, ni * ncols, s);
+  TT_CUDA(cudaMemcpyAsync(out, raw, sizeof(float) * (size_t)Rin * ni * ncols, cudaMemcpyDeviceToDevice, s));
   return TT_OK;
 }
 
@@ -376,6 +400,7 @@ __global__ void k_eye(double* p, int m) {
 // Accounting of the bulk passes: algorithmic FLOPs/bytes always, device time when profiling.
 struct PassRec {
   int kind;
+  int step;
   double bytes;
   cudaEvent_t a, b;
 };
@@ -383,6 +408,7 @@ struct Passes {
   tt_ctx* c = nullptr;
   cudaStream_t s = nullptr;
   bool on = false;
+  int cur_step = 0;
   size_t next = 0;
   double flops = 0.0, bytes = 0.0;
   std::vector<PassRec> recs;
@@ -407,7 +433,7 @@ struct Passes {
     const int st = fn();
     if (a) {
       cudaEventRecord(b, s);
-      recs.push_back({kind, by, a, b});
+      recs.push_back({kind, cur_step, by, a, b});
     }
     return st;
   }
@@ -453,14 +479,17 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
 
   const float* cur = x;
   int slot = 0;
-  const double* pend = nullptr;  // pending rotation (rows_prev x rows_prev), or null
+  const double* pend = nullptr;  // pending rotation (rows_in x rows_in), or null
   int pend_slot = 0;
-  long long rows_prev = 1;
   const int nsteps = (int)P.steps.size();
   for (int k = 0; k < nsteps; ++k) {
     const Step& st = P.steps[k];
+    pass.cur_step = k;
     const long long m = st.m, cols = st.cols;
     const int rq = st.r_req, re = st.r_eff;
+    const int nout = st.n_out;                      // rows of the next data (compacted)
+    const int pr1 = st.perm231 ? st.r1_out : 1;     // TR bond r1 carried after step 1
+    const int rin = st.rows_in, rcore = st.core_rows;
     const int engine = engine_for(o, m, cols);
     float* next = B.data[slot];
     double* sigdst = c->dsig + (size_t)k * TT_STATS_MAX_SIGMA;
@@ -470,20 +499,19 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
     const long long ni = P.n[k];
 
     if (st.path == PATH_IDENTITY) {
-      // Core = (I (x) P^T) I_m as an (rows_prev n_k) x m matrix; no pending rotation afterwards.
+      // Core = (I (x) P^T) I_m as an (rows_in n_k) x m matrix; no pending rotation afterwards.
       k_eye<<<ceil_div(m * m, 256), 256, 0, s>>>(B.w, (int)m);
       count_launch();
       TT_LAUNCH_CHECK();
       if (pend) {
         TT_TRY(launch_f64_to_f32_cols(B.w, m, m, (int)m, B.corebuf, m, (int)m, s));
-        TT_TRY(launch_fold_rows(B.corebuf, core_dst, pend, (int)rows_prev, ni, (int)m, s));
+        TT_TRY(launch_fold_rows(B.corebuf, core_dst, pend, rin, ni, (int)m, s));
       } else {
         TT_TRY(launch_f64_to_f32_cols(B.w, m, m, (int)m, core_dst, m, (int)m, s));
       }
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, 0, sigdst);
       count_launch();
       pend = nullptr;
-      rows_prev = rq;
       continue;  // data unchanged
     }
 
@@ -504,7 +532,7 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
       if (ring1) {
         TT_TRY(launch_ring_core1(B.ef, (int)m, P.r[0], P.r[1], cores[0], s));
       } else {
-        TT_TRY(emit_core(B.ef, core_dst, pend, (int)rows_prev, ni, rq, s));
+        TT_TRY(emit_core(B.ef, core_dst, pend, rin, rcore, ni, rq, s));
       }
       if (st.fold) {
         // next data = raw data; pending rotation = eigenvectors of the raw Gram
@@ -512,12 +540,11 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
         TT_CUDA(cudaMemcpyAsync(pnew, B.evecs, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, s));
         pend = pnew;
         pend_slot ^= 1;
-        rows_prev = rq;
         continue;
       }
-      TT_TRY(pass.run(TT_PASS_PROJECT, 2.0 * m * cols * rq, 4.0 * m * cols + 4.0 * rq * cols, [&] {
-        return launch_project(cur, m, cols, B.ef, rq, m, next, st.perm231 ? 0 : rq,
-                              st.perm231 ? OUT_PERM231 : OUT_ROWMAJOR, P.r[0], P.r[1],
+      TT_TRY(pass.run(TT_PASS_PROJECT, 2.0 * m * cols * nout, 4.0 * m * cols + 4.0 * nout * cols, [&] {
+        return launch_project(cur, m, cols, B.ef, nout, m, next, st.perm231 ? 0 : nout,
+                              st.perm231 ? OUT_PERM231 : OUT_ROWMAJOR, P.r[0], pr1,
                               engine == TT_GEMM_TC && re < m ? TT_GEMM_TC : TT_GEMM_FP32, ws, c->dstat, s);
       }));
     } else if (st.path == PATH_EXACT_COLS) {
@@ -536,14 +563,14 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
       if (ring1) {
         TT_TRY(launch_ring_core1(ubuf, (int)m, P.r[0], P.r[1], cores[0], s));
       } else {
-        TT_TRY(emit_core(ubuf, core_dst, pend, (int)rows_prev, ni, rq, s));
+        TT_TRY(emit_core(ubuf, core_dst, pend, rin, rcore, ni, rq, s));
       }
       if (st.perm231) {
         float* tmp = B.bt;  // q x cols scratch (q <= 128, cols <= 128)
-        TT_TRY(launch_sigma_vt(B.evals, B.evecs, (int)cols, rq, re, tmp, s));
-        TT_TRY(launch_permute231(tmp, next, P.r[0], P.r[1], cols, s));
+        TT_TRY(launch_sigma_vt(B.evals, B.evecs, (int)cols, nout, re, tmp, s));
+        TT_TRY(launch_permute231(tmp, next, P.r[0], pr1, cols, s));
       } else {
-        TT_TRY(launch_sigma_vt(B.evals, B.evecs, (int)cols, rq, re, next, s));
+        TT_TRY(launch_sigma_vt(B.evals, B.evecs, (int)cols, nout, re, next, s));
       }
     } else {  // PATH_RAND
       const int ks = st.ks;
@@ -590,27 +617,27 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
       TT_TRY(launch_canon_cols(ubuf, m, re, m, B.evecs, ks, ks, s));
       // next = E_r^T B  (rotation of the small factor; plain FP32 keeps it exact to FP32)
       TT_TRY(launch_f64_to_f32_cols(B.evecs, ks, ks, re, B.ef, ks, rq, s));
-      TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * ks * cols * rq, 4.0 * ks * cols + 4.0 * rq * cols, [&] {
-        return launch_project(B.bt, ks, cols, B.ef, rq, ks, next, st.perm231 ? 0 : rq,
-                              st.perm231 ? OUT_PERM231 : OUT_ROWMAJOR, P.r[0], P.r[1], TT_GEMM_FP32,
+      TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * ks * cols * nout, 4.0 * ks * cols + 4.0 * nout * cols, [&] {
+        return launch_project(B.bt, ks, cols, B.ef, nout, ks, next, st.perm231 ? 0 : nout,
+                              st.perm231 ? OUT_PERM231 : OUT_ROWMAJOR, P.r[0], pr1, TT_GEMM_FP32,
                               ws, c->dstat, s);
       }));
       if (ring1) {
         TT_TRY(launch_ring_core1(ubuf, (int)m, P.r[0], P.r[1], cores[0], s));
       } else {
-        TT_TRY(emit_core(ubuf, core_dst, pend, (int)rows_prev, ni, rq, s));
+        TT_TRY(emit_core(ubuf, core_dst, pend, rin, rcore, ni, rq, s));
       }
     }
     pend = nullptr;
     cur = next;
     slot ^= 1;
-    rows_prev = ring1 ? P.r[1] : rq;
   }
-  // last core: (rows_prev, n_d, r_d) = current data, with a pending rotation folded in
+  // last core: (r_{d-1}, n_d, r_d) from the current data (P.last_rows rows per index), with a
+  // pending rotation folded in or compacted rows restored as zeros
   {
     const int k = P.d - 1;
     const long long ni = P.n[k] * (long long)P.r[P.d];
-    TT_TRY(emit_core(cur, cores[k], pend, (int)rows_prev, ni, 1, s));
+    TT_TRY(emit_core(cur, cores[k], pend, P.last_rows, P.r[k], ni, 1, s));
   }
   TT_CUDA(cudaEventRecord(c->ev1, s));
   if (host_io) {
@@ -643,12 +670,20 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
     stats->kernels = g_kernel_launches;
     stats->flops = pass.flops;
     stats->bytes = pass.bytes;
+    stats->top_kind = -1;
+    stats->top_step = -1;
     for (const PassRec& rec : pass.recs) {
       float pm = 0.f;
       cudaEventElapsedTime(&pm, rec.a, rec.b);
       stats->pass_ms[rec.kind] += pm;
       stats->pass_bytes[rec.kind] += rec.bytes;
       stats->pass_launches[rec.kind] += 1;
+      if (pm > stats->top_ms) {
+        stats->top_ms = pm;
+        stats->top_kind = rec.kind;
+        stats->top_step = rec.step;
+        stats->top_bytes = rec.bytes;
+      }
     }
   }
   if (c->hstat->code != 0) {

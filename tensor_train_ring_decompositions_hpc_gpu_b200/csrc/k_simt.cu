@@ -49,11 +49,14 @@ __global__ void k_gaussian(float* __restrict__ out, long long rows, long long to
     const float sc = 2.3283064365386963e-10f;  // 2^-32
     const float u0 = ((float)w.x + 0.5f) * sc, u1 = ((float)w.y + 0.5f) * sc;
     const float u2 = ((float)w.z + 0.5f) * sc, u3 = ((float)w.w + 0.5f) * sc;
-    const float r0 = sqrtf(-2.0f * logf(u0)), r1 = sqrtf(-2.0f * logf(u2));
+    // Box-Muller with the hardware approximations (absolute error ~1e-6 on the normals): the
+    // angle is taken in [-pi, pi), where __sincosf is accurate, and the sign flip restores
+    // sin/cos of 2*pi*u.
+    const float r0 = sqrtf(-2.0f * __logf(u0)), r1 = sqrtf(-2.0f * __logf(u2));
     float s0, c0, s1, c1;
-    sincospif(2.0f * u1, &s0, &c0);
-    sincospif(2.0f * u3, &s1, &c1);
-    const float g[4] = {r0 * c0, r0 * s0, r1 * c1, r1 * s1};
+    __sincosf(6.283185307179586f * (u1 - 0.5f), &s0, &c0);
+    __sincosf(6.283185307179586f * (u3 - 0.5f), &s1, &c1);
+    const float g[4] = {-r0 * c0, -r0 * s0, -r1 * c1, -r1 * s1};
     // element e = row + rows * col; one 64-bit division per call, then step through rows
     long long col = (4 * c) / rows;
     long long row = 4 * c - col * rows;
@@ -382,23 +385,28 @@ __global__ void __launch_bounds__(256) k_project_simt(const float* __restrict__ 
 }
 
 // Small-K projection out = Q^T A for K = m <= 64 (the rotation E_r^T B of a small factor, or
-// an m <= 64 unfolding): one column of A per thread.  A's columns are contiguous, so a tile of
-// 256 columns is one contiguous block: it is staged through shared memory with coalesced
-// float4 loads (odd row stride, conflict-free), Q sits in shared memory as float4 rows, and
-// row-major outputs leave through shared memory as one contiguous block.
-template <int NP>
+// an m <= 64 unfolding).  A's columns are contiguous, so a tile of TJ columns is one contiguous
+// block: it is staged through shared memory with coalesced float4 loads (odd row stride,
+// conflict-free), Q sits in shared memory as float4 rows, and each column's NP outputs are
+// computed by SPLIT threads (NP / SPLIT each, which keeps registers low enough for several
+// blocks per SM).  Row-major outputs and the TR bond permute leave through shared memory as
+// contiguous runs.
+template <int NP, int SPLIT>
 __global__ void __launch_bounds__(256) k_proj_smallk(const float* __restrict__ a, int m, long long n,
                                                      const float* __restrict__ q, int N, long long ldq,
                                                      float* __restrict__ out, long long ldo, int mode,
                                                      int r0, int r1) {
-  constexpr int TJ = 256;
+  constexpr int TJ = 256 / SPLIT;   // columns per tile
+  constexpr int NPT = NP / SPLIT;   // outputs per thread
+  static_assert(NPT % 4 == 0, "outputs per thread");
   extern __shared__ __align__(16) float sm_pk[];
   float* Es = sm_pk;            // m x NP: Es[k * NP + c] = Q[k + ldq c]
   float* Xs = Es + 64 * NP;     // TJ x S input tile, then TJ x (NP + 1) output tile
   const int S = (m & 1) ? m : m + 1;
   constexpr int OS = NP + 1;
   const int tid = threadIdx.x;
-  for (int idx = tid; idx < m * NP; idx += TJ) {
+  const int col_t = tid % TJ, grp = tid / TJ;
+  for (int idx = tid; idx < m * NP; idx += 256) {
     const int k = idx / NP, c = idx - (idx / NP) * NP;
     Es[idx] = (c < N) ? q[k + ldq * (long long)c] : 0.f;
   }
@@ -413,7 +421,7 @@ __global__ void __launch_bounds__(256) k_proj_smallk(const float* __restrict__ a
     const int cnt = nj * m;
     __syncthreads();
     if (vec) {
-      for (int f4 = tid; f4 < (cnt >> 2); f4 += TJ) {
+      for (int f4 = tid; f4 < (cnt >> 2); f4 += 256) {
         const float4 v = __ldg(reinterpret_cast<const float4*>(src) + f4);
         const int e = 4 * f4, col = e / m, k = e - col * m;
         float* d = Xs + col * S + k;
@@ -423,22 +431,22 @@ __global__ void __launch_bounds__(256) k_proj_smallk(const float* __restrict__ a
         d[3] = v.w;
       }
     } else {
-      for (int f = tid; f < cnt; f += TJ) {
+      for (int f = tid; f < cnt; f += 256) {
         const int col = f / m, k = f - col * m;
         Xs[col * S + k] = __ldg(src + f);
       }
     }
     __syncthreads();
-    float acc[NP];
+    float acc[NPT];
 #pragma unroll
-    for (int c = 0; c < NP; ++c) acc[c] = 0.f;
-    if (tid < nj) {
-      const float* xr = Xs + tid * S;
+    for (int c = 0; c < NPT; ++c) acc[c] = 0.f;
+    if (col_t < nj) {
+      const float* xr = Xs + col_t * S;
       for (int k = 0; k < m; ++k) {
         const float x = xr[k];
-        const float4* er = reinterpret_cast<const float4*>(Es + k * NP);
+        const float4* er = reinterpret_cast<const float4*>(Es + k * NP + grp * NPT);
 #pragma unroll
-        for (int c4 = 0; c4 < NP / 4; ++c4) {
+        for (int c4 = 0; c4 < NPT / 4; ++c4) {
           const float4 e = er[c4];
           acc[4 * c4] = fmaf(x, e.x, acc[4 * c4]);
           acc[4 * c4 + 1] = fmaf(x, e.y, acc[4 * c4 + 1]);
@@ -449,15 +457,15 @@ __global__ void __launch_bounds__(256) k_proj_smallk(const float* __restrict__ a
     }
     if (staged_out) {
       __syncthreads();
-      if (tid < nj) {
+      if (col_t < nj) {
 #pragma unroll
-        for (int c = 0; c < NP; ++c)
-          if (c < N) Xs[tid * OS + c] = acc[c];
+        for (int c = 0; c < NPT; ++c)
+          if (grp * NPT + c < N) Xs[col_t * OS + grp * NPT + c] = acc[c];
       }
       __syncthreads();
       if (mode == OUT_ROWMAJOR) {
         float* dst = out + j0 * N;
-        for (int f = tid; f < nj * N; f += TJ) {
+        for (int f = tid; f < nj * N; f += 256) {
           const int col = f / N, c = f - col * N;
           dst[f] = Xs[col * OS + c];
         }
@@ -465,22 +473,23 @@ __global__ void __launch_bounds__(256) k_proj_smallk(const float* __restrict__ a
         const int run = r1 * nj;
         for (int ai = 0; ai < r0; ++ai) {
           float* dst = out + (long long)r1 * (j0 + n * (long long)ai);
-          for (int f = tid; f < run; f += TJ) {
+          for (int f = tid; f < run; f += 256) {
             const int col = f / r1, bi = f - col * r1;
             dst[f] = Xs[col * OS + ai + r0 * bi];
           }
         }
       }
-    } else if (tid < nj) {
-      const long long j = j0 + tid;
+    } else if (col_t < nj) {
+      const long long j = j0 + col_t;
 #pragma unroll
-      for (int c = 0; c < NP; ++c) {
+      for (int cc = 0; cc < NPT; ++cc) {
+        const int c = grp * NPT + cc;
         if (c >= N) continue;
         if (mode == OUT_ROWMAJOR) {
-          out[j * ldo + c] = acc[c];
+          out[j * ldo + c] = acc[cc];
         } else {
           const int ai = c % r0, bi = c / r0;
-          out[(long long)bi + (long long)r1 * (j + n * (long long)ai)] = acc[c];
+          out[(long long)bi + (long long)r1 * (j + n * (long long)ai)] = acc[cc];
         }
       }
     }
@@ -543,22 +552,25 @@ int launch_project(const float* a, long long m, long long n, const float* q, int
   }
   const int NT = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : 64;
   if (m <= 64 && N <= 64) {
-    const size_t shm = (64 * (size_t)NT + 256 * (size_t)std::max<long long>(m + 1, NT + 1)) * sizeof(float);
+    // SPLIT threads per column: 1 for NP = 16, 2 for 32 and 48, 4 for 64.
+    const int split = NT <= 16 ? 1 : NT <= 48 ? 2 : 4;
+    const int tj = 256 / split;
+    const size_t shm = (64 * (size_t)NT + (size_t)tj * std::max<long long>(m + 1, NT + 1)) * sizeof(float);
     static bool attr = false;
     if (!attr) {
-      cudaFuncSetAttribute(k_proj_smallk<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-      cudaFuncSetAttribute(k_proj_smallk<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-      cudaFuncSetAttribute(k_proj_smallk<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-      cudaFuncSetAttribute(k_proj_smallk<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+      cudaFuncSetAttribute(k_proj_smallk<16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+      cudaFuncSetAttribute(k_proj_smallk<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+      cudaFuncSetAttribute(k_proj_smallk<48, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+      cudaFuncSetAttribute(k_proj_smallk<64, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
       attr = true;
     }
-    const int grid = (int)std::min<long long>(ceil_div_ll(n, 256), 4LL * num_sms());
+    const int grid = (int)std::min<long long>(ceil_div_ll(n, tj), 64LL * num_sms());
     const int mi = (int)m;
     switch (NT) {
-      case 16: k_proj_smallk<16><<<grid, 256, shm, s>>>(a, mi, n, q, N, ldq, out, ldo, mode, r0, r1); break;
-      case 32: k_proj_smallk<32><<<grid, 256, shm, s>>>(a, mi, n, q, N, ldq, out, ldo, mode, r0, r1); break;
-      case 48: k_proj_smallk<48><<<grid, 256, shm, s>>>(a, mi, n, q, N, ldq, out, ldo, mode, r0, r1); break;
-      default: k_proj_smallk<64><<<grid, 256, shm, s>>>(a, mi, n, q, N, ldq, out, ldo, mode, r0, r1); break;
+      case 16: k_proj_smallk<16, 1><<<grid, 256, shm, s>>>(a, mi, n, q, N, ldq, out, ldo, mode, r0, r1); break;
+      case 32: k_proj_smallk<32, 2><<<grid, 256, shm, s>>>(a, mi, n, q, N, ldq, out, ldo, mode, r0, r1); break;
+      case 48: k_proj_smallk<48, 2><<<grid, 256, shm, s>>>(a, mi, n, q, N, ldq, out, ldo, mode, r0, r1); break;
+      default: k_proj_smallk<64, 4><<<grid, 256, shm, s>>>(a, mi, n, q, N, ldq, out, ldo, mode, r0, r1); break;
     }
     count_launch();
     TT_LAUNCH_CHECK();
@@ -1043,11 +1055,12 @@ __global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, in
     for (int k = 0; k < N; ++k) {
       const double d = W[k * N + k];
       if (d > tol && dmax > 0.0) {
+        // trailing update of the upper triangle: thread (row group tid >> 6, column tid & 63)
         const double inv = 1.0 / d;
-        const int rm = N - k - 1;
-        for (int idx = tid; idx < rm * rm; idx += NT) {
-          const int i = k + 1 + idx / rm, j = k + 1 + idx % rm;
-          if (j >= i) W[i * N + j] -= W[k * N + i] * W[k * N + j] * inv;
+        const int j = k + 1 + (tid & 63);
+        if (j < N) {
+          const double wkj = W[k * N + j] * inv;
+          for (int i = k + 1 + (tid >> 6); i <= j; i += NT / 64) W[i * N + j] -= W[k * N + i] * wkj;
         }
       }
       __syncthreads();
@@ -1257,7 +1270,8 @@ __global__ void __launch_bounds__(256) k_syev_jacobi(const double* __restrict__ 
   const int tid = threadIdx.x, nt = blockDim.x;
   for (int idx = tid; idx < Np * Np; idx += nt) {
     const int i = idx / Np, j = idx % Np;
-    W[idx] = (i < N && j < N) ? w_in[i + (long long)N * j] : 0.0;
+    // symmetrised: Grams from the tensor cores differ between (i, j) and (j, i) by rounding
+    W[idx] = (i < N && j < N) ? 0.5 * (w_in[i + (long long)N * j] + w_in[j + (long long)N * i]) : 0.0;
     V[idx] = (i == j) ? 1.0 : 0.0;
   }
   __syncthreads();
@@ -1355,190 +1369,262 @@ __global__ void __launch_bounds__(256) k_syev_jacobi(const double* __restrict__ 
   for (int a = tid; a < N; a += nt) evals[a] = W[order[a] * Np + order[a]];
 }
 
-// Small-N variant (N <= 64), latency-oriented: one barrier per round.
-//  * W and V are double-buffered in shared memory; a round computes W' = J^T W J and V' = V J
-//    for all Np/2 rotations at once (each entry from at most four old entries), 31 warps
-//    covering the entries with their (row, column) fixed for the whole solve.
-//  * The round-robin pairing of every round (partner, pair slot, which side) is tabulated
-//    once at start-up.
-//  * The last warp computes the NEXT round's rotations while the others apply the current
-//    one: it evaluates the three entries of J^T W J it needs directly from the current W.
-//  * Rotation angle: t from an FP32 evaluation of theta on the matrix scaled by its largest
-//    diagonal entry, then c = 1/sqrt(1 + t^2), s = t c in FP64, so every applied J is
-//    orthogonal to FP64 precision (an inexact t only leaves a tiny a_pq for a later sweep).
-//  * Rotations are skipped when a_pq^2 <= 1e-28 |a_pp a_qq| (relative accuracy) or
-//    |a_pq| <= 1e-15 max|diag| (FP64 rounding floor); the solve ends after Np-1 consecutive
-//    rounds without a rotation.  Eigenvalues are ordered by a parallel rank count.
-__device__ __forceinline__ int rr_slot_index(int x, int r, int NR) {
-  if (x == 0) return 0;
-  int v = x - 1 + r;
-  if (v >= NR) v -= NR;
-  return 1 + v;
+// Small-N variant (N <= 64): parallel cyclic Jacobi in the Brent-Luk layout.
+// W and V are stored by physical position: the two indices of rotation pair k always sit at
+// positions 2k and 2k+1, so a round is a block-local update W' = J^T W J (each 2 x 2 block of
+// W from itself and the two rotations of its row and column pairs) and V' = V J (each row's
+// 1 x 2 blocks), written straight to the positions the indices take next round (a fixed map
+// `mv`: the round-robin tournament shifts every index but index 0 by one slot per round).
+// The last warp computes the next round's rotations meanwhile, from the current blocks and
+// rotations, so a round needs one barrier.  W is symmetrised on input ((W + W^T) / 2), and
+// only the upper blocks are computed (mirrored on store).
+// Rotation angle: t from an FP32 evaluation of theta on the matrix scaled by its largest
+// diagonal entry, then c = 1/sqrt(1 + t^2), s = t c in FP64, so every applied rotation is
+// orthogonal to FP64 precision (an inexact t leaves a tiny a_pq for a later sweep).  Pairs
+// with a_pq^2 <= 1e-28 |a_pp a_qq| (relative accuracy) or |a_pq| <= 1e-15 max|diag| (FP64
+// rounding floor) are not rotated; the solve ends after Np - 1 consecutive rounds without a
+// rotation.  Eigenvalues are ordered by a parallel rank count.
+__device__ __forceinline__ bool jacobi_rotation(double app, double aqq, double apq, double inv_s, double& c,
+                                                double& s) {
+  const double ps = app * inv_s, qs = aqq * inv_s, as = apq * inv_s;
+  c = 1.0;
+  s = 0.0;
+  if (!(fabs(as) > 1e-15 && as * as > 1e-28 * fabs(ps * qs))) return false;
+  // t = sign(d) e / (|d| + sqrt(d^2 + e^2)) with d = a_qq - a_pp, e = 2 a_pq: the smaller root
+  // of t^2 + 2 (d / e) t - 1 = 0, without the quotient d / e.  FP32 suffices for t.
+  const float d = (float)(qs - ps), e = 2.0f * (float)as;
+  const float h = sqrtf(fmaf(d, d, e * e));
+  const float tf = (d >= 0.0f ? e : -e) * __frcp_rn(fabsf(d) + h);
+  const double t = (double)tf;
+  // c = 1 / sqrt(1 + t^2) to FP64 precision: FP32 estimate, then two Newton steps
+  // y <- y (3 - x y^2) / 2, each squaring the relative error.
+  const double x = fma(t, t, 1.0);
+  double y = (double)rsqrtf((float)x);
+  y = y * fma(-0.5 * x, y * y, 1.5);
+  y = y * fma(-0.5 * x, y * y, 1.5);
+  c = y;
+  s = t * y;
+  return true;
 }
 
-__global__ void __launch_bounds__(1024) k_syev_fast(const double* __restrict__ w_in, int N,
-                                                     double* __restrict__ evals,
-                                                     double* __restrict__ evecs, int max_sweeps,
-                                                     DevStatus* st) {
-  constexpr int PW = 31;            // warp that computes the next round's rotations
-  constexpr int NE = PW * 32;       // threads applying rotations
-  constexpr int MAXE = (64 * 64 + NE - 1) / NE;
-  extern __shared__ __align__(16) double sm_fast[];
+// Slot of index i in round-robin round r (slot 0 fixed, slots 1..NR cycle), and its position.
+__device__ __forceinline__ int bl_slot(int i, int r, int NR) {
+  if (i == 0) return 0;
+  int v = i - 1 - r % NR;
+  if (v < 0) v += NR;
+  return 1 + v;
+}
+__device__ __forceinline__ int bl_pos(int x, int Np) { return x < Np / 2 ? 2 * x : 2 * (Np - 1 - x) + 1; }
+
+__global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_in, int N,
+                                                   double* __restrict__ evals,
+                                                   double* __restrict__ evecs, int max_sweeps,
+                                                   DevStatus* st) {
+  constexpr int PW = 31;   // warp computing the next round's rotations
+  constexpr int NE = PW * 32;
+  extern __shared__ __align__(16) double sm_bl[];
   const int Np = N + (N & 1);
   const int NR = Np - 1;
+  const int H = Np / 2;
   const int NN = Np * Np;
-  double* W0 = sm_fast;
-  double* W1 = W0 + NN;
-  double* V0 = W1 + NN;
-  double* V1 = V0 + NN;
-  int* tab = reinterpret_cast<int*>(V1 + NN);  // NR x Np: partner | pair << 8 | (index < partner) << 16
-  __shared__ double csb[2][32], snb[2][32];
-  __shared__ int order[64];
+  double* Wb0 = sm_bl;
+  double* Wb1 = Wb0 + NN;
+  double* Vb0 = Wb1 + NN;
+  double* Vb1 = Vb0 + NN;
+  __shared__ double pc[2][32], ps[2][32];
+  __shared__ int mv[64], imv[64];
+  __shared__ double dg[64];
+  __shared__ int rk[64];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  // position map: slot x -> x - 1 (x >= 2), 1 -> NR, 0 -> 0
+  for (int P = tid; P < Np; P += blockDim.x) {
+    const int x = P % 2 == 0 ? P / 2 : Np - 1 - P / 2;
+    const int xn = x == 0 ? 0 : (x == 1 ? NR : x - 1);
+    const int Pn = bl_pos(xn, Np);
+    mv[P] = Pn;
+    imv[Pn] = P;
+  }
   for (int idx = tid; idx < NN; idx += blockDim.x) {
     const int i = idx / Np, j = idx - (idx / Np) * Np;
-    W0[idx] = (i < N && j < N) ? w_in[i + (long long)N * j] : 0.0;
-    V0[idx] = (i == j) ? 1.0 : 0.0;
+    const int Pi = bl_pos(i, Np), Pj = bl_pos(j, Np);  // round 0: index i sits in slot i
+    double v = 0.0;
+    if (i < N && j < N) v = 0.5 * (w_in[i + (long long)N * j] + w_in[j + (long long)N * i]);
+    Wb0[Pi * Np + Pj] = v;
+    Vb0[i * Np + Pj] = (i == j) ? 1.0 : 0.0;  // V rows: original index; columns: position
   }
-  for (int idx = tid; idx < NR * Np; idx += blockDim.x) {
-    const int r = idx / Np, x = idx - (idx / Np) * Np;
-    const int i = rr_slot_index(x, r, NR);
-    const int y = Np - 1 - x;
-    const int pi = rr_slot_index(y, r, NR);
-    const int k = x < y ? x : y;
-    tab[r * Np + i] = pi | (k << 8) | ((i < pi ? 1 : 0) << 16);
-  }
-  __syncthreads();
   double dm = 0.0;
-  for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(W0[i * Np + i]));
+  for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(w_in[i + (long long)N * i]));
   const double inv_s = dm > 0.0 ? 1.0 / dm : 1.0;
-
-  // Rotation (c, s) annihilating a_pq; false when the pair is already below the thresholds.
-  auto rotation = [&](double app, double aqq, double apq, double& c, double& s) -> bool {
-    const double ps = app * inv_s, qs = aqq * inv_s, as = apq * inv_s;
-    c = 1.0;
-    s = 0.0;
-    if (!(fabs(as) > 1e-15 && as * as > 1e-28 * fabs(ps * qs))) return false;
-    const float th = (float)(qs - ps) / (2.0f * (float)as);
-    const float tf = copysignf(1.0f, th) / (fabsf(th) + sqrtf(fmaf(th, th, 1.0f)));
-    const double t = (double)tf;
-    c = rsqrt(fma(t, t, 1.0));
-    s = t * c;
-    return true;
-  };
-  // Entry (a, b) of J^T W J for the round whose pairing row is `tb` and rotations (cs, sn).
-  auto rotated_entry = [&](const double* W, const int* tb, const double* cs, const double* sn, int a,
-                           int b) -> double {
-    const int ta = tb[a], tbb = tb[b];
-    const int pa = ta & 255, ka = (ta >> 8) & 255, pb = tbb & 255, kb = (tbb >> 8) & 255;
-    const double jaa = cs[ka], jpa = (ta >> 16) ? -sn[ka] : sn[ka];
-    const double jbb = cs[kb], jpb = (tbb >> 16) ? -sn[kb] : sn[kb];
-    return jaa * (W[a * Np + b] * jbb + W[a * Np + pb] * jpb) +
-           jpa * (W[pa * Np + b] * jbb + W[pa * Np + pb] * jpb);
-  };
-
+  __syncthreads();
+  // Positions holding real indices in round 0 (the pad index, when N is odd, is N = Np - 1).
   // Rotations of round 0.
   if (warp == PW) {
-    for (int k = lane; k < Np / 2; k += 32) {
-      int p = rr_slot_index(k, 0, NR), q = rr_slot_index(Np - 1 - k, 0, NR);
-      if (p > q) {
-        const int t = p;
-        p = q;
-        q = t;
-      }
-      double c = 1.0, s = 0.0;
-      if (q < N) rotation(W0[p * Np + p], W0[q * Np + q], W0[p * Np + q], c, s);
-      csb[0][k] = c;
-      snb[0][k] = s;
+    for (int k = lane; k < H; k += 32) {
+      double c = 1.0, sn = 0.0;
+      const int i0 = k, i1 = Np - 1 - k;  // indices in slots k and Np-1-k at round 0
+      if (i0 < N && i1 < N) jacobi_rotation(Wb0[(2 * k) * Np + 2 * k], Wb0[(2 * k + 1) * Np + 2 * k + 1],
+                                            Wb0[(2 * k) * Np + 2 * k + 1], inv_s, c, sn);
+      pc[0][k] = c;
+      ps[0][k] = sn;
     }
-  }
-  int eij[MAXE];  // row | column << 8 of this thread's entries
-#pragma unroll
-  for (int u = 0; u < MAXE; ++u) {
-    const int e = tid + u * NE;
-    eij[u] = (e / Np) | ((e - (e / Np) * Np) << 8);
   }
   __syncthreads();
 
-  int cur = 0;
-  int R = 0;  // global round counter (parity selects the rotation buffer)
+  const int NWB = H * (H + 1) / 2;  // upper blocks (a <= b)
+  const int NITEMS = NWB + N * H;   // + V half-rows (rows < N)
+  // This thread's work items, fixed for the whole solve: a | b << 8 (W block) or
+  // i | b << 8 | 1 << 16 (V row i, column pair b); -1 for none.
+  constexpr int MAXIT = (32 * 33 / 2 + 64 * 32 + NE - 1) / NE;
+  int dsc[MAXIT];
+#pragma unroll
+  for (int u = 0; u < MAXIT; ++u) {
+    const int it = tid + u * NE;
+    if (warp == PW || it >= NITEMS) {
+      dsc[u] = -1;
+    } else if (it < NWB) {
+      int a = 0, rem = it;
+      while (rem >= H - a) {
+        rem -= H - a;
+        ++a;
+      }
+      dsc[u] = a | ((a + rem) << 8);
+    } else {
+      const int e = it - NWB;
+      dsc[u] = (e / H) | ((e % H) << 8) | (1 << 16);
+    }
+  }
+  // Param-warp constants: positions (this round) of the indices that form pair `lane` next
+  // round, as (pair, side).
+  int aP = 0, xP = 0, aQ = 0, xQ = 0;
+  if (warp == PW && lane < H) {
+    const int P = imv[2 * lane], Q = imv[2 * lane + 1];
+    aP = P >> 1;
+    xP = P & 1;
+    aQ = Q >> 1;
+    xQ = Q & 1;
+  }
+  int R = 0;
   int sweep = 0;
   bool converged = false;
   for (; sweep < max_sweeps; ++sweep) {
     int rotated = 0;
+    bool stop = false;
     for (int rnd = 0; rnd < NR; ++rnd, ++R) {
-      const double* W = cur ? W1 : W0;
-      const double* V = cur ? V1 : V0;
-      double* Wn = cur ? W0 : W1;
-      double* Vn = cur ? V0 : V1;
-      const int pb = R & 1;
-      const double* cs = csb[pb];
-      const double* sn = snb[pb];
-      const int* tb = tab + rnd * Np;
+      const int cb = R & 1;
+      const double* W = cb ? Wb1 : Wb0;
+      double* Wn = cb ? Wb0 : Wb1;
+      const double* V = cb ? Vb1 : Vb0;
+      double* Vn = cb ? Vb0 : Vb1;
+      const double* c_ = pc[cb];
+      const double* s_ = ps[cb];
       if (warp != PW) {
 #pragma unroll
-        for (int u = 0; u < MAXE; ++u) {
-          const int e = tid + u * NE;
-          if (e < NN) {
-            const int i = eij[u] & 255, j = eij[u] >> 8;
-            Wn[e] = rotated_entry(W, tb, cs, sn, i, j);
-            const int tj = tb[j];
-            const int pj = tj & 255, kj = (tj >> 8) & 255;
-            const double jjj = cs[kj], jpj = (tj >> 16) ? -sn[kj] : sn[kj];
-            Vn[e] = V[i * Np + j] * jjj + V[i * Np + pj] * jpj;
+        for (int u = 0; u < MAXIT; ++u) {
+          const int dd = dsc[u];
+          if (dd < 0) continue;
+          if (!(dd >> 16)) {
+            const int a = dd & 255, b = (dd >> 8) & 255;
+            const double ca = c_[a], sa = s_[a], cbv = c_[b], sb = s_[b];
+            const double w00 = W[(2 * a) * Np + 2 * b], w01 = W[(2 * a) * Np + 2 * b + 1];
+            const double w10 = W[(2 * a + 1) * Np + 2 * b], w11 = W[(2 * a + 1) * Np + 2 * b + 1];
+            // X = J_a^T B: rows (c, -s), (s, c)
+            const double x00 = ca * w00 - sa * w10, x01 = ca * w01 - sa * w11;
+            const double x10 = sa * w00 + ca * w10, x11 = sa * w01 + ca * w11;
+            // X J_b: columns (c, -s)^T, (s, c)^T
+            const double y00 = x00 * cbv - x01 * sb, y01 = x00 * sb + x01 * cbv;
+            const double y10 = x10 * cbv - x11 * sb, y11 = x10 * sb + x11 * cbv;
+            const int r0 = mv[2 * a], r1 = mv[2 * a + 1], q0 = mv[2 * b], q1 = mv[2 * b + 1];
+            Wn[r0 * Np + q0] = y00;
+            Wn[r0 * Np + q1] = y01;
+            Wn[r1 * Np + q0] = y10;
+            Wn[r1 * Np + q1] = y11;
+            if (a != b) {
+              Wn[q0 * Np + r0] = y00;
+              Wn[q1 * Np + r0] = y01;
+              Wn[q0 * Np + r1] = y10;
+              Wn[q1 * Np + r1] = y11;
+            }
+          } else {
+            const int i = dd & 255, b = (dd >> 8) & 255;
+            const double cbv = c_[b], sb = s_[b];
+            const double v0 = V[i * Np + 2 * b], v1 = V[i * Np + 2 * b + 1];
+            Vn[i * Np + mv[2 * b]] = v0 * cbv - v1 * sb;
+            Vn[i * Np + mv[2 * b + 1]] = v0 * sb + v1 * cbv;
           }
         }
-      } else {
+      } else if (lane < H) {
+        // Rotation of pair `lane` in the next round.  Its two indices sit at the current
+        // positions P = imv[2 lane], Q = imv[2 lane + 1]; the three entries of J^T W J it needs
+        // come from the 2 x 2 blocks (P/2, P/2), (Q/2, Q/2), (P/2, Q/2) and the rotations of
+        // pairs P/2 and Q/2 (row x of J_a^T equals column x of J_a: (c, -s) or (s, c)).
         const int rn = (rnd + 1 == NR) ? 0 : rnd + 1;
-        for (int k = lane; k < Np / 2; k += 32) {
-          int p = rr_slot_index(k, rn, NR), q = rr_slot_index(Np - 1 - k, rn, NR);
-          if (p > q) {
-            const int t = p;
-            p = q;
-            q = t;
-          }
-          double c = 1.0, s = 0.0;
-          if (q < N) {
-            const double app = rotated_entry(W, tb, cs, sn, p, p);
-            const double aqq = rotated_entry(W, tb, cs, sn, q, q);
-            const double apq = rotated_entry(W, tb, cs, sn, p, q);
-            if (rotation(app, aqq, apq, c, s)) rotated = 1;
-          }
-          csb[pb ^ 1][k] = c;
-          snb[pb ^ 1][k] = s;
+        bool live = true;
+        if (Np != N) {  // the padding index N = Np - 1 never rotates
+          const int xs = bl_slot(Np - 1, rn, NR);
+          live = (xs != lane) && (xs != Np - 1 - lane);
         }
+        double c = 1.0, sn = 0.0;
+        if (live) {
+          const double cP = c_[aP], sP = s_[aP], cQ = c_[aQ], sQ = s_[aQ];
+          const double tP0 = xP ? sP : cP, tP1 = xP ? cP : -sP;
+          const double tQ0 = xQ ? sQ : cQ, tQ1 = xQ ? cQ : -sQ;
+          const double* Bpp = W + (2 * aP) * Np + 2 * aP;
+          const double* Bqq = W + (2 * aQ) * Np + 2 * aQ;
+          const double* Bpq = W + (2 * aP) * Np + 2 * aQ;
+          const double p0 = tP0 * Bpp[0] + tP1 * Bpp[Np], p1 = tP0 * Bpp[1] + tP1 * Bpp[Np + 1];
+          const double q0 = tQ0 * Bqq[0] + tQ1 * Bqq[Np], q1 = tQ0 * Bqq[1] + tQ1 * Bqq[Np + 1];
+          const double m0 = tP0 * Bpq[0] + tP1 * Bpq[Np], m1 = tP0 * Bpq[1] + tP1 * Bpq[Np + 1];
+          const double app = p0 * tP0 + p1 * tP1;
+          const double aqq = q0 * tQ0 + q1 * tQ1;
+          const double apq = m0 * tQ0 + m1 * tQ1;
+          if (jacobi_rotation(app, aqq, apq, inv_s, c, sn)) rotated = 1;
+        }
+        pc[cb ^ 1][lane] = c;
+        ps[cb ^ 1][lane] = sn;
       }
-      cur ^= 1;
-      if (rnd + 1 < NR) __syncthreads();
+      if (rnd + 1 < NR) {
+        __syncthreads();
+      } else if (!__syncthreads_or(rotated)) {
+        stop = true;
+      }
     }
-    if (!__syncthreads_or(rotated)) {
+    if (stop) {
       converged = true;
+      ++sweep;
       break;
     }
   }
-  const double* Wf = cur ? W1 : W0;
-  const double* Vf = cur ? V1 : V0;
+  // After R rounds the current buffers are (R & 1); index i sits in slot bl_slot(i, R, NR).
+  const double* Wf = (R & 1) ? Wb1 : Wb0;
+  const double* Vf = (R & 1) ? Vb1 : Vb0;
   if (tid < N) {
-    double la = Wf[tid * Np + tid];
+    const int P = bl_pos(bl_slot(tid, R, NR), Np);
+    dg[tid] = Wf[P * Np + P];
+  }
+  __syncthreads();
+  if (tid < N) {
+    const int a = tid;
+    double la = dg[a];
     if (la != la) la = -INFINITY;
     int rank = 0;
     for (int b = 0; b < N; ++b) {
-      double lb = Wf[b * Np + b];
+      double lb = dg[b];
       if (lb != lb) lb = -INFINITY;
-      rank += (lb > la || (lb == la && b < tid)) ? 1 : 0;
+      rank += (lb > la || (lb == la && b < a)) ? 1 : 0;
     }
-    order[rank] = tid;
+    rk[a] = rank;
+    evals[rank] = dg[a];
   }
   if (tid == 0 && st) {
-    atomicMax(&st->sweeps, sweep + 1);
+    atomicMax(&st->sweeps, sweep);
     if (!converged) dev_fail(st, TT_ERR_NOCONV, sweep);
   }
   __syncthreads();
   for (int idx = tid; idx < N * N; idx += blockDim.x) {
-    const int i = idx % N, a = idx / N;
-    evecs[i + (long long)N * a] = Vf[i * Np + order[a]];
+    const int i = idx % N, a = idx / N;  // eigenvector of index a, component i
+    const int P = bl_pos(bl_slot(a, R, NR), Np);
+    evecs[i + (long long)N * rk[a]] = Vf[i * Np + P];
   }
-  for (int a = tid; a < N; a += blockDim.x) evals[a] = Wf[order[a] * Np + order[a]];
 }
 
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps, Arena& ws,
@@ -1550,13 +1636,13 @@ int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sw
   }
   if (N <= 64) {
     const int Nps = N + (N & 1);
-    const size_t shm_fast = 4 * (size_t)Nps * Nps * sizeof(double) + (size_t)(Nps - 1) * Nps * sizeof(int);
-    static bool attr_fast = false;
-    if (!attr_fast) {
-      cudaFuncSetAttribute(k_syev_fast, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-      attr_fast = true;
+    const size_t shm_bl = 4 * (size_t)Nps * Nps * sizeof(double);
+    static bool attr_bl = false;
+    if (!attr_bl) {
+      cudaFuncSetAttribute(k_syev_bl, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+      attr_bl = true;
     }
-    k_syev_fast<<<1, 1024, shm_fast, s>>>(w, N, evals, evecs, max_sweeps, st);
+    k_syev_bl<<<1, 1024, shm_bl, s>>>(w, N, evals, evecs, max_sweeps, st);
     count_launch();
     TT_LAUNCH_CHECK();
     return TT_OK;
@@ -1681,6 +1767,28 @@ int launch_fold_rows(const float* in, float* out, const double* p, int R, long l
   if (total <= 0) return TT_OK;
   k_fold_rows<<<(int)std::min<long long>(ceil_div_ll(total, 256), 8LL * num_sms()), 256, 0, s>>>(
       in, out, p, R, ni, ncols);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  return TT_OK;
+}
+
+// out (Rout, cols) <- in (Rin, cols), rows Rin..Rout-1 zero (Rin <= Rout), column-major.
+__global__ void k_expand_rows(const float* __restrict__ in, int Rin, float* __restrict__ out, int Rout,
+                              long long cols) {
+  const long long total = (long long)Rout * cols;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long c = idx / Rout;
+    const int a = (int)(idx - c * Rout);
+    out[idx] = (a < Rin) ? in[a + (long long)Rin * c] : 0.f;
+  }
+}
+
+int launch_expand_rows(const float* in, int Rin, float* out, int Rout, long long cols, cudaStream_t s) {
+  const long long total = (long long)Rout * cols;
+  if (total <= 0) return TT_OK;
+  k_expand_rows<<<(int)std::min<long long>(ceil_div_ll(total, 256), 8LL * num_sms()), 256, 0, s>>>(
+      in, Rin, out, Rout, cols);
   count_launch();
   TT_LAUNCH_CHECK();
   return TT_OK;

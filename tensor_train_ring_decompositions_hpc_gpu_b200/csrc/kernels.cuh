@@ -109,6 +109,9 @@ int launch_gemm_nn(const float* a, long long M, int K, const float* b, long long
 int launch_recon_err(const float* x, int n1, long long N, const float* g1, int r0, int r1,
                      const float* mrg, double* acc, cudaStream_t s);
 
+// out (Rout x cols) from in (Rin x cols), rows Rin..Rout-1 zero; column-major.
+int launch_expand_rows(const float* in, int Rin, float* out, int Rout, long long cols, cudaStream_t s);
+
 // Sketch variants that take their split-K scratch from the caller (no allocation).
 int launch_sketch_tc_static(const float* a, long long m, long long n, const float* w, int N,
                             long long wj, long long wc, double* y, double* part, size_t part_cap,

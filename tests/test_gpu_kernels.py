@@ -164,6 +164,26 @@ def test_syev_rank_deficient_terminates(gpu, N, rank):
     assert 1 <= sweeps < 40
 
 
+@pytest.mark.parametrize("N", [16, 40, 96])
+def test_syev_asymmetric_rounding_converges(gpu, N):
+    """Tensor-core Grams are symmetric only to FP32 rounding; the solver symmetrises its input
+    and must converge to the eigen-decomposition of (W + W^T) / 2."""
+    import torch
+    ttr = _ttr()
+    rng = np.random.default_rng(N)
+    b = rng.standard_normal((N, 3 * N))
+    w = b @ b.T
+    w_in = w + 1e-7 * np.abs(w).max() * np.triu(rng.standard_normal((N, N)), 1)
+    ev, vec, sweeps = ttr.syev(torch.from_numpy(w_in).to(gpu))
+    ev = ev.cpu().numpy()
+    vec = vec.cpu().numpy()
+    ws = 0.5 * (w_in + w_in.T)
+    ref = np.sort(np.linalg.eigvalsh(ws))[::-1]
+    np.testing.assert_allclose(ev, ref, rtol=1e-11, atol=1e-11 * ref[0])
+    assert np.linalg.norm(ws @ vec - vec * ev) < 1e-10 * ref[0] * N
+    assert sweeps < 20
+
+
 def test_syev_graded_spectrum_relative_accuracy(gpu):
     import torch
     ttr = _ttr()
