@@ -145,6 +145,12 @@ int tt_rel_error(tt_ctx* ctx, const float* x, int d, const int* n, const int* r,
 int tt_k_gaussian(tt_ctx* ctx, float* out, long long rows, int cols, long long ld,
                   unsigned long long seed, unsigned stream_id);
 
+/* Rows [row0, row0 + nrows) of the Gaussian matrix tt_k_gaussian makes with total_rows rows
+ * (same seed / stream): the Omega block of one rank's columns in a column-sharded EDrSVD.
+ * No counterpart in the reference (single GPU per unfolding). */
+int tt_k_gaussian_rows(tt_ctx* ctx, float* out, long long row0, long long nrows, long long total_rows, int cols,
+                       long long ld, unsigned long long seed, unsigned stream_id);
+
 /* Sketch Y = A * W: A (m x n, lda = m), W (n x N, ldw), Y (m x N, FP64, ldy = m).
  * Replaces GemmEx Y = A*Omega / Y = A*Q (ttdec_gpu_float_rsvd_lu_half.cu:601-619,657-675). */
 int tt_k_sketch(tt_ctx* ctx, const float* a, long long m, long long n, const float* w, int N,
@@ -189,6 +195,21 @@ int tt_k_syev(tt_ctx* ctx, const double* w, int N, double* evals, double* evecs,
  * after the result is complete.  This entry point has no counterpart in the reference. */
 int tt_k_sketch_noalloc(const float* a, long long m, long long n, const float* w, int N,
                         long long ldw, double* y, int gemm, void* stream);
+
+/* Batched TT-SVD of many small tensors in one persistent launch (one CTA per tensor at a
+ * time, a work counter spreads the tensors over the SMs).  `n` holds count x d mode sizes,
+ * `x` the packed column-major tensors at element offsets `x_off`; all host arrays except x and
+ * cores (device).  eps > 0: delta-truncation per tensor as in tt_svd (ranks capped by rmax);
+ * eps = 0: ranks min(rmax, unfolding size).  rmax <= 32; unfoldings whose small side exceeds
+ * 32 are sketched (EDrSVD with `oversample`, Philox `seed`) and may have at most 512 rows.
+ * Cores of tensor t are written compactly from element core_off[t] (core k after core k-1,
+ * each column-major (r_k, n_k, r_{k+1})); tt_batch_core_capacity gives the room one tensor
+ * needs.  ranks receives count x (d + 1) ranks, err_est (optional) the per-tensor error bound
+ * sqrt(discarded energy / ||X||^2).  No counterpart in the reference (one tensor per call). */
+int tt_svd_batched(tt_ctx* ctx, int count, int d, const int* n, const float* x, const long long* x_off,
+                   double eps, int rmax, int oversample, unsigned long long seed, float* cores,
+                   const long long* core_off, int* ranks, double* err_est);
+long long tt_batch_core_capacity(int d, const int* n, int rmax);
 
 /* Core files.  The reference frees its cores before returning (ttdec6_singleGPU.cu:947-952)
  * and has no file format; this one stores a decomposition for later use.  Layout

@@ -30,7 +30,7 @@ __all__ = [
     "rel_error", "tt_random_cores", "tr_random_cores", "add_noise", "make_tt_tensor",
     "make_tr_tensor", "edrsvd_plain", "edrsvd_gram", "gram_eig_step", "ttdec6_gram",
     "trdec6_gram", "philox4x32_10", "gaussian_from_philox", "ref_uniform_tt_tensor",
-    "tt_flops_model",
+    "tt_flops_model", "tt_svd_eps",
 ]
 
 
@@ -205,6 +205,36 @@ def _merge_right(cores, order: str):
 def tt_full(cores, convention: str = "gpu") -> np.ndarray:
     """Reconstruct X from TT cores (restates ``calMSE``'s right-to-left contraction ``TT6:134-182``)."""
     return tr_full(cores, convention)
+
+
+def tt_svd_eps(x: np.ndarray, eps: float, max_ranks=None, dtype=np.float64):
+    """TT-SVD with delta-truncation (Oseledets, TT-SVD algorithm): every unfolding keeps the
+    smallest rank r whose discarded squared singular values sum to at most
+    eps^2 ||X||_F^2 / (d - 1), capped by ``max_ranks``; then ||X - X^|| <= eps ||X||.
+    Column-major chain with canonical signs (the GPU convention).  Returns (cores, ranks)."""
+    n = list(x.shape)
+    d = len(n)
+    flat = np.asarray(x, dtype=dtype).ravel(order="F")
+    delta2 = eps * eps * float(np.sum(flat * flat)) / (d - 1)
+    cores, ranks = [], [1]
+    r_prev = 1
+    for k in range(d - 1):
+        m = r_prev * n[k]
+        a = flat.reshape(m, flat.size // m, order="F")
+        u, s, vt = np.linalg.svd(a, full_matrices=False)
+        cap = s.size if max_ranks is None else min(s.size, max_ranks[k + 1])
+        tail = np.concatenate([np.cumsum((s ** 2)[::-1])[::-1], [0.0]])  # tail[r] = sum_{i>=r} s_i^2
+        r = 1
+        while r < cap and tail[r] > delta2:
+            r += 1
+        u, svt = canon_signs(u[:, :r].copy(), (s[:r, None] * vt[:r]).copy(), r)
+        cores.append(u.reshape(r_prev, n[k], r, order="F"))
+        flat = svt.ravel(order="F")
+        r_prev = r
+        ranks.append(r)
+    cores.append(flat.reshape(r_prev, n[-1], 1, order="F"))
+    ranks.append(1)
+    return cores, ranks
 
 
 def tr_full(cores, convention: str = "gpu") -> np.ndarray:

@@ -102,6 +102,7 @@ class Result:
     ranks: list = field(default_factory=list)
     kernels: int = 0
     jacobi_sweeps: int = 0
+    est_rel_err: float = 0.0
 
 
 def _opts(gemm, method, oversample, power_iters, seed, flags, max_sweeps):
@@ -118,7 +119,7 @@ def _opts(gemm, method, oversample, power_iters, seed, flags, max_sweeps):
 
 
 def _run(ring: bool, x, ranks, gemm="auto", method="edrsvd", oversample=8, power_iters=0,
-         seed=1234, flags=0, max_sweeps=40, shape=None):
+         seed=1234, flags=0, max_sweeps=40, shape=None, eps=0.0):
     ranks = [int(r) for r in ranks]
     host = isinstance(x, np.ndarray)
     if host:
@@ -129,6 +130,7 @@ def _run(ring: bool, x, ranks, gemm="auto", method="edrsvd", oversample=8, power
                     for k in range(d)]
         ptrs = (C.c_void_p * d)(*[c.ctypes.data for c in cores_np])
         o = _opts(gemm, method, oversample, power_iters, seed, flags | TT_FLAG_HOST_IO, max_sweeps)
+        o.eps = float(eps)
         torch = _torch()
         ctx = _ctx_for()
         st = _lib.TTStats()
@@ -136,6 +138,10 @@ def _run(ring: bool, x, ranks, gemm="auto", method="edrsvd", oversample=8, power
         check(fn(ctx, C.c_void_p(xa.ctypes.data), d, _lib.int_array(shape), _lib.int_array(ranks),
                  C.byref(o), ptrs, C.byref(st)))
         cores = cores_np
+        if eps > 0:  # adaptive ranks: core k occupies the first r_k n_k r_{k+1} values of its buffer
+            rr = list(st.ranks[: d + 1])
+            cores = [np.asfortranarray(cores_np[k].reshape(-1, order="F")[: rr[k] * shape[k] * rr[k + 1]]
+                                       .reshape(rr[k], shape[k], rr[k + 1], order="F")) for k in range(d)]
     else:
         torch = _torch()
         if shape is None:
@@ -148,21 +154,27 @@ def _run(ring: bool, x, ranks, gemm="auto", method="edrsvd", oversample=8, power
                 for k in range(d)]
         ptrs = (C.c_void_p * d)(*[t.data_ptr() for t in flat])
         o = _opts(gemm, method, oversample, power_iters, seed, flags, max_sweeps)
+        o.eps = float(eps)
         ctx = _ctx_for(buf.device.index)
         st = _lib.TTStats()
         fn = lib().tr_svd if ring else lib().tt_svd
         check(fn(ctx, _ptr(buf), d, _lib.int_array(shape), _lib.int_array(ranks), C.byref(o), ptrs,
                  C.byref(st)))
-        cores = [_core_view(flat[k], ranks[k], shape[k], ranks[k + 1]) for k in range(d)]
+        rr = list(st.ranks[: d + 1]) if eps > 0 else ranks
+        cores = [_core_view(flat[k][: rr[k] * shape[k] * rr[k + 1]], rr[k], shape[k], rr[k + 1])
+                 for k in range(d)]
     sig = [np.array(st.sigma[k][: st.nsigma[k]], dtype=np.float64) for k in range(st.nsteps)]
     return Result(cores=cores, ms=st.ms, sigmas=sig, ranks=list(st.ranks[: len(ranks)]),
-                  kernels=st.kernels, jacobi_sweeps=st.jacobi_sweeps)
+                  kernels=st.kernels, jacobi_sweeps=st.jacobi_sweeps, est_rel_err=st.est_rel_err)
 
 
 def tt_svd(x, ranks, **kw) -> Result:
     """TT-SVD of ``x`` (torch CUDA tensor or NumPy array, logical shape (n1..nd)) at fixed
     ranks ``[1, r1, ..., r_{d-1}, 1]``.  Keyword options: gemm ('auto' | 'tc' | 'fp32'),
-    method ('edrsvd' | 'exact'), oversample, power_iters, seed, flags, max_sweeps."""
+    method ('edrsvd' | 'exact'), oversample, power_iters, seed, flags, max_sweeps, eps.
+    With eps > 0 the ranks are upper bounds and every unfolding is truncated to the smallest
+    rank whose discarded energy is <= eps^2 ||X||^2 / (d - 1) (TT-SVD delta-truncation);
+    Result.ranks holds the ranks chosen and Result.est_rel_err the implied error bound."""
     return _run(False, x, ranks, **kw)
 
 
@@ -283,6 +295,71 @@ def permute231(x, r0: int, r1: int, n: int):
     out = torch.empty_like(x)
     check(lib().tt_k_permute231(_ctx_for(x.device.index), _ptr(x), _ptr(out), r0, r1, n))
     return out
+
+
+# ---- batched small tensors ----
+class Batch:
+    """A packed batch of small tensors for ``tt_svd_batched``: the column-major tensors in one
+    device buffer, their offsets, and the room for their cores."""
+
+    def __init__(self, tensors, rmax=16, device=None):
+        torch = _torch()
+        self.device = device or torch.device("cuda")
+        self.shapes = [list(t.shape) for t in tensors]
+        self.d = len(self.shapes[0])
+        if any(len(sh) != self.d for sh in self.shapes):
+            raise ValueError("all tensors need the same order")
+        self.rmax = int(rmax)
+        sizes = [int(np.prod(sh)) for sh in self.shapes]
+        self.x_off = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+        self.flat = torch.empty(int(sum(sizes)), dtype=torch.float32, device=self.device)
+        for t, off, sz in zip(tensors, self.x_off, sizes):
+            if isinstance(t, np.ndarray):
+                src = torch.from_numpy(np.ascontiguousarray(np.asarray(t, dtype=np.float32).ravel(order="F")))
+            else:
+                src = t.permute(*reversed(range(t.dim()))).reshape(-1).float()
+            self.flat[int(off):int(off) + sz] = src.to(self.device)
+        caps = [int(lib().tt_batch_core_capacity(self.d, _lib.int_array(sh), self.rmax)) for sh in self.shapes]
+        self.core_off = np.concatenate([[0], np.cumsum(caps)[:-1]]).astype(np.int64)
+        self.cores = torch.zeros(int(sum(caps)), dtype=torch.float32, device=self.device)
+        self.count = len(tensors)
+        self.n_arr = (C.c_int * (self.count * self.d))(*[int(v) for sh in self.shapes for v in sh])
+        self.ranks = (C.c_int * (self.count * (self.d + 1)))()
+        self.err = (C.c_double * self.count)()
+
+    def run(self, eps=1e-2, oversample=8, seed=20261203):
+        """One batched launch over the packed tensors (results stay in the Batch)."""
+        ctx = _ctx_for(self.device.index)
+        check(lib().tt_svd_batched(ctx, self.count, self.d, self.n_arr, C.c_void_p(self.flat.data_ptr()),
+                                   self.x_off.ctypes.data_as(C.POINTER(C.c_longlong)), float(eps), self.rmax,
+                                   int(oversample), int(seed), C.c_void_p(self.cores.data_ptr()),
+                                   self.core_off.ctypes.data_as(C.POINTER(C.c_longlong)), self.ranks, self.err))
+
+    def results(self):
+        """Per tensor: (cores as CUDA tensors of logical shape (r_k, n_k, r_{k+1}), ranks, err_est)."""
+        d = self.d
+        out = []
+        for t in range(self.count):
+            rr = [self.ranks[t * (d + 1) + k] for k in range(d + 1)]
+            off = int(self.core_off[t])
+            cs = []
+            for k in range(d):
+                cnt = rr[k] * self.shapes[t][k] * rr[k + 1]
+                cs.append(_core_view(self.cores[off:off + cnt], rr[k], self.shapes[t][k], rr[k + 1]))
+                off += cnt
+            out.append((cs, rr, self.err[t]))
+        return out
+
+
+def tt_svd_batched(tensors, eps=1e-2, rmax=16, oversample=8, seed=20261203, device=None):
+    """TT-SVD of many small tensors in one persistent launch (``tt_svd_batched``).
+
+    ``tensors``: list of NumPy arrays (same order d, any mode sizes) or of CUDA tensors with
+    their logical shapes.  Returns a list of (cores, ranks, err_est) per tensor; cores are CUDA
+    tensors with logical shape (r_k, n_k, r_{k+1})."""
+    b = Batch(tensors, rmax=rmax, device=device)
+    b.run(eps=eps, oversample=oversample, seed=seed)
+    return b.results()
 
 
 # ---- core files ----

@@ -26,9 +26,10 @@ TT_STATS_MAX_SIGMA = 64
 # Every extern "C" symbol declared in include/ttrsvd.h.
 EXPORTED = [
     "tt_ctx_create", "tt_ctx_destroy", "tt_ctx_set_stream", "tt_ctx_reserve", "tt_last_error",
-    "tt_default_opts", "tt_abi_version", "tt_svd", "tr_svd", "tt_rel_error", "tt_k_gaussian",
+    "tt_default_opts", "tt_abi_version", "tt_svd", "tr_svd", "tt_rel_error", "tt_k_gaussian", "tt_k_gaussian_rows",
     "tt_k_sketch", "tt_k_project", "tt_k_gram_rows", "tt_k_gram_tall", "tt_k_cholqr2",
-    "tt_k_syev", "tt_k_sketch_noalloc", "tt_cores_save", "tt_cores_header", "tt_cores_load",
+    "tt_k_syev", "tt_k_sketch_noalloc", "tt_svd_batched", "tt_batch_core_capacity",
+    "tt_cores_save", "tt_cores_header", "tt_cores_load",
     "tt_k_permute231", "tt_ref_ttdec_gpu_float", "tt_ref_trdec_gpu_float",
     "tt_ref_ttdec_half_lu_device_6", "tt_ref_trdec_half_lu_device_6",
 ]
@@ -93,6 +94,9 @@ def load():
         "tt_k_syev": (i, [vp, vp, i, vp, vp, P(i)]),
         "tt_k_permute231": (i, [vp, vp, vp, i, i, ll]),
         "tt_k_sketch_noalloc": (i, [vp, ll, ll, vp, i, ll, vp, i, vp]),
+        "tt_k_gaussian_rows": (i, [vp, vp, ll, ll, ll, i, ll, ull, C.c_uint]),
+        "tt_svd_batched": (i, [vp, i, i, P(i), vp, P(ll), d, i, i, C.c_ulonglong, vp, P(ll), P(i), P(d)]),
+        "tt_batch_core_capacity": (ll, [i, P(i), i]),
         "tt_cores_save": (i, [C.c_char_p, i, P(i), P(i), i, P(vp), i]),
         "tt_cores_header": (i, [C.c_char_p, P(i), P(i), P(i), P(i)]),
         "tt_cores_load": (i, [C.c_char_p, P(vp), i]),

@@ -1,0 +1,674 @@
+// Batched TT-SVD of many small tensors in one persistent launch.
+//
+// One CTA decomposes one tensor at a time and takes the next tensor index from a global work
+// counter, so the SMs stay busy whatever the size mix.  Every step of a tensor runs inside the
+// CTA: the exact Gram-eigen step when the small side of the unfolding is <= 32 (Gram in FP64,
+// Jacobi in shared memory), otherwise EDrSVD (Philox Gaussian sketch generated on the fly, both
+// CholeskyQR passes in shared memory, projection B = Q^T A with the Gram B B^T accumulated
+// alongside, Jacobi).  Ranks follow the delta-truncation rule of tt_svd (eps > 0) or are the
+// largest allowed (eps = 0), capped by rmax.  The unfoldings of the tensor being processed
+// live in a per-CTA scratch (ping-pong), cores are written compactly in the caller's buffer.
+// The reference decomposes one tensor per call (ttdec_gpu_float, ttdec_half_lu_device_6) and
+// has no batched path.
+#include <math.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "kernels.cuh"
+#include "philox.cuh"
+
+namespace ttr {
+namespace {
+
+constexpr int BT = 512;       // threads per CTA
+constexpr int BMAXM = 512;    // largest row count of a randomized unfolding
+constexpr int BSMALL = 32;    // largest exact small side / sketch width
+constexpr int BCH = 32;       // columns per staged chunk
+constexpr int BMAXD = 8;      // largest order
+
+struct BatchShape {
+  int d;
+  int n[BMAXD];
+  long long size;
+  long long x_off;
+  long long core_off;
+};
+
+// Shared-memory layout of the kernel (bytes).
+constexpr size_t SM_CHUNK = (size_t)BMAXM * BCH * sizeof(float);            // A chunk / U
+constexpr size_t SM_YQ = (size_t)BMAXM * (BSMALL + 1) * sizeof(float);        // Y, Q (stride ks|1)
+constexpr size_t SM_W = (size_t)BSMALL * BSMALL * sizeof(double);             // Gram
+constexpr size_t SM_JAC = 4 * (size_t)BSMALL * BSMALL * sizeof(double);       // Jacobi buffers
+constexpr size_t SM_OM = (size_t)BCH * BSMALL * sizeof(float);                // Omega chunk
+constexpr size_t SM_RED = (size_t)BT * 2 * sizeof(double);                    // reductions
+constexpr size_t SM_TOTAL = SM_CHUNK + SM_YQ + SM_W + SM_JAC + SM_OM + SM_RED + 1024;
+
+struct Smem {
+  float* chunk;   // BMAXM x BCH
+  float* yq;      // BMAXM x (BSMALL+1)
+  double* w;      // BSMALL x BSMALL (row-major, stride Np)
+  double* jac;    // 4 x BSMALL^2
+  float* om;      // BCH x BSMALL
+  double* red;    // 2 * BT
+};
+
+__device__ double cta_sum(double v, double* red) {
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  __syncthreads();
+  if ((tid & 31) == 0) red[tid >> 5] = v;
+  __syncthreads();
+  double t = 0.0;
+  for (int w = 0; w < BT / 32; ++w) t += red[w];
+  __syncthreads();
+  return t;
+}
+
+// W (N x N, row-major, stride N) = sum over `nvec` vectors of v v^T, where component p of
+// vector j is at base[p * ps + j * vs] (N <= BSMALL).  4 x 4 register tiles of the upper
+// triangle, vectors split into groups of threads, groups added in order through W.
+__device__ void cta_gram(const float* __restrict__ base, long long ps, long long vs, int N, long long nvec,
+                         double* W) {
+  const int tid = threadIdx.x;
+  const int TT = (N + 3) / 4;
+  const int nt = TT * (TT + 1) / 2;
+  const int groups = min(32, max(1, BT / nt));
+  const int t = tid % nt, g = tid / nt;
+  const bool act = g < groups;
+  int ta = 0, rem = act ? t : 0;
+  while (rem >= TT - ta) {
+    rem -= TT - ta;
+    ++ta;
+  }
+  const int tb = ta + rem;
+  double acc[16];
+#pragma unroll
+  for (int e = 0; e < 16; ++e) acc[e] = 0.0;
+  if (act) {
+    for (long long j = g; j < nvec; j += groups) {
+      float a[4], b[4];
+#pragma unroll
+      for (int p = 0; p < 4; ++p) {
+        const int ia = 4 * ta + p, ib = 4 * tb + p;
+        a[p] = ia < N ? base[ia * ps + j * vs] : 0.f;
+        b[p] = ib < N ? base[ib * ps + j * vs] : 0.f;
+      }
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p * 4 + q] = fma((double)a[p], (double)b[q], acc[p * 4 + q]);
+    }
+  }
+  for (int gg = 0; gg < groups; ++gg) {
+    if (act && g == gg) {
+#pragma unroll
+      for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const int i = 4 * ta + p, j = 4 * tb + q;
+          if (i < N && j < N && i <= j) {  // upper triangle, mirrored (diagonal tiles hold both halves)
+            const double v = (gg == 0 ? 0.0 : W[i * N + j]) + acc[p * 4 + q];
+            W[i * N + j] = v;
+            if (i != j) W[j * N + i] = v;
+          }
+        }
+    }
+    __syncthreads();
+  }
+}
+
+// Jacobi rotation annihilating a_pq (same rule as the single-tensor solver).
+__device__ __forceinline__ bool b_rotation(double app, double aqq, double apq, double inv_s, double& c, double& s) {
+  const double ps = app * inv_s, qs = aqq * inv_s, as = apq * inv_s;
+  c = 1.0;
+  s = 0.0;
+  if (!(fabs(as) > 1e-15 && as * as > 1e-28 * fabs(ps * qs))) return false;
+  const float d = (float)(qs - ps), e = 2.0f * (float)as;
+  const float h = sqrtf(fmaf(d, d, e * e));
+  const float tf = (d >= 0.0f ? e : -e) * __frcp_rn(fabsf(d) + h);
+  const double t = (double)tf;
+  const double x = fma(t, t, 1.0);
+  double y = (double)rsqrtf((float)x);
+  y = y * fma(-0.5 * x, y * y, 1.5);
+  y = y * fma(-0.5 * x, y * y, 1.5);
+  c = y;
+  s = t * y;
+  return true;
+}
+
+// Eigen-decomposition of the symmetric W (N x N row-major, N <= BSMALL) by cyclic Jacobi with
+// the round-robin pairing, all rotations of a round applied together as W' = J^T W J, V' = V J
+// (double-buffered).  Output: evals[N] descending, evecs (N x N column-major, stride N).
+// Returns the sweep count (max_sweeps + 1 when not converged).
+__device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, double* evecs, int max_sweeps,
+                          double* red) {
+  const int tid = threadIdx.x;
+  const int Np = N + (N & 1);
+  const int NR = Np - 1;
+  const int NN = Np * Np;
+  double* Wb[2] = {jac, jac + NN};
+  double* Vb[2] = {jac + 2 * NN, jac + 3 * NN};
+  double* cs = red;             // Np/2
+  double* sn = red + 32;        // Np/2
+  int* pr = reinterpret_cast<int*>(red + 64);  // partner, pair, first (3 x Np)
+  for (int idx = tid; idx < NN; idx += BT) {
+    const int i = idx / Np, j = idx - (idx / Np) * Np;
+    Wb[0][idx] = (i < N && j < N) ? W[i * N + j] : 0.0;
+    Vb[0][idx] = (i == j) ? 1.0 : 0.0;
+  }
+  double dm = 0.0;
+  for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(W[i * N + i]));
+  const double inv_s = dm > 0.0 ? 1.0 / dm : 1.0;
+  __syncthreads();
+  int cur = 0, sweep = 0;
+  bool conv = false;
+  for (; sweep < max_sweeps; ++sweep) {
+    int rot = 0;
+    for (int rnd = 0; rnd < NR; ++rnd) {
+      const double* Wc = Wb[cur];
+      if (tid < Np / 2) {
+        const int k = tid, x = k, y = Np - 1 - k;
+        int p = x == 0 ? 0 : 1 + (x - 1 + rnd) % NR;
+        int q = y == 0 ? 0 : 1 + (y - 1 + rnd) % NR;
+        if (p > q) {
+          const int tt = p;
+          p = q;
+          q = tt;
+        }
+        double c = 1.0, s = 0.0;
+        if (q < N && b_rotation(Wc[p * Np + p], Wc[q * Np + q], Wc[p * Np + q], inv_s, c, s)) rot = 1;
+        cs[k] = c;
+        sn[k] = s;
+        pr[p] = q;
+        pr[q] = p;
+        pr[Np + p] = k;
+        pr[Np + q] = k;
+        pr[2 * Np + p] = 1;
+        pr[2 * Np + q] = 0;
+      }
+      __syncthreads();
+      double* Wn = Wb[cur ^ 1];
+      const double* Vc = Vb[cur];
+      double* Vn = Vb[cur ^ 1];
+      for (int idx = tid; idx < NN; idx += BT) {
+        const int i = idx / Np, j = idx - (idx / Np) * Np;
+        const int pi = pr[i], pj = pr[j];
+        const double ci = cs[pr[Np + i]], si = sn[pr[Np + i]];
+        const double cj = cs[pr[Np + j]], sj = sn[pr[Np + j]];
+        const double jpi = pr[2 * Np + i] ? -si : si, jpj = pr[2 * Np + j] ? -sj : sj;
+        Wn[idx] = ci * (Wc[i * Np + j] * cj + Wc[i * Np + pj] * jpj) + jpi * (Wc[pi * Np + j] * cj + Wc[pi * Np + pj] * jpj);
+        Vn[idx] = Vc[i * Np + j] * cj + Vc[i * Np + pj] * jpj;
+      }
+      __syncthreads();
+      cur ^= 1;
+    }
+    if (!__syncthreads_or(rot)) {
+      conv = true;
+      ++sweep;
+      break;
+    }
+  }
+  const double* Wf = Wb[cur];
+  const double* Vf = Vb[cur];
+  int* rk = pr;  // reuse
+  if (tid < N) {
+    double la = Wf[tid * Np + tid];
+    if (la != la) la = -INFINITY;
+    int rank = 0;
+    for (int b = 0; b < N; ++b) {
+      double lb = Wf[b * Np + b];
+      if (lb != lb) lb = -INFINITY;
+      rank += (lb > la || (lb == la && b < tid)) ? 1 : 0;
+    }
+    rk[tid] = rank;
+    evals[rank] = Wf[tid * Np + tid];
+  }
+  __syncthreads();
+  for (int idx = tid; idx < N * N; idx += BT) {
+    const int i = idx % N, a = idx / N;
+    evecs[i + N * rk[a]] = Vf[i * Np + a];
+  }
+  __syncthreads();
+  return conv ? sweep : max_sweeps + 1;
+}
+
+// Largest-|entry| of each of the first r columns of U (rows x r, stride ld) made positive;
+// the sign is recorded in sgn[c] (+1/-1) and applied to U.
+__device__ void cta_canon(float* U, int rows, int ld, int r, float* sgn) {
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  for (int c = warp; c < r; c += BT / 32) {
+    float best = 0.f;
+    int bi = rows;
+    for (int i = lane; i < rows; i += 32) {
+      const float v = fabsf(U[i + (long long)ld * c]);
+      if (v > best || (v == best && i < bi)) {
+        best = v;
+        bi = i;
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const float ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    const float s = (bi < rows && U[bi + (long long)ld * c] < 0.f) ? -1.f : 1.f;
+    for (int i = lane; i < rows; i += 32) U[i + (long long)ld * c] *= s;
+    if (lane == 0) sgn[c] = s;
+  }
+  __syncthreads();
+}
+
+// Rank from eigenvalues (descending) of an unfolding whose energy is `energy`: the smallest r
+// (<= cap) whose discarded energy is <= delta2; eps = 0 keeps cap.  Returns r and updates the
+// energy carried and the discarded total.
+__device__ int pick_rank(const double* lam, int nev, int cap, double delta2, bool adaptive, double energy,
+                         double* kept_out, double* tail_out) {
+  int r = 0;
+  double kept = 0.0;
+  if (!adaptive) {
+    for (; r < cap; ++r) kept += fmax(lam[r], 0.0);
+  } else {
+    while (r < cap && (r == 0 || energy - kept > delta2)) kept += fmax(lam[r++], 0.0);
+  }
+  (void)nev;
+  *kept_out = kept;
+  *tail_out = fmax(energy - kept, 0.0);
+  return r;
+}
+
+__global__ void __launch_bounds__(BT, 1)
+    k_tt_batched(const BatchShape* __restrict__ shp, int count, const float* __restrict__ x,
+                 float* __restrict__ cores, int* __restrict__ ranks_out, double* __restrict__ err_out,
+                 float* __restrict__ scratch, long long scratch_per_cta, long long half, double eps, int rmax,
+                 int oversample, unsigned long long seed, int max_sweeps, int* __restrict__ counter,
+                 DevStatus* st) {
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Smem S;
+  {
+    unsigned char* p = smraw;
+    S.chunk = reinterpret_cast<float*>(p);
+    p += SM_CHUNK;
+    S.yq = reinterpret_cast<float*>(p);
+    p += SM_YQ;
+    S.w = reinterpret_cast<double*>(p);
+    p += SM_W;
+    S.jac = reinterpret_cast<double*>(p);
+    p += SM_JAC;
+    S.om = reinterpret_cast<float*>(p);
+    p += SM_OM;
+    S.red = reinterpret_cast<double*>(p);
+  }
+  __shared__ double lam[BSMALL], evec[BSMALL * BSMALL];
+  __shared__ float sgn[BSMALL], sig_inv[BSMALL];
+  __shared__ int sh_i[4];
+  const int tid = threadIdx.x;
+  float* buf0 = scratch + (long long)blockIdx.x * scratch_per_cta;
+  float* buf1 = buf0 + half;
+  float* Bg = buf1 + half;  // ks x cols of the randomized steps
+
+  for (;;) {
+    if (tid == 0) sh_i[0] = atomicAdd(counter, 1);
+    __syncthreads();
+    const int t = sh_i[0];
+    __syncthreads();
+    if (t >= count) break;
+    const BatchShape sh = shp[t];
+    const int d = sh.d;
+    const float* src = x + sh.x_off;
+    float* cp = cores + sh.core_off;
+    long long size = sh.size;
+    // ||X||^2
+    double s2 = 0.0;
+    for (long long i = tid; i < size; i += BT) s2 = fma((double)src[i], (double)src[i], s2);
+    const double xn2 = cta_sum(s2, S.red);
+    const bool adaptive = eps > 0.0;
+    const double delta2 = eps * eps * xn2 / (double)max(d - 1, 1);
+    double energy = xn2, tails = 0.0;
+    int r_prev = 1;
+    if (tid == 0) ranks_out[(long long)t * (BMAXD + 1)] = 1;
+    bool fail = false;
+    for (int k = 0; k < d - 1 && !fail; ++k) {
+      const long long m = (long long)r_prev * sh.n[k];
+      const long long cols = size / m;
+      const long long small = m < cols ? m : cols;
+      const int cap = (int)min((long long)rmax, small);
+      float* dst = (k & 1) ? buf0 : buf1;
+      int r = 1;
+      if (small <= BSMALL) {
+        // ---- exact Gram-eigen step ----
+        const int N = (int)small;
+        if (m <= cols) cta_gram(src, 1, m, N, cols, S.w);   // W = A A^T, vectors = columns
+        else cta_gram(src, m, 1, N, m, S.w);                // W = A^T A, vectors = rows
+        const int sw = cta_jacobi(S.w, N, S.jac, lam, evec, max_sweeps, S.red);
+        if (tid == 0 && st) {
+          atomicMax(&st->sweeps, sw);
+          if (sw > max_sweeps) dev_fail(st, TT_ERR_NOCONV, t);
+        }
+        double full = 0.0;
+        for (int i = 0; i < N; ++i) full += fmax(lam[i], 0.0);
+        double kept, tail;
+        r = pick_rank(lam, N, cap, delta2, adaptive, adaptive ? full : energy, &kept, &tail);
+        tails += tail;
+        energy = kept;
+        if (m <= cols) {
+          // U = E_r (m x r): canonical signs, core, next = U^T A (r x cols, column-major)
+          float* U = S.chunk;  // m x r
+          for (int idx = tid; idx < (int)m * r; idx += BT) U[idx] = (float)evec[(idx % m) + m * (idx / m)];
+          __syncthreads();
+          cta_canon(U, (int)m, (int)m, r, sgn);
+          for (int idx = tid; idx < (int)m * r; idx += BT) cp[idx] = U[idx];
+          for (long long j = tid; j < cols; j += BT) {
+            float acc[BSMALL];
+#pragma unroll
+            for (int c = 0; c < BSMALL; ++c) acc[c] = 0.f;
+            const float* a = src + j * m;
+            for (int i = 0; i < (int)m; ++i) {
+              const float av = a[i];
+#pragma unroll
+              for (int c = 0; c < BSMALL; ++c)
+                if (c < r) acc[c] = fmaf(av, U[i + m * c], acc[c]);
+            }
+#pragma unroll
+            for (int c = 0; c < BSMALL; ++c)
+              if (c < r) dst[j * r + c] = acc[c];
+          }
+        } else {
+          // cols <= 32 < m: V (cols x cols), U = A V_r / sigma (m x r), next = sigma V_r^T
+          for (int c = tid; c < r; c += BT) sig_inv[c] = lam[c] > 0.0 ? (float)(1.0 / sqrt(lam[c])) : 0.f;
+          __syncthreads();
+          const int nc = (int)cols;
+          for (long long i = tid; i < m; i += BT) {
+            float arow[BSMALL];
+#pragma unroll
+            for (int q = 0; q < BSMALL; ++q) arow[q] = q < nc ? src[i + m * q] : 0.f;
+            for (int c = 0; c < r; ++c) {
+              float acc = 0.f;
+#pragma unroll
+              for (int q = 0; q < BSMALL; ++q)
+                if (q < nc) acc = fmaf(arow[q], (float)evec[q + nc * c], acc);
+              cp[i + m * c] = acc * sig_inv[c];
+            }
+          }
+          __syncthreads();
+          // canonical signs on the core columns (global memory), mirrored on the rows of sigma V^T
+          cta_canon(cp, (int)m, (int)m, r, sgn);
+          for (int idx = tid; idx < r * nc; idx += BT) {
+            const int c = idx % r, q = idx / r;  // dst column-major r x cols: dst[c + r q]
+            dst[idx] = sgn[c] * (float)(sqrt(fmax(lam[c], 0.0)) * evec[q + nc * c]);
+          }
+        }
+      } else if (m <= BMAXM) {
+        // ---- randomized step (EDrSVD) ----
+        const int ks = (int)min((long long)min(cap + oversample, BSMALL), small);
+        const int SY = ks | 1;  // odd row stride of Y / Q in shared memory
+        const int mi = (int)m;
+        // Y = A Omega, Omega (cols x ks) N(0,1) from Philox: element (j, c) is component j & 3 of
+        // call (c * cols4 + (j & ~3)) / 4, cols4 = cols rounded up to a multiple of 4.
+        const long long cols4 = (cols + 3) & ~3LL;
+        const unsigned stream = (unsigned)(t * BMAXD + k);
+        float yacc[BSMALL];
+#pragma unroll
+        for (int c = 0; c < BSMALL; ++c) yacc[c] = 0.f;
+        for (long long j0 = 0; j0 < cols; j0 += BCH) {
+          const int nj = (int)min((long long)BCH, cols - j0);
+          __syncthreads();
+          for (int q = tid; q < (BCH / 4) * ks; q += BT) {
+            const int c = q / (BCH / 4), j4 = 4 * (q % (BCH / 4));
+            const float4 g = philox_normal4((unsigned long long)((c * cols4 + j0 + j4) >> 2), stream, seed);
+            S.om[(j4 + 0) * BSMALL + c] = g.x;
+            S.om[(j4 + 1) * BSMALL + c] = g.y;
+            S.om[(j4 + 2) * BSMALL + c] = g.z;
+            S.om[(j4 + 3) * BSMALL + c] = g.w;
+          }
+          __syncthreads();
+          if (tid < mi) {
+            for (int jj = 0; jj < nj; ++jj) {
+              const float av = src[tid + m * (j0 + jj)];
+#pragma unroll
+              for (int c = 0; c < BSMALL; ++c)
+                if (c < ks) yacc[c] = fmaf(av, S.om[jj * BSMALL + c], yacc[c]);
+            }
+          }
+        }
+        __syncthreads();
+        if (tid < mi)
+#pragma unroll
+          for (int c = 0; c < BSMALL; ++c)
+            if (c < ks) S.yq[tid * SY + c] = yacc[c];
+        __syncthreads();
+        // CholeskyQR2 on Y (rows x ks in shared memory): Gram in FP64, Cholesky, substitution
+        for (int pass = 0; pass < 2; ++pass) {
+          cta_gram(S.yq, 1, SY, ks, mi, S.w);
+          double* Wc = S.w;
+          double dmax = 0.0;
+          for (int i = 0; i < ks; ++i) dmax = fmax(dmax, Wc[i * ks + i]);
+          const double tol = 1e-12 * dmax;
+          for (int kk = 0; kk < ks; ++kk) {
+            const double dk = Wc[kk * ks + kk];
+            if (dk > tol && dmax > 0.0) {
+              const double inv = 1.0 / dk;
+              const int j = kk + 1 + (tid & 31);
+              if (j < ks) {
+                const double wkj = Wc[kk * ks + j] * inv;
+                for (int i = kk + 1 + (tid >> 5); i <= j; i += BT / 32) Wc[i * ks + j] -= Wc[kk * ks + i] * wkj;
+              }
+            }
+            __syncthreads();
+          }
+          // row i: q R = y (forward substitution, R[k][c] = W[k][c] / sqrt(W[k][k]) on live rows)
+          if (tid < mi) {
+            float* yr = S.yq + tid * SY;
+            for (int c = 0; c < ks; ++c) {
+              const double dc = Wc[c * ks + c];
+              if (!(dc > tol && dmax > 0.0)) {
+                yr[c] = 0.f;
+                continue;
+              }
+              float a = yr[c];
+              for (int kk = 0; kk < c; ++kk) {
+                const double dk = Wc[kk * ks + kk];
+                if (dk > tol && dmax > 0.0) a = fmaf(-yr[kk], (float)(Wc[kk * ks + c] / sqrt(dk)), a);
+              }
+              yr[c] = a * (float)(1.0 / sqrt(dc));
+            }
+          }
+          __syncthreads();
+        }
+        // B = Q^T A (ks x cols, column-major in Bg), then W = B B^T in FP64
+        for (long long j = tid; j < cols; j += BT) {
+          float b[BSMALL];
+#pragma unroll
+          for (int c = 0; c < BSMALL; ++c) b[c] = 0.f;
+          const float* a = src + j * m;
+          for (int i = 0; i < mi; ++i) {
+            const float av = a[i];
+            const float* qr = S.yq + i * SY;
+#pragma unroll
+            for (int c = 0; c < BSMALL; ++c)
+              if (c < ks) b[c] = fmaf(av, qr[c], b[c]);
+          }
+#pragma unroll
+          for (int c = 0; c < BSMALL; ++c)
+            if (c < ks) Bg[j * ks + c] = b[c];
+        }
+        __syncthreads();
+        cta_gram(Bg, 1, ks, ks, cols, S.w);  // W = B B^T (vectors = columns of B)
+        const int sw = cta_jacobi(S.w, ks, S.jac, lam, evec, max_sweeps, S.red);
+        if (tid == 0 && st) {
+          atomicMax(&st->sweeps, sw);
+          if (sw > max_sweeps) dev_fail(st, TT_ERR_NOCONV, t);
+        }
+        double kept, tail;
+        r = pick_rank(lam, ks, min(cap, ks), delta2, adaptive, energy, &kept, &tail);
+        tails += tail;
+        energy = kept;
+        // U = Q E_r (m x r) -> canonical signs -> core; next = E_r^T B with the same signs
+        float* U = S.chunk;
+        for (int idx = tid; idx < mi * r; idx += BT) {
+          const int i = idx % mi, c = idx / mi;
+          float acc = 0.f;
+          for (int q = 0; q < ks; ++q) acc = fmaf(S.yq[i * SY + q], (float)evec[q + ks * c], acc);
+          U[idx] = acc;
+        }
+        __syncthreads();
+        cta_canon(U, mi, mi, r, sgn);
+        for (int idx = tid; idx < mi * r; idx += BT) cp[idx] = U[idx];
+        for (long long j = tid; j < cols; j += BT) {
+          float b[BSMALL];
+#pragma unroll
+          for (int q = 0; q < BSMALL; ++q) b[q] = q < ks ? Bg[j * ks + q] : 0.f;
+          for (int c = 0; c < r; ++c) {
+            float acc = 0.f;
+#pragma unroll
+            for (int q = 0; q < BSMALL; ++q)
+              if (q < ks) acc = fmaf(b[q], (float)evec[q + ks * c], acc);
+            dst[j * r + c] = sgn[c] * acc;
+          }
+        }
+      } else {
+        fail = true;
+        if (tid == 0 && st) dev_fail(st, TT_ERR_UNSUPPORTED, t);
+        break;
+      }
+      __syncthreads();
+      cp += m * r;
+      src = dst;
+      size = (long long)r * cols;
+      r_prev = r;
+      if (tid == 0) ranks_out[(long long)t * (BMAXD + 1) + k + 1] = r;
+    }
+    if (!fail) {
+      // last core = the remaining data (r_{d-1}, n_d, 1)
+      for (long long i = tid; i < size; i += BT) cp[i] = src[i];
+      if (tid == 0) {
+        ranks_out[(long long)t * (BMAXD + 1) + d] = 1;
+        err_out[t] = xn2 > 0.0 ? sqrt(tails / xn2) : 0.0;
+      }
+    }
+    __syncthreads();
+  }
+}
+
+}  // namespace
+}  // namespace ttr
+
+using namespace ttr;
+
+extern "C" long long tt_batch_core_capacity(int d, const int* n, int rmax) {
+  if (d < 2 || d > BMAXD || !n || rmax < 1) return -1;
+  long long total = 0, left = 1, right = 1;
+  for (int k = 0; k < d; ++k) right *= n[k];
+  long long rp = 1;
+  for (int k = 0; k < d; ++k) {
+    left *= n[k];
+    right /= n[k];
+    const long long rn = (k == d - 1) ? 1 : std::min<long long>({(long long)rmax, left, right});
+    total += rp * n[k] * rn;
+    rp = rn;
+  }
+  return total;
+}
+
+extern "C" int tt_svd_batched(tt_ctx* ctx, int count, int d, const int* n, const float* x,
+                              const long long* x_off, double eps, int rmax, int oversample,
+                              unsigned long long seed, float* cores, const long long* core_off, int* ranks,
+                              double* err_est) {
+  if (!ctx || !n || !x || !x_off || !cores || !core_off || !ranks || count < 0) {
+    set_error(TT_ERR_ARG, "null argument");
+    return TT_ERR_ARG;
+  }
+  if (d < 2 || d > BMAXD || rmax < 1 || rmax > BSMALL || !(eps >= 0.0) || oversample < 0) {
+    set_error(TT_ERR_SHAPE, "batched: order %d (2..%d), rmax %d (1..%d), eps %g", d, BMAXD, rmax, BSMALL, eps);
+    return TT_ERR_SHAPE;
+  }
+  if (count == 0) return TT_OK;
+  std::vector<BatchShape> hs((size_t)count);
+  long long maxsize = 0, maxbg = 0;
+  for (int t = 0; t < count; ++t) {
+    BatchShape& b = hs[(size_t)t];
+    b.d = d;
+    b.size = 1;
+    for (int k = 0; k < BMAXD; ++k) b.n[k] = k < d ? n[(size_t)t * d + k] : 1;
+    for (int k = 0; k < d; ++k) {
+      if (b.n[k] < 1) {
+        set_error(TT_ERR_SHAPE, "batched: tensor %d mode %d size %d", t, k, b.n[k]);
+        return TT_ERR_SHAPE;
+      }
+      b.size *= b.n[k];
+    }
+    b.x_off = x_off[t];
+    b.core_off = core_off[t];
+    maxsize = std::max(maxsize, b.size);
+    // randomized steps keep B (ks x cols) and need rows <= BMAXM
+    long long rp = 1, sz = b.size;
+    for (int k = 0; k < d - 1; ++k) {
+      const long long m = rp * b.n[k], cols = sz / m, small = std::min(m, cols);
+      if (small > BSMALL) {
+        if (m > BMAXM) {
+          set_error(TT_ERR_UNSUPPORTED, "batched: tensor %d step %d has %lld rows (> %d) on a sketched step", t, k, m,
+                    BMAXM);
+          return TT_ERR_UNSUPPORTED;
+        }
+        maxbg = std::max(maxbg, (long long)BSMALL * cols);
+      }
+      const long long rn = std::min<long long>((long long)rmax, small);
+      sz = rn * cols;
+      rp = rn;
+    }
+  }
+  int dev = 0, sms = 148;
+  TT_CUDA(cudaGetDevice(&dev));
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  const int grid = std::min(count, sms);
+  const long long half = (maxsize + 63) & ~63LL;
+  const long long per_cta = 2 * half + ((maxbg + 63) & ~63LL);
+  const size_t bytes = sizeof(BatchShape) * (size_t)count + sizeof(int) * (size_t)count * (BMAXD + 1) +
+                       sizeof(double) * (size_t)count + sizeof(float) * (size_t)per_cta * grid + 4096;
+  Arena ws;
+  TT_TRY(ctx_arena(ctx, bytes, &ws));
+  BatchShape* dshp = ws.take<BatchShape>((size_t)count);
+  int* dranks = ws.take<int>((size_t)count * (BMAXD + 1));
+  double* derr = ws.take<double>((size_t)count);
+  int* dcounter = ws.take<int>(1);
+  float* scratch = ws.take<float>((size_t)per_cta * grid);
+  if (!dshp || !dranks || !derr || !dcounter || !scratch) {
+    set_error(TT_ERR_NOMEM, "batched workspace");
+    return TT_ERR_NOMEM;
+  }
+  cudaStream_t s = ctx_stream(ctx);
+  DevStatus* dst = ctx_status(ctx);
+  TT_CUDA(cudaMemsetAsync(dst, 0, sizeof(DevStatus), s));
+  TT_CUDA(cudaMemcpyAsync(dshp, hs.data(), sizeof(BatchShape) * (size_t)count, cudaMemcpyHostToDevice, s));
+  TT_CUDA(cudaMemsetAsync(dcounter, 0, sizeof(int), s));
+  static bool attr = false;
+  if (!attr) {
+    if (cudaFuncSetAttribute(k_tt_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_TOTAL) != cudaSuccess) {
+      set_error(TT_ERR_CUDA, "batched kernel shared-memory attribute");
+      return TT_ERR_CUDA;
+    }
+    attr = true;
+  }
+  k_tt_batched<<<grid, BT, SM_TOTAL, s>>>(dshp, count, x, cores, dranks, derr, scratch, per_cta, half, eps, rmax,
+                                            oversample, seed, 40, dcounter, dst);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  std::vector<int> hr((size_t)count * (BMAXD + 1));
+  TT_CUDA(cudaMemcpyAsync(hr.data(), dranks, sizeof(int) * hr.size(), cudaMemcpyDeviceToHost, s));
+  if (err_est) TT_CUDA(cudaMemcpyAsync(err_est, derr, sizeof(double) * (size_t)count, cudaMemcpyDeviceToHost, s));
+  DevStatus hst;
+  TT_CUDA(cudaMemcpyAsync(&hst, dst, sizeof(hst), cudaMemcpyDeviceToHost, s));
+  TT_CUDA(cudaStreamSynchronize(s));
+  for (int t = 0; t < count; ++t)
+    for (int k = 0; k <= d; ++k) ranks[(size_t)t * (d + 1) + k] = hr[(size_t)t * (BMAXD + 1) + k];
+  if (hst.code) {
+    set_error(hst.code, "batched: device status %d (tensor %d)", hst.code, hst.detail);
+    return hst.code;
+  }
+  return TT_OK;
+}

@@ -439,7 +439,7 @@ struct Passes {
   }
 };
 
-int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, float* const* cores_out,
+int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* const* cores_out,
               tt_stats* stats) {
   const bool host_io = (o.flags & TT_FLAG_HOST_IO) != 0;
   TT_CUDA(cudaSetDevice(c->device));
@@ -477,17 +477,68 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
     }
   }
 
+  // Adaptive ranks (o.eps > 0): delta-truncation of every unfolding, delta^2 = eps^2 ||X||^2 /
+  // (d - 1) (the TT-SVD error bound); the caller's ranks are upper bounds.  Each decision reads
+  // the eigenvalues back to the host, and the rest of the plan is rebuilt with the chosen rank.
+  const bool adaptive = o.eps > 0.0;
+  double delta2 = 0.0, energy = 0.0, xnorm2 = 0.0, tail_sum = 0.0;
+  if (adaptive) {
+    const size_t mk = ws.mark();
+    double* acc = ws.take<double>(2);
+    if (!acc) {
+      set_error(TT_ERR_NOMEM, "norm accumulator");
+      return TT_ERR_NOMEM;
+    }
+    TT_CUDA(cudaMemsetAsync(acc, 0, 2 * sizeof(double), s));
+    TT_TRY(launch_diff_norm(x, nullptr, P.total, acc, s));
+    double h[2];
+    TT_CUDA(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    TT_CUDA(cudaStreamSynchronize(s));
+    ws.reset(mk);
+    xnorm2 = h[1];
+    energy = xnorm2;
+    delta2 = o.eps * o.eps * xnorm2 / (double)(P.d - 1);
+  }
+  std::vector<int> rmax(P.r);  // caller's ranks (upper bounds in adaptive mode)
+  tt_opts oplan = o;
+  oplan.flags |= TT_FLAG_NO_FOLD;
+
   const float* cur = x;
   int slot = 0;
   const double* pend = nullptr;  // pending rotation (rows_in x rows_in), or null
   int pend_slot = 0;
   const int nsteps = (int)P.steps.size();
   for (int k = 0; k < nsteps; ++k) {
-    const Step& st = P.steps[k];
+    Step& st = P.steps[k];
     pass.cur_step = k;
     const long long m = st.m, cols = st.cols;
-    const int rq = st.r_req, re = st.r_eff;
-    const int nout = st.n_out;                      // rows of the next data (compacted)
+    int rq = st.r_req, re = st.r_eff;
+    int nout = st.n_out;                            // rows of the next data (compacted)
+    // Adaptive rank of this step from the first `nev` eigenvalues in B.evals: the smallest r
+    // whose discarded energy (energy of the unfolding minus the kept eigenvalues) is <= delta^2.
+    auto decide = [&](int nev) -> int {
+      if (!adaptive) return TT_OK;
+      std::vector<double> lam((size_t)nev);
+      TT_CUDA(cudaMemcpyAsync(lam.data(), B.evals, sizeof(double) * nev, cudaMemcpyDeviceToHost, s));
+      TT_CUDA(cudaStreamSynchronize(s));
+      const int cap = std::min(rmax[k + 1], std::min(nev, re));
+      int r = 0;
+      double tail = energy;
+      while (r < cap && (r == 0 || tail > delta2)) tail -= std::max(lam[(size_t)r++], 0.0);
+      tail = std::max(tail, 0.0);
+      tail_sum += tail;
+      energy = std::max(energy - tail, 0.0);
+      rq = re = nout = r;
+      st.r_req = st.r_eff = st.n_out = r;
+      st.next_elems = (long long)r * cols;
+      P.r[k + 1] = r;
+      Plan P2;
+      const std::vector<int> nn(P.n.begin(), P.n.end());
+      TT_TRY(make_plan(P.d, nn.data(), P.r.data(), P.ring, oplan, P2));
+      for (size_t j = (size_t)k + 1; j < P.steps.size(); ++j) P.steps[j] = P2.steps[j];
+      P.last_rows = P2.last_rows;
+      return TT_OK;
+    };
     const int pr1 = st.perm231 ? st.r1_out : 1;     // TR bond r1 carried after step 1
     const int rin = st.rows_in, rcore = st.core_rows;
     const int engine = engine_for(o, m, cols);
@@ -526,6 +577,7 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
       TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
+      TT_TRY(decide((int)m));
       // basis (m x r_req, zero-padded beyond r_eff), FP32, canonical column signs
       TT_TRY(launch_f64_to_f32_cols(B.evecs, m, m, re, B.ef, m, rq, s));
       TT_TRY(launch_canon_cols(B.ef, m, re, m, B.evecs, (int)m, m, s));
@@ -545,7 +597,7 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
       TT_TRY(pass.run(TT_PASS_PROJECT, 2.0 * m * cols * nout, 4.0 * m * cols + 4.0 * nout * cols, [&] {
         return launch_project(cur, m, cols, B.ef, nout, m, next, st.perm231 ? 0 : nout,
                               st.perm231 ? OUT_PERM231 : OUT_ROWMAJOR, P.r[0], pr1,
-                              engine == TT_GEMM_TC && re < m ? TT_GEMM_TC : TT_GEMM_FP32, ws, c->dstat, s);
+                              engine, ws, c->dstat, s);
       }));
     } else if (st.path == PATH_EXACT_COLS) {
       // W = A^T A over the rows of A (vectors = rows i, components = columns)
@@ -554,6 +606,7 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
       TT_TRY(launch_syev(B.w, (int)cols, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(cols, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
+      TT_TRY(decide((int)cols));
       TT_TRY(launch_inv_sigma(B.evals, re, B.colscale, 1e-30, s));
       float* ubuf = B.corebuf;
       TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * m * cols * rq, 4.0 * m * cols + 4.0 * m * rq, [&] {
@@ -583,14 +636,15 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
       TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, ks, B.yf, m, ks, s));
       TT_TRY(launch_cholqr2(B.yf, m, ks, 1, m, nullptr, ws, c->dstat, s));
       for (int it = 0; it < o.power_iters; ++it) {
+        // Z = A^T Q written column-major (cols x ks), the layout the sketch reads W in
         TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
-          return launch_project(cur, m, cols, B.yf, ks, m, B.bt, ks, OUT_ROWMAJOR, 1, 1, engine, ws, c->dstat, s);
+          return launch_project(cur, m, cols, B.yf, ks, m, B.bt, cols, OUT_COLMAJOR, 1, 1, engine, ws, c->dstat, s);
         }));
         TT_TRY(pass.run(TT_PASS_OTHER, 6.0 * cols * ks * ks, 24.0 * cols * ks, [&] {
-          return launch_cholqr2(B.bt, cols, ks, ks, 1, nullptr, ws, c->dstat, s);
+          return launch_orth_power(B.bt, cols, ks, 1, cols, ws, c->dstat, s);
         }));
         TT_TRY(pass.run(TT_PASS_SKETCH, fl_pass, by_pass, [&] {
-          return launch_sketch(cur, m, cols, B.bt, ks, ks, 1, B.yd, engine, ws, c->dstat, s);
+          return launch_sketch(cur, m, cols, B.bt, ks, 1, cols, B.yd, engine, ws, c->dstat, s);
         }));
         TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, ks, B.yf, m, ks, s));
         TT_TRY(launch_cholqr2(B.yf, m, ks, 1, m, nullptr, ws, c->dstat, s));
@@ -611,6 +665,7 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
       TT_TRY(launch_syev(B.w, ks, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, std::min(ks, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
+      TT_TRY(decide(ks));
       // core = Q E_r with canonical column signs (E's columns follow)
       float* ubuf = B.corebuf;
       TT_TRY(launch_small_nn(B.yf, m, ks, m, B.evecs, rq, ks, nullptr, re, ubuf, m, s));
@@ -656,6 +711,7 @@ int run_chain(tt_ctx* c, const float* x_in, const Plan& P, const tt_opts& o, flo
     stats->ms = ms;
     stats->nsteps = nsteps;
     for (int k = 0; k <= P.d; ++k) stats->ranks[k] = P.r[k];
+    stats->est_rel_err = adaptive && xnorm2 > 0.0 ? std::sqrt(tail_sum / xnorm2) : 0.0;
     for (int k = 0; k < nsteps; ++k) {
       int cnt = 0;
       for (int i = 0; i < TT_STATS_MAX_SIGMA; ++i) {
@@ -704,6 +760,17 @@ int run_entry(tt_ctx* c, const float* x, int d, const int* n, const int* r, cons
     o = *opts;
   else
     tt_default_opts(&o);
+  if (o.eps < 0.0 || o.eps != o.eps) {
+    set_error(TT_ERR_ARG, "eps must be >= 0");
+    return TT_ERR_ARG;
+  }
+  if (o.eps > 0.0) {
+    if (ring) {
+      set_error(TT_ERR_UNSUPPORTED, "adaptive ranks (eps > 0) are implemented for TT-SVD only");
+      return TT_ERR_UNSUPPORTED;
+    }
+    o.flags |= TT_FLAG_NO_FOLD;  // the rank of a full-rank step is not known in advance
+  }
   Plan P;
   TT_TRY(make_plan(d, n, r, ring, o, P));
   for (int k = 0; k < d; ++k)
@@ -784,6 +851,19 @@ int ws_for(tt_ctx* c, size_t bytes, Arena& ws) {
   ws = Arena{c->arena, c->cap, 0};
   return TT_OK;
 }
+}  // namespace
+
+// Context accessors for the other translation units (batched path).
+namespace ttr {
+int ctx_arena(tt_ctx* c, size_t bytes, Arena* ws) {
+  TT_CUDA(cudaSetDevice(c->device));
+  return ws_for(c, bytes, *ws);
+}
+cudaStream_t ctx_stream(tt_ctx* c) { return c->stream; }
+DevStatus* ctx_status(tt_ctx* c) { return c->dstat; }
+}  // namespace ttr
+
+namespace {
 int check_status(tt_ctx* c) {
   TT_CUDA(cudaMemcpyAsync(c->hstat, c->dstat, sizeof(DevStatus), cudaMemcpyDeviceToHost, c->stream));
   TT_CUDA(cudaStreamSynchronize(c->stream));
@@ -834,6 +914,19 @@ extern "C" int tt_k_sketch(tt_ctx* c, const float* a, long long m, long long n, 
   TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
   TT_TRY(launch_sketch(a, m, n, w, N, 1, ldw, y, eng, ws, c->dstat, c->stream));
   return check_status(c);
+}
+
+extern "C" int tt_k_gaussian_rows(tt_ctx* c, float* out, long long row0, long long nrows, long long total_rows,
+                                  int cols, long long ld, unsigned long long seed, unsigned stream_id) {
+  TT_NEED(c);
+  TT_NEED(out);
+  if (row0 < 0 || nrows < 0 || row0 + nrows > total_rows || cols < 0 || ld < nrows) {
+    set_error(TT_ERR_SHAPE, "gaussian_rows shape");
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  TT_TRY(launch_gaussian_rows(out, row0, nrows, total_rows, cols, ld, seed, stream_id, c->stream));
+  return TT_OK;
 }
 
 extern "C" int tt_k_project(tt_ctx* c, const float* a, long long m, long long n, const float* q,

@@ -7,6 +7,7 @@
 #include <algorithm>
 
 #include "kernels.cuh"
+#include "philox.cuh"
 
 namespace ttr {
 
@@ -26,37 +27,14 @@ static int num_sms() {
 // ---------------------------------------------------------------------------------------
 // Philox4x32-10 Gaussian generator (replaces curandGenerateNormal, TT3O:585-587)
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
-#pragma unroll
-  for (int i = 0; i < 10; ++i) {
-    const unsigned hi0 = __umulhi(0xD2511F53u, c.x), lo0 = 0xD2511F53u * c.x;
-    const unsigned hi1 = __umulhi(0xCD9E8D57u, c.z), lo1 = 0xCD9E8D57u * c.z;
-    c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
-    k.x += 0x9E3779B9u;
-    k.y += 0xBB67AE85u;
-  }
-  return c;
-}
 
 __global__ void k_gaussian(float* __restrict__ out, long long rows, long long total, long long ld,
                            unsigned long long seed, unsigned stream_id) {
   const long long ncall = (total + 3) / 4;
-  const uint2 key = make_uint2((unsigned)(seed & 0xFFFFFFFFull), (unsigned)(seed >> 32));
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncall;
        c += (long long)gridDim.x * blockDim.x) {
-    const uint4 w = philox4x32_10(
-        make_uint4((unsigned)(c & 0xFFFFFFFFll), stream_id, (unsigned)(c >> 32), 0u), key);
-    const float sc = 2.3283064365386963e-10f;  // 2^-32
-    const float u0 = ((float)w.x + 0.5f) * sc, u1 = ((float)w.y + 0.5f) * sc;
-    const float u2 = ((float)w.z + 0.5f) * sc, u3 = ((float)w.w + 0.5f) * sc;
-    // Box-Muller with the hardware approximations (absolute error ~1e-6 on the normals): the
-    // angle is taken in [-pi, pi), where __sincosf is accurate, and the sign flip restores
-    // sin/cos of 2*pi*u.
-    const float r0 = sqrtf(-2.0f * __logf(u0)), r1 = sqrtf(-2.0f * __logf(u2));
-    float s0, c0, s1, c1;
-    __sincosf(6.283185307179586f * (u1 - 0.5f), &s0, &c0);
-    __sincosf(6.283185307179586f * (u3 - 0.5f), &s1, &c1);
-    const float g[4] = {-r0 * c0, -r0 * s0, -r1 * c1, -r1 * s1};
+    const float4 gv = philox_normal4((unsigned long long)c, stream_id, seed);
+    const float g[4] = {gv.x, gv.y, gv.z, gv.w};
     // element e = row + rows * col; one 64-bit division per call, then step through rows
     long long col = (4 * c) / rows;
     long long row = 4 * c - col * rows;
@@ -69,6 +47,33 @@ __global__ void k_gaussian(float* __restrict__ out, long long rows, long long to
       }
     }
   }
+}
+
+// Rows [row0, row0 + nrows) of the (total_rows x cols) matrix k_gaussian generates (its element
+// (i, c) is component e % 4 of Philox call e / 4, e = i + total_rows * c): the block of a
+// column-sharded Omega that one rank multiplies with its columns.
+__global__ void k_gaussian_rows(float* __restrict__ out, long long row0, long long nrows, long long total_rows,
+                                int cols, long long ld, unsigned long long seed, unsigned stream_id) {
+  const long long total = nrows * cols;
+  for (long long idx = blockIdx.x * (long long)blockDim.x + threadIdx.x; idx < total;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const long long c = idx / nrows, i = idx - c * nrows;
+    const long long e = row0 + i + total_rows * c;
+    const float4 g = philox_normal4((unsigned long long)(e >> 2), stream_id, seed);
+    const int l = (int)(e & 3);
+    out[i + ld * c] = l == 0 ? g.x : l == 1 ? g.y : l == 2 ? g.z : g.w;
+  }
+}
+
+int launch_gaussian_rows(float* out, long long row0, long long nrows, long long total_rows, int cols, long long ld,
+                         unsigned long long seed, unsigned stream_id, cudaStream_t s) {
+  const long long total = nrows * (long long)cols;
+  if (total <= 0) return TT_OK;
+  k_gaussian_rows<<<(int)std::min<long long>(ceil_div_ll(total, 256), 8LL * num_sms()), 256, 0, s>>>(
+      out, row0, nrows, total_rows, cols, ld, seed, stream_id);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  return TT_OK;
 }
 
 int launch_gaussian(float* out, long long rows, int cols, long long ld, unsigned long long seed,
@@ -376,6 +381,8 @@ __global__ void __launch_bounds__(256) k_project_simt(const float* __restrict__ 
       if (col >= N) continue;
       if (mode == OUT_ROWMAJOR) {
         out[j * ldo + col] = acc[e][c];
+      } else if (mode == OUT_COLMAJOR) {
+        out[j + ldo * col] = acc[e][c];
       } else {
         const int ai = col % r0, bi = col / r0;
         out[(long long)bi + (long long)r1 * (j + n * (long long)ai)] = acc[e][c];
@@ -487,6 +494,8 @@ __global__ void __launch_bounds__(256) k_proj_smallk(const float* __restrict__ a
         if (c >= N) continue;
         if (mode == OUT_ROWMAJOR) {
           out[j * ldo + c] = acc[cc];
+        } else if (mode == OUT_COLMAJOR) {
+          out[j + ldo * c] = acc[cc];
         } else {
           const int ai = c % r0, bi = c / r0;
           out[(long long)bi + (long long)r1 * (j + n * (long long)ai)] = acc[cc];
@@ -508,6 +517,8 @@ __global__ void k_project_reduce(const float* __restrict__ part, long long n, in
     const int c = (int)(idx - j * N);
     if (mode == OUT_ROWMAJOR) {
       out[j * ldo + c] = v;
+    } else if (mode == OUT_COLMAJOR) {
+      out[j + ldo * c] = v;
     } else {
       const int ai = c % r0, bi = c / r0;
       out[(long long)bi + (long long)r1 * (j + n * (long long)ai)] = v;
@@ -1166,8 +1177,24 @@ static size_t cholqr2_small_smem(long long n, int N, bool want_r, int* S_out) {
   return bytes;
 }
 
+static int cholqr_passes(float* y, long long n, int N, long long vs, long long es, double* r, Arena& ws,
+                         DevStatus* st, cudaStream_t s, int passes, bool acc64);
+
 int launch_cholqr2(float* y, long long n, int N, long long vs, long long es, double* r,
                    Arena& ws, DevStatus* st, cudaStream_t s) {
+  return cholqr_passes(y, n, N, vs, es, r, ws, st, s, 2, true);
+}
+
+// One CholeskyQR pass with the FP32-accumulated Gram (FP64 across chunks of vectors): the
+// orthonormalisation between power iterations, which only has to keep the basis well
+// conditioned (the sketch that follows is orthonormalised by CholeskyQR2).
+int launch_orth_power(float* y, long long n, int N, long long vs, long long es, Arena& ws, DevStatus* st,
+                      cudaStream_t s) {
+  return cholqr_passes(y, n, N, vs, es, nullptr, ws, st, s, 1, false);
+}
+
+static int cholqr_passes(float* y, long long n, int N, long long vs, long long es, double* r, Arena& ws,
+                         DevStatus* st, cudaStream_t s, int passes, bool acc64) {
   if (N <= 0 || n <= 0) return TT_OK;
   if (N > TT_MAX_SMALL) {
     set_error(TT_ERR_UNSUPPORTED, "cholqr2 width %d > %d", N, TT_MAX_SMALL);
@@ -1220,8 +1247,8 @@ int launch_cholqr2(float* y, long long n, int N, long long vs, long long es, dou
     cudaFuncSetAttribute(k_apply_rinv<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
     attr_set = true;
   }
-  for (int pass = 0; pass < 2; ++pass) {
-    TT_TRY(launch_gram(y, n, N, vs, es, w, true, ws, s));
+  for (int pass = 0; pass < passes; ++pass) {
+    TT_TRY(launch_gram(y, n, N, vs, es, w, acc64, ws, s));
     k_chol_inv<<<1, 256, shm, s>>>(w, N, pass == 0 ? r1 : r2, rinv, 1e-12, ri_smem, st);
     count_launch();
     TT_LAUNCH_CHECK();
@@ -1237,7 +1264,7 @@ int launch_cholqr2(float* y, long long n, int N, long long vs, long long es, dou
     count_launch();
     TT_LAUNCH_CHECK();
   }
-  if (r) {
+  if (r && passes == 2) {
     k_mul_upper<<<ceil_div(N * N, 256), 256, 0, s>>>(r2, r1, N, r);
     count_launch();
     TT_LAUNCH_CHECK();

@@ -348,7 +348,24 @@ __global__ void __launch_bounds__(192, 1)
       __syncwarp();
       if (lane == 0) mbar_arrive(bars.tempty(buf));
       const long long j = tile * BM + q * 32 + lane;
-      if (j < n) {
+      if (mode == OUT_PERM231) {
+        // Bond permute through shared memory: for each a, the warp's 32 columns j form one
+        // contiguous run of r1 * 32 outputs (b fastest), written with coalesced stores.
+        float* stg = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(barmem) + 256) + (warp - 2) * 32 * (BN + 1);
+#pragma unroll
+        for (int c = 0; c < BN; ++c) stg[lane * (BN + 1) + c] = __uint_as_float(r[c]);
+        __syncwarp();
+        const long long jw = tile * BM + q * 32;
+        const int nj = (int)((n - jw) < 32 ? (n - jw) : 32);
+        for (int ai = 0; ai < r0; ++ai) {
+          float* dst = out + (long long)r1 * (jw + n * (long long)ai);
+          for (int f = lane; f < r1 * nj; f += 32) {
+            const int jl = f / r1, bi = f - jl * r1;
+            dst[f] = stg[jl * (BN + 1) + ai + r0 * bi];
+          }
+        }
+        __syncwarp();
+      } else if (j < n) {
         if (mode == OUT_ROWMAJOR) {
           float* o = out + j * ldo;
           if (vec) {
@@ -363,14 +380,10 @@ __global__ void __launch_bounds__(192, 1)
             for (int c = 0; c < BN; ++c)
               if (c < N) o[c] = __uint_as_float(r[c]);
           }
-        } else {
+        } else {  // OUT_COLMAJOR
 #pragma unroll
-          for (int c = 0; c < BN; ++c) {
-            if (c < N) {
-              const int ai = c % r0, bi = c / r0;
-              out[(long long)bi + (long long)r1 * (j + n * (long long)ai)] = __uint_as_float(r[c]);
-            }
-          }
+          for (int c = 0; c < BN; ++c)
+            if (c < N) out[j + ldo * (long long)c] = __uint_as_float(r[c]);
         }
       }
     }
@@ -580,7 +593,8 @@ __global__ void __launch_bounds__(192, 1)
   constexpr int BK = 32;
   constexpr uint32_t ABLK = BK * 128;           // one 32-row block, BK columns
   constexpr uint32_t STAGE_BYTES = 4 * ABLK;    // 128 rows
-  constexpr uint32_t TMEM_COLS = pow2_cols(NB);
+  constexpr uint32_t NBP = pow2_cols(NB);
+  constexpr uint32_t TMEM_COLS = pow2_cols(2 * NBP);  // two accumulators: MMA fills one while the epilogue drains the other
   constexpr uint32_t IDESC = idesc_tf32(128, NB, 1, 1);
 
   extern __shared__ uint8_t smem_raw[];
@@ -658,11 +672,13 @@ __global__ void __launch_bounds__(192, 1)
         const long long jb = (long long)u * kchunk;
         const long long je = (jb + kchunk < ncols) ? jb + kchunk : ncols;
         const int KB = (int)((je - jb + BK - 1) / BK);
-        if (!mbar_wait(bars.tempty(0), (uint32_t)(t & 1) ^ 1u, abort_flag)) {
+        const int buf = t & 1;
+        if (!mbar_wait(bars.tempty(buf), (uint32_t)((t >> 1) & 1) ^ 1u, abort_flag)) {
           ok = false;
           break;
         }
         tc_fence_after();
+        const uint32_t dacc = tmem_base + (uint32_t)buf * NBP;
         for (int kb = 0; kb < KB; ++kb) {
           if (!mbar_wait(bars.full(stage), phase, abort_flag)) {
             ok = false;
@@ -673,7 +689,7 @@ __global__ void __launch_bounds__(192, 1)
 #pragma unroll
           for (int ks = 0; ks < BK / 8; ++ks) {
             const uint64_t da = desc_mn_sw128_32b(sa + ks * 1024, ABLK, 512);
-            mma_tf32(tmem_base, da, da, IDESC, (kb | ks) ? 1u : 0u);
+            mma_tf32(dacc, da, da, IDESC, (kb | ks) ? 1u : 0u);
           }
           mma_commit(bars.empty(stage));
           if (++stage == STAGES) {
@@ -682,7 +698,7 @@ __global__ void __launch_bounds__(192, 1)
           }
         }
         if (!ok) break;
-        mma_commit(bars.tfull(0));
+        mma_commit(bars.tfull(buf));
       }
       if (!ok) {
         *abort_flag = 1;
@@ -698,7 +714,8 @@ __global__ void __launch_bounds__(192, 1)
     int t = 0;
     for (int u = blockIdx.x; u < nsplit; u += gridDim.x, ++t) {
       for (int idx = et; idx < m * m; idx += 128) gsum[(idx / m) * (m + 1) + idx % m] = 0.f;
-      const bool ok = mbar_wait(bars.tfull(0), (uint32_t)(t & 1), abort_flag);
+      const int buf = t & 1;
+      const bool ok = mbar_wait(bars.tfull(buf), (uint32_t)((t >> 1) & 1), abort_flag);
       // all four epilogue warps leave together if any of them gave up
       if (named_bar_or(1, 128, !ok)) {
         *abort_flag = 1;
@@ -706,7 +723,7 @@ __global__ void __launch_bounds__(192, 1)
         break;
       }
       tc_fence_after();
-      const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16);
+      const uint32_t taddr = tmem_base + ((uint32_t)(q * 32) << 16) + (uint32_t)buf * NBP;
       uint32_t r[NB];
 #pragma unroll
       for (int c = 0; c < NB; c += 16) tmem_ld16(taddr + c, &r[c]);
@@ -715,7 +732,7 @@ __global__ void __launch_bounds__(192, 1)
       for (int c = 0; c < NB; ++c) asm volatile("" : "+r"(r[c])::"memory");
       tc_fence_before();
       __syncwarp();
-      if (lane == 0) mbar_arrive(bars.tempty(0));
+      if (lane == 0) mbar_arrive(bars.tempty(buf));
       // Gram row (row % m) gets columns [blk*m, blk*m + m) of its diagonal block.
       const int gi = grouped ? row % m : row;
       const int c0 = grouped ? (row / m) * m : 0;
@@ -837,8 +854,9 @@ int run_project(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap&
                 int N, int KB, float* out, long long ldo, int mode, int r0, int r1, DevStatus* st,
                 cudaStream_t s) {
   constexpr uint32_t STAGE = 128 * 128 + (SPLIT ? 2 : 1) * BN * 128;
-  constexpr int STAGES = (int)std::min<size_t>(10, kSmemBudget / STAGE);
-  const size_t smem = (size_t)STAGES * STAGE + 1024 + 256;
+  constexpr size_t STAGING = 4 * 32 * (BN + 1) * sizeof(float);  // bond-permute epilogue
+  constexpr int STAGES = (int)std::min<size_t>(10, (kSmemBudget - STAGING) / STAGE);
+  const size_t smem = (size_t)STAGES * STAGE + 1024 + 256 + STAGING;
   auto kern = k_project_tc<BN, STAGES, SPLIT>;
   static bool attr = false;
   if (!attr) {
@@ -933,9 +951,11 @@ void gram_tc_plan(long long m, long long n, int* grouped, long long* ncols, int*
   const bool g = (128 % m == 0) && ((n * m) % 128 == 0);
   *grouped = g ? 1 : 0;
   *ncols = g ? (n * m) / 128 : n;
+  // Each unit's MMA accumulation runs in FP32 (TMEM); units of at most 2048 columns keep its
+  // rounding small before the FP64 sum of the unit partials.
   const int sms = g_sms > 0 ? g_sms : 148;
   long long kc = (*ncols + sms - 1) / sms;
-  kc = std::max<long long>(kc, 128);
+  kc = std::min<long long>(std::max<long long>(kc, 128), 2048);
   kc = (kc + 31) / 32 * 32;
   *kchunk = kc;
   *nsplit = (int)((*ncols + kc - 1) / kc);

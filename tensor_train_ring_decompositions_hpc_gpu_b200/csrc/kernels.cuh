@@ -29,6 +29,9 @@ size_t project_ws_bytes(long long m, long long n, int N);
 // Philox Gaussian fill (column-major rows x cols, ld).
 int launch_gaussian(float* out, long long rows, int cols, long long ld, unsigned long long seed,
                     unsigned stream_id, cudaStream_t s);
+// Rows [row0, row0 + nrows) of the (total_rows x cols) matrix launch_gaussian would produce.
+int launch_gaussian_rows(float* out, long long row0, long long nrows, long long total_rows, int cols, long long ld,
+                         unsigned long long seed, unsigned stream_id, cudaStream_t s);
 
 // Y (m x N, FP64, ld = m) = A (m x n, lda = m) * W, W element (j, c) at w[j*wj + c*wc].
 // engine: TT_GEMM_FP32 or TT_GEMM_TC.
@@ -39,10 +42,11 @@ int launch_sketch(const float* a, long long m, long long n, const float* w, int 
 int launch_reduce_splits(const double* part, long long count, int nsplit, double* y, cudaStream_t s);
 
 // Output modes of the projection.
-enum { OUT_ROWMAJOR = 0, OUT_PERM231 = 1 };
+enum { OUT_ROWMAJOR = 0, OUT_PERM231 = 1, OUT_COLMAJOR = 2 };
 
 // out = A^T Q: A (m x n, lda = m), Q (m x N, ldq).  OUT_ROWMAJOR: out[j*ldo + c];
 // OUT_PERM231: column c = a + r0*b of Q^T A goes to out[b + r1*(j + n*a)] (TR bond permute).
+// OUT_COLMAJOR: out[j + ldo*c] (A^T Q as a column-major n x N matrix).
 int launch_project(const float* a, long long m, long long n, const float* q, int N, long long ldq,
                    float* out, long long ldo, int mode, int r0, int r1, int engine, Arena& ws,
                    DevStatus* st, cudaStream_t s);
@@ -56,6 +60,9 @@ int launch_gram(const float* x, long long nvec, int M, long long vs, long long e
 // Writes R (N x N, FP64, upper) when r != nullptr.
 int launch_cholqr2(float* y, long long n, int N, long long vs, long long es, double* r,
                    Arena& ws, DevStatus* st, cudaStream_t s);
+// One CholeskyQR pass with an FP32-accumulated Gram (between power iterations).
+int launch_orth_power(float* y, long long n, int N, long long vs, long long es, Arena& ws, DevStatus* st,
+                      cudaStream_t s);
 
 // Symmetric eigen-decomposition by parallel cyclic Jacobi (FP64, N <= 128).
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps,
@@ -108,6 +115,12 @@ int launch_gemm_nn(const float* a, long long M, int K, const float* b, long long
 // and ||X||^2, where G1 is (r0, n1, r1) and M is (r1, N, r0).
 int launch_recon_err(const float* x, int n1, long long N, const float* g1, int r0, int r1,
                      const float* mrg, double* acc, cudaStream_t s);
+
+// Context accessors (driver.cu): a workspace arena of at least `bytes`, the context stream and
+// its device status word.
+int ctx_arena(tt_ctx* c, size_t bytes, Arena* ws);
+cudaStream_t ctx_stream(tt_ctx* c);
+DevStatus* ctx_status(tt_ctx* c);
 
 // out (Rout x cols) from in (Rin x cols), rows Rin..Rout-1 zero; column-major.
 int launch_expand_rows(const float* in, int Rin, float* out, int Rout, long long cols, cudaStream_t s);

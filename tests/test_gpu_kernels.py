@@ -229,3 +229,30 @@ def test_tc_rounding_bias(gpu, kind):
         assert abs(bias) < 5e-5, f"projection bias {bias:.3e}"
     else:
         assert abs(bias) < 2e-3, f"sketch bias {bias:.3e}"
+
+
+@pytest.mark.parametrize("n", [1 << 21, 3 << 20])
+def test_gram_rows_tc_resolves_graded_spectrum(gpu, n):
+    """A 32-row unfolding with singular values from 1 down to 3e-3 (eigenvalues over 5 decades,
+    like unfolding 1 of the 32^6 TT).  The tensor-core Gram accumulates in FP32 over units of
+    at most 2048 columns and in FP64 across units, so the leading eigenvalues (above 1e-2 of the
+    largest) stay within 1e-4 relative of the FP64 ones; every eigenvalue stays within 2e-6 of
+    the largest in absolute terms, the floor the TF32 rounding of the operand sets (the
+    smallest, 1e-5 of the largest, move by up to ~5 %)."""
+    import torch
+    ttr = _ttr()
+    m = 32
+    g = torch.Generator(device="cpu").manual_seed(9)
+    u, _ = torch.linalg.qr(torch.randn(m, m, generator=g, dtype=torch.float64))
+    sig = torch.logspace(0, -2.5, m, dtype=torch.float64)
+    z = torch.randn(n, m, generator=g, dtype=torch.float32).to(gpu)
+    z = z / torch.linalg.vector_norm(z, dim=0, keepdim=True)
+    a_t = (z.double() @ (u * sig).T.to(gpu)).float()  # (n x m) row-major = A (m x n) column-major
+    a = a_t.t()
+    w = ttr.gram_rows(a, "tc").cpu().numpy()
+    ad = a_t.double().cpu().numpy()
+    ref = np.sort(np.linalg.eigvalsh(ad.T @ ad))[::-1]
+    got = np.sort(np.linalg.eigvalsh(0.5 * (w + w.T)))[::-1]
+    lead = ref >= 1e-2 * ref[0]
+    np.testing.assert_allclose(got[lead], ref[lead], rtol=1e-4)
+    np.testing.assert_allclose(got, ref, rtol=0, atol=2e-6 * ref[0])

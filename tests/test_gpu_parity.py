@@ -230,3 +230,34 @@ def test_engines_agree_and_deterministic(gpu):
     ec = ttr.rel_error(xd, c.cores)
     # TF32 operands (round to nearest) add ~1e-4-level white error per projected step
     assert ea < ERR_ABS and ec < ERR_ABS and abs(ea - ec) < 5e-4
+
+
+@pytest.mark.parametrize("gemm", ["fp32", "auto"])
+@pytest.mark.parametrize("shape,ranks,noise,eps", [
+    ([16, 12, 10, 14], [1, 4, 6, 3, 1], 1e-5, 1e-3),
+    ([8, 9, 10, 11, 12], [1, 3, 5, 5, 4, 1], 1e-5, 1e-3),
+    ([32, 32, 32, 32], [1, 8, 16, 8, 1], 1e-3, 0.02),
+])
+def test_adaptive_eps_matches_oracle(gpu, gemm, shape, ranks, noise, eps):
+    """eps > 0: the ranks chosen by delta-truncation equal the oracle's and the error is <= eps."""
+    ttr = _ttr()
+    import torch
+    x = oracle.make_tt_tensor(shape, ranks, noise, seed=21)
+    xt = torch.from_numpy(np.ascontiguousarray(x.ravel(order="F"))).to(gpu)
+    maxr = [1] + [64] * (len(shape) - 1) + [1]
+    res = ttr.tt_svd(xt, maxr, gemm=gemm, eps=eps, shape=list(shape))
+    ocores, oranks = oracle.tt_svd_eps(x.astype(np.float64), eps, max_ranks=maxr)
+    assert res.ranks == oranks
+    cores = [c.double().cpu().numpy() for c in res.cores]
+    err = oracle.rel_error(x, oracle.tt_full(cores))
+    assert err <= eps * 1.001
+    # the estimate is the discarded energy carried in FP32 data: it can round down to 0
+    assert 0.0 <= res.est_rel_err <= eps * 1.001
+
+
+def test_adaptive_eps_rejects_ring(gpu):
+    ttr = _ttr()
+    import torch
+    x = torch.randn(8 * 8 * 8, device=gpu)
+    with pytest.raises(Exception):
+        ttr.tr_svd(x, [2, 2, 2, 2], eps=1e-2, shape=[8, 8, 8])

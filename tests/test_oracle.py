@@ -102,3 +102,15 @@ def test_edrsvd_restatements_recover_low_rank():
 def test_flops_model_c2():
     f = oracle.tt_flops_model([32] * 6, [1, 32, 32, 32, 32, 32, 1], 8, 0)
     assert f > 1e11
+
+
+def test_tt_svd_eps_meets_tolerance_and_recovers_ranks():
+    """delta-truncation: error <= eps and, on a noisy low-rank TT, the generating ranks."""
+    x = oracle.make_tt_tensor([6, 7, 5, 8], [1, 3, 4, 2, 1], 1e-6, seed=11).astype(np.float64)
+    cores, ranks = oracle.tt_svd_eps(x, 1e-3)
+    assert ranks == [1, 3, 4, 2, 1]
+    err = oracle.rel_error(x, oracle.tt_full(cores))
+    assert err <= 1e-3
+    cores, ranks = oracle.tt_svd_eps(x, 0.3)
+    assert oracle.rel_error(x, oracle.tt_full(cores)) <= 0.3
+    assert all(a <= b for a, b in zip(ranks, [1, 3, 4, 2, 1]))
