@@ -338,7 +338,7 @@ def run_batch(args):
         b.run(eps=BATCH["eps"])
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    clk = ClockSampler()
+    clk = ClockSampler(0)
     clk.start()
     e0.record()
     for _ in range(args.steps):

@@ -19,9 +19,13 @@
 extern "C" {
 #endif
 
-#define TTRSVD_ABI_VERSION 2
+#define TTRSVD_ABI_VERSION 3
 #define TT_MAX_ORDER 16
 #define TT_MAX_SMALL 128 /* largest Gram / Jacobi size handled on chip */
+#define TT_MLP_INPUTS 8    /* probe features per unfolding (tt_probe_features) */
+#define TT_MLP_OUTPUTS 3   /* predicted log2 rank / 10, log2 oversampling / 5, power iterations / 2 */
+#define TT_MLP_PARAMS 4931 /* 8 -> 64 -> 64 -> 3 ReLU network, packed W1 b1 W2 b2 W3 b3 */
+#define TT_PROBE_COLS 16   /* Gaussian probe columns behind the features */
 
 /* Status codes.  The reference aborts through assert() on every library status
  * (e.g. ttdecomposition/high_order_GPUs/ttdec6_singleGPU.cu:826-831); here every failure
@@ -60,7 +64,17 @@ enum {
   TT_FLAG_NO_FOLD = 4,        /* materialise full-rank steps instead of folding their rotation */
   TT_FLAG_IDENTITY_GAUGE = 8, /* full-rank steps keep the identity basis (no Gram pass) */
   TT_FLAG_KEEP_SIGMA = 16,    /* fill tt_stats.sigma */
-  TT_FLAG_PROFILE = 32        /* time the bulk passes over the largest unfolding (tt_stats.top_*) */
+  TT_FLAG_PROFILE = 32,       /* time the bulk passes over the largest unfolding (tt_stats.top_*) */
+  /* eps > 0 only.  Plain adaptive EDrSVD: the sketch width of a randomized step starts at
+   * 16 + s and doubles (up to r + s, r the caller's rank bound) until the a-posteriori error
+   * estimate ||A||^2 - ||Q^T A||^2 meets the step tolerance. */
+  TT_FLAG_ADAPTIVE_KS = 64,
+  /* eps > 0 only.  Learned EDrSVD: the context's predictor (tt_ctx_set_predictor) chooses
+   * rank, oversampling and power iterations of each randomized step from Gaussian-probe
+   * features (tt_probe_features); when the a-posteriori estimate of that attempt exceeds the
+   * step tolerance the plain adaptive EDrSVD takes over from twice its sketch width (at least
+ * the plain method's first width). */
+  TT_FLAG_LEARNED = 128
 };
 
 typedef struct tt_opts {
@@ -83,7 +97,7 @@ typedef struct tt_stats {
   float sigma[TT_MAX_ORDER][TT_STATS_MAX_SIGMA];
   int jacobi_sweeps;                           /* largest sweep count of any eigen-solve */
   int kernels;                                 /* kernels launched by the call */
-  double est_rel_err;                          /* reserved (adaptive-rank error estimate) */
+  double est_rel_err;                          /* eps > 0: sqrt(discarded energy / ||X||^2) */
   double flops;                                /* algorithmic FLOPs of the bulk GEMM passes executed */
   double bytes;                                /* algorithmic HBM bytes of those passes (operands once) */
   /* TT_FLAG_PROFILE: per pass kind (TT_PASS_*), summed device time (CUDA events on the
@@ -97,6 +111,11 @@ typedef struct tt_stats {
   int top_step;
   double top_ms;
   double top_bytes;
+  int passes;                      /* bulk passes over unfoldings (Gram, sketch, projection, probe) */
+  int fallbacks;                   /* TT_FLAG_LEARNED: steps the plain adaptive EDrSVD took over */
+  int step_ks[TT_MAX_ORDER];       /* sketch width finally used per unfolding (0: exact step) */
+  int step_power[TT_MAX_ORDER];    /* power iterations finally used per unfolding */
+  int step_attempts[TT_MAX_ORDER]; /* EDrSVD attempts per unfolding */
 } tt_stats;
 
 /* Bulk pass kinds reported in tt_stats.pass_*. */
@@ -210,6 +229,31 @@ int tt_svd_batched(tt_ctx* ctx, int count, int d, const int* n, const float* x, 
                    double eps, int rmax, int oversample, unsigned long long seed, float* cores,
                    const long long* core_off, int* ranks, double* err_est);
 long long tt_batch_core_capacity(int d, const int* n, int rmax);
+
+/* Learned EDrSVD parameters.  A 8 -> 64 -> 64 -> 3 ReLU network maps the probe features of
+ * an unfolding to (log2 rank / 10, log2 oversampling / 5, power iterations / 2); it is trained
+ * by the library's own kernels (tt_mlp_train) on labels of the plain method.  All pointers
+ * are device pointers unless stated.  No counterpart in the reference, whose EDrSVD takes
+ * fixed s and p (ttdecomposition/third_order_GPUs/opt/ttdec_gpu_float_rsvd_lu_half.cu:797-798). */
+/* Install (host params, TT_MLP_PARAMS floats) or clear (NULL) the predictor of TT_FLAG_LEARNED. */
+int tt_ctx_set_predictor(tt_ctx* ctx, const float* params);
+/* Features of the (m x n) unfolding a: a Gaussian probe Y = A Omega with TT_PROBE_COLS columns
+ * (Philox `seed`, stream `stream_id`), the eigenvalues mu of Y^T Y, and
+ * [log2(min(m,n))/10, log10(mu_j/mu_1)/4 for j = 2,4,8,12,16, log10(16 E/mu_1)/4, log10(tol)/4]
+ * with E = ||A||_F^2 (`energy`; computed when < 0) and `tol` the step's relative tolerance. */
+int tt_probe_features(tt_ctx* ctx, const float* a, long long m, long long n, double energy, double tol,
+                      unsigned long long seed, unsigned stream_id, float* features);
+/* y (n x 3, row-major) = network(x (n x 8, row-major)). */
+int tt_mlp_forward(tt_ctx* ctx, const float* params, const float* x, int n, float* y);
+/* Gradient (TT_MLP_PARAMS floats) and value (1 float, may be NULL) of the mean over the n
+ * samples of the summed squared output error against t (n x 3). */
+int tt_mlp_grad(tt_ctx* ctx, const float* params, const float* x, const float* t, int n, float* grad, float* loss);
+/* `steps` Adam steps (lr, beta 0.9 / 0.999, bias-corrected from step step0 + 1) on minibatches
+ * of `batch` samples drawn with replacement from the n samples (Philox `seed`); params,
+ * adam_m and adam_v are updated in place; loss_trace (steps floats, may be NULL) receives
+ * each minibatch's loss before its update.  One persistent single-CTA launch. */
+int tt_mlp_train(tt_ctx* ctx, float* params, float* adam_m, float* adam_v, const float* x, const float* t, int n,
+                 int steps, int batch, float lr, int step0, unsigned long long seed, float* loss_trace);
 
 /* Core files.  The reference frees its cores before returning (ttdec6_singleGPU.cu:947-952)
  * and has no file format; this one stores a decomposition for later use.  Layout

@@ -19,14 +19,15 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import (TT_FLAG_CHECK_FINITE, TT_FLAG_HOST_IO, TT_FLAG_IDENTITY_GAUGE, TT_FLAG_KEEP_SIGMA,
-                   TT_FLAG_NO_FOLD, TT_GEMM_AUTO, TT_GEMM_FP32, TT_GEMM_TC, TT_METHOD_EDRSVD,
-                   TT_METHOD_EXACT, TTError, check)
+from ._lib import (TT_FLAG_ADAPTIVE_KS, TT_FLAG_CHECK_FINITE, TT_FLAG_HOST_IO, TT_FLAG_IDENTITY_GAUGE,
+                   TT_FLAG_KEEP_SIGMA, TT_FLAG_LEARNED, TT_FLAG_NO_FOLD, TT_GEMM_AUTO, TT_GEMM_FP32, TT_GEMM_TC,
+                   TT_METHOD_EDRSVD, TT_METHOD_EXACT, TTError, check)
 
 __all__ = [
     "tt_svd", "tr_svd", "rel_error", "Result", "gaussian", "sketch", "project", "gram_rows",
     "gram_tall", "cholqr2", "syev", "permute231", "ttdec_gpu_float", "trdec_gpu_float",
     "ttdec_half_lu_device_6", "trdec_half_lu_device_6", "TTError", "lib", "GEMM", "METHOD",
+    "set_predictor", "probe_features", "mlp_forward", "mlp_grad", "mlp_train",
 ]
 
 GEMM = {"auto": TT_GEMM_AUTO, "tc": TT_GEMM_TC, "fp32": TT_GEMM_FP32}
@@ -103,6 +104,11 @@ class Result:
     kernels: int = 0
     jacobi_sweeps: int = 0
     est_rel_err: float = 0.0
+    passes: int = 0
+    fallbacks: int = 0
+    step_ks: list = field(default_factory=list)
+    step_power: list = field(default_factory=list)
+    step_attempts: list = field(default_factory=list)
 
 
 def _opts(gemm, method, oversample, power_iters, seed, flags, max_sweeps):
@@ -164,8 +170,11 @@ def _run(ring: bool, x, ranks, gemm="auto", method="edrsvd", oversample=8, power
         cores = [_core_view(flat[k][: rr[k] * shape[k] * rr[k + 1]], rr[k], shape[k], rr[k + 1])
                  for k in range(d)]
     sig = [np.array(st.sigma[k][: st.nsigma[k]], dtype=np.float64) for k in range(st.nsteps)]
+    ns = int(st.nsteps)
     return Result(cores=cores, ms=st.ms, sigmas=sig, ranks=list(st.ranks[: len(ranks)]),
-                  kernels=st.kernels, jacobi_sweeps=st.jacobi_sweeps, est_rel_err=st.est_rel_err)
+                  kernels=st.kernels, jacobi_sweeps=st.jacobi_sweeps, est_rel_err=st.est_rel_err,
+                  passes=st.passes, fallbacks=st.fallbacks, step_ks=list(st.step_ks[:ns]),
+                  step_power=list(st.step_power[:ns]), step_attempts=list(st.step_attempts[:ns]))
 
 
 def tt_svd(x, ranks, **kw) -> Result:
@@ -295,6 +304,64 @@ def permute231(x, r0: int, r1: int, n: int):
     out = torch.empty_like(x)
     check(lib().tt_k_permute231(_ctx_for(x.device.index), _ptr(x), _ptr(out), r0, r1, n))
     return out
+
+
+# ---- learned EDrSVD parameters ----
+def set_predictor(params, device=None):
+    """Install the predictor (TT_MLP_PARAMS floats; None clears it) in the device's context."""
+    torch = _torch()
+    dev = device if device is not None else torch.device("cuda", torch.cuda.current_device())
+    ctx = _ctx_for(dev.index if isinstance(dev, torch.device) else dev)
+    if params is None:
+        check(lib().tt_ctx_set_predictor(ctx, None))
+        return
+    p = np.ascontiguousarray(np.asarray(params, dtype=np.float32).ravel())
+    if p.size != _lib.TT_MLP_PARAMS:
+        raise ValueError(f"predictor needs {_lib.TT_MLP_PARAMS} parameters, got {p.size}")
+    check(lib().tt_ctx_set_predictor(ctx, C.c_void_p(p.ctypes.data)))
+
+
+def probe_features(a, energy=-1.0, tol=1e-3, seed=1234, stream_id=0):
+    """The TT_MLP_INPUTS probe features of a column-major (m x n) FP32 CUDA matrix."""
+    torch = _torch()
+    a = _as_colmajor(a.float())
+    m, n = a.shape
+    out = torch.empty(_lib.TT_MLP_INPUTS, dtype=torch.float32, device=a.device)
+    check(lib().tt_probe_features(_ctx_for(a.device.index), _ptr(a), m, n, float(energy), float(tol), int(seed),
+                                  int(stream_id), _ptr(out)))
+    return out
+
+
+def mlp_forward(params, x):
+    """Network outputs (n x 3) for features x (n x 8), both CUDA FP32 row-major."""
+    torch = _torch()
+    x = x.float().contiguous()
+    y = torch.empty((x.shape[0], _lib.TT_MLP_OUTPUTS), dtype=torch.float32, device=x.device)
+    check(lib().tt_mlp_forward(_ctx_for(x.device.index), _ptr(params.contiguous()), _ptr(x), int(x.shape[0]), _ptr(y)))
+    return y
+
+
+def mlp_grad(params, x, t):
+    """(gradient, loss) of the mean summed squared error over the batch."""
+    torch = _torch()
+    x = x.float().contiguous()
+    t = t.float().contiguous()
+    g = torch.empty(_lib.TT_MLP_PARAMS, dtype=torch.float32, device=x.device)
+    loss = torch.empty(1, dtype=torch.float32, device=x.device)
+    check(lib().tt_mlp_grad(_ctx_for(x.device.index), _ptr(params.contiguous()), _ptr(x), _ptr(t),
+                            int(x.shape[0]), _ptr(g), _ptr(loss)))
+    return g, loss
+
+
+def mlp_train(params, adam_m, adam_v, x, t, steps, batch=256, lr=1e-3, step0=0, seed=1234):
+    """Adam steps in place on CUDA tensors params / adam_m / adam_v; returns the loss trace."""
+    torch = _torch()
+    x = x.float().contiguous()
+    t = t.float().contiguous()
+    trace = torch.empty(max(int(steps), 1), dtype=torch.float32, device=x.device)
+    check(lib().tt_mlp_train(_ctx_for(x.device.index), _ptr(params), _ptr(adam_m), _ptr(adam_v), _ptr(x), _ptr(t),
+                             int(x.shape[0]), int(steps), int(batch), float(lr), int(step0), int(seed), _ptr(trace)))
+    return trace[: int(steps)]
 
 
 # ---- batched small tensors ----

@@ -17,6 +17,8 @@ TT_GEMM_AUTO, TT_GEMM_TC, TT_GEMM_FP32 = 0, 1, 2
 TT_METHOD_EDRSVD, TT_METHOD_EXACT = 0, 1
 TT_FLAG_HOST_IO, TT_FLAG_CHECK_FINITE, TT_FLAG_NO_FOLD, TT_FLAG_IDENTITY_GAUGE, TT_FLAG_KEEP_SIGMA = 1, 2, 4, 8, 16
 TT_FLAG_PROFILE = 32
+TT_FLAG_ADAPTIVE_KS, TT_FLAG_LEARNED = 64, 128
+TT_MLP_INPUTS, TT_MLP_OUTPUTS, TT_MLP_PARAMS, TT_PROBE_COLS = 8, 3, 4931, 16
 TT_PASS_GRAM, TT_PASS_SKETCH, TT_PASS_PROJECT, TT_PASS_OTHER = 0, 1, 2, 3
 PASS_NAMES = ["gram", "sketch", "project", "other"]
 TT_MAX_ORDER = 16
@@ -30,6 +32,7 @@ EXPORTED = [
     "tt_k_sketch", "tt_k_project", "tt_k_gram_rows", "tt_k_gram_tall", "tt_k_cholqr2",
     "tt_k_syev", "tt_k_sketch_noalloc", "tt_svd_batched", "tt_batch_core_capacity",
     "tt_cores_save", "tt_cores_header", "tt_cores_load",
+    "tt_ctx_set_predictor", "tt_probe_features", "tt_mlp_forward", "tt_mlp_grad", "tt_mlp_train",
     "tt_k_permute231", "tt_ref_ttdec_gpu_float", "tt_ref_trdec_gpu_float",
     "tt_ref_ttdec_half_lu_device_6", "tt_ref_trdec_half_lu_device_6",
 ]
@@ -51,6 +54,8 @@ class TTStats(C.Structure):
         ("flops", C.c_double), ("bytes", C.c_double), ("pass_ms", C.c_double * 4),
         ("pass_bytes", C.c_double * 4), ("pass_launches", C.c_int * 4),
         ("top_kind", C.c_int), ("top_step", C.c_int), ("top_ms", C.c_double), ("top_bytes", C.c_double),
+        ("passes", C.c_int), ("fallbacks", C.c_int), ("step_ks", C.c_int * TT_MAX_ORDER),
+        ("step_power", C.c_int * TT_MAX_ORDER), ("step_attempts", C.c_int * TT_MAX_ORDER),
     ]
 
 
@@ -97,6 +102,11 @@ def load():
         "tt_k_gaussian_rows": (i, [vp, vp, ll, ll, ll, i, ll, ull, C.c_uint]),
         "tt_svd_batched": (i, [vp, i, i, P(i), vp, P(ll), d, i, i, C.c_ulonglong, vp, P(ll), P(i), P(d)]),
         "tt_batch_core_capacity": (ll, [i, P(i), i]),
+        "tt_ctx_set_predictor": (i, [vp, vp]),
+        "tt_probe_features": (i, [vp, vp, ll, ll, d, d, ull, C.c_uint, vp]),
+        "tt_mlp_forward": (i, [vp, vp, vp, i, vp]),
+        "tt_mlp_grad": (i, [vp, vp, vp, vp, i, vp, vp]),
+        "tt_mlp_train": (i, [vp, vp, vp, vp, vp, vp, i, i, i, C.c_float, i, ull, vp]),
         "tt_cores_save": (i, [C.c_char_p, i, P(i), P(i), i, P(vp), i]),
         "tt_cores_header": (i, [C.c_char_p, P(i), P(i), P(i), P(i)]),
         "tt_cores_load": (i, [C.c_char_p, P(vp), i]),

@@ -43,6 +43,7 @@ struct tt_ctx {
   double* hsig = nullptr;
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> pool;  // per-pass timing events (TT_FLAG_PROFILE)
+  float* pred = nullptr;          // predictor parameters, then features (8) and outputs (3)
 };
 
 extern "C" const char* tt_last_error(void) { return ttr::g_err; }
@@ -109,6 +110,7 @@ extern "C" int tt_ctx_destroy(tt_ctx* c) {
   if (c->ev0) cudaEventDestroy(c->ev0);
   if (c->ev1) cudaEventDestroy(c->ev1);
   for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
+  if (c->pred) cudaFree(c->pred);
   delete c;
   return TT_OK;
 }
@@ -119,6 +121,30 @@ extern "C" int tt_ctx_set_stream(tt_ctx* c, void* stream) {
     return TT_ERR_ARG;
   }
   c->stream = reinterpret_cast<cudaStream_t>(stream);
+  return TT_OK;
+}
+
+extern "C" int tt_ctx_set_predictor(tt_ctx* c, const float* params) {
+  if (!c) {
+    set_error(TT_ERR_ARG, "null ctx");
+    return TT_ERR_ARG;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  if (!params) {
+    if (c->pred) {
+      if (c->stream) TT_CUDA(cudaStreamSynchronize(c->stream));
+      cudaFree(c->pred);
+    }
+    c->pred = nullptr;
+    return TT_OK;
+  }
+  if (!c->pred && cudaMalloc(&c->pred, sizeof(float) * (TT_MLP_PARAMS + 16)) != cudaSuccess) {
+    c->pred = nullptr;
+    set_error(TT_ERR_NOMEM, "predictor allocation");
+    return TT_ERR_NOMEM;
+  }
+  TT_CUDA(cudaMemcpyAsync(c->pred, params, sizeof(float) * TT_MLP_PARAMS, cudaMemcpyHostToDevice, c->stream));
+  TT_CUDA(cudaStreamSynchronize(c->stream));
   return TT_OK;
 }
 
@@ -286,11 +312,16 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
       P.max_omega = std::max<size_t>(P.max_omega, (size_t)st.cols * st.ks);
       P.max_y = std::max<size_t>(P.max_y, (size_t)st.m * st.ks);
       P.max_bt = std::max<size_t>(P.max_bt, (size_t)st.cols * st.ks);
-      P.max_ws = std::max(P.max_ws, sketch_ws_bytes(st.m, st.cols, st.ks));
-      P.max_ws = std::max(P.max_ws, gram_ws_bytes(st.cols, st.ks));
-      P.max_ws = std::max(P.max_ws, gram_ws_bytes(st.m, st.ks));
-      P.max_ws = std::max(P.max_ws, gram_tc_ws_bytes(st.ks, st.cols));
-      P.max_ws = std::max(P.max_ws, project_ws_bytes(st.m, st.cols, st.ks));
+      // the adaptive modes run narrower sketches (and the probe) within the same buffers
+      const bool narrow = (o.flags & (TT_FLAG_ADAPTIVE_KS | TT_FLAG_LEARNED)) != 0;
+      for (int w = narrow ? 1 : st.ks; w <= st.ks; ++w) {
+        P.max_ws = std::max(P.max_ws, sketch_ws_bytes(st.m, st.cols, w));
+        P.max_ws = std::max(P.max_ws, gram_ws_bytes(st.cols, w));
+        P.max_ws = std::max(P.max_ws, gram_ws_bytes(st.m, w));
+        P.max_ws = std::max(P.max_ws, gram_tc_ws_bytes(w, st.cols));
+        P.max_ws = std::max(P.max_ws, project_ws_bytes(st.m, st.cols, w));
+        P.max_ws = std::max(P.max_ws, project_ws_bytes(w, st.cols, std::min(w, st.r_req)));
+      }
       P.max_ws = std::max(P.max_ws, project_ws_bytes(st.ks, st.cols, st.r_req));
     } else {
       P.max_ws = std::max(P.max_ws, project_ws_bytes(st.m, st.cols, st.r_req));
@@ -508,9 +539,12 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
   const double* pend = nullptr;  // pending rotation (rows_in x rows_in), or null
   int pend_slot = 0;
   const int nsteps = (int)P.steps.size();
+  int npasses = 0, natt = 0, nfall = 0;  // bulk passes, EDrSVD attempts, learned fallbacks
+  std::vector<int> step_ks((size_t)nsteps, 0), step_pw((size_t)nsteps, 0), step_att((size_t)nsteps, 0);
   for (int k = 0; k < nsteps; ++k) {
     Step& st = P.steps[k];
     pass.cur_step = k;
+    const int natt0 = natt;
     const long long m = st.m, cols = st.cols;
     int rq = st.r_req, re = st.r_eff;
     int nout = st.n_out;                            // rows of the next data (compacted)
@@ -567,6 +601,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
     }
 
     if (st.path == PATH_EXACT_ROWS) {
+      npasses += st.fold ? 1 : 2;
       TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols, [&] {
         if (engine == TT_GEMM_TC) {
           const int rc = launch_gram_tc(cur, m, cols, B.w, ws, c->dstat, s);
@@ -600,6 +635,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
                               engine, ws, c->dstat, s);
       }));
     } else if (st.path == PATH_EXACT_COLS) {
+      npasses += 2;
       // W = A^T A over the rows of A (vectors = rows i, components = columns)
       TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * cols * cols, 4.0 * m * cols,
                       [&] { return launch_gram(cur, m, (int)cols, 1, m, B.w, true, ws, s); }));
@@ -626,45 +662,124 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         TT_TRY(launch_sigma_vt(B.evals, B.evecs, (int)cols, nout, re, next, s));
       }
     } else {  // PATH_RAND
-      const int ks = st.ks;
-      TT_TRY(launch_gaussian(B.omega, cols, ks, cols, o.seed, (unsigned)k, s));
-      const double fl_pass = 2.0 * m * cols * ks;
-      const double by_pass = 4.0 * m * cols + 4.0 * cols * ks;
-      TT_TRY(pass.run(TT_PASS_SKETCH, fl_pass, by_pass, [&] {
-        return launch_sketch(cur, m, cols, B.omega, ks, 1, cols, B.yd, engine, ws, c->dstat, s);
-      }));
-      TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, ks, B.yf, m, ks, s));
-      TT_TRY(launch_cholqr2(B.yf, m, ks, 1, m, nullptr, ws, c->dstat, s));
-      for (int it = 0; it < o.power_iters; ++it) {
-        // Z = A^T Q written column-major (cols x ks), the layout the sketch reads W in
-        TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
-          return launch_project(cur, m, cols, B.yf, ks, m, B.bt, cols, OUT_COLMAJOR, 1, 1, engine, ws, c->dstat, s);
-        }));
-        TT_TRY(pass.run(TT_PASS_OTHER, 6.0 * cols * ks * ks, 24.0 * cols * ks, [&] {
-          return launch_orth_power(B.bt, cols, ks, 1, cols, ws, c->dstat, s);
-        }));
+      // One EDrSVD attempt with sketch width ksa and pwa power iterations: Q (B.yf), B^T
+      // (B.bt), the eigen-decomposition of B B^T (B.evals / B.evecs), sigma stored.
+      auto attempt = [&](int ksa, int pwa, unsigned sid) -> int {
+        TT_TRY(launch_gaussian(B.omega, cols, ksa, cols, o.seed, sid, s));
+        const double fl_pass = 2.0 * m * cols * ksa;
+        const double by_pass = 4.0 * m * cols + 4.0 * cols * ksa;
         TT_TRY(pass.run(TT_PASS_SKETCH, fl_pass, by_pass, [&] {
-          return launch_sketch(cur, m, cols, B.bt, ks, 1, cols, B.yd, engine, ws, c->dstat, s);
+          return launch_sketch(cur, m, cols, B.omega, ksa, 1, cols, B.yd, engine, ws, c->dstat, s);
         }));
-        TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, ks, B.yf, m, ks, s));
-        TT_TRY(launch_cholqr2(B.yf, m, ks, 1, m, nullptr, ws, c->dstat, s));
-      }
-      // B^T = A^T Q (cols x ks, row-major) = B (ks x cols, column-major)
-      TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
-        return launch_project(cur, m, cols, B.yf, ks, m, B.bt, ks, OUT_ROWMAJOR, 1, 1, engine, ws, c->dstat, s);
-      }));
-      // Gram of the small factor B (ks x cols, column-major = B^T row-major): the input of the
-      // eigen-based small SVD (TT3O:717), on the tensor cores for long B.
-      TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ks * ks, 4.0 * cols * ks, [&] {
-        if (engine == TT_GEMM_TC) {
-          const int rc = launch_gram_tc(B.bt, ks, cols, B.w, ws, c->dstat, s);
-          if (rc != TT_ERR_UNSUPPORTED) return rc;
+        TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, ksa, B.yf, m, ksa, s));
+        TT_TRY(launch_cholqr2(B.yf, m, ksa, 1, m, nullptr, ws, c->dstat, s));
+        for (int it = 0; it < pwa; ++it) {
+          // Z = A^T Q written column-major (cols x ksa), the layout the sketch reads W in
+          TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
+            return launch_project(cur, m, cols, B.yf, ksa, m, B.bt, cols, OUT_COLMAJOR, 1, 1, engine, ws, c->dstat,
+                                  s);
+          }));
+          TT_TRY(pass.run(TT_PASS_OTHER, 6.0 * cols * ksa * ksa, 24.0 * cols * ksa, [&] {
+            return launch_orth_power(B.bt, cols, ksa, 1, cols, ws, c->dstat, s);
+          }));
+          TT_TRY(pass.run(TT_PASS_SKETCH, fl_pass, by_pass, [&] {
+            return launch_sketch(cur, m, cols, B.bt, ksa, 1, cols, B.yd, engine, ws, c->dstat, s);
+          }));
+          TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, ksa, B.yf, m, ksa, s));
+          TT_TRY(launch_cholqr2(B.yf, m, ksa, 1, m, nullptr, ws, c->dstat, s));
         }
-        return launch_gram(B.bt, cols, ks, ks, 1, B.w, true, ws, s);
-      }));
-      TT_TRY(launch_syev(B.w, ks, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
-      k_store_sigma<<<1, 64, 0, s>>>(B.evals, std::min(ks, TT_STATS_MAX_SIGMA), sigdst);
-      count_launch();
+        // B^T = A^T Q (cols x ksa, row-major) = B (ksa x cols, column-major)
+        TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
+          return launch_project(cur, m, cols, B.yf, ksa, m, B.bt, ksa, OUT_ROWMAJOR, 1, 1, engine, ws, c->dstat, s);
+        }));
+        // Gram of the small factor B (ksa x cols, column-major = B^T row-major): the input of
+        // the eigen-based small SVD (TT3O:717), on the tensor cores for long B.
+        TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ksa * ksa, 4.0 * cols * ksa, [&] {
+          if (engine == TT_GEMM_TC) {
+            const int rc = launch_gram_tc(B.bt, ksa, cols, B.w, ws, c->dstat, s);
+            if (rc != TT_ERR_UNSUPPORTED) return rc;
+          }
+          return launch_gram(B.bt, cols, ksa, ksa, 1, B.w, true, ws, s);
+        }));
+        TT_TRY(launch_syev(B.w, ksa, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
+        k_store_sigma<<<1, 64, 0, s>>>(B.evals, std::min(ksa, TT_STATS_MAX_SIGMA), sigdst);
+        count_launch();
+        npasses += 2 + 2 * pwa;
+        ++natt;
+        return TT_OK;
+      };
+      // Energy outside the attempt's subspace plus nothing discarded yet: ||A||^2 - ||B||^2.
+      auto outside = [&](int ksa, double* out) -> int {
+        std::vector<double> lam((size_t)ksa);
+        TT_CUDA(cudaMemcpyAsync(lam.data(), B.evals, sizeof(double) * ksa, cudaMemcpyDeviceToHost, s));
+        TT_CUDA(cudaStreamSynchronize(s));
+        double kept = 0.0;
+        for (double v : lam) kept += std::max(v, 0.0);
+        *out = energy - kept;
+        return TT_OK;
+      };
+      const int ks_cap = st.ks;
+      int ks = ks_cap, pw = o.power_iters;
+      const bool adapt_ks = adaptive && (o.flags & (TT_FLAG_ADAPTIVE_KS | TT_FLAG_LEARNED));
+      if (!adapt_ks) {
+        TT_TRY(attempt(ks, pw, (unsigned)k));
+      } else {
+        bool done = false;
+        int ks_next = std::min(ks_cap, 16 + std::max(0, o.oversample));
+        unsigned sid = (unsigned)k;
+        if ((o.flags & TT_FLAG_LEARNED) && ks_cap >= TT_PROBE_COLS) {
+          if (!c->pred) {
+            set_error(TT_ERR_ARG, "TT_FLAG_LEARNED without a predictor (tt_ctx_set_predictor)");
+            return TT_ERR_ARG;
+          }
+          // probe: Y0 = A Omega0 (TT_PROBE_COLS columns), eigenvalues of Y0^T Y0, features
+          float* feat = c->pred + TT_MLP_PARAMS;
+          float* yout = feat + TT_MLP_INPUTS;
+          TT_TRY(launch_gaussian(B.omega, cols, TT_PROBE_COLS, cols, o.seed, 0x40000000u + (unsigned)k, s));
+          TT_TRY(pass.run(TT_PASS_SKETCH, 2.0 * m * cols * TT_PROBE_COLS, 4.0 * m * cols + 4.0 * cols * TT_PROBE_COLS,
+                          [&] {
+                            return launch_sketch(cur, m, cols, B.omega, TT_PROBE_COLS, 1, cols, B.yd, engine, ws,
+                                                 c->dstat, s);
+                          }));
+          ++npasses;
+          TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, TT_PROBE_COLS, B.yf, m, TT_PROBE_COLS, s));
+          TT_TRY(launch_gram(B.yf, m, TT_PROBE_COLS, 1, m, B.w, true, ws, s));
+          TT_TRY(launch_syev(B.w, TT_PROBE_COLS, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
+          const double tol = energy > 0.0 ? std::sqrt(delta2 / energy) : 1.0;
+          TT_TRY(launch_probe_features(B.evals, energy, tol, m, cols, feat, s));
+          TT_TRY(launch_mlp_forward(c->pred, feat, 1, yout, s));
+          float hy[TT_MLP_OUTPUTS];
+          TT_CUDA(cudaMemcpyAsync(hy, yout, sizeof(hy), cudaMemcpyDeviceToHost, s));
+          TT_CUDA(cudaStreamSynchronize(s));
+          // decode: rank 2^(10 y0), oversampling 2^(5 y1), power iterations 2 y2
+          const double rh = std::max(1.0, std::round(std::exp2(std::min(10.0 * (double)hy[0], 10.0))));
+          const int sh = (int)std::lround(std::exp2(std::min(std::max(5.0 * (double)hy[1], 1.0), 5.0)));
+          pw = (int)std::lround(std::min(std::max(2.0 * (double)hy[2], 0.0), 3.0));
+          ks = (int)std::min<double>((double)ks_cap, std::max(1.0, rh + sh));
+          TT_TRY(attempt(ks, pw, sid));
+          double out = 0.0;
+          TT_TRY(outside(ks, &out));
+          if (out <= delta2 || ks >= ks_cap) {
+            done = true;
+          } else {
+            ++nfall;
+            ks_next = std::min(ks_cap, std::max(2 * ks, ks_next));
+            pw = o.power_iters;
+          }
+        }
+        while (!done) {
+          ks = ks_next;
+          pw = o.power_iters;
+          TT_TRY(attempt(ks, pw, sid + 0x1000u * (unsigned)natt));
+          double out = 0.0;
+          TT_TRY(outside(ks, &out));
+          if (out <= delta2 || ks >= ks_cap) done = true;
+          ks_next = std::min(ks_cap, 2 * ks);
+        }
+      }
+      step_ks[k] = ks;
+      step_pw[k] = pw;
+      step_att[k] = natt - natt0;
       TT_TRY(decide(ks));
       // core = Q E_r with canonical column signs (E's columns follow)
       float* ubuf = B.corebuf;
@@ -712,6 +827,13 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
     stats->nsteps = nsteps;
     for (int k = 0; k <= P.d; ++k) stats->ranks[k] = P.r[k];
     stats->est_rel_err = adaptive && xnorm2 > 0.0 ? std::sqrt(tail_sum / xnorm2) : 0.0;
+    stats->passes = npasses;
+    stats->fallbacks = nfall;
+    for (int k = 0; k < nsteps && k < TT_MAX_ORDER; ++k) {
+      stats->step_ks[k] = step_ks[(size_t)k];
+      stats->step_power[k] = step_pw[(size_t)k];
+      stats->step_attempts[k] = step_att[(size_t)k];
+    }
     for (int k = 0; k < nsteps; ++k) {
       int cnt = 0;
       for (int i = 0; i < TT_STATS_MAX_SIGMA; ++i) {
@@ -762,6 +884,14 @@ int run_entry(tt_ctx* c, const float* x, int d, const int* n, const int* r, cons
     tt_default_opts(&o);
   if (o.eps < 0.0 || o.eps != o.eps) {
     set_error(TT_ERR_ARG, "eps must be >= 0");
+    return TT_ERR_ARG;
+  }
+  if ((o.flags & (TT_FLAG_ADAPTIVE_KS | TT_FLAG_LEARNED)) && !(o.eps > 0.0)) {
+    set_error(TT_ERR_ARG, "TT_FLAG_ADAPTIVE_KS / TT_FLAG_LEARNED need eps > 0");
+    return TT_ERR_ARG;
+  }
+  if ((o.flags & TT_FLAG_LEARNED) && !c->pred) {
+    set_error(TT_ERR_ARG, "TT_FLAG_LEARNED without a predictor (tt_ctx_set_predictor)");
     return TT_ERR_ARG;
   }
   if (o.eps > 0.0) {
@@ -926,6 +1056,106 @@ extern "C" int tt_k_gaussian_rows(tt_ctx* c, float* out, long long row0, long lo
   }
   TT_CUDA(cudaSetDevice(c->device));
   TT_TRY(launch_gaussian_rows(out, row0, nrows, total_rows, cols, ld, seed, stream_id, c->stream));
+  return TT_OK;
+}
+
+extern "C" int tt_probe_features(tt_ctx* c, const float* a, long long m, long long n, double energy, double tol,
+                                 unsigned long long seed, unsigned stream_id, float* features) {
+  TT_NEED(c);
+  TT_NEED(a);
+  TT_NEED(features);
+  if (m < 1 || n < 1) {
+    set_error(TT_ERR_SHAPE, "probe_features shape %lld x %lld", m, n);
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  const int P = TT_PROBE_COLS;
+  tt_opts o;
+  tt_default_opts(&o);
+  const int engine = engine_for(o, m, n);
+  const size_t bytes = sizeof(float) * (size_t)n * P + sizeof(double) * (size_t)m * P + sizeof(float) * (size_t)m * P +
+                       sizeof(double) * (2 * P * P + P + 2) + sketch_ws_bytes(m, n, P) + gram_ws_bytes(m, P) +
+                       (size_t)TT_MAX_SMALL * TT_MAX_SMALL * sizeof(double) * 8 + 16 * 4096;
+  Arena ws;
+  TT_TRY(ws_for(c, bytes, ws));
+  float* om = ws.take<float>((size_t)n * P);
+  double* yd = ws.take<double>((size_t)m * P);
+  float* yf = ws.take<float>((size_t)m * P);
+  double* w = ws.take<double>((size_t)P * P);
+  double* ev = ws.take<double>((size_t)P);
+  double* vec = ws.take<double>((size_t)P * P);
+  double* acc = ws.take<double>(2);
+  if (!om || !yd || !yf || !w || !ev || !vec || !acc) {
+    set_error(TT_ERR_NOMEM, "probe workspace");
+    return TT_ERR_NOMEM;
+  }
+  cudaStream_t s = c->stream;
+  TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), s));
+  if (energy < 0.0) {
+    TT_CUDA(cudaMemsetAsync(acc, 0, 2 * sizeof(double), s));
+    TT_TRY(launch_diff_norm(a, nullptr, m * n, acc, s));
+    double h[2];
+    TT_CUDA(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, s));
+    TT_CUDA(cudaStreamSynchronize(s));
+    energy = h[1];
+  }
+  TT_TRY(launch_gaussian(om, n, P, n, seed, stream_id, s));
+  TT_TRY(launch_sketch(a, m, n, om, P, 1, n, yd, engine, ws, c->dstat, s));
+  TT_TRY(launch_f64_to_f32_cols(yd, m, m, P, yf, m, P, s));
+  TT_TRY(launch_gram(yf, m, P, 1, m, w, true, ws, s));
+  TT_TRY(launch_syev(w, P, ev, vec, 40, ws, c->dstat, s));
+  TT_TRY(launch_probe_features(ev, energy, tol, m, n, features, s));
+  return check_status(c);
+}
+
+extern "C" int tt_mlp_forward(tt_ctx* c, const float* params, const float* x, int n, float* y) {
+  TT_NEED(c);
+  TT_NEED(params);
+  TT_NEED(x);
+  TT_NEED(y);
+  if (n < 0) {
+    set_error(TT_ERR_SHAPE, "mlp_forward n = %d", n);
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  TT_TRY(launch_mlp_forward(params, x, n, y, c->stream));
+  return TT_OK;
+}
+
+extern "C" int tt_mlp_grad(tt_ctx* c, const float* params, const float* x, const float* t, int n, float* grad,
+                           float* loss) {
+  TT_NEED(c);
+  TT_NEED(params);
+  TT_NEED(x);
+  TT_NEED(t);
+  TT_NEED(grad);
+  if (n < 1) {
+    set_error(TT_ERR_SHAPE, "mlp_grad n = %d", n);
+    return TT_ERR_SHAPE;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  TT_TRY(launch_mlp_train(const_cast<float*>(params), nullptr, nullptr, x, t, n, 1, n, 0.f, 0, 0ull, loss, grad, 1,
+                          c->stream));
+  return TT_OK;
+}
+
+extern "C" int tt_mlp_train(tt_ctx* c, float* params, float* adam_m, float* adam_v, const float* x, const float* t,
+                            int n, int steps, int batch, float lr, int step0, unsigned long long seed,
+                            float* loss_trace) {
+  TT_NEED(c);
+  TT_NEED(params);
+  TT_NEED(adam_m);
+  TT_NEED(adam_v);
+  TT_NEED(x);
+  TT_NEED(t);
+  if (n < 1 || steps < 0 || batch < 1 || step0 < 0 || !(lr >= 0.f)) {
+    set_error(TT_ERR_ARG, "mlp_train n %d steps %d batch %d step0 %d lr %g", n, steps, batch, step0, (double)lr);
+    return TT_ERR_ARG;
+  }
+  if (steps == 0) return TT_OK;
+  TT_CUDA(cudaSetDevice(c->device));
+  TT_TRY(launch_mlp_train(params, adam_m, adam_v, x, t, n, steps, batch, lr, step0, seed, loss_trace, nullptr, 0,
+                          c->stream));
   return TT_OK;
 }
 

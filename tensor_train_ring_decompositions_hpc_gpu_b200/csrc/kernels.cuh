@@ -116,6 +116,16 @@ int launch_gemm_nn(const float* a, long long M, int K, const float* b, long long
 int launch_recon_err(const float* x, int n1, long long N, const float* g1, int r0, int r1,
                      const float* mrg, double* acc, cudaStream_t s);
 
+// Learned predictor (mlp.cu).  Features from the descending probe eigenvalues mu
+// (TT_PROBE_COLS of them); network inference; training (mode 0: Adam steps on Philox-drawn
+// minibatches; mode 1: gradient over samples 0..batch-1 into grad_out).
+int launch_probe_features(const double* mu, double energy, double tol, long long m, long long n, float* out,
+                          cudaStream_t s);
+int launch_mlp_forward(const float* params, const float* x, int n, float* y, cudaStream_t s);
+int launch_mlp_train(float* params, float* adam_m, float* adam_v, const float* x, const float* t, int n, int steps,
+                     int batch, float lr, int step0, unsigned long long seed, float* loss_trace, float* grad_out,
+                     int mode, cudaStream_t s);
+
 // Context accessors (driver.cu): a workspace arena of at least `bytes`, the context stream and
 // its device status word.
 int ctx_arena(tt_ctx* c, size_t bytes, Arena* ws);

@@ -1,0 +1,245 @@
+"""Training data, training run and weights of the learned EDrSVD parameter predictor.
+
+The predictor (kernels in ``csrc/mlp.cu``) maps 8 Gaussian-probe features of an unfolding
+(``tt_probe_features``) to its truncation rank, oversampling and power-iteration count.  This
+module builds its training set and trains it with the library's own GPU kernels:
+
+* Unfoldings: spectra sigma_i = i^-alpha (i = 1..k) with alpha ~ U[0.5, 2], k = min(m, n)
+  log-uniform in [129, 2048] (sizes where a TT step of an order-6 tensor with modes 24..40
+  takes the randomized path), and a step tolerance tol log-uniform in [2e-4, 3e-3] (the
+  per-unfolding share eps / sqrt(d - 1) of eps = 1e-3 for orders 2..6, with margin).
+* Features: ``tt_probe_features`` on the k x k matrix diag(sigma).  For A = U diag(sigma) V^T
+  with orthonormal U, V and a Gaussian probe Omega, V^T Omega is Gaussian again, so the probe
+  statistics (and every EDrSVD quantity) of A and of diag(sigma) have the same distribution.
+* Labels (the plain method in FP64): the rank r* of the exact truncated SVD at tolerance tol
+  (smallest r with sum_{i>r} sigma_i^2 <= tol^2 sum sigma_i^2), and the cheapest (power
+  iterations p, oversampling s) for which the FP64 EDrSVD with r* + s columns leaves at most
+  tol^2 of the energy outside its subspace in every trial: fewer passes over A first
+  (2 + 2p), then the narrower sketch.  Ranks above RANK_CAP (most spectra with alpha < 1.8 at
+  these tolerances) cannot be met within the sketch-width limit of 128; they are labelled
+  with the widest sketch (see ``label``).
+* Training: ``tt_mlp_train`` (Adam, one persistent launch), on 90 % of the samples; the rest
+  measure the validation loss.
+
+``python -m tensor_train_ring_decompositions_hpc_gpu_b200.learned train --out FILE`` runs it on a
+GPU and writes the parameters (``TT_MLP_PARAMS`` float32 values in a .npy file).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+from . import _lib
+
+RANK_CAP = 120            # largest rank the randomized step can return (sketch width <= 128)
+OVERSAMPLE = (4, 8, 16, 32)
+POWER = (0, 1, 2)
+WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "predictor_weights.npy")
+
+
+def sample_specs(count, seed, kmin=129, kmax=2048, amin=0.5, amax=2.0, tmin=2e-4, tmax=3e-3):
+    """(k, alpha, tol) of `count` training unfoldings."""
+    rng = np.random.default_rng(seed)
+    k = np.exp(rng.uniform(np.log(kmin), np.log(kmax + 1), count)).astype(np.int64)
+    alpha = rng.uniform(amin, amax, count)
+    tol = np.exp(rng.uniform(np.log(tmin), np.log(tmax), count))
+    return k, alpha, tol
+
+
+def spectrum(k, alpha):
+    return np.arange(1, int(k) + 1, dtype=np.float64) ** (-float(alpha))
+
+
+def exact_rank(sig, tol, cap=RANK_CAP):
+    """Smallest r with sum_{i>r} sigma_i^2 <= tol^2 ||sigma||^2 (the exact FP64 truncated SVD)."""
+    e = sig * sig
+    tail = np.concatenate([np.cumsum(e[::-1])[::-1], [0.0]])  # tail[r] = sum_{i>=r} e_i (0-based)
+    ok = np.nonzero(tail <= tol * tol * e.sum())[0]
+    r = int(ok[0]) if ok.size else int(sig.size)
+    return max(1, min(r, cap))
+
+
+def _orth(y):
+    q, _ = np.linalg.qr(y)
+    return q
+
+
+def edrsvd_outside(sig, ks, p, rng):
+    """Energy share outside the EDrSVD subspace of diag(sig) (ks columns, p power iterations)."""
+    k = sig.size
+    q = _orth(sig[:, None] * rng.standard_normal((k, ks)))
+    for _ in range(p):
+        z = _orth(sig[:, None] * q)      # A^T Q (A = diag(sig) is symmetric)
+        q = _orth(sig[:, None] * z)      # A Z
+    e = sig * sig
+    captured = float(np.sum(e[:, None] * q * q))
+    return max(e.sum() - captured, 0.0) / e.sum()
+
+
+def label(k, alpha, tol, seed, trials=2):
+    """(r*, s*, p*, feasible) of one unfolding.  When the exact rank exceeds RANK_CAP no sketch
+    within the width limit meets tol; the label is then the widest sketch with the plain
+    method's power count (s = 8, p = 1: r* + s reaches the limit), so that the step ends where
+    the plain adaptive method's doubling would."""
+    sig = spectrum(k, alpha)
+    r = exact_rank(sig, tol, cap=int(k))
+    if r > RANK_CAP:
+        return RANK_CAP, 8, 1, False
+    rng = np.random.default_rng(seed)
+    for p in POWER:
+        for s in OVERSAMPLE:
+            ks = min(r + s, _lib.TT_MAX_SMALL, int(k))
+            if all(edrsvd_outside(sig, ks, p, rng) <= tol * tol for _ in range(trials)):
+                return r, s, p, True
+    return r, OVERSAMPLE[-1], POWER[-1], False
+
+
+def _label_chunk(args):
+    k, alpha, tol, seeds = args
+    return [label(int(a), float(b), float(c), int(d)) for a, b, c, d in zip(k, alpha, tol, seeds)]
+
+
+def labels(k, alpha, tol, seed, workers=None):
+    """Labels of all samples, over a spawn process pool (started before any GPU call)."""
+    seeds = np.random.default_rng(seed + 1).integers(1 << 31, size=k.size)
+    workers = workers or max(1, min(16, os.cpu_count() or 1))
+    chunks = np.array_split(np.arange(k.size), workers * 4)
+    jobs = [(k[c], alpha[c], tol[c], seeds[c]) for c in chunks]
+    if workers == 1:
+        res = [_label_chunk(j) for j in jobs]
+    else:
+        import multiprocessing as mp
+        with mp.get_context("spawn").Pool(workers) as pool:
+            res = pool.map(_label_chunk, jobs)
+    out = np.array([x for part in res for x in part], dtype=np.float64)
+    return out[:, 0], out[:, 1], out[:, 2], out[:, 3].astype(bool)
+
+
+def targets(r, s, p):
+    """Network targets: log2 r / 10, log2 s / 5, p / 2 (decoded by the library as
+    round(2^(10 y0)), round(2^(5 y1)), round(2 y2))."""
+    return np.stack([np.log2(r) / 10.0, np.log2(s) / 5.0, p / 2.0], axis=1).astype(np.float32)
+
+
+def features(k, alpha, tol, seed, device=None):
+    """Probe features of diag(sigma) for every sample, computed by tt_probe_features."""
+    import torch
+    from . import probe_features
+    dev = device or torch.device("cuda")
+    out = np.empty((k.size, _lib.TT_MLP_INPUTS), dtype=np.float32)
+    for i in range(k.size):
+        sig = spectrum(k[i], alpha[i])
+        a = torch.diag(torch.from_numpy(sig).float()).to(dev)  # symmetric: its column-major view is itself
+        e = float(np.sum(sig * sig))
+        out[i] = probe_features(a, energy=e, tol=float(tol[i]), seed=int(seed) + i, stream_id=0).cpu().numpy()
+    return out
+
+
+def init_params(seed):
+    """He-uniform weights, zero biases, packed W1 b1 W2 b2 W3 b3."""
+    rng = np.random.default_rng(seed)
+    parts = []
+    for rows, cols in ((64, 8), (64, 64), (3, 64)):
+        lim = np.sqrt(6.0 / cols)
+        parts += [rng.uniform(-lim, lim, rows * cols), np.zeros(rows)]
+    return np.concatenate(parts).astype(np.float32)
+
+
+def train(x, t, steps=8000, batch=256, lr=1e-3, seed=7, device=None, log=None):
+    """Train on the GPU with tt_mlp_train; returns (params as NumPy, loss trace)."""
+    import torch
+    from . import mlp_train
+    dev = device or torch.device("cuda")
+    p = torch.from_numpy(init_params(seed)).to(dev)
+    m = torch.zeros_like(p)
+    v = torch.zeros_like(p)
+    xt = torch.from_numpy(x).to(dev)
+    tt = torch.from_numpy(t).to(dev)
+    traces, done = [], 0
+    # two phases: lr, then lr / 4 for the last quarter
+    for n_steps, rate in ((steps - steps // 4, lr), (steps // 4, lr / 4)):
+        traces.append(mlp_train(p, m, v, xt, tt, n_steps, batch=batch, lr=rate, step0=done, seed=seed).cpu().numpy())
+        done += n_steps
+        if log:
+            log(f"step {done}: minibatch loss {float(traces[-1][-20:].mean()):.5f}")
+    return p.cpu().numpy(), np.concatenate(traces)
+
+
+def decode(y, ks_cap=_lib.TT_MAX_SMALL):
+    """(rank, oversampling, power iterations, sketch width) the library derives from outputs y."""
+    y = np.asarray(y, dtype=np.float64)
+    r = np.maximum(1.0, np.rint(np.exp2(np.minimum(10.0 * y[..., 0], 10.0))))
+    s = np.rint(np.exp2(np.clip(5.0 * y[..., 1], 1.0, 5.0)))
+    p = np.rint(np.clip(2.0 * y[..., 2], 0.0, 3.0))
+    ks = np.clip(r + s, 1, ks_cap)
+    return r.astype(int), s.astype(int), p.astype(int), ks.astype(int)
+
+
+def save_params(path, params):
+    np.save(path, np.asarray(params, dtype=np.float32).ravel())
+
+
+def load_params(path=WEIGHTS):
+    p = np.load(path).astype(np.float32).ravel()
+    if p.size != _lib.TT_MLP_PARAMS:
+        raise ValueError(f"{path}: {p.size} parameters, expected {_lib.TT_MLP_PARAMS}")
+    return p
+
+
+def build_dataset(count, seed, workers=None, log=print):
+    """Specs, labels (CPU) and features (GPU) of `count` training unfoldings."""
+    t0 = time.time()
+    k, alpha, tol = sample_specs(count, seed)
+    r, s, p, feas = labels(k, alpha, tol, seed, workers)
+    log(f"labels of {count} unfoldings: {time.time() - t0:.1f} s, feasible {feas.mean():.3f}")
+    t0 = time.time()
+    x = features(k, alpha, tol, seed)
+    log(f"features: {time.time() - t0:.1f} s")
+    return dict(k=k, alpha=alpha, tol=tol, r=r, s=s, p=p, feasible=feas, x=x, t=targets(r, s, p))
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
+    sub = ap.add_subparsers(dest="cmd", required=True)
+    tr = sub.add_parser("train")
+    tr.add_argument("--count", type=int, default=20000)
+    tr.add_argument("--steps", type=int, default=8000)
+    tr.add_argument("--batch", type=int, default=256)
+    tr.add_argument("--lr", type=float, default=1e-3)
+    tr.add_argument("--seed", type=int, default=20261203)
+    tr.add_argument("--workers", type=int, default=None)
+    tr.add_argument("--out", required=True)
+    tr.add_argument("--report", default=None, help="JSON summary of the run")
+    args = ap.parse_args(argv)
+    data = build_dataset(args.count, args.seed, args.workers)  # the pool runs before the first GPU call
+    n = args.count
+    ntr = int(0.9 * n)
+    t0 = time.time()
+    params, trace = train(data["x"][:ntr], data["t"][:ntr], steps=args.steps, batch=args.batch, lr=args.lr,
+                          seed=args.seed, log=print)
+    train_s = time.time() - t0
+    import torch
+    from . import mlp_forward
+    y = mlp_forward(torch.from_numpy(params).cuda(), torch.from_numpy(data["x"][ntr:]).cuda()).cpu().numpy()
+    val = float(np.mean(np.sum((y - data["t"][ntr:]) ** 2, axis=1)))
+    r, s, p, ks = decode(y)
+    rt = data["r"][ntr:]
+    save_params(args.out, params)
+    rep = {"samples": n, "train": ntr, "steps": args.steps, "batch": args.batch, "train_seconds": train_s,
+           "final_minibatch_loss": float(trace[-50:].mean()), "validation_loss": val,
+           "validation_rank_within_10pct": float(np.mean(np.abs(r - rt) <= 0.1 * rt + 1)),
+           "validation_power_exact": float(np.mean(p == data["p"][ntr:])),
+           "feasible_share": float(data["feasible"].mean())}
+    print(json.dumps(rep))
+    if args.report:
+        with open(args.report, "w") as f:
+            json.dump(rep, f, indent=1)
+    return 0
+
+
+if __name__ == "__main__":
+    raise SystemExit(main())

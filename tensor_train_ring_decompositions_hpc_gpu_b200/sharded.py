@@ -55,6 +55,9 @@ class DeviceBackend:
     def flat(self, a):
         return a.t().contiguous().reshape(-1)
 
+    def transpose(self, a):
+        return a.t()
+
     def gram_rows(self, a):
         return self.ttr.gram_rows(a, "tc" if self.gemm != "fp32" and a.shape[1] >= (1 << 16) else "fp32")
 
@@ -90,9 +93,18 @@ class DeviceBackend:
         return t.t().contiguous().t()  # column-major
 
     def allreduce(self, t, group):
+        """In-place sum over the ranks; column-major matrices are reduced through their
+        (contiguous) transpose, which shares the storage."""
         import torch.distributed as dist
-        dist.all_reduce(t, group=group)
-        return t
+        if t.is_contiguous():
+            dist.all_reduce(t, group=group)
+            return t
+        if t.dim() == 2 and t.t().is_contiguous():
+            dist.all_reduce(t.t(), group=group)
+            return t
+        c = t.contiguous()
+        dist.all_reduce(c, group=group)
+        return c
 
     def allgather_cols(self, a, group):
         """Concatenate the ranks' column blocks (rank order) of a (rows x cols_local) matrix."""
@@ -155,10 +167,10 @@ def tt_svd_sharded(x_local, shape, ranks, *, oversample=8, power_iters=0, seed=1
             y = be.allreduce(be.sketch(a, om), group)
             q = be.cholqr(y)
             for _ in range(power_iters):
-                z = be.project(a, q).t()                      # cols_loc x ks
-                wz = be.allreduce(be.gram_rows(z.t()), group)  # Z^T Z (ks x ks)
+                zt = be.project(a, q)                         # Z^T = Q^T A (ks x cols_loc)
+                wz = be.allreduce(be.gram_rows(zt), group)     # Z^T Z (ks x ks)
                 rz = np.linalg.cholesky(be.to_host(wz) + 1e-300 * np.eye(ks)).T  # upper
-                z = be.sketch(z, be.from_host(np.linalg.inv(rz))).float()
+                z = be.sketch(be.transpose(zt), be.from_host(np.linalg.inv(rz)))  # Z R^-1
                 y = be.allreduce(be.sketch(a, z), group)
                 q = be.cholqr(y)
             b = be.project(a, q)                              # ks x cols_loc
