@@ -334,8 +334,11 @@ def run_batch(args):
     xs = batch_tensors_torch(args.seed, dev)
     b = ttr.Batch(xs, rmax=BATCH["rmax"], device=dev)
     elems = float(b.flat.numel())
+    b.make_plan(eps=BATCH["eps"])
+    tune_ms = b.tune(reps=2)  # autotuner: sketch chunk width x work order, fastest kept
+    chunk, largest_first = b.variant()
     for _ in range(max(args.warmup, 3)):
-        b.run(eps=BATCH["eps"])
+        b.run(eps=BATCH["eps"])  # first run captures the CUDA graph
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     clk = ClockSampler(0)
@@ -368,7 +371,13 @@ def run_batch(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32+fp64",
         "data": "synthetic (seeded N(0,1) TT cores, modes U{8..32}, ranks U{2..16}, 1e-3 noise)",
         "config": {"workload": "batch4", "tensors": len(xs), "elements": elems, "eps": BATCH["eps"],
-                   "rmax": BATCH["rmax"], "launch": "one persistent kernel (one CTA per tensor at a time)"},
+                   "rmax": BATCH["rmax"],
+                   "launch": "CUDA graph replay: counter/status reset, one persistent kernel (one CTA per tensor "
+                             "at a time), read-back of ranks and error estimates",
+                   "autotuner": {"chunk": chunk, "largest_first": largest_first,
+                                 "variant_ms": {f"{'lpt' if i >= 3 else 'natural'}_chunk{c}": round(v, 3)
+                                                for i, (c, v) in enumerate(zip([16, 32, 64] * 2, tune_ms))}},
+                   "l2": f"inputs {elems * 4 / 1e9:.2f} GB > L2, no flush needed"},
         "parity": {"sample": len(sample), "rank_agreement": agree, "max_rel_err": worst,
                    "max_err_estimate": float(errs.max())},
         "cpu_baseline": {"value": 1.0 / t_cpu, "unit": "tensors/s", "cores": blas_threads(), "kind": "port",

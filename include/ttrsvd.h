@@ -230,6 +230,24 @@ int tt_svd_batched(tt_ctx* ctx, int count, int d, const int* n, const float* x, 
                    const long long* core_off, int* ranks, double* err_est);
 long long tt_batch_core_capacity(int d, const int* n, int rmax);
 
+/* Batch plans: the same decomposition as tt_svd_batched for a batch that is run repeatedly.
+ * tt_batch_plan_create validates the shapes once and keeps the shape table, a largest-first
+ * work order and the kernel scratch on the device (own allocation and stream; inputs are
+ * ordered after the context stream's prior work).  tt_batch_plan_tune times every variant
+ * (sketch chunk width 16 / 32 / 64 x natural or largest-first work order; `reps` launches
+ * each, ms_out receives the 6 averages or may be NULL) on the caller's batch and keeps the
+ * fastest; otherwise chunk 32, largest-first.  tt_batch_plan_run replays the launch sequence
+ * (status and work-counter reset, the persistent kernel, read-back of ranks / error estimates)
+ * as one CUDA graph, captured on the first run and again when x, cores or the variant change;
+ * ranks and err_est as in tt_svd_batched (host arrays, may be NULL). */
+typedef struct tt_batch_plan tt_batch_plan;
+int tt_batch_plan_create(tt_ctx* ctx, int count, int d, const int* n, const long long* x_off, double eps, int rmax,
+                         int oversample, unsigned long long seed, const long long* core_off, tt_batch_plan** plan);
+int tt_batch_plan_tune(tt_batch_plan* plan, const float* x, float* cores, int reps, float* ms_out);
+int tt_batch_plan_variant(const tt_batch_plan* plan, int* chunk, int* largest_first);
+int tt_batch_plan_run(tt_batch_plan* plan, const float* x, float* cores, int* ranks, double* err_est);
+int tt_batch_plan_destroy(tt_batch_plan* plan);
+
 /* Learned EDrSVD parameters.  A 8 -> 64 -> 64 -> 3 ReLU network maps the probe features of
  * an unfolding to (log2 rank / 10, log2 oversampling / 5, power iterations / 2); it is trained
  * by the library's own kernels (tt_mlp_train) on labels of the plain method.  All pointers

@@ -393,14 +393,62 @@ class Batch:
         self.n_arr = (C.c_int * (self.count * self.d))(*[int(v) for sh in self.shapes for v in sh])
         self.ranks = (C.c_int * (self.count * (self.d + 1)))()
         self.err = (C.c_double * self.count)()
+        self.plan = None
+        self.plan_args = None
 
-    def run(self, eps=1e-2, oversample=8, seed=20261203):
-        """One batched launch over the packed tensors (results stay in the Batch)."""
+    def make_plan(self, eps=1e-2, oversample=8, seed=20261203):
+        """Create the batch plan (shape table, work orders and scratch kept on the device)."""
+        self.close()
+        ctx = _ctx_for(self.device.index)
+        p = C.c_void_p()
+        check(lib().tt_batch_plan_create(ctx, self.count, self.d, self.n_arr,
+                                         self.x_off.ctypes.data_as(C.POINTER(C.c_longlong)), float(eps), self.rmax,
+                                         int(oversample), int(seed),
+                                         self.core_off.ctypes.data_as(C.POINTER(C.c_longlong)), C.byref(p)))
+        self.plan = p
+        self.plan_args = (float(eps), int(oversample), int(seed))
+
+    def tune(self, reps=2):
+        """Time every kernel variant on this batch and keep the fastest; returns the 6 times
+        (ms; chunk 16/32/64 in natural order, then largest-first)."""
+        if self.plan is None:
+            self.make_plan()
+        ms = (C.c_float * 6)()
+        check(lib().tt_batch_plan_tune(self.plan, C.c_void_p(self.flat.data_ptr()), C.c_void_p(self.cores.data_ptr()),
+                                       int(reps), ms))
+        return list(ms)
+
+    def variant(self):
+        """(sketch chunk width, largest-first work order) of the plan."""
+        ch, lf = C.c_int(), C.c_int()
+        check(lib().tt_batch_plan_variant(self.plan, C.byref(ch), C.byref(lf)))
+        return ch.value, bool(lf.value)
+
+    def run(self, eps=1e-2, oversample=8, seed=20261203, graph=True):
+        """Decompose the packed tensors (results stay in the Batch).  graph=True replays the
+        plan's CUDA graph (created on first use); graph=False makes one tt_svd_batched call."""
+        if graph:
+            if self.plan is None or self.plan_args != (float(eps), int(oversample), int(seed)):
+                self.make_plan(eps, oversample, seed)
+            check(lib().tt_batch_plan_run(self.plan, C.c_void_p(self.flat.data_ptr()),
+                                          C.c_void_p(self.cores.data_ptr()), self.ranks, self.err))
+            return
         ctx = _ctx_for(self.device.index)
         check(lib().tt_svd_batched(ctx, self.count, self.d, self.n_arr, C.c_void_p(self.flat.data_ptr()),
                                    self.x_off.ctypes.data_as(C.POINTER(C.c_longlong)), float(eps), self.rmax,
                                    int(oversample), int(seed), C.c_void_p(self.cores.data_ptr()),
                                    self.core_off.ctypes.data_as(C.POINTER(C.c_longlong)), self.ranks, self.err))
+
+    def close(self):
+        if getattr(self, "plan", None) is not None:
+            lib().tt_batch_plan_destroy(self.plan)
+            self.plan = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def results(self):
         """Per tensor: (cores as CUDA tensors of logical shape (r_k, n_k, r_{k+1}), ranks, err_est)."""
@@ -425,7 +473,7 @@ def tt_svd_batched(tensors, eps=1e-2, rmax=16, oversample=8, seed=20261203, devi
     their logical shapes.  Returns a list of (cores, ranks, err_est) per tensor; cores are CUDA
     tensors with logical shape (r_k, n_k, r_{k+1})."""
     b = Batch(tensors, rmax=rmax, device=device)
-    b.run(eps=eps, oversample=oversample, seed=seed)
+    b.run(eps=eps, oversample=oversample, seed=seed, graph=False)
     return b.results()
 
 

@@ -31,6 +31,8 @@ EXPORTED = [
     "tt_default_opts", "tt_abi_version", "tt_svd", "tr_svd", "tt_rel_error", "tt_k_gaussian", "tt_k_gaussian_rows",
     "tt_k_sketch", "tt_k_project", "tt_k_gram_rows", "tt_k_gram_tall", "tt_k_cholqr2",
     "tt_k_syev", "tt_k_sketch_noalloc", "tt_svd_batched", "tt_batch_core_capacity",
+    "tt_batch_plan_create", "tt_batch_plan_tune", "tt_batch_plan_variant", "tt_batch_plan_run",
+    "tt_batch_plan_destroy",
     "tt_cores_save", "tt_cores_header", "tt_cores_load",
     "tt_ctx_set_predictor", "tt_probe_features", "tt_mlp_forward", "tt_mlp_grad", "tt_mlp_train",
     "tt_k_permute231", "tt_ref_ttdec_gpu_float", "tt_ref_trdec_gpu_float",
@@ -102,6 +104,11 @@ def load():
         "tt_k_gaussian_rows": (i, [vp, vp, ll, ll, ll, i, ll, ull, C.c_uint]),
         "tt_svd_batched": (i, [vp, i, i, P(i), vp, P(ll), d, i, i, C.c_ulonglong, vp, P(ll), P(i), P(d)]),
         "tt_batch_core_capacity": (ll, [i, P(i), i]),
+        "tt_batch_plan_create": (i, [vp, i, i, P(i), P(ll), d, i, i, ull, P(ll), P(vp)]),
+        "tt_batch_plan_tune": (i, [vp, vp, vp, i, P(C.c_float)]),
+        "tt_batch_plan_variant": (i, [vp, P(i), P(i)]),
+        "tt_batch_plan_run": (i, [vp, vp, vp, P(i), P(d)]),
+        "tt_batch_plan_destroy": (i, [vp]),
         "tt_ctx_set_predictor": (i, [vp, vp]),
         "tt_probe_features": (i, [vp, vp, ll, ll, d, d, ull, C.c_uint, vp]),
         "tt_mlp_forward": (i, [vp, vp, vp, i, vp]),

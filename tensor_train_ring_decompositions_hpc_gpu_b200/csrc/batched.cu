@@ -11,6 +11,7 @@
 // The reference decomposes one tensor per call (ttdec_gpu_float, ttdec_half_lu_device_6) and
 // has no batched path.
 #include <math.h>
+#include <string.h>
 
 #include <algorithm>
 #include <vector>
@@ -24,8 +25,11 @@ namespace {
 constexpr int BT = 512;       // threads per CTA
 constexpr int BMAXM = 512;    // largest row count of a randomized unfolding
 constexpr int BSMALL = 32;    // largest exact small side / sketch width
-constexpr int BCH = 32;       // columns per staged chunk
 constexpr int BMAXD = 8;      // largest order
+// Tunable: columns of the Gaussian test matrix generated per chunk of the sketch (BCH, a
+// template parameter) and the order in which the work counter hands out tensors.
+constexpr int kChunks[3] = {16, 32, 64};
+enum { SCHED_NATURAL = 0, SCHED_LARGEST_FIRST = 1 };
 
 struct BatchShape {
   int d;
@@ -36,16 +40,18 @@ struct BatchShape {
 };
 
 // Shared-memory layout of the kernel (bytes).
-constexpr size_t SM_CHUNK = (size_t)BMAXM * BCH * sizeof(float);            // A chunk / U
+constexpr size_t SM_CHUNK = (size_t)BMAXM * BSMALL * sizeof(float);         // U (m x r)
 constexpr size_t SM_YQ = (size_t)BMAXM * (BSMALL + 1) * sizeof(float);        // Y, Q (stride ks|1)
 constexpr size_t SM_W = (size_t)BSMALL * BSMALL * sizeof(double);             // Gram
 constexpr size_t SM_JAC = 4 * (size_t)BSMALL * BSMALL * sizeof(double);       // Jacobi buffers
-constexpr size_t SM_OM = (size_t)BCH * BSMALL * sizeof(float);                // Omega chunk
 constexpr size_t SM_RED = (size_t)BT * 2 * sizeof(double);                    // reductions
-constexpr size_t SM_TOTAL = SM_CHUNK + SM_YQ + SM_W + SM_JAC + SM_OM + SM_RED + 1024;
+template <int BCH>
+constexpr size_t sm_om() { return (size_t)BCH * BSMALL * sizeof(float); }   // Omega chunk
+template <int BCH>
+constexpr size_t sm_total() { return SM_CHUNK + SM_YQ + SM_W + SM_JAC + sm_om<BCH>() + SM_RED + 1024; }
 
 struct Smem {
-  float* chunk;   // BMAXM x BCH
+  float* chunk;   // BMAXM x BSMALL
   float* yq;      // BMAXM x (BSMALL+1)
   double* w;      // BSMALL x BSMALL (row-major, stride Np)
   double* jac;    // 4 x BSMALL^2
@@ -282,8 +288,10 @@ __device__ int pick_rank(const double* lam, int nev, int cap, double delta2, boo
   return r;
 }
 
+template <int BCH>
 __global__ void __launch_bounds__(BT, 1)
-    k_tt_batched(const BatchShape* __restrict__ shp, int count, const float* __restrict__ x,
+    k_tt_batched(const BatchShape* __restrict__ shp, const int* __restrict__ order, int count,
+                 const float* __restrict__ x,
                  float* __restrict__ cores, int* __restrict__ ranks_out, double* __restrict__ err_out,
                  float* __restrict__ scratch, long long scratch_per_cta, long long half, double eps, int rmax,
                  int oversample, unsigned long long seed, int max_sweeps, int* __restrict__ counter,
@@ -301,7 +309,7 @@ __global__ void __launch_bounds__(BT, 1)
     S.jac = reinterpret_cast<double*>(p);
     p += SM_JAC;
     S.om = reinterpret_cast<float*>(p);
-    p += SM_OM;
+    p += sm_om<BCH>();
     S.red = reinterpret_cast<double*>(p);
   }
   __shared__ double lam[BSMALL], evec[BSMALL * BSMALL];
@@ -315,9 +323,10 @@ __global__ void __launch_bounds__(BT, 1)
   for (;;) {
     if (tid == 0) sh_i[0] = atomicAdd(counter, 1);
     __syncthreads();
-    const int t = sh_i[0];
+    const int slot = sh_i[0];
     __syncthreads();
-    if (t >= count) break;
+    if (slot >= count) break;
+    const int t = order ? order[slot] : slot;
     const BatchShape sh = shp[t];
     const int d = sh.d;
     const float* src = x + sh.x_off;
@@ -555,43 +564,18 @@ __global__ void __launch_bounds__(BT, 1)
   }
 }
 
-}  // namespace
-}  // namespace ttr
+// Shape table of a batch: validation and the per-CTA scratch the kernel needs.
+struct BatchLayout {
+  std::vector<BatchShape> hs;
+  long long half = 0, per_cta = 0;
+};
 
-using namespace ttr;
-
-extern "C" long long tt_batch_core_capacity(int d, const int* n, int rmax) {
-  if (d < 2 || d > BMAXD || !n || rmax < 1) return -1;
-  long long total = 0, left = 1, right = 1;
-  for (int k = 0; k < d; ++k) right *= n[k];
-  long long rp = 1;
-  for (int k = 0; k < d; ++k) {
-    left *= n[k];
-    right /= n[k];
-    const long long rn = (k == d - 1) ? 1 : std::min<long long>({(long long)rmax, left, right});
-    total += rp * n[k] * rn;
-    rp = rn;
-  }
-  return total;
-}
-
-extern "C" int tt_svd_batched(tt_ctx* ctx, int count, int d, const int* n, const float* x,
-                              const long long* x_off, double eps, int rmax, int oversample,
-                              unsigned long long seed, float* cores, const long long* core_off, int* ranks,
-                              double* err_est) {
-  if (!ctx || !n || !x || !x_off || !cores || !core_off || !ranks || count < 0) {
-    set_error(TT_ERR_ARG, "null argument");
-    return TT_ERR_ARG;
-  }
-  if (d < 2 || d > BMAXD || rmax < 1 || rmax > BSMALL || !(eps >= 0.0) || oversample < 0) {
-    set_error(TT_ERR_SHAPE, "batched: order %d (2..%d), rmax %d (1..%d), eps %g", d, BMAXD, rmax, BSMALL, eps);
-    return TT_ERR_SHAPE;
-  }
-  if (count == 0) return TT_OK;
-  std::vector<BatchShape> hs((size_t)count);
+int batch_layout(int count, int d, const int* n, const long long* x_off, const long long* core_off, int rmax,
+                 BatchLayout& L) {
+  L.hs.assign((size_t)count, BatchShape{});
   long long maxsize = 0, maxbg = 0;
   for (int t = 0; t < count; ++t) {
-    BatchShape& b = hs[(size_t)t];
+    BatchShape& b = L.hs[(size_t)t];
     b.d = d;
     b.size = 1;
     for (int k = 0; k < BMAXD; ++k) b.n[k] = k < d ? n[(size_t)t * d + k] : 1;
@@ -622,21 +606,122 @@ extern "C" int tt_svd_batched(tt_ctx* ctx, int count, int d, const int* n, const
       rp = rn;
     }
   }
+  L.half = (maxsize + 63) & ~63LL;
+  L.per_cta = 2 * L.half + ((maxbg + 63) & ~63LL);
+  return TT_OK;
+}
+
+int check_batch_args(int count, int d, int rmax, double eps, int oversample) {
+  if (count < 0 || d < 2 || d > BMAXD || rmax < 1 || rmax > BSMALL || !(eps >= 0.0) || oversample < 0) {
+    set_error(TT_ERR_SHAPE, "batched: count %d, order %d (2..%d), rmax %d (1..%d), eps %g, oversample %d", count, d,
+              BMAXD, rmax, BSMALL, eps, oversample);
+    return TT_ERR_SHAPE;
+  }
+  return TT_OK;
+}
+
+template <int BCH>
+int set_smem_attr() {
+  static bool done = false;
+  if (!done) {
+    if (cudaFuncSetAttribute(k_tt_batched<BCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_total<BCH>()) !=
+        cudaSuccess) {
+      set_error(TT_ERR_CUDA, "batched kernel shared-memory attribute");
+      return TT_ERR_CUDA;
+    }
+    done = true;
+  }
+  return TT_OK;
+}
+
+struct BatchArgs {
+  const BatchShape* shp;
+  const int* order;
+  int count;
+  const float* x;
+  float* cores;
+  int* ranks;
+  double* err;
+  float* scratch;
+  long long per_cta, half;
+  double eps;
+  int rmax, oversample;
+  unsigned long long seed;
+  int* counter;
+  DevStatus* st;
+};
+
+template <int BCH>
+int launch_bch(int grid, cudaStream_t s, const BatchArgs& a) {
+  TT_TRY(set_smem_attr<BCH>());
+  k_tt_batched<BCH><<<grid, BT, sm_total<BCH>(), s>>>(a.shp, a.order, a.count, a.x, a.cores, a.ranks, a.err,
+                                                       a.scratch, a.per_cta, a.half, a.eps, a.rmax, a.oversample,
+                                                       a.seed, 40, a.counter, a.st);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  return TT_OK;
+}
+
+int launch_batched(int bch, int grid, cudaStream_t s, const BatchArgs& a) {
+  switch (bch) {
+    case 16: return launch_bch<16>(grid, s, a);
+    case 32: return launch_bch<32>(grid, s, a);
+    case 64: return launch_bch<64>(grid, s, a);
+    default:
+      set_error(TT_ERR_ARG, "batched: chunk width %d", bch);
+      return TT_ERR_ARG;
+  }
+}
+
+int persistent_grid(int count) {
   int dev = 0, sms = 148;
   TT_CUDA(cudaGetDevice(&dev));
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  const int grid = std::min(count, sms);
-  const long long half = (maxsize + 63) & ~63LL;
-  const long long per_cta = 2 * half + ((maxbg + 63) & ~63LL);
+  return std::max(1, std::min(count, sms));
+}
+
+}  // namespace
+}  // namespace ttr
+
+using namespace ttr;
+
+extern "C" long long tt_batch_core_capacity(int d, const int* n, int rmax) {
+  if (d < 2 || d > BMAXD || !n || rmax < 1) return -1;
+  long long total = 0, left = 1, right = 1;
+  for (int k = 0; k < d; ++k) right *= n[k];
+  long long rp = 1;
+  for (int k = 0; k < d; ++k) {
+    left *= n[k];
+    right /= n[k];
+    const long long rn = (k == d - 1) ? 1 : std::min<long long>({(long long)rmax, left, right});
+    total += rp * n[k] * rn;
+    rp = rn;
+  }
+  return total;
+}
+
+extern "C" int tt_svd_batched(tt_ctx* ctx, int count, int d, const int* n, const float* x,
+                              const long long* x_off, double eps, int rmax, int oversample,
+                              unsigned long long seed, float* cores, const long long* core_off, int* ranks,
+                              double* err_est) {
+  if (!ctx || !n || !x || !x_off || !cores || !core_off || !ranks || count < 0) {
+    set_error(TT_ERR_ARG, "null argument");
+    return TT_ERR_ARG;
+  }
+  TT_TRY(check_batch_args(count, d, rmax, eps, oversample));
+  if (count == 0) return TT_OK;
+  BatchLayout L;
+  TT_TRY(batch_layout(count, d, n, x_off, core_off, rmax, L));
+  const int grid = persistent_grid(count);
   const size_t bytes = sizeof(BatchShape) * (size_t)count + sizeof(int) * (size_t)count * (BMAXD + 1) +
-                       sizeof(double) * (size_t)count + sizeof(float) * (size_t)per_cta * grid + 4096;
+                       sizeof(double) * (size_t)count + sizeof(float) * (size_t)L.per_cta * grid + 4096;
   Arena ws;
   TT_TRY(ctx_arena(ctx, bytes, &ws));
   BatchShape* dshp = ws.take<BatchShape>((size_t)count);
   int* dranks = ws.take<int>((size_t)count * (BMAXD + 1));
   double* derr = ws.take<double>((size_t)count);
   int* dcounter = ws.take<int>(1);
-  float* scratch = ws.take<float>((size_t)per_cta * grid);
+  float* scratch = ws.take<float>((size_t)L.per_cta * grid);
   if (!dshp || !dranks || !derr || !dcounter || !scratch) {
     set_error(TT_ERR_NOMEM, "batched workspace");
     return TT_ERR_NOMEM;
@@ -644,20 +729,11 @@ extern "C" int tt_svd_batched(tt_ctx* ctx, int count, int d, const int* n, const
   cudaStream_t s = ctx_stream(ctx);
   DevStatus* dst = ctx_status(ctx);
   TT_CUDA(cudaMemsetAsync(dst, 0, sizeof(DevStatus), s));
-  TT_CUDA(cudaMemcpyAsync(dshp, hs.data(), sizeof(BatchShape) * (size_t)count, cudaMemcpyHostToDevice, s));
+  TT_CUDA(cudaMemcpyAsync(dshp, L.hs.data(), sizeof(BatchShape) * (size_t)count, cudaMemcpyHostToDevice, s));
   TT_CUDA(cudaMemsetAsync(dcounter, 0, sizeof(int), s));
-  static bool attr = false;
-  if (!attr) {
-    if (cudaFuncSetAttribute(k_tt_batched, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SM_TOTAL) != cudaSuccess) {
-      set_error(TT_ERR_CUDA, "batched kernel shared-memory attribute");
-      return TT_ERR_CUDA;
-    }
-    attr = true;
-  }
-  k_tt_batched<<<grid, BT, SM_TOTAL, s>>>(dshp, count, x, cores, dranks, derr, scratch, per_cta, half, eps, rmax,
-                                            oversample, seed, 40, dcounter, dst);
-  count_launch();
-  TT_LAUNCH_CHECK();
+  const BatchArgs args{dshp, nullptr, count, x, cores, dranks, derr, scratch, L.per_cta, L.half,
+                       eps, rmax, oversample, seed, dcounter, dst};
+  TT_TRY(launch_batched(32, grid, s, args));
   std::vector<int> hr((size_t)count * (BMAXD + 1));
   TT_CUDA(cudaMemcpyAsync(hr.data(), dranks, sizeof(int) * hr.size(), cudaMemcpyDeviceToHost, s));
   if (err_est) TT_CUDA(cudaMemcpyAsync(err_est, derr, sizeof(double) * (size_t)count, cudaMemcpyDeviceToHost, s));
@@ -669,6 +745,265 @@ extern "C" int tt_svd_batched(tt_ctx* ctx, int count, int d, const int* n, const
   if (hst.code) {
     set_error(hst.code, "batched: device status %d (tensor %d)", hst.code, hst.detail);
     return hst.code;
+  }
+  return TT_OK;
+}
+
+// ---------------------------------------------------------------------------------------
+// Batch plans: the batch's shape table, work orders and scratch allocated once, a variant
+// (chunk width x work order) picked by timing every candidate on the batch, and the launch
+// sequence (status reset, counter reset, persistent kernel, result read-back) captured in a
+// CUDA graph that every later run replays with one cudaGraphLaunch.
+// ---------------------------------------------------------------------------------------
+struct tt_batch_plan {
+  tt_ctx* ctx = nullptr;
+  int count = 0, d = 0, rmax = 0, oversample = 0, grid = 1;
+  double eps = 0.0;
+  unsigned long long seed = 0;
+  long long per_cta = 0, half = 0;
+  char* dmem = nullptr;
+  BatchShape* dshp = nullptr;
+  int* dorder = nullptr;  // largest-first order
+  int* dranks = nullptr;
+  double* derr = nullptr;
+  int* dcounter = nullptr;
+  DevStatus* dst = nullptr;
+  float* scratch = nullptr;
+  int* hranks = nullptr;  // pinned
+  double* herr = nullptr;
+  DevStatus* hst = nullptr;
+  cudaStream_t stream = nullptr;
+  cudaEvent_t ev_in = nullptr, e0 = nullptr, e1 = nullptr;
+  int bch = 32, sched = SCHED_LARGEST_FIRST;
+  float tune_ms[6] = {0, 0, 0, 0, 0, 0};
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  const float* gx = nullptr;
+  float* gcores = nullptr;
+  int gbch = 0, gsched = -1;
+};
+
+namespace {
+BatchArgs plan_args(tt_batch_plan* p, const float* x, float* cores, int sched) {
+  return BatchArgs{p->dshp, sched == SCHED_LARGEST_FIRST ? p->dorder : nullptr, p->count, x, cores, p->dranks,
+                   p->derr, p->scratch, p->per_cta, p->half, p->eps, p->rmax, p->oversample, p->seed, p->dcounter,
+                   p->dst};
+}
+
+// The launch sequence of one run, on the plan's stream (also what the graph records).
+int plan_enqueue(tt_batch_plan* p, const float* x, float* cores, int bch, int sched, bool readback) {
+  cudaStream_t s = p->stream;
+  TT_CUDA(cudaMemsetAsync(p->dst, 0, sizeof(DevStatus), s));
+  TT_CUDA(cudaMemsetAsync(p->dcounter, 0, sizeof(int), s));
+  TT_TRY(launch_batched(bch, p->grid, s, plan_args(p, x, cores, sched)));
+  if (readback) {
+    TT_CUDA(cudaMemcpyAsync(p->hranks, p->dranks, sizeof(int) * (size_t)p->count * (BMAXD + 1),
+                            cudaMemcpyDeviceToHost, s));
+    TT_CUDA(cudaMemcpyAsync(p->herr, p->derr, sizeof(double) * (size_t)p->count, cudaMemcpyDeviceToHost, s));
+    TT_CUDA(cudaMemcpyAsync(p->hst, p->dst, sizeof(DevStatus), cudaMemcpyDeviceToHost, s));
+  }
+  return TT_OK;
+}
+
+void plan_drop_graph(tt_batch_plan* p) {
+  if (p->exec) cudaGraphExecDestroy(p->exec);
+  if (p->graph) cudaGraphDestroy(p->graph);
+  p->exec = nullptr;
+  p->graph = nullptr;
+  p->gx = nullptr;
+  p->gcores = nullptr;
+  p->gsched = -1;
+}
+
+int plan_capture(tt_batch_plan* p, const float* x, float* cores) {
+  plan_drop_graph(p);
+  TT_TRY(set_smem_attr<16>());
+  TT_TRY(set_smem_attr<32>());
+  TT_TRY(set_smem_attr<64>());
+  TT_CUDA(cudaStreamBeginCapture(p->stream, cudaStreamCaptureModeThreadLocal));
+  const int rc = plan_enqueue(p, x, cores, p->bch, p->sched, true);
+  cudaGraph_t g = nullptr;
+  const cudaError_t ec = cudaStreamEndCapture(p->stream, &g);
+  if (rc != TT_OK) {
+    if (g) cudaGraphDestroy(g);
+    return rc;
+  }
+  if (ec != cudaSuccess || !g) {
+    set_error(TT_ERR_CUDA, "batched: graph capture: %s", cudaGetErrorString(ec));
+    return TT_ERR_CUDA;
+  }
+  p->graph = g;
+  if (cudaGraphInstantiate(&p->exec, g, 0) != cudaSuccess) {
+    p->exec = nullptr;
+    plan_drop_graph(p);
+    set_error(TT_ERR_CUDA, "batched: graph instantiation");
+    return TT_ERR_CUDA;
+  }
+  p->gx = x;
+  p->gcores = cores;
+  p->gbch = p->bch;
+  p->gsched = p->sched;
+  return TT_OK;
+}
+}  // namespace
+
+extern "C" int tt_batch_plan_destroy(tt_batch_plan* p) {
+  if (!p) return TT_OK;
+  if (p->stream) cudaStreamSynchronize(p->stream);
+  plan_drop_graph(p);
+  if (p->dmem) cudaFree(p->dmem);
+  if (p->hranks) cudaFreeHost(p->hranks);
+  if (p->herr) cudaFreeHost(p->herr);
+  if (p->hst) cudaFreeHost(p->hst);
+  if (p->ev_in) cudaEventDestroy(p->ev_in);
+  if (p->e0) cudaEventDestroy(p->e0);
+  if (p->e1) cudaEventDestroy(p->e1);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+  return TT_OK;
+}
+
+extern "C" int tt_batch_plan_create(tt_ctx* ctx, int count, int d, const int* n, const long long* x_off, double eps,
+                                    int rmax, int oversample, unsigned long long seed, const long long* core_off,
+                                    tt_batch_plan** out) {
+  if (!ctx || !n || !x_off || !core_off || !out || count < 1) {
+    set_error(TT_ERR_ARG, "batch plan: null argument or empty batch");
+    return TT_ERR_ARG;
+  }
+  *out = nullptr;
+  TT_TRY(check_batch_args(count, d, rmax, eps, oversample));
+  BatchLayout L;
+  TT_TRY(batch_layout(count, d, n, x_off, core_off, rmax, L));
+  tt_batch_plan* p = new tt_batch_plan();
+  p->ctx = ctx;
+  p->count = count;
+  p->d = d;
+  p->rmax = rmax;
+  p->oversample = oversample;
+  p->eps = eps;
+  p->seed = seed;
+  p->per_cta = L.per_cta;
+  p->half = L.half;
+  p->grid = persistent_grid(count);
+  size_t off = 0;
+  auto carve = [&](size_t bytes) {
+    const size_t o = off;
+    off += (bytes + 255) & ~size_t(255);
+    return o;
+  };
+  const size_t o_shp = carve(sizeof(BatchShape) * (size_t)count);
+  const size_t o_ord = carve(sizeof(int) * (size_t)count);
+  const size_t o_rk = carve(sizeof(int) * (size_t)count * (BMAXD + 1));
+  const size_t o_err = carve(sizeof(double) * (size_t)count);
+  const size_t o_cnt = carve(sizeof(int));
+  const size_t o_st = carve(sizeof(DevStatus));
+  const size_t o_scr = carve(sizeof(float) * (size_t)L.per_cta * p->grid);
+  if (cudaMalloc(&p->dmem, off) != cudaSuccess ||
+      cudaMallocHost(&p->hranks, sizeof(int) * (size_t)count * (BMAXD + 1)) != cudaSuccess ||
+      cudaMallocHost(&p->herr, sizeof(double) * (size_t)count) != cudaSuccess ||
+      cudaMallocHost(&p->hst, sizeof(DevStatus)) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&p->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&p->ev_in, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreate(&p->e0) != cudaSuccess || cudaEventCreate(&p->e1) != cudaSuccess) {
+    tt_batch_plan_destroy(p);
+    set_error(TT_ERR_NOMEM, "batch plan allocation");
+    return TT_ERR_NOMEM;
+  }
+  p->dshp = reinterpret_cast<BatchShape*>(p->dmem + o_shp);
+  p->dorder = reinterpret_cast<int*>(p->dmem + o_ord);
+  p->dranks = reinterpret_cast<int*>(p->dmem + o_rk);
+  p->derr = reinterpret_cast<double*>(p->dmem + o_err);
+  p->dcounter = reinterpret_cast<int*>(p->dmem + o_cnt);
+  p->dst = reinterpret_cast<DevStatus*>(p->dmem + o_st);
+  p->scratch = reinterpret_cast<float*>(p->dmem + o_scr);
+  // largest-first order: the longest tensors start first, so the work counter's tail holds
+  // only small ones (longest-processing-time rule for the SM makespan)
+  std::vector<int> ord((size_t)count);
+  for (int t = 0; t < count; ++t) ord[(size_t)t] = t;
+  std::stable_sort(ord.begin(), ord.end(),
+                   [&](int a, int b) { return L.hs[(size_t)a].size > L.hs[(size_t)b].size; });
+  if (cudaMemcpyAsync(p->dshp, L.hs.data(), sizeof(BatchShape) * (size_t)count, cudaMemcpyHostToDevice, p->stream) !=
+          cudaSuccess ||
+      cudaMemcpyAsync(p->dorder, ord.data(), sizeof(int) * (size_t)count, cudaMemcpyHostToDevice, p->stream) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(p->stream) != cudaSuccess) {
+    tt_batch_plan_destroy(p);
+    set_error(TT_ERR_CUDA, "batch plan upload");
+    return TT_ERR_CUDA;
+  }
+  *out = p;
+  return TT_OK;
+}
+
+extern "C" int tt_batch_plan_tune(tt_batch_plan* p, const float* x, float* cores, int reps, float* ms_out) {
+  if (!p || !x || !cores) {
+    set_error(TT_ERR_ARG, "batch plan tune: null argument");
+    return TT_ERR_ARG;
+  }
+  reps = std::max(1, reps);
+  TT_CUDA(cudaEventRecord(p->ev_in, ctx_stream(p->ctx)));
+  TT_CUDA(cudaStreamWaitEvent(p->stream, p->ev_in, 0));
+  float best = 0.f;
+  int vi = 0;
+  for (int sched = 0; sched < 2; ++sched)
+    for (int c = 0; c < 3; ++c, ++vi) {
+      TT_TRY(plan_enqueue(p, x, cores, kChunks[c], sched, false));  // warm-up
+      TT_CUDA(cudaEventRecord(p->e0, p->stream));
+      for (int r = 0; r < reps; ++r) TT_TRY(plan_enqueue(p, x, cores, kChunks[c], sched, false));
+      TT_CUDA(cudaEventRecord(p->e1, p->stream));
+      TT_CUDA(cudaEventSynchronize(p->e1));
+      float ms = 0.f;
+      TT_CUDA(cudaEventElapsedTime(&ms, p->e0, p->e1));
+      ms /= (float)reps;
+      p->tune_ms[vi] = ms;
+      if (vi == 0 || ms < best) {
+        best = ms;
+        p->bch = kChunks[c];
+        p->sched = sched;
+      }
+    }
+  DevStatus h;
+  TT_CUDA(cudaMemcpyAsync(&h, p->dst, sizeof(h), cudaMemcpyDeviceToHost, p->stream));
+  TT_CUDA(cudaStreamSynchronize(p->stream));
+  if (h.code) {
+    set_error(h.code, "batched: device status %d (tensor %d)", h.code, h.detail);
+    return h.code;
+  }
+  if (ms_out)
+    for (int i = 0; i < 6; ++i) ms_out[i] = p->tune_ms[i];
+  return TT_OK;
+}
+
+extern "C" int tt_batch_plan_variant(const tt_batch_plan* p, int* chunk, int* largest_first) {
+  if (!p) {
+    set_error(TT_ERR_ARG, "batch plan: null");
+    return TT_ERR_ARG;
+  }
+  if (chunk) *chunk = p->bch;
+  if (largest_first) *largest_first = p->sched == SCHED_LARGEST_FIRST;
+  return TT_OK;
+}
+
+extern "C" int tt_batch_plan_run(tt_batch_plan* p, const float* x, float* cores, int* ranks, double* err_est) {
+  if (!p || !x || !cores) {
+    set_error(TT_ERR_ARG, "batch plan run: null argument");
+    return TT_ERR_ARG;
+  }
+  if (!p->exec || p->gx != x || p->gcores != cores || p->gbch != p->bch || p->gsched != p->sched)
+    TT_TRY(plan_capture(p, x, cores));
+  TT_CUDA(cudaEventRecord(p->ev_in, ctx_stream(p->ctx)));
+  TT_CUDA(cudaStreamWaitEvent(p->stream, p->ev_in, 0));
+  TT_CUDA(cudaGraphLaunch(p->exec, p->stream));
+  count_launch();
+  TT_CUDA(cudaStreamSynchronize(p->stream));
+  if (ranks)
+    for (int t = 0; t < p->count; ++t)
+      for (int k = 0; k <= p->d; ++k)
+        ranks[(size_t)t * (p->d + 1) + k] = p->hranks[(size_t)t * (BMAXD + 1) + k];
+  if (err_est) memcpy(err_est, p->herr, sizeof(double) * (size_t)p->count);
+  if (p->hst->code) {
+    set_error(p->hst->code, "batched: device status %d (tensor %d)", p->hst->code, p->hst->detail);
+    return p->hst->code;
   }
   return TT_OK;
 }

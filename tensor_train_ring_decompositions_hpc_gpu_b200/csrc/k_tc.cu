@@ -357,11 +357,26 @@ __global__ void __launch_bounds__(192, 1)
         __syncwarp();
         const long long jw = tile * BM + q * 32;
         const int nj = (int)((n - jw) < 32 ? (n - jw) : 32);
-        for (int ai = 0; ai < r0; ++ai) {
-          float* dst = out + (long long)r1 * (jw + n * (long long)ai);
-          for (int f = lane; f < r1 * nj; f += 32) {
-            const int jl = f / r1, bi = f - jl * r1;
-            dst[f] = stg[jl * (BN + 1) + ai + r0 * bi];
+        if ((r1 & 3) == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0) {
+          // lane = column j: its r1 outputs of bond index a are contiguous (b fastest), so each
+          // lane stores them as float4s and a warp store covers 32 consecutive 16-byte chunks
+          if (lane < nj) {
+            const float* sr = stg + lane * (BN + 1);
+            for (int ai = 0; ai < r0; ++ai) {
+              float* dst = out + (long long)r1 * (jw + lane + n * (long long)ai);
+              for (int bi = 0; bi < r1; bi += 4)
+                *reinterpret_cast<float4*>(dst + bi) =
+                    make_float4(sr[ai + r0 * bi], sr[ai + r0 * (bi + 1)], sr[ai + r0 * (bi + 2)],
+                                sr[ai + r0 * (bi + 3)]);
+            }
+          }
+        } else {
+          for (int ai = 0; ai < r0; ++ai) {
+            float* dst = out + (long long)r1 * (jw + n * (long long)ai);
+            for (int f = lane; f < r1 * nj; f += 32) {
+              const int jl = f / r1, bi = f - jl * r1;
+              dst[f] = stg[jl * (BN + 1) + ai + r0 * bi];
+            }
           }
         }
         __syncwarp();

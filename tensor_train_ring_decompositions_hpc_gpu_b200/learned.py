@@ -99,16 +99,20 @@ def label(k, alpha, tol, seed, trials=2):
 
 
 def _label_chunk(args):
-    k, alpha, tol, seeds = args
+    k, alpha, tol, seeds, one_thread = args
+    if one_thread:  # one BLAS thread per pool worker: the pool already fills the cores
+        from threadpoolctl import threadpool_limits
+        with threadpool_limits(1):
+            return [label(int(a), float(b), float(c), int(d)) for a, b, c, d in zip(k, alpha, tol, seeds)]
     return [label(int(a), float(b), float(c), int(d)) for a, b, c, d in zip(k, alpha, tol, seeds)]
 
 
 def labels(k, alpha, tol, seed, workers=None):
     """Labels of all samples, over a spawn process pool (started before any GPU call)."""
     seeds = np.random.default_rng(seed + 1).integers(1 << 31, size=k.size)
-    workers = workers or max(1, min(16, os.cpu_count() or 1))
+    workers = workers or max(1, min(32, len(os.sched_getaffinity(0))))
     chunks = np.array_split(np.arange(k.size), workers * 4)
-    jobs = [(k[c], alpha[c], tol[c], seeds[c]) for c in chunks]
+    jobs = [(k[c], alpha[c], tol[c], seeds[c], workers > 1) for c in chunks]
     if workers == 1:
         res = [_label_chunk(j) for j in jobs]
     else:
@@ -125,18 +129,21 @@ def targets(r, s, p):
     return np.stack([np.log2(r) / 10.0, np.log2(s) / 5.0, p / 2.0], axis=1).astype(np.float32)
 
 
-def features(k, alpha, tol, seed, device=None):
+def features(k, alpha, tol, seed, device=None, log=None):
     """Probe features of diag(sigma) for every sample, computed by tt_probe_features."""
     import torch
     from . import probe_features
     dev = device or torch.device("cuda")
-    out = np.empty((k.size, _lib.TT_MLP_INPUTS), dtype=np.float32)
+    out = torch.empty((k.size, _lib.TT_MLP_INPUTS), dtype=torch.float32, device=dev)
+    t0 = time.time()
     for i in range(k.size):
         sig = spectrum(k[i], alpha[i])
-        a = torch.diag(torch.from_numpy(sig).float()).to(dev)  # symmetric: its column-major view is itself
+        a = torch.diag(torch.from_numpy(sig).float().to(dev))  # symmetric: its column-major view is itself
         e = float(np.sum(sig * sig))
-        out[i] = probe_features(a, energy=e, tol=float(tol[i]), seed=int(seed) + i, stream_id=0).cpu().numpy()
-    return out
+        out[i] = probe_features(a, energy=e, tol=float(tol[i]), seed=int(seed) + i, stream_id=0)
+        if log and (i + 1) % 5000 == 0:
+            log(f"features {i + 1}/{k.size}: {time.time() - t0:.1f} s")
+    return out.cpu().numpy()
 
 
 def init_params(seed):
@@ -190,14 +197,15 @@ def load_params(path=WEIGHTS):
     return p
 
 
-def build_dataset(count, seed, workers=None, log=print):
+def build_dataset(count, seed, workers=None, log=None):
     """Specs, labels (CPU) and features (GPU) of `count` training unfoldings."""
+    log = log or (lambda msg: print(msg, flush=True))
     t0 = time.time()
     k, alpha, tol = sample_specs(count, seed)
     r, s, p, feas = labels(k, alpha, tol, seed, workers)
     log(f"labels of {count} unfoldings: {time.time() - t0:.1f} s, feasible {feas.mean():.3f}")
     t0 = time.time()
-    x = features(k, alpha, tol, seed)
+    x = features(k, alpha, tol, seed, log=log)
     log(f"features: {time.time() - t0:.1f} s")
     return dict(k=k, alpha=alpha, tol=tol, r=r, s=s, p=p, feasible=feas, x=x, t=targets(r, s, p))
 
@@ -214,13 +222,16 @@ def main(argv=None):
     tr.add_argument("--workers", type=int, default=None)
     tr.add_argument("--out", required=True)
     tr.add_argument("--report", default=None, help="JSON summary of the run")
+    tr.add_argument("--save-data", default=None, help="write the training set (.npz)")
     args = ap.parse_args(argv)
     data = build_dataset(args.count, args.seed, args.workers)  # the pool runs before the first GPU call
+    if args.save_data:
+        np.savez_compressed(args.save_data, **data)
     n = args.count
     ntr = int(0.9 * n)
     t0 = time.time()
     params, trace = train(data["x"][:ntr], data["t"][:ntr], steps=args.steps, batch=args.batch, lr=args.lr,
-                          seed=args.seed, log=print)
+                          seed=args.seed, log=lambda msg: print(msg, flush=True))
     train_s = time.time() - t0
     import torch
     from . import mlp_forward

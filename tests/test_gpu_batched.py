@@ -63,3 +63,40 @@ def test_batched_rejects_bad_arguments(gpu):
     from tensor_train_ring_decompositions_hpc_gpu_b200._lib import TTError
     with pytest.raises(TTError):
         ttr.tt_svd_batched([np.ones((4, 4, 4), np.float32)], eps=1e-2, rmax=64)
+
+
+def test_plan_graph_replay_matches_one_shot_call(gpu):
+    """Every autotuner variant (chunk width x work order) and the graph replay give the same
+    ranks and cores as the one-shot tt_svd_batched call: the variants change the schedule,
+    not the arithmetic of a tensor (each tensor is decomposed by one CTA in a fixed order)."""
+    import torch
+    ttr = _ttr()
+    xs = _batch(40, seed=9)
+    ref = ttr.Batch(xs, rmax=16)
+    ref.run(eps=1e-2, graph=False)
+    b = ttr.Batch(xs, rmax=16)
+    b.make_plan(eps=1e-2)
+    ms = b.tune(reps=1)
+    assert len(ms) == 6 and all(v > 0 for v in ms)
+    chunk, largest_first = b.variant()
+    assert chunk in (16, 32, 64)
+    for _ in range(3):  # first run captures the graph, the others replay it
+        b.cores.zero_()
+        b.run(eps=1e-2)
+        assert list(b.ranks) == list(ref.ranks)
+        assert torch.equal(b.cores, ref.cores)
+        assert list(b.err) == list(ref.err)
+    b.close()
+
+
+def test_plan_recaptures_for_new_buffers(gpu):
+    import torch
+    ttr = _ttr()
+    xs = _batch(12, seed=10)
+    b = ttr.Batch(xs, rmax=16)
+    b.run(eps=1e-2)
+    first = b.cores.clone()
+    b.cores = torch.zeros_like(b.cores)  # a different output buffer: the plan re-captures
+    b.run(eps=1e-2)
+    assert torch.equal(b.cores, first)
+    b.close()
