@@ -18,6 +18,7 @@
 
 #include "kernels.cuh"
 #include "philox.cuh"
+#include "jacobi_warp.cuh"
 
 namespace ttr {
 namespace {
@@ -125,32 +126,24 @@ __device__ void cta_gram(const float* __restrict__ base, long long ps, long long
   }
 }
 
-// Jacobi rotation annihilating a_pq (same rule as the single-tensor solver).
-__device__ __forceinline__ bool b_rotation(double app, double aqq, double apq, double inv_s, double& c, double& s) {
-  const double ps = app * inv_s, qs = aqq * inv_s, as = apq * inv_s;
-  c = 1.0;
-  s = 0.0;
-  if (!(fabs(as) > 1e-15 && as * as > 1e-28 * fabs(ps * qs))) return false;
-  const float d = (float)(qs - ps), e = 2.0f * (float)as;
-  const float h = sqrtf(fmaf(d, d, e * e));
-  const float tf = (d >= 0.0f ? e : -e) * __frcp_rn(fabsf(d) + h);
-  const double t = (double)tf;
-  const double x = fma(t, t, 1.0);
-  double y = (double)rsqrtf((float)x);
-  y = y * fma(-0.5 * x, y * y, 1.5);
-  y = y * fma(-0.5 * x, y * y, 1.5);
-  c = y;
-  s = t * y;
-  return true;
-}
-
-// Eigen-decomposition of the symmetric W (N x N row-major, N <= BSMALL) by cyclic Jacobi with
-// the round-robin pairing, all rotations of a round applied together as W' = J^T W J, V' = V J
-// (double-buffered).  Output: evals[N] descending, evecs (N x N column-major, stride N).
+// Eigen-decomposition of the symmetric W (N x N row-major, N <= BSMALL): one warp with the
+// register-resident solver for N <= 32; otherwise cyclic Jacobi with the round-robin pairing,
+// all rotations of a round applied together as W' = J^T W J, V' = V J (double-buffered).  Output: evals[N] descending, evecs (N x N column-major, stride N).
 // Returns the sweep count (max_sweeps + 1 when not converged).
 __device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, double* evecs, int max_sweeps,
                           double* red) {
   const int tid = threadIdx.x;
+  if (N <= 32) {  // one warp, matrix in registers (warp_jacobi32); the other warps wait
+    int* shw = reinterpret_cast<int*>(red);
+    if (tid < 32) {
+      const int sw = warp_jacobi32<false>(W, N, 1, N, jac, max_sweeps, evals, evecs, N);
+      if (tid == 0) shw[0] = sw;
+    }
+    __syncthreads();
+    const int sw = shw[0];
+    __syncthreads();
+    return sw;
+  }
   const int Np = N + (N & 1);
   const int NR = Np - 1;
   const int NN = Np * Np;
@@ -184,7 +177,7 @@ __device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, do
           q = tt;
         }
         double c = 1.0, s = 0.0;
-        if (q < N && b_rotation(Wc[p * Np + p], Wc[q * Np + q], Wc[p * Np + q], inv_s, c, s)) rot = 1;
+        if (q < N && jacobi_rotation(Wc[p * Np + p], Wc[q * Np + q], Wc[p * Np + q], inv_s, c, s)) rot = 1;
         cs[k] = c;
         sn[k] = s;
         pr[p] = q;

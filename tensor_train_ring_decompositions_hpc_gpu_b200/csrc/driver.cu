@@ -603,11 +603,13 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
     if (st.path == PATH_EXACT_ROWS) {
       npasses += st.fold ? 1 : 2;
       TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols, [&] {
-        if (engine == TT_GEMM_TC) {
+        // adaptive ranks: FP64-accumulated Gram unless the unfolding is long enough (>= 2^22
+        // columns, >= 2048 units of the tensor-core Gram) for the unit errors to average out
+        if (engine == TT_GEMM_TC && (!adaptive || cols >= (1LL << 22))) {
           const int rc = launch_gram_tc(cur, m, cols, B.w, ws, c->dstat, s);
           if (rc != TT_ERR_UNSUPPORTED) return rc;
         }
-        return launch_gram(cur, cols, (int)m, m, 1, B.w, false, ws, s);
+        return launch_gram(cur, cols, (int)m, m, 1, B.w, adaptive, ws, s);
       }));
       TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
@@ -694,8 +696,11 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         }));
         // Gram of the small factor B (ksa x cols, column-major = B^T row-major): the input of
         // the eigen-based small SVD (TT3O:717), on the tensor cores for long B.
+        // Adaptive ranks read ||A||^2 - sum(lambda) down to delta^2 = eps^2 ||X||^2 / (d - 1): the
+        // eigenvalue sum must then hold ~1e-8 relative, which the tensor-core Gram (TF32
+        // operands, FP32 accumulation within 2048-column units) does not guarantee on short B.
         TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ksa * ksa, 4.0 * cols * ksa, [&] {
-          if (engine == TT_GEMM_TC) {
+          if (engine == TT_GEMM_TC && !adaptive) {
             const int rc = launch_gram_tc(B.bt, ksa, cols, B.w, ws, c->dstat, s);
             if (rc != TT_ERR_UNSUPPORTED) return rc;
           }
@@ -756,6 +761,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
           const int sh = (int)std::lround(std::exp2(std::min(std::max(5.0 * (double)hy[1], 1.0), 5.0)));
           pw = (int)std::lround(std::min(std::max(2.0 * (double)hy[2], 0.0), 3.0));
           ks = (int)std::min<double>((double)ks_cap, std::max(1.0, rh + sh));
+          if (10 * ks >= 9 * ks_cap) ks = ks_cap;  // within 10 % of the width limit: use the limit
           TT_TRY(attempt(ks, pw, sid));
           double out = 0.0;
           TT_TRY(outside(ks, &out));

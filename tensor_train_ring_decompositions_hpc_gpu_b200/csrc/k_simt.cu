@@ -8,6 +8,7 @@
 
 #include "kernels.cuh"
 #include "philox.cuh"
+#include "jacobi_warp.cuh"
 
 namespace ttr {
 
@@ -1411,29 +1412,6 @@ __global__ void __launch_bounds__(256) k_syev_jacobi(const double* __restrict__ 
 // with a_pq^2 <= 1e-28 |a_pp a_qq| (relative accuracy) or |a_pq| <= 1e-15 max|diag| (FP64
 // rounding floor) are not rotated; the solve ends after Np - 1 consecutive rounds without a
 // rotation.  Eigenvalues are ordered by a parallel rank count.
-__device__ __forceinline__ bool jacobi_rotation(double app, double aqq, double apq, double inv_s, double& c,
-                                                double& s) {
-  const double ps = app * inv_s, qs = aqq * inv_s, as = apq * inv_s;
-  c = 1.0;
-  s = 0.0;
-  if (!(fabs(as) > 1e-15 && as * as > 1e-28 * fabs(ps * qs))) return false;
-  // t = sign(d) e / (|d| + sqrt(d^2 + e^2)) with d = a_qq - a_pp, e = 2 a_pq: the smaller root
-  // of t^2 + 2 (d / e) t - 1 = 0, without the quotient d / e.  FP32 suffices for t.
-  const float d = (float)(qs - ps), e = 2.0f * (float)as;
-  const float h = sqrtf(fmaf(d, d, e * e));
-  const float tf = (d >= 0.0f ? e : -e) * __frcp_rn(fabsf(d) + h);
-  const double t = (double)tf;
-  // c = 1 / sqrt(1 + t^2) to FP64 precision: FP32 estimate, then two Newton steps
-  // y <- y (3 - x y^2) / 2, each squaring the relative error.
-  const double x = fma(t, t, 1.0);
-  double y = (double)rsqrtf((float)x);
-  y = y * fma(-0.5 * x, y * y, 1.5);
-  y = y * fma(-0.5 * x, y * y, 1.5);
-  c = y;
-  s = t * y;
-  return true;
-}
-
 // Slot of index i in round-robin round r (slot 0 fixed, slots 1..NR cycle), and its position.
 __device__ __forceinline__ int bl_slot(int i, int r, int NR) {
   if (i == 0) return 0;
@@ -1654,12 +1632,29 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
   }
 }
 
+// One warp: the register-resident XOR-tournament Jacobi (N <= 32).
+__global__ void __launch_bounds__(32) k_syev_w32(const double* __restrict__ w, int N, double* __restrict__ evals,
+                                                 double* __restrict__ evecs, int max_sweeps, DevStatus* st) {
+  __shared__ double vsm[32 * 33];
+  const int sw = warp_jacobi32<false>(w, 1, N, N, vsm, max_sweeps, evals, evecs, N);
+  if (threadIdx.x == 0 && st) {
+    atomicMax(&st->sweeps, sw > max_sweeps ? max_sweeps : sw);
+    if (sw > max_sweeps) dev_fail(st, TT_ERR_NOCONV, max_sweeps);
+  }
+}
+
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps, Arena& ws,
                 DevStatus* st, cudaStream_t s) {
   if (N <= 0) return TT_OK;
   if (N > TT_MAX_SMALL) {
     set_error(TT_ERR_UNSUPPORTED, "eigen-solver size %d > %d", N, TT_MAX_SMALL);
     return TT_ERR_UNSUPPORTED;
+  }
+  if (N <= 32) {
+    k_syev_w32<<<1, 32, 0, s>>>(w, N, evals, evecs, max_sweeps, st);
+    count_launch();
+    TT_LAUNCH_CHECK();
+    return TT_OK;
   }
   if (N <= 64) {
     const int Nps = N + (N & 1);

@@ -175,10 +175,10 @@ struct Bars {
   int stages;
   __device__ uint32_t full(int s) const { return base + 8u * s; }
   __device__ uint32_t empty(int s) const { return base + 8u * (stages + s); }
-  __device__ uint32_t tfull(int b) const { return base + 8u * (2 * stages + b); }
-  __device__ uint32_t tempty(int b) const { return base + 8u * (2 * stages + 2 + b); }
-  __device__ uint32_t drain() const { return base + 8u * (2 * stages + 4); }
-  __host__ __device__ static constexpr int count(int stages) { return 2 * stages + 5; }
+  __device__ uint32_t tfull(int b) const { return base + 8u * (2 * stages + b); }       // b < 4
+  __device__ uint32_t tempty(int b) const { return base + 8u * (2 * stages + 4 + b); }  // b < 4
+  __device__ uint32_t drain() const { return base + 8u * (2 * stages + 8); }
+  __host__ __device__ static constexpr int count(int stages) { return 2 * stages + 9; }
 };
 
 // Wait (bounded) until the most recent TMA fill of every stage has landed; fill number f used
@@ -198,7 +198,7 @@ __device__ __forceinline__ void drain_fills(const Bars& bars, int stages, long l
 // SPLIT: Q arrives as an exactly-TF32 high part (tmB) and its FP32 remainder (tmB2); each
 // K-step issues A*Qhi and A*Qlo into the same accumulator, so Q carries FP32 precision.
 template <int BN, int STAGES, bool SPLIT>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(320, 1)
     k_project_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  const __grid_constant__ CUtensorMap tmB2, long long n, int N, int KB,
                  float* __restrict__ out, long long ldo, int mode, int r0, int r1, DevStatus* st) {
@@ -207,7 +207,7 @@ __global__ void __launch_bounds__(192, 1)
   constexpr uint32_t B_BYTES = BN * 128;
   constexpr uint32_t STAGE_BYTES = A_BYTES + (SPLIT ? 2 : 1) * B_BYTES;  // 1 KB aligned
   constexpr uint32_t BNP = pow2_cols(BN);
-  constexpr uint32_t TMEM_COLS = pow2_cols(2 * BNP);
+  constexpr uint32_t TMEM_COLS = pow2_cols(4 * BNP);  // four accumulators, two per epilogue group
   constexpr uint32_t IDESC = idesc_tf32(BM, BN, 0, 0);
   static_assert(STAGE_BYTES % 1024 == 0, "stage alignment");
 
@@ -226,7 +226,7 @@ __global__ void __launch_bounds__(192, 1)
       mbar_init(bars.full(s), 1);
       mbar_init(bars.empty(s), 1);
     }
-    for (int b = 0; b < 2; ++b) {
+    for (int b = 0; b < 4; ++b) {
       mbar_init(bars.tfull(b), 1);
       mbar_init(bars.tempty(b), 4);
     }
@@ -284,8 +284,8 @@ __global__ void __launch_bounds__(192, 1)
       bool ok = true;
       int t = 0;
       for (long long tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x, ++t) {
-        const int buf = t & 1;
-        const uint32_t tph = (uint32_t)((t >> 1) & 1);
+        const int buf = t & 3;
+        const uint32_t tph = (uint32_t)((t >> 2) & 1);
         if (!mbar_wait(bars.tempty(buf), tph ^ 1u, abort_flag)) {
           ok = false;
           break;
@@ -324,13 +324,16 @@ __global__ void __launch_bounds__(192, 1)
       mbar_wait_bounded(bars.drain(), 0);
     }
   } else {
+    // Two epilogue groups of four warps (one per TMEM lane quadrant each) take alternate tiles:
+    // group e drains accumulators e and e + 2, so up to four tiles are in flight.
     const int q = warp & 3;  // TMEM lane quadrant this warp may access
-    int t = 0;
+    const int e = (warp - 2) >> 2;
+    int t = e;
     const bool vec = (mode == OUT_ROWMAJOR) && ((ldo & 3) == 0) && ((N & 3) == 0) &&
                      ((reinterpret_cast<uintptr_t>(out) & 15) == 0);
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x, ++t) {
-      const int buf = t & 1;
-      const uint32_t tph = (uint32_t)((t >> 1) & 1);
+    for (long long tile = blockIdx.x + (long long)e * gridDim.x; tile < ntiles; tile += 2LL * gridDim.x, t += 2) {
+      const int buf = t & 3;
+      const uint32_t tph = (uint32_t)((t >> 2) & 1);
       if (!mbar_wait(bars.tfull(buf), tph, abort_flag)) {
         *abort_flag = 1;
         dev_fail(st, TT_ERR_TIMEOUT, 3);
@@ -348,7 +351,7 @@ __global__ void __launch_bounds__(192, 1)
       __syncwarp();
       if (lane == 0) mbar_arrive(bars.tempty(buf));
       const long long j = tile * BM + q * 32 + lane;
-      if (mode == OUT_PERM231) {
+      if (BN <= 32 && mode == OUT_PERM231) {  // the launcher sends the bond permute only for BN <= 32
         // Bond permute through shared memory: for each a, the warp's 32 columns j form one
         // contiguous run of r1 * 32 outputs (b fastest), written with coalesced stores.
         float* stg = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(barmem) + 256) + (warp - 2) * 32 * (BN + 1);
@@ -869,7 +872,8 @@ int run_project(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap&
                 int N, int KB, float* out, long long ldo, int mode, int r0, int r1, DevStatus* st,
                 cudaStream_t s) {
   constexpr uint32_t STAGE = 128 * 128 + (SPLIT ? 2 : 1) * BN * 128;
-  constexpr size_t STAGING = 4 * 32 * (BN + 1) * sizeof(float);  // bond-permute epilogue
+  // bond-permute staging of the 8 epilogue warps (that epilogue runs for BN <= 32 only)
+  constexpr size_t STAGING = BN <= 32 ? 8 * 32 * (BN + 1) * sizeof(float) : 0;
   constexpr int STAGES = (int)std::min<size_t>(10, (kSmemBudget - STAGING) / STAGE);
   const size_t smem = (size_t)STAGES * STAGE + 1024 + 256 + STAGING;
   auto kern = k_project_tc<BN, STAGES, SPLIT>;
@@ -883,7 +887,7 @@ int run_project(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap&
   }
   const long long ntiles = (n + 127) / 128;
   const int grid = (int)std::min<long long>(ntiles, (long long)g_sms);
-  kern<<<grid, 192, smem, s>>>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st);
+  kern<<<grid, 320, smem, s>>>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st);
   count_launch();
   TT_LAUNCH_CHECK();
   return TT_OK;
@@ -1041,6 +1045,7 @@ int launch_project_tc(const float* a, long long m, long long n, const float* q, 
       m > (1LL << 31))
     return TT_ERR_UNSUPPORTED;
   const int BN = pad_bn(N);
+  if (mode == OUT_PERM231 && BN > 32) return TT_ERR_UNSUPPORTED;
   // Q = Qhi + Qlo, Qhi exactly representable in TF32 (round to nearest), Qlo the FP32 remainder.
   const size_t mk = ws.mark();
   const long long ldh = (m + 3) & ~3LL;

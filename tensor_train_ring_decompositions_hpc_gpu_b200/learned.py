@@ -183,6 +183,7 @@ def decode(y, ks_cap=_lib.TT_MAX_SMALL):
     s = np.rint(np.exp2(np.clip(5.0 * y[..., 1], 1.0, 5.0)))
     p = np.rint(np.clip(2.0 * y[..., 2], 0.0, 3.0))
     ks = np.clip(r + s, 1, ks_cap)
+    ks = np.where(10 * ks >= 9 * ks_cap, ks_cap, ks)  # the library snaps widths within 10 % to the limit
     return r.astype(int), s.astype(int), p.astype(int), ks.astype(int)
 
 

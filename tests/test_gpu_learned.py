@@ -183,3 +183,30 @@ def test_learned_flag_needs_predictor_and_eps(gpu):
         ttr.tt_svd(a, [1, 64, 1], eps=1e-3, flags=ttr.TT_FLAG_LEARNED)
     with pytest.raises(ttr.TTError):
         ttr.tt_svd(a, [1, 64, 1], eps=0.0, flags=ttr.TT_FLAG_ADAPTIVE_KS)
+
+
+def test_trained_predictor_saves_passes_at_equal_error(gpu):
+    """The shipped predictor (trained by the library's kernels, learned.py) against the plain
+    adaptive EDrSVD on held-out power-law unfoldings U diag(i^-alpha) V^T: fewer passes over A
+    in total, and per matrix the same achieved error (the tolerance, or what the 128-column
+    sketch limit allows when the exact rank is above it)."""
+    import torch
+    ttr = _ttr()
+    from tensor_train_ring_decompositions_hpc_gpu_b200 import learned
+    ttr.set_predictor(learned.load_params())
+    tol = 1e-3
+    tot = {"plain": 0, "learned": 0}
+    try:
+        for i, (m, alpha) in enumerate([(300, 0.7), (600, 1.3), (300, 1.9), (600, 2.0), (450, 1.6), (600, 1.85)]):
+            a, _ = _lowrank(m, 32768, alpha, 50 + i, gpu)
+            errs = {}
+            for name, flag in (("plain", ttr.TT_FLAG_ADAPTIVE_KS), ("learned", ttr.TT_FLAG_LEARNED)):
+                res = ttr.tt_svd(a, [1, 120, 1], eps=tol, power_iters=1, flags=flag)
+                errs[name] = _err(ttr, a, res)
+                tot[name] += res.passes
+                # the a-posteriori estimate is the achieved error
+                assert abs(res.est_rel_err - errs[name]) <= 0.05 * errs[name] + 1e-5, (m, alpha, name)
+            assert errs["learned"] <= max(tol, errs["plain"]) * 1.05, (m, alpha, errs)
+    finally:
+        ttr.set_predictor(None)
+    assert tot["learned"] <= 0.6 * tot["plain"], tot
