@@ -169,7 +169,12 @@ def tt_svd_sharded(x_local, shape, ranks, *, oversample=8, power_iters=0, seed=1
             for _ in range(power_iters):
                 zt = be.project(a, q)                         # Z^T = Q^T A (ks x cols_loc)
                 wz = be.allreduce(be.gram_rows(zt), group)     # Z^T Z (ks x ks)
-                rz = np.linalg.cholesky(be.to_host(wz) + 1e-300 * np.eye(ks)).T  # upper
+                # Z^T Z is singular to working precision when A's rank is below ks; a shift of
+                # 1e-12 of its trace keeps the Cholesky factor finite (R^-1 only conditions Z)
+                wzh = be.to_host(wz)
+                wzh = 0.5 * (wzh + wzh.T)
+                shift = 1e-12 * max(float(np.trace(wzh)), 1e-300)
+                rz = np.linalg.cholesky(wzh + shift * np.eye(ks)).T  # upper
                 z = be.sketch(be.transpose(zt), be.from_host(np.linalg.inv(rz)))  # Z R^-1
                 y = be.allreduce(be.sketch(a, z), group)
                 q = be.cholqr(y)
