@@ -18,7 +18,7 @@
 
 #include "kernels.cuh"
 #include "philox.cuh"
-#include "jacobi_warp.cuh"
+#include "jacobi_rot.cuh"
 
 namespace ttr {
 namespace {
@@ -126,24 +126,14 @@ __device__ void cta_gram(const float* __restrict__ base, long long ps, long long
   }
 }
 
-// Eigen-decomposition of the symmetric W (N x N row-major, N <= BSMALL): one warp with the
-// register-resident solver for N <= 32; otherwise cyclic Jacobi with the round-robin pairing,
-// all rotations of a round applied together as W' = J^T W J, V' = V J (double-buffered).  Output: evals[N] descending, evecs (N x N column-major, stride N).
+// Eigen-decomposition of the symmetric W (N x N row-major, N <= BSMALL) by cyclic Jacobi with
+// the round-robin pairing, all rotations of a round applied together as W' = J^T W J, V' = V J
+// (double-buffered).  Output: evals[N] descending, evecs (N x N column-major, stride N).
 // Returns the sweep count (max_sweeps + 1 when not converged).
 __device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, double* evecs, int max_sweeps,
                           double* red) {
   const int tid = threadIdx.x;
-  if (N <= 32) {  // one warp, matrix in registers (warp_jacobi32); the other warps wait
-    int* shw = reinterpret_cast<int*>(red);
-    if (tid < 32) {
-      const int sw = warp_jacobi32<false>(W, N, 1, N, jac, max_sweeps, evals, evecs, N);
-      if (tid == 0) shw[0] = sw;
-    }
-    __syncthreads();
-    const int sw = shw[0];
-    __syncthreads();
-    return sw;
-  }
+
   const int Np = N + (N & 1);
   const int NR = Np - 1;
   const int NN = Np * Np;

@@ -1,0 +1,32 @@
+// The Jacobi rotation shared by the single-matrix and the batched eigen-solvers.
+#pragma once
+#include <math.h>
+
+namespace ttr {
+
+// Rotation (c, s) annihilating a_pq of the 2 x 2 block [[a_pp, a_pq], [a_pq, a_qq]] (values
+// scaled by inv_s for the skip test).  Returns false (c = 1, s = 0) when a_pq is negligible.
+// t = sign(d) e / (|d| + sqrt(d^2 + e^2)) with d = a_qq - a_pp, e = 2 a_pq is the smaller root of
+// t^2 + 2 (d / e) t - 1 = 0, formed without the quotient d / e; FP32 suffices for t.
+// c = 1 / sqrt(1 + t^2) to FP64 precision: FP32 estimate, then two Newton steps
+// y <- y (3 - x y^2) / 2, each squaring the relative error.
+__device__ __forceinline__ bool jacobi_rotation(double app, double aqq, double apq, double inv_s, double& c,
+                                                double& s) {
+  const double ps = app * inv_s, qs = aqq * inv_s, as = apq * inv_s;
+  c = 1.0;
+  s = 0.0;
+  if (!(fabs(as) > 1e-15 && as * as > 1e-28 * fabs(ps * qs))) return false;
+  const float d = (float)(qs - ps), e = 2.0f * (float)as;
+  const float h = sqrtf(fmaf(d, d, e * e));
+  const float tf = (d >= 0.0f ? e : -e) * __frcp_rn(fabsf(d) + h);
+  const double t = (double)tf;
+  const double x = fma(t, t, 1.0);
+  double y = (double)rsqrtf((float)x);
+  y = y * fma(-0.5 * x, y * y, 1.5);
+  y = y * fma(-0.5 * x, y * y, 1.5);
+  c = y;
+  s = t * y;
+  return true;
+}
+
+}  // namespace ttr

@@ -8,7 +8,7 @@
 
 #include "kernels.cuh"
 #include "philox.cuh"
-#include "jacobi_warp.cuh"
+#include "jacobi_rot.cuh"
 
 namespace ttr {
 
@@ -1632,29 +1632,12 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
   }
 }
 
-// One warp: the register-resident XOR-tournament Jacobi (N <= 32).
-__global__ void __launch_bounds__(32) k_syev_w32(const double* __restrict__ w, int N, double* __restrict__ evals,
-                                                 double* __restrict__ evecs, int max_sweeps, DevStatus* st) {
-  __shared__ double vsm[32 * 33];
-  const int sw = warp_jacobi32<false>(w, 1, N, N, vsm, max_sweeps, evals, evecs, N);
-  if (threadIdx.x == 0 && st) {
-    atomicMax(&st->sweeps, sw > max_sweeps ? max_sweeps : sw);
-    if (sw > max_sweeps) dev_fail(st, TT_ERR_NOCONV, max_sweeps);
-  }
-}
-
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps, Arena& ws,
                 DevStatus* st, cudaStream_t s) {
   if (N <= 0) return TT_OK;
   if (N > TT_MAX_SMALL) {
     set_error(TT_ERR_UNSUPPORTED, "eigen-solver size %d > %d", N, TT_MAX_SMALL);
     return TT_ERR_UNSUPPORTED;
-  }
-  if (N <= 32) {
-    k_syev_w32<<<1, 32, 0, s>>>(w, N, evals, evecs, max_sweeps, st);
-    count_launch();
-    TT_LAUNCH_CHECK();
-    return TT_OK;
   }
   if (N <= 64) {
     const int Nps = N + (N & 1);

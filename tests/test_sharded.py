@@ -171,5 +171,5 @@ def test_sharded_device_backend_one_rank_matches_library(gpu):
     assert used == RANKS
     err = oracle.rel_error(x, oracle.tt_full(cores))
     res = ttr.tt_svd(x, RANKS, gemm="fp32")
-    lerr = oracle.rel_error(x, oracle.tt_full([c.double().cpu().numpy() for c in res.cores]))
+    lerr = oracle.rel_error(x, oracle.tt_full([np.asarray(c, dtype=np.float64) for c in res.cores]))
     assert abs(err - lerr) < 1e-5, (err, lerr)
