@@ -603,13 +603,14 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
     if (st.path == PATH_EXACT_ROWS) {
       npasses += st.fold ? 1 : 2;
       TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols, [&] {
-        // adaptive ranks: FP64-accumulated Gram unless the unfolding is long enough (>= 2^22
-        // columns, >= 2048 units of the tensor-core Gram) for the unit errors to average out
-        if (engine == TT_GEMM_TC && (!adaptive || cols >= (1LL << 22))) {
+        // adaptive ranks read energies to ~1e-8 relative: FP32 products (unbiased rounding)
+        // instead of TF32 ones, FP64 accumulation (per product for short unfoldings, per 1024
+        // columns for long ones, whose many partial sums average the FP32 rounding out)
+        if (engine == TT_GEMM_TC && !adaptive) {
           const int rc = launch_gram_tc(cur, m, cols, B.w, ws, c->dstat, s);
           if (rc != TT_ERR_UNSUPPORTED) return rc;
         }
-        return launch_gram(cur, cols, (int)m, m, 1, B.w, adaptive, ws, s);
+        return launch_gram(cur, cols, (int)m, m, 1, B.w, adaptive && cols < (1LL << 22), ws, s);
       }));
       TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
@@ -690,9 +691,13 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
           TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, ksa, B.yf, m, ksa, s));
           TT_TRY(launch_cholqr2(B.yf, m, ksa, 1, m, nullptr, ws, c->dstat, s));
         }
-        // B^T = A^T Q (cols x ksa, row-major) = B (ksa x cols, column-major)
+        // B^T = A^T Q (cols x ksa, row-major) = B (ksa x cols, column-major).  Adaptive ranks
+        // take ||B||^2 as the captured energy, which must hold ~1e-8 relative: TF32 operands
+        // (round-to-nearest in the TMA unit, a measured product bias of ~-2e-6) would shift it
+        // by more than delta^2, so that mode forms B on the FP32 engine.
         TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
-          return launch_project(cur, m, cols, B.yf, ksa, m, B.bt, ksa, OUT_ROWMAJOR, 1, 1, engine, ws, c->dstat, s);
+          return launch_project(cur, m, cols, B.yf, ksa, m, B.bt, ksa, OUT_ROWMAJOR, 1, 1,
+                                adaptive ? TT_GEMM_FP32 : engine, ws, c->dstat, s);
         }));
         // Gram of the small factor B (ksa x cols, column-major = B^T row-major): the input of
         // the eigen-based small SVD (TT3O:717), on the tensor cores for long B.

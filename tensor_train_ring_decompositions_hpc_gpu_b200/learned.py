@@ -22,7 +22,8 @@ module builds its training set and trains it with the library's own GPU kernels:
   measure the validation loss.
 
 ``python -m tensor_train_ring_decompositions_hpc_gpu_b200.learned train --out FILE`` runs it on a
-GPU and writes the parameters (``TT_MLP_PARAMS`` float32 values in a .npy file).
+GPU and writes the parameters (``TT_MLP_PARAMS`` float32 values in a .npy file);
+``... learned evaluate`` compares the shipped predictor with the plain adaptive method.
 """
 from __future__ import annotations
 
@@ -211,6 +212,53 @@ def build_dataset(count, seed, workers=None, log=None):
     return dict(k=k, alpha=alpha, tol=tol, r=r, s=s, p=p, feasible=feas, x=x, t=targets(r, s, p))
 
 
+def evaluate(weights=WEIGHTS, count=24, n=32768, tol=1e-3, seed=5, reps=3, log=None):
+    """Learned against plain adaptive EDrSVD on `count` held-out unfoldings U diag(i^-alpha) V^T
+    (m ~ U{200..1024}, alpha ~ U[0.5, 2], orthonormal U, V drawn on the GPU): passes over A,
+    device time (median of `reps` after a warm-up), achieved error and its estimate."""
+    import torch
+    from . import TT_FLAG_ADAPTIVE_KS, TT_FLAG_LEARNED, set_predictor, tt_svd
+    dev = torch.device("cuda", 0)
+    set_predictor(load_params(weights))
+    rng = np.random.default_rng(seed)
+    rows = []
+    try:
+        for i in range(count):
+            m = int(rng.integers(200, 1025))
+            alpha = float(rng.uniform(0.5, 2.0))
+            g = torch.Generator(device=dev).manual_seed(i)
+            u, _ = torch.linalg.qr(torch.randn(m, m, generator=g, device=dev))
+            v, _ = torch.linalg.qr(torch.randn(n, m, generator=g, device=dev))
+            sig = torch.arange(1, m + 1, device=dev, dtype=torch.float32) ** (-alpha)
+            a = (u * sig) @ v.T
+            out = {"m": m, "n": n, "alpha": alpha}
+            for name, flags in (("plain", TT_FLAG_ADAPTIVE_KS), ("learned", TT_FLAG_LEARNED)):
+                tt_svd(a, [1, 120, 1], eps=tol, power_iters=1, flags=flags)
+                ms = []
+                for _ in range(reps):
+                    res = tt_svd(a, [1, 120, 1], eps=tol, power_iters=1, flags=flags)
+                    ms.append(res.ms)
+                uu = res.cores[0].reshape(m, -1).double()
+                ww = res.cores[1].reshape(res.cores[1].shape[0], -1).double()
+                err = float(torch.linalg.matrix_norm(a.double() - uu @ ww) / torch.linalg.matrix_norm(a.double()))
+                out[name] = dict(ms=float(np.median(ms)), passes=res.passes, ks=res.step_ks[0], p=res.step_power[0],
+                                 attempts=res.step_attempts[0], fallbacks=res.fallbacks, rank=res.ranks[1],
+                                 est=res.est_rel_err, err=err)
+            rows.append(out)
+            if log:
+                log(json.dumps(out))
+    finally:
+        set_predictor(None)
+    summ = {"unfoldings": count, "tol": tol,
+            "passes_plain": int(sum(r["plain"]["passes"] for r in rows)),
+            "passes_learned": int(sum(r["learned"]["passes"] for r in rows)),
+            "ms_plain": float(sum(r["plain"]["ms"] for r in rows)),
+            "ms_learned": float(sum(r["learned"]["ms"] for r in rows)),
+            "fallbacks": int(sum(r["learned"]["fallbacks"] for r in rows)),
+            "max_err_ratio_learned_over_plain": float(max(r["learned"]["err"] / r["plain"]["err"] for r in rows))}
+    return summ, rows
+
+
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
@@ -224,7 +272,15 @@ def main(argv=None):
     tr.add_argument("--out", required=True)
     tr.add_argument("--report", default=None, help="JSON summary of the run")
     tr.add_argument("--save-data", default=None, help="write the training set (.npz)")
+    ev = sub.add_parser("evaluate")
+    ev.add_argument("--weights", default=WEIGHTS)
+    ev.add_argument("--count", type=int, default=24)
+    ev.add_argument("--tol", type=float, default=1e-3)
     args = ap.parse_args(argv)
+    if args.cmd == "evaluate":
+        summ, _ = evaluate(args.weights, args.count, tol=args.tol, log=lambda msg: print(msg, flush=True))
+        print(json.dumps({"summary": summ}))
+        return 0
     data = build_dataset(args.count, args.seed, args.workers)  # the pool runs before the first GPU call
     if args.save_data:
         np.savez_compressed(args.save_data, **data)
