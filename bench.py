@@ -554,6 +554,48 @@ def run_ours(args, wl):
                "d2h_bytes_per_step": int(sum(t.numel() * 4 for t in hc)), "steps": args.e2e_steps}
         del xh, hc
 
+    # The north-star comparison on the same tensor and GPU: the plain FP32 form (FP32 CUDA-core
+    # GEMMs, the reference's EDrSVD defaults s = 8, p = 1, fixed ranks) and the learned form
+    # (tensor cores, eps = 1e-3 with the caller's ranks as bounds, the shipped predictor
+    # choosing sketch width and power count per randomized step).
+    forms = None
+    if not args.no_forms:
+        def timed(opts, steps=3):
+            st = _lib.TTStats()
+            _lib.check(fn(ctx, C.c_void_p(x.data_ptr()), d, n_arr, r_arr, C.byref(opts), ptrs, C.byref(st)))
+            torch.cuda.synchronize(dev)
+            f0 = torch.cuda.Event(enable_timing=True)
+            f1 = torch.cuda.Event(enable_timing=True)
+            f0.record(stream)
+            for _ in range(steps):
+                _lib.check(fn(ctx, C.c_void_p(x.data_ptr()), d, n_arr, r_arr, C.byref(opts), ptrs, C.byref(st)))
+            f1.record(stream)
+            torch.cuda.synchronize(dev)
+            rr = list(st.ranks[: d + 1])
+            e = C.c_double()
+            _lib.check(ttr.lib().tt_rel_error(ctx, C.c_void_p(x.data_ptr()), d, n_arr, _lib.int_array(rr),
+                                              1 if ring else 0, (C.c_void_p * d)(*[t.data_ptr() for t in flat]),
+                                              C.byref(e)))
+            return {"ms": f0.elapsed_time(f1) / steps, "rel_err": e.value, "ranks": rr, "passes": int(st.passes)}
+        forms = {}
+        po = ttr._opts("fp32", "edrsvd", 8, 1, args.seed, _lib.TT_FLAG_KEEP_SIGMA, 40)
+        forms["plain_fp32"] = timed(po)
+        forms["plain_fp32"]["config"] = "FP32 CUDA-core GEMMs, s = 8, p = 1, fixed ranks"
+        if not ring:
+            from tensor_train_ring_decompositions_hpc_gpu_b200 import learned as _learned
+            ttr.set_predictor(_learned.load_params(), device=dev)
+            lo = ttr._opts(args.gemm, "edrsvd", args.oversample, 1, args.seed,
+                           _lib.TT_FLAG_KEEP_SIGMA | _lib.TT_FLAG_LEARNED, 40)
+            lo.eps = 1e-3
+            forms["learned"] = timed(lo)
+            forms["learned"]["config"] = "tensor cores, eps = 1e-3, shipped predictor (fallback p = 1)"
+            ttr.set_predictor(None, device=dev)
+        forms["this_line"] = {"ms": ms, "rel_err": err.value, "config": "tensor cores, fixed ranks, "
+                              f"s = {args.oversample}, p = {args.power_iters}"}
+        forms["speedup_vs_plain_fp32"] = forms["plain_fp32"]["ms"] / ms
+        if "learned" in forms:
+            forms["learned_speedup_vs_plain_fp32"] = forms["plain_fp32"]["ms"] / forms["learned"]["ms"]
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         xh_np = x.cpu().numpy()
@@ -577,6 +619,7 @@ def run_ours(args, wl):
             "parity": exact_chain_parity(args, wl, err.value, stats[-1]),
             "jacobi_sweeps_max": int(max(st.jacobi_sweeps for st in stats)),
             "roofline": roof,
+            "forms": forms,
             "cpu_baseline": cpu,
             "e2e": e2e,
             "gpu_launches": int(sum(st.kernels for st in stats)),
@@ -605,6 +648,8 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--ref-frac", type=float, default=1.0 / 32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-forms", action="store_true",
+                    help="skip the plain-FP32 and learned comparison on the same tensor")
     ap.add_argument("--shape", default=None, help="override the mode sizes, e.g. 32,32,32,32,24,24")
     ap.add_argument("--ranks", default=None, help="override the ranks, e.g. 1,32,32,32,32,24,1")
     args = ap.parse_args()
