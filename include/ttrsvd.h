@@ -74,7 +74,17 @@ enum {
    * features (tt_probe_features); when the a-posteriori estimate of that attempt exceeds the
    * step tolerance the plain adaptive EDrSVD takes over from twice its sketch width (at least
  * the plain method's first width). */
-  TT_FLAG_LEARNED = 128
+  TT_FLAG_LEARNED = 128,
+  /* x is a host pointer (pinned memory recommended) that is never copied whole to the device:
+   * the passes over the first unfolding (its Gram and its projection) stream it in column
+   * chunks (tt_ctx_set_stream_chunk) through two device buffers, the copy of chunk c + 1
+   * overlapping the kernels of chunk c; the rest of the chain runs on the projected data.  For
+   * tensors larger than device memory whose first unfolding has at most TT_MAX_SMALL rows and
+   * whose projected data (r1 x n2...nd) fits.  TT-SVD with fixed ranks; cores are device
+   * pointers unless TT_FLAG_HOST_IO is also set.  Replaces ttdec_half_lu_host_6
+   * (ttdecomposition/high_order_GPUs/ttdec6_singleGPU.cu:656-796; its per-slice Gram at :567
+   * restarts the accumulation with beta = 0 on every slice, here the slices are summed). */
+  TT_FLAG_HOST_STREAM = 256
 };
 
 typedef struct tt_opts {
@@ -130,6 +140,8 @@ int tt_ctx_create(tt_ctx** out, int device, void* stream);
 int tt_ctx_destroy(tt_ctx* ctx);
 int tt_ctx_set_stream(tt_ctx* ctx, void* stream);
 int tt_ctx_reserve(tt_ctx* ctx, size_t bytes);
+/* Bytes of one host-streaming chunk (TT_FLAG_HOST_STREAM; default 256 MiB, minimum one column). */
+int tt_ctx_set_stream_chunk(tt_ctx* ctx, size_t bytes);
 const char* tt_last_error(void);
 void tt_default_opts(tt_opts* o);
 int tt_abi_version(void);

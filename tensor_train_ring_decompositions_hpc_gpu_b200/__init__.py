@@ -19,7 +19,8 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _lib
-from ._lib import (TT_FLAG_ADAPTIVE_KS, TT_FLAG_CHECK_FINITE, TT_FLAG_HOST_IO, TT_FLAG_IDENTITY_GAUGE,
+from ._lib import (TT_FLAG_ADAPTIVE_KS, TT_FLAG_CHECK_FINITE, TT_FLAG_HOST_IO, TT_FLAG_HOST_STREAM,
+                   TT_FLAG_IDENTITY_GAUGE,
                    TT_FLAG_KEEP_SIGMA, TT_FLAG_LEARNED, TT_FLAG_NO_FOLD, TT_GEMM_AUTO, TT_GEMM_FP32, TT_GEMM_TC,
                    TT_METHOD_EDRSVD, TT_METHOD_EXACT, TTError, check)
 
@@ -27,7 +28,7 @@ __all__ = [
     "tt_svd", "tr_svd", "rel_error", "Result", "gaussian", "sketch", "project", "gram_rows",
     "gram_tall", "cholqr2", "syev", "permute231", "ttdec_gpu_float", "trdec_gpu_float",
     "ttdec_half_lu_device_6", "trdec_half_lu_device_6", "TTError", "lib", "GEMM", "METHOD",
-    "set_predictor", "probe_features", "mlp_forward", "mlp_grad", "mlp_train",
+    "set_predictor", "probe_features", "mlp_forward", "mlp_grad", "mlp_train", "set_stream_chunk",
 ]
 
 GEMM = {"auto": TT_GEMM_AUTO, "tc": TT_GEMM_TC, "fp32": TT_GEMM_FP32}
@@ -124,12 +125,21 @@ def _opts(gemm, method, oversample, power_iters, seed, flags, max_sweeps):
     return o
 
 
+def set_stream_chunk(nbytes, device=None):
+    """Chunk size (bytes) of the host-streamed first unfolding (tt_svd(..., stream=True))."""
+    check(lib().tt_ctx_set_stream_chunk(_ctx_for(device), int(nbytes)))
+
+
 def _run(ring: bool, x, ranks, gemm="auto", method="edrsvd", oversample=8, power_iters=0,
-         seed=1234, flags=0, max_sweeps=40, shape=None, eps=0.0):
+         seed=1234, flags=0, max_sweeps=40, shape=None, eps=0.0, stream=False):
     ranks = [int(r) for r in ranks]
     host = isinstance(x, np.ndarray)
+    if stream:
+        if not host:
+            raise ValueError("stream=True takes a host (NumPy) tensor, ideally backed by pinned memory")
+        flags |= TT_FLAG_HOST_STREAM
     if host:
-        xa = np.asfortranarray(x, dtype=np.float32)
+        xa = x if (x.dtype == np.float32 and x.flags.f_contiguous) else np.asfortranarray(x, dtype=np.float32)
         shape = list(xa.shape)
         d = len(shape)
         cores_np = [np.zeros((ranks[k], shape[k], ranks[k + 1]), dtype=np.float32, order="F")
@@ -183,7 +193,9 @@ def tt_svd(x, ranks, **kw) -> Result:
     method ('edrsvd' | 'exact'), oversample, power_iters, seed, flags, max_sweeps, eps.
     With eps > 0 the ranks are upper bounds and every unfolding is truncated to the smallest
     rank whose discarded energy is <= eps^2 ||X||^2 / (d - 1) (TT-SVD delta-truncation);
-    Result.ranks holds the ranks chosen and Result.est_rel_err the implied error bound."""
+    Result.ranks holds the ranks chosen and Result.est_rel_err the implied error bound.
+    stream=True (NumPy input, fixed ranks): the first unfolding is streamed from host memory in
+    chunks (set_stream_chunk) instead of being copied to the device whole."""
     return _run(False, x, ranks, **kw)
 
 

@@ -17,7 +17,7 @@ TT_GEMM_AUTO, TT_GEMM_TC, TT_GEMM_FP32 = 0, 1, 2
 TT_METHOD_EDRSVD, TT_METHOD_EXACT = 0, 1
 TT_FLAG_HOST_IO, TT_FLAG_CHECK_FINITE, TT_FLAG_NO_FOLD, TT_FLAG_IDENTITY_GAUGE, TT_FLAG_KEEP_SIGMA = 1, 2, 4, 8, 16
 TT_FLAG_PROFILE = 32
-TT_FLAG_ADAPTIVE_KS, TT_FLAG_LEARNED = 64, 128
+TT_FLAG_ADAPTIVE_KS, TT_FLAG_LEARNED, TT_FLAG_HOST_STREAM = 64, 128, 256
 TT_MLP_INPUTS, TT_MLP_OUTPUTS, TT_MLP_PARAMS, TT_PROBE_COLS = 8, 3, 4931, 16
 TT_PASS_GRAM, TT_PASS_SKETCH, TT_PASS_PROJECT, TT_PASS_OTHER = 0, 1, 2, 3
 PASS_NAMES = ["gram", "sketch", "project", "other"]
@@ -27,7 +27,8 @@ TT_STATS_MAX_SIGMA = 64
 
 # Every extern "C" symbol declared in include/ttrsvd.h.
 EXPORTED = [
-    "tt_ctx_create", "tt_ctx_destroy", "tt_ctx_set_stream", "tt_ctx_reserve", "tt_last_error",
+    "tt_ctx_create", "tt_ctx_destroy", "tt_ctx_set_stream", "tt_ctx_reserve", "tt_ctx_set_stream_chunk",
+    "tt_last_error",
     "tt_default_opts", "tt_abi_version", "tt_svd", "tr_svd", "tt_rel_error", "tt_k_gaussian", "tt_k_gaussian_rows",
     "tt_k_sketch", "tt_k_project", "tt_k_gram_rows", "tt_k_gram_tall", "tt_k_cholqr2",
     "tt_k_syev", "tt_k_sketch_noalloc", "tt_svd_batched", "tt_batch_core_capacity",
@@ -86,6 +87,7 @@ def load():
         "tt_ctx_destroy": (i, [vp]),
         "tt_ctx_set_stream": (i, [vp, vp]),
         "tt_ctx_reserve": (i, [vp, C.c_size_t]),
+        "tt_ctx_set_stream_chunk": (i, [vp, C.c_size_t]),
         "tt_last_error": (C.c_char_p, []),
         "tt_default_opts": (None, [P(TTOpts)]),
         "tt_abi_version": (i, []),

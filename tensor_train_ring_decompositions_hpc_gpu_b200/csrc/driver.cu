@@ -44,6 +44,9 @@ struct tt_ctx {
   cudaEvent_t ev0 = nullptr, ev1 = nullptr;
   std::vector<cudaEvent_t> pool;  // per-pass timing events (TT_FLAG_PROFILE)
   float* pred = nullptr;          // predictor parameters, then features (8) and outputs (3)
+  size_t chunk_bytes = 256ull << 20;  // host-streaming chunk
+  cudaStream_t copy_stream = nullptr;  // host-streaming copies
+  cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_used[2] = {nullptr, nullptr};
 };
 
 extern "C" const char* tt_last_error(void) { return ttr::g_err; }
@@ -111,6 +114,11 @@ extern "C" int tt_ctx_destroy(tt_ctx* c) {
   if (c->ev1) cudaEventDestroy(c->ev1);
   for (cudaEvent_t e : c->pool) cudaEventDestroy(e);
   if (c->pred) cudaFree(c->pred);
+  for (int b = 0; b < 2; ++b) {
+    if (c->ev_copied[b]) cudaEventDestroy(c->ev_copied[b]);
+    if (c->ev_used[b]) cudaEventDestroy(c->ev_used[b]);
+  }
+  if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
   delete c;
   return TT_OK;
 }
@@ -145,6 +153,15 @@ extern "C" int tt_ctx_set_predictor(tt_ctx* c, const float* params) {
   }
   TT_CUDA(cudaMemcpyAsync(c->pred, params, sizeof(float) * TT_MLP_PARAMS, cudaMemcpyHostToDevice, c->stream));
   TT_CUDA(cudaStreamSynchronize(c->stream));
+  return TT_OK;
+}
+
+extern "C" int tt_ctx_set_stream_chunk(tt_ctx* c, size_t bytes) {
+  if (!c) {
+    set_error(TT_ERR_ARG, "null ctx");
+    return TT_ERR_ARG;
+  }
+  c->chunk_bytes = bytes;
   return TT_OK;
 }
 
@@ -201,6 +218,7 @@ struct Plan {
   size_t max_ef = (size_t)TT_MAX_SMALL * TT_MAX_SMALL;  // FP32 basis (m x r or ks x r)
   int max_small = 0;
   int last_rows = 1;  // rows per mode index of the data left for the last core
+  long long stream_cols = 0;  // host streaming: columns of the first unfolding per chunk (0: off)
 };
 
 int engine_of(const tt_opts& o) {
@@ -351,13 +369,19 @@ struct Bufs {
   double* pend[2] = {nullptr, nullptr};
   int* flag = nullptr;
   std::vector<float*> cores;  // device cores
+  float* chunk[2] = {nullptr, nullptr};  // host streaming
+  double* wacc = nullptr;
 };
 
 size_t plan_bytes(const Plan& P, bool host_io) {
   const size_t S = TT_MAX_SMALL;
   size_t b = 0;
   auto add = [&](size_t bytes) { b += (bytes + 255) & ~size_t(255); };
-  if (host_io) add(P.total * sizeof(float));
+  if (host_io && !P.stream_cols) add(P.total * sizeof(float));
+  if (P.stream_cols) {
+    add((size_t)P.steps[0].m * P.stream_cols * sizeof(float) * 2);
+    add(S * S * sizeof(double));
+  }
   add(P.max_data * sizeof(float));
   add(P.max_data * sizeof(float));
   add(P.max_omega * sizeof(float));
@@ -379,7 +403,16 @@ size_t plan_bytes(const Plan& P, bool host_io) {
 int carve(tt_ctx* c, const Plan& P, bool host_io, Bufs& B, Arena& ws) {
   Arena a{c->arena, c->cap, 0};
   const size_t S = TT_MAX_SMALL;
-  if (host_io) B.x = a.take<float>(P.total);
+  if (host_io && !P.stream_cols) B.x = a.take<float>(P.total);
+  if (P.stream_cols) {
+    B.chunk[0] = a.take<float>((size_t)P.steps[0].m * P.stream_cols);
+    B.chunk[1] = a.take<float>((size_t)P.steps[0].m * P.stream_cols);
+    B.wacc = a.take<double>(S * S);
+    if (!B.chunk[1] || !B.wacc) {
+      set_error(TT_ERR_NOMEM, "streaming buffers");
+      return TT_ERR_NOMEM;
+    }
+  }
   B.data[0] = a.take<float>(std::max<size_t>(P.max_data, 1));
   B.data[1] = a.take<float>(std::max<size_t>(P.max_data, 1));
   B.omega = a.take<float>(std::max<size_t>(P.max_omega, 1));
@@ -470,6 +503,11 @@ struct Passes {
   }
 };
 
+__global__ void k_add_f64(const double* __restrict__ a, double* __restrict__ acc, int n) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) acc[i] += a[i];
+}
+
 int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* const* cores_out,
               tt_stats* stats) {
   const bool host_io = (o.flags & TT_FLAG_HOST_IO) != 0;
@@ -489,10 +527,47 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
   TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), s));
   TT_CUDA(cudaEventRecord(c->ev0, s));
   const float* x = x_in;
-  if (host_io) {
+  const bool stream = P.stream_cols > 0;  // x stays on the host; step 0 streams it
+  if (host_io && !stream) {
     TT_CUDA(cudaMemcpyAsync(B.x, x_in, sizeof(float) * P.total, cudaMemcpyHostToDevice, s));
     x = B.x;
   }
+  // One pass over the host-resident first unfolding: chunk ch (stream_cols columns) is copied
+  // on the copy stream into buffer ch & 1 while the kernels of chunk ch - 1 run on s; fn(chunk,
+  // first column, columns) enqueues a chunk's kernels on s.
+  auto stream_pass = [&](auto&& fn) -> int {
+    const long long m0 = P.steps[0].m, cols0 = P.steps[0].cols, cc = P.stream_cols;
+    const long long nch = (cols0 + cc - 1) / cc;
+    if (!c->copy_stream) {
+      TT_CUDA(cudaStreamCreateWithFlags(&c->copy_stream, cudaStreamNonBlocking));
+      for (int b = 0; b < 2; ++b) {
+        TT_CUDA(cudaEventCreateWithFlags(&c->ev_copied[b], cudaEventDisableTiming));
+        TT_CUDA(cudaEventCreateWithFlags(&c->ev_used[b], cudaEventDisableTiming));
+      }
+    }
+    // buffers are free once the work already on s (an earlier pass) is done
+    for (int b = 0; b < 2; ++b) TT_CUDA(cudaEventRecord(c->ev_used[b], s));
+    auto issue = [&](long long ch) -> int {
+      const int b = (int)(ch & 1);
+      const long long c0 = ch * cc, nc = std::min(cc, cols0 - c0);
+      TT_CUDA(cudaStreamWaitEvent(c->copy_stream, c->ev_used[b], 0));
+      TT_CUDA(cudaMemcpyAsync(B.chunk[b], x_in + c0 * m0, sizeof(float) * (size_t)(nc * m0), cudaMemcpyHostToDevice,
+                              c->copy_stream));
+      TT_CUDA(cudaEventRecord(c->ev_copied[b], c->copy_stream));
+      return TT_OK;
+    };
+    TT_TRY(issue(0));
+    if (nch > 1) TT_TRY(issue(1));
+    for (long long ch = 0; ch < nch; ++ch) {
+      const int b = (int)(ch & 1);
+      const long long c0 = ch * cc, nc = std::min(cc, cols0 - c0);
+      TT_CUDA(cudaStreamWaitEvent(s, c->ev_copied[b], 0));
+      TT_TRY(fn((const float*)B.chunk[b], c0, nc));
+      TT_CUDA(cudaEventRecord(c->ev_used[b], s));
+      if (ch + 2 < nch) TT_TRY(issue(ch + 2));
+    }
+    return TT_OK;
+  };
   std::vector<float*> cores(P.d);
   for (int k = 0; k < P.d; ++k) cores[k] = host_io ? B.cores[k] : cores_out[k];
 
@@ -600,7 +675,38 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       continue;  // data unchanged
     }
 
-    if (st.path == PATH_EXACT_ROWS) {
+    if (st.path == PATH_EXACT_ROWS && stream && k == 0) {
+      // host-streamed first unfolding: Gram summed over the chunks in FP64, projection per chunk
+      npasses += 2;
+      TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols, [&]() -> int {
+        TT_CUDA(cudaMemsetAsync(B.wacc, 0, sizeof(double) * m * m, s));
+        TT_TRY(stream_pass([&](const float* a, long long, long long nc) -> int {
+          const int eng = engine_for(o, m, nc);
+          int rc = TT_ERR_UNSUPPORTED;
+          if (eng == TT_GEMM_TC) rc = launch_gram_tc(a, m, nc, B.w, ws, c->dstat, s);
+          if (rc == TT_ERR_UNSUPPORTED) rc = launch_gram(a, nc, (int)m, m, 1, B.w, false, ws, s);
+          TT_TRY(rc);
+          k_add_f64<<<ceil_div(m * m, 256), 256, 0, s>>>(B.w, B.wacc, (int)(m * m));
+          count_launch();
+          TT_LAUNCH_CHECK();
+          return TT_OK;
+        }));
+        TT_CUDA(cudaMemcpyAsync(B.w, B.wacc, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, s));
+        return TT_OK;
+      }));
+      TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
+      k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
+      count_launch();
+      TT_TRY(launch_f64_to_f32_cols(B.evecs, m, m, re, B.ef, m, rq, s));
+      TT_TRY(launch_canon_cols(B.ef, m, re, m, B.evecs, (int)m, m, s));
+      TT_TRY(emit_core(B.ef, core_dst, pend, rin, rcore, ni, rq, s));
+      TT_TRY(pass.run(TT_PASS_PROJECT, 2.0 * m * cols * nout, 4.0 * m * cols + 4.0 * nout * cols, [&]() -> int {
+        return stream_pass([&](const float* a, long long c0, long long nc) -> int {
+          return launch_project(a, m, nc, B.ef, nout, m, next + c0 * nout, nout, OUT_ROWMAJOR, 1, 1,
+                                engine_for(o, m, nc), ws, c->dstat, s);
+        });
+      }));
+    } else if (st.path == PATH_EXACT_ROWS) {
       npasses += st.fold ? 1 : 2;
       TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols, [&] {
         // adaptive ranks read energies to ~1e-8 relative: FP32 products (unbiased rounding)
@@ -905,6 +1011,14 @@ int run_entry(tt_ctx* c, const float* x, int d, const int* n, const int* r, cons
     set_error(TT_ERR_ARG, "TT_FLAG_LEARNED without a predictor (tt_ctx_set_predictor)");
     return TT_ERR_ARG;
   }
+  if (o.flags & TT_FLAG_HOST_STREAM) {
+    if (ring || o.eps > 0.0 || (o.flags & (TT_FLAG_CHECK_FINITE | TT_FLAG_ADAPTIVE_KS | TT_FLAG_LEARNED))) {
+      set_error(TT_ERR_UNSUPPORTED, "TT_FLAG_HOST_STREAM: TT-SVD with fixed ranks only");
+      return TT_ERR_UNSUPPORTED;
+    }
+    o.flags |= TT_FLAG_NO_FOLD;  // the first projection is materialised from the streamed chunks
+    o.flags &= ~TT_FLAG_IDENTITY_GAUGE;
+  }
   if (o.eps > 0.0) {
     if (ring) {
       set_error(TT_ERR_UNSUPPORTED, "adaptive ranks (eps > 0) are implemented for TT-SVD only");
@@ -914,6 +1028,19 @@ int run_entry(tt_ctx* c, const float* x, int d, const int* n, const int* r, cons
   }
   Plan P;
   TT_TRY(make_plan(d, n, r, ring, o, P));
+  if (o.flags & TT_FLAG_HOST_STREAM) {
+    const Step& s0 = P.steps[0];
+    if (s0.path != PATH_EXACT_ROWS) {
+      set_error(TT_ERR_UNSUPPORTED, "TT_FLAG_HOST_STREAM needs a first unfolding with <= %d rows (got %lld x %lld)",
+                TT_MAX_SMALL, s0.m, s0.cols);
+      return TT_ERR_UNSUPPORTED;
+    }
+    P.stream_cols = std::max<long long>(1, std::min<long long>(s0.cols, (long long)(c->chunk_bytes / (4 * s0.m))));
+    // the Gram and projection kernels see one chunk at a time
+    P.max_ws = std::max(P.max_ws, gram_ws_bytes(P.stream_cols, (int)s0.m));
+    P.max_ws = std::max(P.max_ws, gram_tc_ws_bytes(s0.m, P.stream_cols));
+    P.max_ws = std::max(P.max_ws, project_ws_bytes(s0.m, P.stream_cols, s0.r_req));
+  }
   for (int k = 0; k < d; ++k)
     if (!cores[k]) {
       set_error(TT_ERR_ARG, "null core pointer %d", k);

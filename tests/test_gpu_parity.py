@@ -261,3 +261,42 @@ def test_adaptive_eps_rejects_ring(gpu):
     x = torch.randn(8 * 8 * 8, device=gpu)
     with pytest.raises(Exception):
         ttr.tr_svd(x, [2, 2, 2, 2], eps=1e-2, shape=[8, 8, 8])
+
+
+@pytest.mark.parametrize("chunk", [4096, 1 << 20])
+def test_host_stream_matches_device_chain(gpu, chunk):
+    """TT_FLAG_HOST_STREAM: the first unfolding streamed from host memory in column chunks
+    (many chunks at 4 KiB) gives the same singular values and error as the chain on a
+    device-resident copy, against the oracle's exact chain."""
+    import torch
+    ttr = _ttr()
+    shape, ranks = [16, 12, 10, 8], [1, 8, 8, 6, 1]
+    x = oracle.make_tt_tensor(shape, ranks, 1e-3, seed=61)
+    pinned = torch.empty(x.size, dtype=torch.float32).pin_memory()
+    xs = pinned.numpy().reshape(shape[::-1]).transpose()  # Fortran-ordered view of pinned memory
+    xs[...] = x
+    ttr.set_stream_chunk(chunk)
+    try:
+        res_s = ttr.tt_svd(xs, ranks, gemm="fp32", stream=True)
+    finally:
+        ttr.set_stream_chunk(256 << 20)
+    res_d = ttr.tt_svd(torch.from_numpy(np.ascontiguousarray(x)).to(gpu), ranks, gemm="fp32")
+    err_s = oracle.rel_error(x, oracle.tt_full([np.asarray(c, dtype=np.float64) for c in res_s.cores]))
+    err_d = oracle.rel_error(x, oracle.tt_full([c.double().cpu().numpy() for c in res_d.cores]))
+    ocores, _ = oracle.tt_svd(x.astype(np.float64), ranks, method="gram")
+    oerr = oracle.rel_error(x, oracle.tt_full(ocores))
+    assert abs(err_s - err_d) < 1e-6 and abs(err_s - oerr) < 1e-4
+    for a, b in zip(res_s.sigmas, res_d.sigmas):
+        np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-6 * b[0])
+
+
+def test_host_stream_rejects_unsupported(gpu):
+    ttr = _ttr()
+    x = oracle.make_tt_tensor([8, 8, 8], [1, 4, 4, 1], 1e-3, seed=2)
+    with pytest.raises(ttr.TTError):
+        ttr.tt_svd(x, [1, 4, 4, 1], eps=1e-2, stream=True)
+    with pytest.raises(ttr.TTError):
+        ttr.tr_svd(x, [2, 2, 2, 2], stream=True)
+    big = np.ones((200, 4, 4), dtype=np.float32)  # first unfolding 200 x 16: randomized step
+    with pytest.raises(ttr.TTError):
+        ttr.tt_svd(big, [1, 4, 4, 1], stream=True)
