@@ -223,8 +223,13 @@ struct Plan {
 
 int engine_of(const tt_opts& o) {
   if (o.gemm == TT_GEMM_FP32) return TT_GEMM_FP32;
-  return tc_available() ? TT_GEMM_TC : TT_GEMM_FP32;
+  if (!tc_available()) return TT_GEMM_FP32;
+  return o.gemm == TT_GEMM_TC3 ? TT_GEMM_TC3 : TT_GEMM_TC;
 }
+
+// Engine of a projection whose output feeds the energy bookkeeping of adaptive ranks: the
+// 3xTF32 tensor-core variant (unbiased to ~2^-21) instead of plain TF32.
+int precise_engine(int engine) { return engine == TT_GEMM_TC ? TT_GEMM_TC3 : engine; }
 
 // Engine of a bulk pass over an m x cols unfolding.  TT_GEMM_AUTO keeps passes below 2^24
 // elements on the FP32 kernels (they are cheap there and carry full FP32 precision); the
@@ -683,7 +688,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         TT_TRY(stream_pass([&](const float* a, long long, long long nc) -> int {
           const int eng = engine_for(o, m, nc);
           int rc = TT_ERR_UNSUPPORTED;
-          if (eng == TT_GEMM_TC) rc = launch_gram_tc(a, m, nc, B.w, ws, c->dstat, s);
+          if (eng != TT_GEMM_FP32) rc = launch_gram_tc(a, m, nc, B.w, ws, c->dstat, s);
           if (rc == TT_ERR_UNSUPPORTED) rc = launch_gram(a, nc, (int)m, m, 1, B.w, false, ws, s);
           TT_TRY(rc);
           k_add_f64<<<ceil_div(m * m, 256), 256, 0, s>>>(B.w, B.wacc, (int)(m * m));
@@ -712,7 +717,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         // adaptive ranks read energies to ~1e-8 relative: FP32 products (unbiased rounding)
         // instead of TF32 ones, FP64 accumulation (per product for short unfoldings, per 1024
         // columns for long ones, whose many partial sums average the FP32 rounding out)
-        if (engine == TT_GEMM_TC && !adaptive) {
+        if (engine != TT_GEMM_FP32 && !adaptive) {
           const int rc = launch_gram_tc(cur, m, cols, B.w, ws, c->dstat, s);
           if (rc != TT_ERR_UNSUPPORTED) return rc;
         }
@@ -741,7 +746,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       TT_TRY(pass.run(TT_PASS_PROJECT, 2.0 * m * cols * nout, 4.0 * m * cols + 4.0 * nout * cols, [&] {
         return launch_project(cur, m, cols, B.ef, nout, m, next, st.perm231 ? 0 : nout,
                               st.perm231 ? OUT_PERM231 : OUT_ROWMAJOR, P.r[0], pr1,
-                              engine, ws, c->dstat, s);
+                              adaptive ? precise_engine(engine) : engine, ws, c->dstat, s);
       }));
     } else if (st.path == PATH_EXACT_COLS) {
       npasses += 2;
@@ -799,11 +804,11 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         }
         // B^T = A^T Q (cols x ksa, row-major) = B (ksa x cols, column-major).  Adaptive ranks
         // take ||B||^2 as the captured energy, which must hold ~1e-8 relative: TF32 operands
-        // (round-to-nearest in the TMA unit, a measured product bias of ~-2e-6) would shift it
-        // by more than delta^2, so that mode forms B on the FP32 engine.
+        // (a measured product bias of ~-2e-6) would shift it by more than delta^2, so that mode
+        // forms B with the 3xTF32 tensor-core projection.
         TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
           return launch_project(cur, m, cols, B.yf, ksa, m, B.bt, ksa, OUT_ROWMAJOR, 1, 1,
-                                adaptive ? TT_GEMM_FP32 : engine, ws, c->dstat, s);
+                                adaptive ? precise_engine(engine) : engine, ws, c->dstat, s);
         }));
         // Gram of the small factor B (ksa x cols, column-major = B^T row-major): the input of
         // the eigen-based small SVD (TT3O:717), on the tensor cores for long B.
@@ -811,7 +816,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         // eigenvalue sum must then hold ~1e-8 relative, which the tensor-core Gram (TF32
         // operands, FP32 accumulation within 2048-column units) does not guarantee on short B.
         TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ksa * ksa, 4.0 * cols * ksa, [&] {
-          if (engine == TT_GEMM_TC && !adaptive) {
+          if (engine != TT_GEMM_FP32 && !adaptive) {
             const int rc = launch_gram_tc(B.bt, ksa, cols, B.w, ws, c->dstat, s);
             if (rc != TT_ERR_UNSUPPORTED) return rc;
           }
@@ -1310,7 +1315,9 @@ extern "C" int tt_k_project(tt_ctx* c, const float* a, long long m, long long n,
   TT_CUDA(cudaSetDevice(c->device));
   Arena ws;
   TT_TRY(ws_for(c, std::max<size_t>(1 << 20, project_ws_bytes(m, n, N)), ws));
-  const int eng = (gemm == TT_GEMM_FP32 || !tc_available()) ? TT_GEMM_FP32 : TT_GEMM_TC;
+  const int eng = (gemm == TT_GEMM_FP32 || !tc_available()) ? TT_GEMM_FP32
+                  : gemm == TT_GEMM_TC3                       ? TT_GEMM_TC3
+                                                              : TT_GEMM_TC;
   TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
   TT_TRY(launch_project(a, m, n, q, N, ldq, out, ldo, OUT_ROWMAJOR, 1, 1, eng, ws, c->dstat, c->stream));
   return check_status(c);

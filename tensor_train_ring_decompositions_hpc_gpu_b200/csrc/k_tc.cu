@@ -178,6 +178,9 @@ struct Bars {
   __device__ uint32_t tfull(int b) const { return base + 8u * (2 * stages + b); }       // b < 4
   __device__ uint32_t tempty(int b) const { return base + 8u * (2 * stages + 4 + b); }  // b < 4
   __device__ uint32_t drain() const { return base + 8u * (2 * stages + 8); }
+  // after the drain barrier: per stage "A split into hi / lo" (the 3xTF32 projection only;
+  // that kernel reserves room for count(stages) + stages barriers)
+  __device__ uint32_t conv(int s) const { return base + 8u * (2 * stages + 9 + s); }
   __host__ __device__ static constexpr int count(int stages) { return 2 * stages + 9; }
 };
 
@@ -195,17 +198,36 @@ __device__ __forceinline__ void drain_fills(const Bars& bars, int stages, long l
 // ---------------------------------------------------------------------------------------
 // projection kernel: out = A^T Q   (persistent over 128-column tiles of A)
 // ---------------------------------------------------------------------------------------
-// SPLIT: Q arrives as an exactly-TF32 high part (tmB) and its FP32 remainder (tmB2); each
-// K-step issues A*Qhi and A*Qlo into the same accumulator, so Q carries FP32 precision.
-template <int BN, int STAGES, bool SPLIT>
-__global__ void __launch_bounds__(320, 1)
+// SPLIT: Q arrives as an exactly-TF32 high part (tmB) and its remainder (tmB2); each K-step
+// issues A*Qhi and A*Qlo into the same accumulator, so Q carries FP32 precision.
+// SPLITA (3xTF32): A is loaded as FP32 and four converter warps split every stage in shared
+// memory into hi = rn_tf32(a) (in place) and lo = rn_tf32(a - hi); the K-step then issues
+// Ahi*Qhi + Ahi*Qlo + Alo*Qhi, products exact to ~2^-21 and unbiased (round to nearest
+// everywhere), for passes whose results feed energy bookkeeping at 1e-8 relative.
+// Round-to-nearest-even FP32 -> TF32 (10 stored mantissa bits).
+__device__ __forceinline__ float tf32_rn(float x) {
+  uint32_t u = __float_as_uint(x);
+  if ((u & 0x7F800000u) != 0x7F800000u) {
+    u += 0x0FFFu + ((u >> 13) & 1u);
+    u &= 0xFFFFE000u;
+  }
+  return __uint_as_float(u);
+}
+
+constexpr uint32_t kProjBarBytes = 512;  // barrier / TMEM-slot region of the projection kernel
+template <int BN, int STAGES, bool SPLIT, bool SPLITA>
+__global__ void __launch_bounds__(SPLITA ? 448 : 320, 1)
     k_project_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  const __grid_constant__ CUtensorMap tmB2, long long n, int N, int KB,
                  float* __restrict__ out, long long ldo, int mode, int r0, int r1, DevStatus* st) {
   constexpr int BM = 128;
   constexpr uint32_t A_BYTES = BM * 128;
   constexpr uint32_t B_BYTES = BN * 128;
-  constexpr uint32_t STAGE_BYTES = A_BYTES + (SPLIT ? 2 : 1) * B_BYTES;  // 1 KB aligned
+  constexpr uint32_t ALO_BYTES = SPLITA ? A_BYTES : 0;
+  constexpr uint32_t STAGE_BYTES = A_BYTES + ALO_BYTES + (SPLIT ? 2 : 1) * B_BYTES;  // 1 KB aligned
+  constexpr uint32_t TMA_BYTES = A_BYTES + (SPLIT ? 2 : 1) * B_BYTES;
+  static_assert(SPLIT || !SPLITA, "3xTF32 needs the Q split");
+  static_assert(8 * (Bars::count(STAGES) + STAGES) + 8 <= kProjBarBytes, "barrier region");
   constexpr uint32_t BNP = pow2_cols(BN);
   constexpr uint32_t TMEM_COLS = pow2_cols(4 * BNP);  // four accumulators, two per epilogue group
   constexpr uint32_t IDESC = idesc_tf32(BM, BN, 0, 0);
@@ -214,7 +236,7 @@ __global__ void __launch_bounds__(320, 1)
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* barmem = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(barmem + Bars::count(STAGES));
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(barmem + Bars::count(STAGES) + STAGES);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const Bars bars{smem_u32(barmem), STAGES};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -225,6 +247,7 @@ __global__ void __launch_bounds__(320, 1)
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(bars.full(s), 1);
       mbar_init(bars.empty(s), 1);
+      if (SPLITA) mbar_init(bars.conv(s), 4);
     }
     for (int b = 0; b < 4; ++b) {
       mbar_init(bars.tfull(b), 1);
@@ -258,11 +281,11 @@ __global__ void __launch_bounds__(320, 1)
             ok = false;
             break;
           }
-          mbar_expect_tx(bars.full(stage), STAGE_BYTES);
+          mbar_expect_tx(bars.full(stage), TMA_BYTES);
           const uint32_t sa = sbase + stage * STAGE_BYTES;
           tma_load_2d(sa, &tmA, bars.full(stage), kb * 32, j0);
-          tma_load_2d(sa + A_BYTES, &tmB, bars.full(stage), kb * 32, 0);
-          if (SPLIT) tma_load_2d(sa + A_BYTES + B_BYTES, &tmB2, bars.full(stage), kb * 32, 0);
+          tma_load_2d(sa + A_BYTES + ALO_BYTES, &tmB, bars.full(stage), kb * 32, 0);
+          if (SPLIT) tma_load_2d(sa + A_BYTES + ALO_BYTES + B_BYTES, &tmB2, bars.full(stage), kb * 32, 0);
           ++nissued;
           if (++stage == STAGES) {
             stage = 0;
@@ -293,19 +316,21 @@ __global__ void __launch_bounds__(320, 1)
         tc_fence_after();
         const uint32_t d = tmem_base + (uint32_t)buf * BNP;
         for (int kb = 0; kb < KB; ++kb) {
-          if (!mbar_wait(bars.full(stage), phase, abort_flag)) {
+          if (!mbar_wait(SPLITA ? bars.conv(stage) : bars.full(stage), phase, abort_flag)) {
             ok = false;
             break;
           }
           tc_fence_after();
           const uint32_t sa = sbase + stage * STAGE_BYTES;
           const uint64_t da = desc_kmajor(sa, 2, 1024);
-          const uint64_t db = desc_kmajor(sa + A_BYTES, 2, 1024);
-          const uint64_t db2 = desc_kmajor(sa + A_BYTES + B_BYTES, 2, 1024);
+          const uint64_t dlo = desc_kmajor(sa + A_BYTES, 2, 1024);
+          const uint64_t db = desc_kmajor(sa + A_BYTES + ALO_BYTES, 2, 1024);
+          const uint64_t db2 = desc_kmajor(sa + A_BYTES + ALO_BYTES + B_BYTES, 2, 1024);
 #pragma unroll
           for (int s = 0; s < 4; ++s) {
             mma_tf32(d, da + 2ull * s, db + 2ull * s, IDESC, (kb | s) ? 1u : 0u);
             if (SPLIT) mma_tf32(d, da + 2ull * s, db2 + 2ull * s, IDESC, 1u);
+            if (SPLITA) mma_tf32(d, dlo + 2ull * s, db + 2ull * s, IDESC, 1u);
           }
           mma_commit(bars.empty(stage));
           if (++stage == STAGES) {
@@ -322,6 +347,40 @@ __global__ void __launch_bounds__(320, 1)
       }
       mma_commit(bars.drain());
       mbar_wait_bounded(bars.drain(), 0);
+    }
+  } else if (SPLITA && warp >= 10) {
+    // converters: split each landed A stage into TF32 hi (in place) and lo; a quarter each
+    const int cw = warp - 10;
+    int stage = 0;
+    uint32_t phase = 0;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+      bool ok = true;
+      for (int kb = 0; kb < KB; ++kb) {
+        if (!mbar_wait(bars.full(stage), phase, abort_flag)) {
+          ok = false;
+          break;
+        }
+        float4* av = reinterpret_cast<float4*>(smem + stage * STAGE_BYTES);
+        float4* lv = reinterpret_cast<float4*>(smem + stage * STAGE_BYTES + A_BYTES);
+        for (int i = cw * 32 + lane; i < (int)(A_BYTES / 16); i += 128) {
+          const float4 v = av[i];
+          const float4 h = make_float4(tf32_rn(v.x), tf32_rn(v.y), tf32_rn(v.z), tf32_rn(v.w));
+          av[i] = h;
+          lv[i] = make_float4(tf32_rn(v.x - h.x), tf32_rn(v.y - h.y), tf32_rn(v.z - h.z), tf32_rn(v.w - h.w));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bars.conv(stage));
+        if (++stage == STAGES) {
+          stage = 0;
+          phase ^= 1u;
+        }
+      }
+      if (!ok) {
+        *abort_flag = 1;
+        dev_fail(st, TT_ERR_TIMEOUT, 4);
+        break;
+      }
     }
   } else {
     // Two epilogue groups of four warps (one per TMEM lane quadrant each) take alternate tiles:
@@ -354,7 +413,7 @@ __global__ void __launch_bounds__(320, 1)
       if (BN <= 32 && mode == OUT_PERM231) {  // the launcher sends the bond permute only for BN <= 32
         // Bond permute through shared memory: for each a, the warp's 32 columns j form one
         // contiguous run of r1 * 32 outputs (b fastest), written with coalesced stores.
-        float* stg = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(barmem) + 256) + (warp - 2) * 32 * (BN + 1);
+        float* stg = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(barmem) + kProjBarBytes) + (warp - 2) * 32 * (BN + 1);
 #pragma unroll
         for (int c = 0; c < BN; ++c) stg[lane * (BN + 1) + c] = __uint_as_float(r[c]);
         __syncwarp();
@@ -844,15 +903,6 @@ int set_smem(K kernel, size_t bytes) {
 
 constexpr size_t kSmemBudget = 200 * 1024;
 
-// Round-to-nearest-even FP32 -> TF32 (10 stored mantissa bits) and the exact remainder.
-__device__ __forceinline__ float tf32_rn(float x) {
-  uint32_t u = __float_as_uint(x);
-  if ((u & 0x7F800000u) != 0x7F800000u) {
-    u += 0x0FFFu + ((u >> 13) & 1u);
-    u &= 0xFFFFE000u;
-  }
-  return __uint_as_float(u);
-}
 
 __global__ void k_split_tf32(const float* __restrict__ q, long long m, int N, long long ldq,
                              float* __restrict__ hi, float* __restrict__ lo, long long ldo) {
@@ -863,20 +913,20 @@ __global__ void k_split_tf32(const float* __restrict__ q, long long m, int N, lo
     const float v = q[i + ldq * c];
     const float h = tf32_rn(v);
     hi[i + ldo * c] = h;
-    lo[i + ldo * c] = v - h;
+    lo[i + ldo * c] = tf32_rn(v - h);  // the MMA reads TF32: round the remainder to nearest too
   }
 }
 
-template <int BN, bool SPLIT>
+template <int BN, bool SPLIT, bool SPLITA>
 int run_project(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap& mb2, long long n,
                 int N, int KB, float* out, long long ldo, int mode, int r0, int r1, DevStatus* st,
                 cudaStream_t s) {
-  constexpr uint32_t STAGE = 128 * 128 + (SPLIT ? 2 : 1) * BN * 128;
+  constexpr uint32_t STAGE = 128 * 128 * (SPLITA ? 2 : 1) + (SPLIT ? 2 : 1) * BN * 128;
   // bond-permute staging of the 8 epilogue warps (that epilogue runs for BN <= 32 only)
   constexpr size_t STAGING = BN <= 32 ? 8 * 32 * (BN + 1) * sizeof(float) : 0;
   constexpr int STAGES = (int)std::min<size_t>(10, (kSmemBudget - STAGING) / STAGE);
-  const size_t smem = (size_t)STAGES * STAGE + 1024 + 256 + STAGING;
-  auto kern = k_project_tc<BN, STAGES, SPLIT>;
+  const size_t smem = (size_t)STAGES * STAGE + 1024 + kProjBarBytes + STAGING;
+  auto kern = k_project_tc<BN, STAGES, SPLIT, SPLITA>;
   static bool attr = false;
   if (!attr) {
     if (set_smem(kern, smem) != TT_OK) {
@@ -887,7 +937,7 @@ int run_project(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap&
   }
   const long long ntiles = (n + 127) / 128;
   const int grid = (int)std::min<long long>(ntiles, (long long)g_sms);
-  kern<<<grid, 320, smem, s>>>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st);
+  kern<<<grid, SPLITA ? 448 : 320, smem, s>>>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st);
   count_launch();
   TT_LAUNCH_CHECK();
   return TT_OK;
@@ -1038,7 +1088,7 @@ size_t sketch_tc_ws_bytes(long long m, long long n, int N) {
 }
 
 int launch_project_tc(const float* a, long long m, long long n, const float* q, int N,
-                      long long ldq, float* out, long long ldo, int mode, int r0, int r1,
+                      long long ldq, float* out, long long ldo, int mode, int r0, int r1, bool split_a,
                       Arena& ws, DevStatus* st, cudaStream_t s) {
   if (!init_tc()) return TT_ERR_UNSUPPORTED;
   if (N > 128 || (m & 3) || (reinterpret_cast<uintptr_t>(a) & 15) || n > (1LL << 31) - 256 ||
@@ -1063,21 +1113,33 @@ int launch_project_tc(const float* a, long long m, long long n, const float* q, 
     TT_LAUNCH_CHECK();
   }
   CUtensorMap ma, mb, mb2;
-  // A through the TFLOAT32 tensor-map type; the MMA then sees TMA-converted operands.
+  // A through the TFLOAT32 tensor-map type (the TMA rounds to TF32), or as FP32 for the
+  // in-kernel hi / lo split of the 3xTF32 variant.
   TT_TRY(make_map(&ma, a, (unsigned long long)m, (unsigned long long)n, (unsigned long long)m * 4, 32, 128,
-                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
+                  CU_TENSOR_MAP_SWIZZLE_128B,
+                  split_a ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
   TT_TRY(make_map(&mb, qhi, (unsigned long long)m, (unsigned long long)N, (unsigned long long)ldh * 4, 32,
                   (unsigned)BN, CU_TENSOR_MAP_SWIZZLE_128B));
   TT_TRY(make_map(&mb2, qlo, (unsigned long long)m, (unsigned long long)N, (unsigned long long)ldh * 4, 32,
                   (unsigned)BN, CU_TENSOR_MAP_SWIZZLE_128B));
   const int KB = (int)((m + 31) / 32);
   int rc;
-  switch (BN) {
-    case 16: rc = run_project<16, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-    case 32: rc = run_project<32, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-    case 48: rc = run_project<48, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-    case 64: rc = run_project<64, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-    default: rc = run_project<128, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+  if (split_a) {
+    switch (BN) {
+      case 16: rc = run_project<16, true, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+      case 32: rc = run_project<32, true, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+      case 48: rc = run_project<48, true, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+      case 64: rc = run_project<64, true, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+      default: rc = run_project<128, true, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+    }
+  } else {
+    switch (BN) {
+      case 16: rc = run_project<16, true, false>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+      case 32: rc = run_project<32, true, false>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+      case 48: rc = run_project<48, true, false>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+      case 64: rc = run_project<64, true, false>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+      default: rc = run_project<128, true, false>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+    }
   }
   ws.reset(mk);  // the split copies are consumed by the launch above (stream-ordered)
   return rc;

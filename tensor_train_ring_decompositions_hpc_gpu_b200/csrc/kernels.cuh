@@ -153,7 +153,7 @@ int launch_gram_tc(const float* a, long long m, long long n, double* w, Arena& w
 int launch_sketch_tc(const float* a, long long m, long long n, const float* w, int N, long long wj,
                      long long wc, double* y, Arena& ws, DevStatus* st, cudaStream_t s);
 int launch_project_tc(const float* a, long long m, long long n, const float* q, int N,
-                      long long ldq, float* out, long long ldo, int mode, int r0, int r1,
+                      long long ldq, float* out, long long ldo, int mode, int r0, int r1, bool split_a,
                       Arena& ws, DevStatus* st, cudaStream_t s);
 
 }  // namespace ttr
