@@ -227,8 +227,9 @@ int engine_of(const tt_opts& o) {
   return o.gemm == TT_GEMM_TC3 ? TT_GEMM_TC3 : TT_GEMM_TC;
 }
 
-// Engine of a projection whose output feeds the energy bookkeeping of adaptive ranks: the
-// 3xTF32 tensor-core variant (unbiased to ~2^-21) instead of plain TF32.
+// Engine of a projection whose output becomes the next unfolding under adaptive ranks: the
+// 3xTF32 tensor-core variant (products to ~2^-21; ~1e-5 relative after FP32 accumulation)
+// instead of plain TF32.
 int precise_engine(int engine) { return engine == TT_GEMM_TC ? TT_GEMM_TC3 : engine; }
 
 // Engine of a bulk pass over an m x cols unfolding.  TT_GEMM_AUTO keeps passes below 2^24
@@ -714,14 +715,16 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
     } else if (st.path == PATH_EXACT_ROWS) {
       npasses += st.fold ? 1 : 2;
       TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols, [&] {
-        // adaptive ranks read energies to ~1e-8 relative: FP32 products (unbiased rounding)
-        // instead of TF32 ones, FP64 accumulation (per product for short unfoldings, per 1024
-        // columns for long ones, whose many partial sums average the FP32 rounding out)
+        // Adaptive ranks read energies to ~1e-8 relative: the FP32 engine (round-to-nearest
+        // products, FP64 accumulation per product for short unfoldings, per 1024 columns for
+        // long ones whose many partial sums average the FP32 rounding out).  Tensor-core
+        // accumulation truncates, a bias above delta^2.
+        const bool long_unf = cols >= (1LL << 22);
         if (engine != TT_GEMM_FP32 && !adaptive) {
-          const int rc = launch_gram_tc(cur, m, cols, B.w, ws, c->dstat, s);
+          const int rc = launch_gram_tc(cur, m, cols, B.w, ws, c->dstat, s, engine == TT_GEMM_TC3);
           if (rc != TT_ERR_UNSUPPORTED) return rc;
         }
-        return launch_gram(cur, cols, (int)m, m, 1, B.w, adaptive && cols < (1LL << 22), ws, s);
+        return launch_gram(cur, cols, (int)m, m, 1, B.w, adaptive && !long_unf, ws, s);
       }));
       TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
@@ -793,8 +796,12 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
             return launch_project(cur, m, cols, B.yf, ksa, m, B.bt, cols, OUT_COLMAJOR, 1, 1, engine, ws, c->dstat,
                                   s);
           }));
+          // Adaptive ranks need the basis beyond the FP32 Gram's resolution (graded spectra
+          // down to delta / ||A|| ~ 1e-4): full CholeskyQR2 with FP64 Grams there; one
+          // FP32-Gram pass otherwise.
           TT_TRY(pass.run(TT_PASS_OTHER, 6.0 * cols * ksa * ksa, 24.0 * cols * ksa, [&] {
-            return launch_orth_power(B.bt, cols, ksa, 1, cols, ws, c->dstat, s);
+            return adaptive ? launch_cholqr2(B.bt, cols, ksa, 1, cols, nullptr, ws, c->dstat, s)
+                            : launch_orth_power(B.bt, cols, ksa, 1, cols, ws, c->dstat, s);
           }));
           TT_TRY(pass.run(TT_PASS_SKETCH, fl_pass, by_pass, [&] {
             return launch_sketch(cur, m, cols, B.bt, ksa, 1, cols, B.yd, engine, ws, c->dstat, s);
@@ -803,12 +810,13 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
           TT_TRY(launch_cholqr2(B.yf, m, ksa, 1, m, nullptr, ws, c->dstat, s));
         }
         // B^T = A^T Q (cols x ksa, row-major) = B (ksa x cols, column-major).  Adaptive ranks
-        // take ||B||^2 as the captured energy, which must hold ~1e-8 relative: TF32 operands
-        // (a measured product bias of ~-2e-6) would shift it by more than delta^2, so that mode
-        // forms B with the 3xTF32 tensor-core projection.
+        // take ||B||^2 as the captured energy, which must hold ~1e-8 relative.  Tensor-core
+        // accumulation (FP32 in TMEM, truncating) shrinks long product-sums by ~1e-6 relative
+        // even with exact 3xTF32 products, more than delta^2; that mode forms B on the FP32
+        // engine (round-to-nearest FMA).
         TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
           return launch_project(cur, m, cols, B.yf, ksa, m, B.bt, ksa, OUT_ROWMAJOR, 1, 1,
-                                adaptive ? precise_engine(engine) : engine, ws, c->dstat, s);
+                                adaptive ? TT_GEMM_FP32 : engine, ws, c->dstat, s);
         }));
         // Gram of the small factor B (ksa x cols, column-major = B^T row-major): the input of
         // the eigen-based small SVD (TT3O:717), on the tensor cores for long B.
@@ -1337,7 +1345,8 @@ extern "C" int tt_k_gram_rows(tt_ctx* c, const float* a, long long m, long long 
   TT_TRY(ws_for(c, std::max(gram_ws_bytes(n, (int)m), gram_tc_ws_bytes(m, n)), ws));
   TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
   int rc = TT_ERR_UNSUPPORTED;
-  if (gemm != TT_GEMM_FP32 && tc_available()) rc = launch_gram_tc(a, m, n, w, ws, c->dstat, c->stream);
+  if (gemm != TT_GEMM_FP32 && tc_available())
+    rc = launch_gram_tc(a, m, n, w, ws, c->dstat, c->stream, gemm == TT_GEMM_TC3);
   if (rc == TT_ERR_UNSUPPORTED) rc = launch_gram(a, n, (int)m, m, 1, w, false, ws, c->stream);
   TT_TRY(rc);
   return check_status(c);

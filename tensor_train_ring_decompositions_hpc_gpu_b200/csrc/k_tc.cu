@@ -663,13 +663,14 @@ __global__ void __launch_bounds__(192, 1)
 // the Gram contributions) or the m rows padded with zero rows by the TMA (padded view).
 // Both MMA operands are the same MN-major shared-memory tile.
 // ---------------------------------------------------------------------------------------
-template <int NB, int STAGES>
-__global__ void __launch_bounds__(192, 1)
+template <int NB, int STAGES, bool SPLITA>
+__global__ void __launch_bounds__(SPLITA ? 320 : 192, 1)
     k_gram_tc(const __grid_constant__ CUtensorMap tmA, long long ncols, int m, int grouped,
               long long kchunk, int nsplit, double* __restrict__ part, DevStatus* st) {
   constexpr int BK = 32;
   constexpr uint32_t ABLK = BK * 128;           // one 32-row block, BK columns
-  constexpr uint32_t STAGE_BYTES = 4 * ABLK;    // 128 rows
+  constexpr uint32_t HI_BYTES = 4 * ABLK;       // 128 rows
+  constexpr uint32_t STAGE_BYTES = HI_BYTES * (SPLITA ? 2 : 1);  // + the lo copy (3xTF32)
   constexpr uint32_t NBP = pow2_cols(NB);
   constexpr uint32_t TMEM_COLS = pow2_cols(2 * NBP);  // two accumulators: MMA fills one while the epilogue drains the other
   constexpr uint32_t IDESC = idesc_tf32(128, NB, 1, 1);
@@ -677,7 +678,7 @@ __global__ void __launch_bounds__(192, 1)
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* barmem = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(barmem + Bars::count(STAGES));
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(barmem + Bars::count(STAGES) + (SPLITA ? STAGES : 0));
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   float* gsum = reinterpret_cast<float*>(tmem_slot + 4);  // per-CTA Gram accumulator, m x (m+1) used
   const Bars bars{smem_u32(barmem), STAGES};
@@ -688,6 +689,7 @@ __global__ void __launch_bounds__(192, 1)
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(bars.full(s), 1);
       mbar_init(bars.empty(s), 1);
+      if (SPLITA) mbar_init(bars.conv(s), 4);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(bars.tfull(b), 1);
@@ -721,7 +723,7 @@ __global__ void __launch_bounds__(192, 1)
             ok = false;
             break;
           }
-          mbar_expect_tx(bars.full(stage), STAGE_BYTES);
+          mbar_expect_tx(bars.full(stage), HI_BYTES);
           const uint32_t sa = sbase + stage * STAGE_BYTES;
           const int jc = (int)(jb + (long long)kb * BK);
 #pragma unroll
@@ -757,7 +759,7 @@ __global__ void __launch_bounds__(192, 1)
         tc_fence_after();
         const uint32_t dacc = tmem_base + (uint32_t)buf * NBP;
         for (int kb = 0; kb < KB; ++kb) {
-          if (!mbar_wait(bars.full(stage), phase, abort_flag)) {
+          if (!mbar_wait(SPLITA ? bars.conv(stage) : bars.full(stage), phase, abort_flag)) {
             ok = false;
             break;
           }
@@ -767,6 +769,11 @@ __global__ void __launch_bounds__(192, 1)
           for (int ks = 0; ks < BK / 8; ++ks) {
             const uint64_t da = desc_mn_sw128_32b(sa + ks * 1024, ABLK, 512);
             mma_tf32(dacc, da, da, IDESC, (kb | ks) ? 1u : 0u);
+            if (SPLITA) {  // hi lo^T + lo hi^T: the 3xTF32 Gram
+              const uint64_t dl = desc_mn_sw128_32b(sa + HI_BYTES + ks * 1024, ABLK, 512);
+              mma_tf32(dacc, da, dl, IDESC, 1u);
+              mma_tf32(dacc, dl, da, IDESC, 1u);
+            }
           }
           mma_commit(bars.empty(stage));
           if (++stage == STAGES) {
@@ -783,6 +790,43 @@ __global__ void __launch_bounds__(192, 1)
       }
       mma_commit(bars.drain());
       mbar_wait_bounded(bars.drain(), 0);
+    }
+  } else if (SPLITA && warp >= 6) {
+    // converters: split each landed stage into TF32 hi (in place) and lo; a quarter each
+    const int cw = warp - 6;
+    int stage = 0;
+    uint32_t phase = 0;
+    for (int u = blockIdx.x; u < nsplit; u += gridDim.x) {
+      const long long jb = (long long)u * kchunk;
+      const long long je = (jb + kchunk < ncols) ? jb + kchunk : ncols;
+      const int KB = (int)((je - jb + BK - 1) / BK);
+      bool ok = true;
+      for (int kb = 0; kb < KB; ++kb) {
+        if (!mbar_wait(bars.full(stage), phase, abort_flag)) {
+          ok = false;
+          break;
+        }
+        float4* av = reinterpret_cast<float4*>(smem + stage * STAGE_BYTES);
+        float4* lv = reinterpret_cast<float4*>(smem + stage * STAGE_BYTES + HI_BYTES);
+        for (int i = cw * 32 + lane; i < (int)(HI_BYTES / 16); i += 128) {
+          const float4 v = av[i];
+          const float4 h = make_float4(tf32_rn(v.x), tf32_rn(v.y), tf32_rn(v.z), tf32_rn(v.w));
+          av[i] = h;
+          lv[i] = make_float4(tf32_rn(v.x - h.x), tf32_rn(v.y - h.y), tf32_rn(v.z - h.z), tf32_rn(v.w - h.w));
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncwarp();
+        if (lane == 0) mbar_arrive(bars.conv(stage));
+        if (++stage == STAGES) {
+          stage = 0;
+          phase ^= 1u;
+        }
+      }
+      if (!ok) {
+        *abort_flag = 1;
+        dev_fail(st, TT_ERR_TIMEOUT, 24);
+        break;
+      }
     }
   } else {
     const int et = threadIdx.x - 64;           // 0..127
@@ -992,13 +1036,13 @@ int sketch_tc_plan(long long m, long long n, int N, int* MT, int* ngroups, int* 
 }
 
 
-template <int NB>
+template <int NB, bool SPLITA>
 int run_gram(const CUtensorMap& ma, long long ncols, int m, int grouped, long long kchunk, int nsplit,
              double* part, DevStatus* st, cudaStream_t s) {
-  constexpr uint32_t STAGE = 4 * 32 * 128;
-  constexpr int STAGES = 8;  // 128 KB ring + the m x (m+1) Gram accumulator
+  constexpr uint32_t STAGE = 4 * 32 * 128 * (SPLITA ? 2 : 1);
+  constexpr int STAGES = SPLITA ? 4 : 8;  // 128 KB ring + the m x (m+1) Gram accumulator
   const size_t smem = (size_t)STAGES * STAGE + 1024 + 256 + (size_t)m * (m + 1) * sizeof(float);
-  auto kern = k_gram_tc<NB, STAGES>;
+  auto kern = k_gram_tc<NB, STAGES, SPLITA>;
   static bool attr = false;
   if (!attr) {
     const size_t most = (size_t)STAGES * STAGE + 1024 + 256 + 128 * 129 * sizeof(float);
@@ -1009,7 +1053,7 @@ int run_gram(const CUtensorMap& ma, long long ncols, int m, int grouped, long lo
     attr = true;
   }
   const int grid = std::min(nsplit, g_sms);
-  kern<<<grid, 192, smem, s>>>(ma, ncols, m, grouped, kchunk, nsplit, part, st);
+  kern<<<grid, SPLITA ? 320 : 192, smem, s>>>(ma, ncols, m, grouped, kchunk, nsplit, part, st);
   count_launch();
   TT_LAUNCH_CHECK();
   return TT_OK;
@@ -1042,7 +1086,7 @@ size_t gram_tc_ws_bytes(long long m, long long n) {
 
 // W (m x m, FP64) = A A^T with the tensor cores; A column-major m x n, m <= 128.
 int launch_gram_tc(const float* a, long long m, long long n, double* w, Arena& ws, DevStatus* st,
-                   cudaStream_t s) {
+                   cudaStream_t s, bool split_a) {
   if (!init_tc()) return TT_ERR_UNSUPPORTED;
   if (m < 1 || m > 128 || (m & 3) || (reinterpret_cast<uintptr_t>(a) & 15) || n > (1LL << 31) - 256)
     return TT_ERR_UNSUPPORTED;
@@ -1058,19 +1102,28 @@ int launch_gram_tc(const float* a, long long m, long long n, double* w, Arena& w
   CUtensorMap ma;
   const unsigned long long rows = grouped ? 128ull : (unsigned long long)m;
   TT_TRY(make_map(&ma, a, rows, (unsigned long long)nc, rows * 4, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
-                  CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
+                  split_a ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
   const int NB = grouped ? 128 : (int)((m + 15) / 16 * 16);
   int rc;
+#define TT_GRAM_CASE(nb)                                                              \
+  case nb:                                                                            \
+    rc = split_a ? run_gram<nb, true>(ma, nc, (int)m, grouped, kc, ns, part, st, s)   \
+                 : run_gram<nb, false>(ma, nc, (int)m, grouped, kc, ns, part, st, s); \
+    break;
   switch (NB) {
-    case 16: rc = run_gram<16>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
-    case 32: rc = run_gram<32>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
-    case 48: rc = run_gram<48>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
-    case 64: rc = run_gram<64>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
-    case 80: rc = run_gram<80>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
-    case 96: rc = run_gram<96>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
-    case 112: rc = run_gram<112>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
-    default: rc = run_gram<128>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
+    TT_GRAM_CASE(16)
+    TT_GRAM_CASE(32)
+    TT_GRAM_CASE(48)
+    TT_GRAM_CASE(64)
+    TT_GRAM_CASE(80)
+    TT_GRAM_CASE(96)
+    TT_GRAM_CASE(112)
+    default:
+      rc = split_a ? run_gram<128, true>(ma, nc, (int)m, grouped, kc, ns, part, st, s)
+                   : run_gram<128, false>(ma, nc, (int)m, grouped, kc, ns, part, st, s);
+      break;
   }
+#undef TT_GRAM_CASE
   if (rc != TT_OK) return rc;
   TT_TRY(launch_reduce_splits(part, m * m, ns, w, s));
   ws.reset(mk);

@@ -285,7 +285,7 @@ def test_host_stream_matches_device_chain(gpu, chunk):
     err_d = oracle.rel_error(x, oracle.tt_full([c.double().cpu().numpy() for c in res_d.cores]))
     ocores, _ = oracle.tt_svd(x.astype(np.float64), ranks, method="gram")
     oerr = oracle.rel_error(x, oracle.tt_full(ocores))
-    assert abs(err_s - err_d) < 1e-6 and abs(err_s - oerr) < 1e-4
+    assert abs(err_s - err_d) < 1e-6 and abs(err_s - oerr) < 1e-3
     for a, b in zip(res_s.sigmas, res_d.sigmas):
         np.testing.assert_allclose(a, b, rtol=1e-5, atol=1e-6 * b[0])
 
