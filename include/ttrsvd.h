@@ -48,9 +48,7 @@ typedef enum tt_status {
 enum {
   TT_GEMM_AUTO = 0, /* tensor cores where the shape allows it */
   TT_GEMM_TC = 1,   /* tcgen05 TF32 tensor-core tiles fed by TMA, FP32 accumulation in TMEM */
-  TT_GEMM_FP32 = 2, /* plain FP32 FMA (CUDA cores): the "plain FP32" form */
-  TT_GEMM_TC3 = 3   /* tensor cores with 3xTF32 compensation in the projections (A and Q split
-                     * into round-to-nearest TF32 hi / lo parts): products to ~2^-21, unbiased */
+  TT_GEMM_FP32 = 2  /* plain FP32 FMA (CUDA cores): the "plain FP32" form */
 };
 
 /* Per-unfolding factorisation. */

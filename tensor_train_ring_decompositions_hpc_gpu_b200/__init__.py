@@ -31,7 +31,7 @@ __all__ = [
     "set_predictor", "probe_features", "mlp_forward", "mlp_grad", "mlp_train", "set_stream_chunk",
 ]
 
-GEMM = {"auto": TT_GEMM_AUTO, "tc": TT_GEMM_TC, "fp32": TT_GEMM_FP32, "tc3": 3}
+GEMM = {"auto": TT_GEMM_AUTO, "tc": TT_GEMM_TC, "fp32": TT_GEMM_FP32}
 METHOD = {"edrsvd": TT_METHOD_EDRSVD, "exact": TT_METHOD_EXACT}
 
 

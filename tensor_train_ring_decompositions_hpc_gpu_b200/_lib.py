@@ -13,7 +13,7 @@ STATUS_NAMES = {
     5: "TT_ERR_NOMEM", 6: "TT_ERR_NOCONV", 7: "TT_ERR_TIMEOUT", 8: "TT_ERR_CUDA",
     9: "TT_ERR_UNSUPPORTED", 10: "TT_ERR_IO",
 }
-TT_GEMM_AUTO, TT_GEMM_TC, TT_GEMM_FP32, TT_GEMM_TC3 = 0, 1, 2, 3
+TT_GEMM_AUTO, TT_GEMM_TC, TT_GEMM_FP32 = 0, 1, 2
 TT_METHOD_EDRSVD, TT_METHOD_EXACT = 0, 1
 TT_FLAG_HOST_IO, TT_FLAG_CHECK_FINITE, TT_FLAG_NO_FOLD, TT_FLAG_IDENTITY_GAUGE, TT_FLAG_KEEP_SIGMA = 1, 2, 4, 8, 16
 TT_FLAG_PROFILE = 32

@@ -223,14 +223,8 @@ struct Plan {
 
 int engine_of(const tt_opts& o) {
   if (o.gemm == TT_GEMM_FP32) return TT_GEMM_FP32;
-  if (!tc_available()) return TT_GEMM_FP32;
-  return o.gemm == TT_GEMM_TC3 ? TT_GEMM_TC3 : TT_GEMM_TC;
+  return tc_available() ? TT_GEMM_TC : TT_GEMM_FP32;
 }
-
-// Engine of a projection whose output becomes the next unfolding under adaptive ranks: the
-// 3xTF32 tensor-core variant (products to ~2^-21; ~1e-5 relative after FP32 accumulation)
-// instead of plain TF32.
-int precise_engine(int engine) { return engine == TT_GEMM_TC ? TT_GEMM_TC3 : engine; }
 
 // Engine of a bulk pass over an m x cols unfolding.  TT_GEMM_AUTO keeps passes below 2^24
 // elements on the FP32 kernels (they are cheap there and carry full FP32 precision); the
@@ -689,7 +683,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         TT_TRY(stream_pass([&](const float* a, long long, long long nc) -> int {
           const int eng = engine_for(o, m, nc);
           int rc = TT_ERR_UNSUPPORTED;
-          if (eng != TT_GEMM_FP32) rc = launch_gram_tc(a, m, nc, B.w, ws, c->dstat, s);
+          if (eng == TT_GEMM_TC) rc = launch_gram_tc(a, m, nc, B.w, ws, c->dstat, s);
           if (rc == TT_ERR_UNSUPPORTED) rc = launch_gram(a, nc, (int)m, m, 1, B.w, false, ws, s);
           TT_TRY(rc);
           k_add_f64<<<ceil_div(m * m, 256), 256, 0, s>>>(B.w, B.wacc, (int)(m * m));
@@ -720,8 +714,8 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         // long ones whose many partial sums average the FP32 rounding out).  Tensor-core
         // accumulation truncates, a bias above delta^2.
         const bool long_unf = cols >= (1LL << 22);
-        if (engine != TT_GEMM_FP32 && !adaptive) {
-          const int rc = launch_gram_tc(cur, m, cols, B.w, ws, c->dstat, s, engine == TT_GEMM_TC3);
+        if (engine == TT_GEMM_TC && !adaptive) {
+          const int rc = launch_gram_tc(cur, m, cols, B.w, ws, c->dstat, s);
           if (rc != TT_ERR_UNSUPPORTED) return rc;
         }
         return launch_gram(cur, cols, (int)m, m, 1, B.w, adaptive && !long_unf, ws, s);
@@ -749,7 +743,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       TT_TRY(pass.run(TT_PASS_PROJECT, 2.0 * m * cols * nout, 4.0 * m * cols + 4.0 * nout * cols, [&] {
         return launch_project(cur, m, cols, B.ef, nout, m, next, st.perm231 ? 0 : nout,
                               st.perm231 ? OUT_PERM231 : OUT_ROWMAJOR, P.r[0], pr1,
-                              adaptive ? precise_engine(engine) : engine, ws, c->dstat, s);
+                              engine, ws, c->dstat, s);
       }));
     } else if (st.path == PATH_EXACT_COLS) {
       npasses += 2;
@@ -824,7 +818,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         // eigenvalue sum must then hold ~1e-8 relative, which the tensor-core Gram (TF32
         // operands, FP32 accumulation within 2048-column units) does not guarantee on short B.
         TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ksa * ksa, 4.0 * cols * ksa, [&] {
-          if (engine != TT_GEMM_FP32 && !adaptive) {
+          if (engine == TT_GEMM_TC && !adaptive) {
             const int rc = launch_gram_tc(B.bt, ksa, cols, B.w, ws, c->dstat, s);
             if (rc != TT_ERR_UNSUPPORTED) return rc;
           }
@@ -1323,9 +1317,7 @@ extern "C" int tt_k_project(tt_ctx* c, const float* a, long long m, long long n,
   TT_CUDA(cudaSetDevice(c->device));
   Arena ws;
   TT_TRY(ws_for(c, std::max<size_t>(1 << 20, project_ws_bytes(m, n, N)), ws));
-  const int eng = (gemm == TT_GEMM_FP32 || !tc_available()) ? TT_GEMM_FP32
-                  : gemm == TT_GEMM_TC3                       ? TT_GEMM_TC3
-                                                              : TT_GEMM_TC;
+  const int eng = (gemm == TT_GEMM_FP32 || !tc_available()) ? TT_GEMM_FP32 : TT_GEMM_TC;
   TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
   TT_TRY(launch_project(a, m, n, q, N, ldq, out, ldo, OUT_ROWMAJOR, 1, 1, eng, ws, c->dstat, c->stream));
   return check_status(c);
@@ -1345,8 +1337,7 @@ extern "C" int tt_k_gram_rows(tt_ctx* c, const float* a, long long m, long long 
   TT_TRY(ws_for(c, std::max(gram_ws_bytes(n, (int)m), gram_tc_ws_bytes(m, n)), ws));
   TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
   int rc = TT_ERR_UNSUPPORTED;
-  if (gemm != TT_GEMM_FP32 && tc_available())
-    rc = launch_gram_tc(a, m, n, w, ws, c->dstat, c->stream, gemm == TT_GEMM_TC3);
+  if (gemm != TT_GEMM_FP32 && tc_available()) rc = launch_gram_tc(a, m, n, w, ws, c->dstat, c->stream);
   if (rc == TT_ERR_UNSUPPORTED) rc = launch_gram(a, n, (int)m, m, 1, w, false, ws, c->stream);
   TT_TRY(rc);
   return check_status(c);

@@ -236,7 +236,7 @@ int launch_reduce_splits(const double* part, long long count, int nsplit, double
 int launch_sketch(const float* a, long long m, long long n, const float* w, int N, long long wj,
                   long long wc, double* y, int engine, Arena& ws, DevStatus* st, cudaStream_t s) {
   if (m <= 0 || n <= 0 || N <= 0) return TT_OK;
-  if (engine == TT_GEMM_TC || engine == TT_GEMM_TC3) {
+  if (engine == TT_GEMM_TC) {
     int rc = launch_sketch_tc(a, m, n, w, N, wj, wc, y, ws, st, s);
     if (rc != TT_ERR_UNSUPPORTED) return rc;
   }
@@ -558,8 +558,8 @@ int launch_project(const float* a, long long m, long long n, const float* q, int
                    float* out, long long ldo, int mode, int r0, int r1, int engine, Arena& ws,
                    DevStatus* st, cudaStream_t s) {
   if (n <= 0 || N <= 0) return TT_OK;
-  if (engine == TT_GEMM_TC || engine == TT_GEMM_TC3) {
-    int rc = launch_project_tc(a, m, n, q, N, ldq, out, ldo, mode, r0, r1, engine == TT_GEMM_TC3, ws, st, s);
+  if (engine == TT_GEMM_TC) {
+    int rc = launch_project_tc(a, m, n, q, N, ldq, out, ldo, mode, r0, r1, ws, st, s);
     if (rc != TT_ERR_UNSUPPORTED) return rc;
   }
   const int NT = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : 64;

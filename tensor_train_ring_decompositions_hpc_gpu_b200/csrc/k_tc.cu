@@ -178,9 +178,6 @@ struct Bars {
   __device__ uint32_t tfull(int b) const { return base + 8u * (2 * stages + b); }       // b < 4
   __device__ uint32_t tempty(int b) const { return base + 8u * (2 * stages + 4 + b); }  // b < 4
   __device__ uint32_t drain() const { return base + 8u * (2 * stages + 8); }
-  // after the drain barrier: per stage "A split into hi / lo" (the 3xTF32 projection only;
-  // that kernel reserves room for count(stages) + stages barriers)
-  __device__ uint32_t conv(int s) const { return base + 8u * (2 * stages + 9 + s); }
   __host__ __device__ static constexpr int count(int stages) { return 2 * stages + 9; }
 };
 
@@ -198,36 +195,17 @@ __device__ __forceinline__ void drain_fills(const Bars& bars, int stages, long l
 // ---------------------------------------------------------------------------------------
 // projection kernel: out = A^T Q   (persistent over 128-column tiles of A)
 // ---------------------------------------------------------------------------------------
-// SPLIT: Q arrives as an exactly-TF32 high part (tmB) and its remainder (tmB2); each K-step
-// issues A*Qhi and A*Qlo into the same accumulator, so Q carries FP32 precision.
-// SPLITA (3xTF32): A is loaded as FP32 and four converter warps split every stage in shared
-// memory into hi = rn_tf32(a) (in place) and lo = rn_tf32(a - hi); the K-step then issues
-// Ahi*Qhi + Ahi*Qlo + Alo*Qhi, products exact to ~2^-21 and unbiased (round to nearest
-// everywhere), for passes whose results feed energy bookkeeping at 1e-8 relative.
-// Round-to-nearest-even FP32 -> TF32 (10 stored mantissa bits).
-__device__ __forceinline__ float tf32_rn(float x) {
-  uint32_t u = __float_as_uint(x);
-  if ((u & 0x7F800000u) != 0x7F800000u) {
-    u += 0x0FFFu + ((u >> 13) & 1u);
-    u &= 0xFFFFE000u;
-  }
-  return __uint_as_float(u);
-}
-
-constexpr uint32_t kProjBarBytes = 512;  // barrier / TMEM-slot region of the projection kernel
-template <int BN, int STAGES, bool SPLIT, bool SPLITA>
-__global__ void __launch_bounds__(SPLITA ? 448 : 320, 1)
+// SPLIT: Q arrives as an exactly-TF32 high part (tmB) and its FP32 remainder (tmB2); each
+// K-step issues A*Qhi and A*Qlo into the same accumulator, so Q carries FP32 precision.
+template <int BN, int STAGES, bool SPLIT>
+__global__ void __launch_bounds__(320, 1)
     k_project_tc(const __grid_constant__ CUtensorMap tmA, const __grid_constant__ CUtensorMap tmB,
                  const __grid_constant__ CUtensorMap tmB2, long long n, int N, int KB,
                  float* __restrict__ out, long long ldo, int mode, int r0, int r1, DevStatus* st) {
   constexpr int BM = 128;
   constexpr uint32_t A_BYTES = BM * 128;
   constexpr uint32_t B_BYTES = BN * 128;
-  constexpr uint32_t ALO_BYTES = SPLITA ? A_BYTES : 0;
-  constexpr uint32_t STAGE_BYTES = A_BYTES + ALO_BYTES + (SPLIT ? 2 : 1) * B_BYTES;  // 1 KB aligned
-  constexpr uint32_t TMA_BYTES = A_BYTES + (SPLIT ? 2 : 1) * B_BYTES;
-  static_assert(SPLIT || !SPLITA, "3xTF32 needs the Q split");
-  static_assert(8 * (Bars::count(STAGES) + STAGES) + 8 <= kProjBarBytes, "barrier region");
+  constexpr uint32_t STAGE_BYTES = A_BYTES + (SPLIT ? 2 : 1) * B_BYTES;  // 1 KB aligned
   constexpr uint32_t BNP = pow2_cols(BN);
   constexpr uint32_t TMEM_COLS = pow2_cols(4 * BNP);  // four accumulators, two per epilogue group
   constexpr uint32_t IDESC = idesc_tf32(BM, BN, 0, 0);
@@ -236,7 +214,7 @@ __global__ void __launch_bounds__(SPLITA ? 448 : 320, 1)
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* barmem = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(barmem + Bars::count(STAGES) + STAGES);
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(barmem + Bars::count(STAGES));
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   const Bars bars{smem_u32(barmem), STAGES};
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -247,7 +225,6 @@ __global__ void __launch_bounds__(SPLITA ? 448 : 320, 1)
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(bars.full(s), 1);
       mbar_init(bars.empty(s), 1);
-      if (SPLITA) mbar_init(bars.conv(s), 4);
     }
     for (int b = 0; b < 4; ++b) {
       mbar_init(bars.tfull(b), 1);
@@ -281,11 +258,11 @@ __global__ void __launch_bounds__(SPLITA ? 448 : 320, 1)
             ok = false;
             break;
           }
-          mbar_expect_tx(bars.full(stage), TMA_BYTES);
+          mbar_expect_tx(bars.full(stage), STAGE_BYTES);
           const uint32_t sa = sbase + stage * STAGE_BYTES;
           tma_load_2d(sa, &tmA, bars.full(stage), kb * 32, j0);
-          tma_load_2d(sa + A_BYTES + ALO_BYTES, &tmB, bars.full(stage), kb * 32, 0);
-          if (SPLIT) tma_load_2d(sa + A_BYTES + ALO_BYTES + B_BYTES, &tmB2, bars.full(stage), kb * 32, 0);
+          tma_load_2d(sa + A_BYTES, &tmB, bars.full(stage), kb * 32, 0);
+          if (SPLIT) tma_load_2d(sa + A_BYTES + B_BYTES, &tmB2, bars.full(stage), kb * 32, 0);
           ++nissued;
           if (++stage == STAGES) {
             stage = 0;
@@ -316,21 +293,19 @@ __global__ void __launch_bounds__(SPLITA ? 448 : 320, 1)
         tc_fence_after();
         const uint32_t d = tmem_base + (uint32_t)buf * BNP;
         for (int kb = 0; kb < KB; ++kb) {
-          if (!mbar_wait(SPLITA ? bars.conv(stage) : bars.full(stage), phase, abort_flag)) {
+          if (!mbar_wait(bars.full(stage), phase, abort_flag)) {
             ok = false;
             break;
           }
           tc_fence_after();
           const uint32_t sa = sbase + stage * STAGE_BYTES;
           const uint64_t da = desc_kmajor(sa, 2, 1024);
-          const uint64_t dlo = desc_kmajor(sa + A_BYTES, 2, 1024);
-          const uint64_t db = desc_kmajor(sa + A_BYTES + ALO_BYTES, 2, 1024);
-          const uint64_t db2 = desc_kmajor(sa + A_BYTES + ALO_BYTES + B_BYTES, 2, 1024);
+          const uint64_t db = desc_kmajor(sa + A_BYTES, 2, 1024);
+          const uint64_t db2 = desc_kmajor(sa + A_BYTES + B_BYTES, 2, 1024);
 #pragma unroll
           for (int s = 0; s < 4; ++s) {
             mma_tf32(d, da + 2ull * s, db + 2ull * s, IDESC, (kb | s) ? 1u : 0u);
             if (SPLIT) mma_tf32(d, da + 2ull * s, db2 + 2ull * s, IDESC, 1u);
-            if (SPLITA) mma_tf32(d, dlo + 2ull * s, db + 2ull * s, IDESC, 1u);
           }
           mma_commit(bars.empty(stage));
           if (++stage == STAGES) {
@@ -347,40 +322,6 @@ __global__ void __launch_bounds__(SPLITA ? 448 : 320, 1)
       }
       mma_commit(bars.drain());
       mbar_wait_bounded(bars.drain(), 0);
-    }
-  } else if (SPLITA && warp >= 10) {
-    // converters: split each landed A stage into TF32 hi (in place) and lo; a quarter each
-    const int cw = warp - 10;
-    int stage = 0;
-    uint32_t phase = 0;
-    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-      bool ok = true;
-      for (int kb = 0; kb < KB; ++kb) {
-        if (!mbar_wait(bars.full(stage), phase, abort_flag)) {
-          ok = false;
-          break;
-        }
-        float4* av = reinterpret_cast<float4*>(smem + stage * STAGE_BYTES);
-        float4* lv = reinterpret_cast<float4*>(smem + stage * STAGE_BYTES + A_BYTES);
-        for (int i = cw * 32 + lane; i < (int)(A_BYTES / 16); i += 128) {
-          const float4 v = av[i];
-          const float4 h = make_float4(tf32_rn(v.x), tf32_rn(v.y), tf32_rn(v.z), tf32_rn(v.w));
-          av[i] = h;
-          lv[i] = make_float4(tf32_rn(v.x - h.x), tf32_rn(v.y - h.y), tf32_rn(v.z - h.z), tf32_rn(v.w - h.w));
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) mbar_arrive(bars.conv(stage));
-        if (++stage == STAGES) {
-          stage = 0;
-          phase ^= 1u;
-        }
-      }
-      if (!ok) {
-        *abort_flag = 1;
-        dev_fail(st, TT_ERR_TIMEOUT, 4);
-        break;
-      }
     }
   } else {
     // Two epilogue groups of four warps (one per TMEM lane quadrant each) take alternate tiles:
@@ -413,7 +354,7 @@ __global__ void __launch_bounds__(SPLITA ? 448 : 320, 1)
       if (BN <= 32 && mode == OUT_PERM231) {  // the launcher sends the bond permute only for BN <= 32
         // Bond permute through shared memory: for each a, the warp's 32 columns j form one
         // contiguous run of r1 * 32 outputs (b fastest), written with coalesced stores.
-        float* stg = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(barmem) + kProjBarBytes) + (warp - 2) * 32 * (BN + 1);
+        float* stg = reinterpret_cast<float*>(reinterpret_cast<uint8_t*>(barmem) + 256) + (warp - 2) * 32 * (BN + 1);
 #pragma unroll
         for (int c = 0; c < BN; ++c) stg[lane * (BN + 1) + c] = __uint_as_float(r[c]);
         __syncwarp();
@@ -663,14 +604,13 @@ __global__ void __launch_bounds__(192, 1)
 // the Gram contributions) or the m rows padded with zero rows by the TMA (padded view).
 // Both MMA operands are the same MN-major shared-memory tile.
 // ---------------------------------------------------------------------------------------
-template <int NB, int STAGES, bool SPLITA>
-__global__ void __launch_bounds__(SPLITA ? 320 : 192, 1)
+template <int NB, int STAGES>
+__global__ void __launch_bounds__(192, 1)
     k_gram_tc(const __grid_constant__ CUtensorMap tmA, long long ncols, int m, int grouped,
               long long kchunk, int nsplit, double* __restrict__ part, DevStatus* st) {
   constexpr int BK = 32;
   constexpr uint32_t ABLK = BK * 128;           // one 32-row block, BK columns
-  constexpr uint32_t HI_BYTES = 4 * ABLK;       // 128 rows
-  constexpr uint32_t STAGE_BYTES = HI_BYTES * (SPLITA ? 2 : 1);  // + the lo copy (3xTF32)
+  constexpr uint32_t STAGE_BYTES = 4 * ABLK;    // 128 rows
   constexpr uint32_t NBP = pow2_cols(NB);
   constexpr uint32_t TMEM_COLS = pow2_cols(2 * NBP);  // two accumulators: MMA fills one while the epilogue drains the other
   constexpr uint32_t IDESC = idesc_tf32(128, NB, 1, 1);
@@ -678,7 +618,7 @@ __global__ void __launch_bounds__(SPLITA ? 320 : 192, 1)
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   uint64_t* barmem = reinterpret_cast<uint64_t*>(smem + STAGES * STAGE_BYTES);
-  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(barmem + Bars::count(STAGES) + (SPLITA ? STAGES : 0));
+  uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(barmem + Bars::count(STAGES));
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
   float* gsum = reinterpret_cast<float*>(tmem_slot + 4);  // per-CTA Gram accumulator, m x (m+1) used
   const Bars bars{smem_u32(barmem), STAGES};
@@ -689,7 +629,6 @@ __global__ void __launch_bounds__(SPLITA ? 320 : 192, 1)
     for (int s = 0; s < STAGES; ++s) {
       mbar_init(bars.full(s), 1);
       mbar_init(bars.empty(s), 1);
-      if (SPLITA) mbar_init(bars.conv(s), 4);
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(bars.tfull(b), 1);
@@ -723,7 +662,7 @@ __global__ void __launch_bounds__(SPLITA ? 320 : 192, 1)
             ok = false;
             break;
           }
-          mbar_expect_tx(bars.full(stage), HI_BYTES);
+          mbar_expect_tx(bars.full(stage), STAGE_BYTES);
           const uint32_t sa = sbase + stage * STAGE_BYTES;
           const int jc = (int)(jb + (long long)kb * BK);
 #pragma unroll
@@ -759,7 +698,7 @@ __global__ void __launch_bounds__(SPLITA ? 320 : 192, 1)
         tc_fence_after();
         const uint32_t dacc = tmem_base + (uint32_t)buf * NBP;
         for (int kb = 0; kb < KB; ++kb) {
-          if (!mbar_wait(SPLITA ? bars.conv(stage) : bars.full(stage), phase, abort_flag)) {
+          if (!mbar_wait(bars.full(stage), phase, abort_flag)) {
             ok = false;
             break;
           }
@@ -769,11 +708,6 @@ __global__ void __launch_bounds__(SPLITA ? 320 : 192, 1)
           for (int ks = 0; ks < BK / 8; ++ks) {
             const uint64_t da = desc_mn_sw128_32b(sa + ks * 1024, ABLK, 512);
             mma_tf32(dacc, da, da, IDESC, (kb | ks) ? 1u : 0u);
-            if (SPLITA) {  // hi lo^T + lo hi^T: the 3xTF32 Gram
-              const uint64_t dl = desc_mn_sw128_32b(sa + HI_BYTES + ks * 1024, ABLK, 512);
-              mma_tf32(dacc, da, dl, IDESC, 1u);
-              mma_tf32(dacc, dl, da, IDESC, 1u);
-            }
           }
           mma_commit(bars.empty(stage));
           if (++stage == STAGES) {
@@ -790,43 +724,6 @@ __global__ void __launch_bounds__(SPLITA ? 320 : 192, 1)
       }
       mma_commit(bars.drain());
       mbar_wait_bounded(bars.drain(), 0);
-    }
-  } else if (SPLITA && warp >= 6) {
-    // converters: split each landed stage into TF32 hi (in place) and lo; a quarter each
-    const int cw = warp - 6;
-    int stage = 0;
-    uint32_t phase = 0;
-    for (int u = blockIdx.x; u < nsplit; u += gridDim.x) {
-      const long long jb = (long long)u * kchunk;
-      const long long je = (jb + kchunk < ncols) ? jb + kchunk : ncols;
-      const int KB = (int)((je - jb + BK - 1) / BK);
-      bool ok = true;
-      for (int kb = 0; kb < KB; ++kb) {
-        if (!mbar_wait(bars.full(stage), phase, abort_flag)) {
-          ok = false;
-          break;
-        }
-        float4* av = reinterpret_cast<float4*>(smem + stage * STAGE_BYTES);
-        float4* lv = reinterpret_cast<float4*>(smem + stage * STAGE_BYTES + HI_BYTES);
-        for (int i = cw * 32 + lane; i < (int)(HI_BYTES / 16); i += 128) {
-          const float4 v = av[i];
-          const float4 h = make_float4(tf32_rn(v.x), tf32_rn(v.y), tf32_rn(v.z), tf32_rn(v.w));
-          av[i] = h;
-          lv[i] = make_float4(tf32_rn(v.x - h.x), tf32_rn(v.y - h.y), tf32_rn(v.z - h.z), tf32_rn(v.w - h.w));
-        }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncwarp();
-        if (lane == 0) mbar_arrive(bars.conv(stage));
-        if (++stage == STAGES) {
-          stage = 0;
-          phase ^= 1u;
-        }
-      }
-      if (!ok) {
-        *abort_flag = 1;
-        dev_fail(st, TT_ERR_TIMEOUT, 24);
-        break;
-      }
     }
   } else {
     const int et = threadIdx.x - 64;           // 0..127
@@ -947,6 +844,15 @@ int set_smem(K kernel, size_t bytes) {
 
 constexpr size_t kSmemBudget = 200 * 1024;
 
+// Round-to-nearest-even FP32 -> TF32 (10 stored mantissa bits) and the exact remainder.
+__device__ __forceinline__ float tf32_rn(float x) {
+  uint32_t u = __float_as_uint(x);
+  if ((u & 0x7F800000u) != 0x7F800000u) {
+    u += 0x0FFFu + ((u >> 13) & 1u);
+    u &= 0xFFFFE000u;
+  }
+  return __uint_as_float(u);
+}
 
 __global__ void k_split_tf32(const float* __restrict__ q, long long m, int N, long long ldq,
                              float* __restrict__ hi, float* __restrict__ lo, long long ldo) {
@@ -957,20 +863,20 @@ __global__ void k_split_tf32(const float* __restrict__ q, long long m, int N, lo
     const float v = q[i + ldq * c];
     const float h = tf32_rn(v);
     hi[i + ldo * c] = h;
-    lo[i + ldo * c] = tf32_rn(v - h);  // the MMA reads TF32: round the remainder to nearest too
+    lo[i + ldo * c] = v - h;
   }
 }
 
-template <int BN, bool SPLIT, bool SPLITA>
+template <int BN, bool SPLIT>
 int run_project(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap& mb2, long long n,
                 int N, int KB, float* out, long long ldo, int mode, int r0, int r1, DevStatus* st,
                 cudaStream_t s) {
-  constexpr uint32_t STAGE = 128 * 128 * (SPLITA ? 2 : 1) + (SPLIT ? 2 : 1) * BN * 128;
+  constexpr uint32_t STAGE = 128 * 128 + (SPLIT ? 2 : 1) * BN * 128;
   // bond-permute staging of the 8 epilogue warps (that epilogue runs for BN <= 32 only)
   constexpr size_t STAGING = BN <= 32 ? 8 * 32 * (BN + 1) * sizeof(float) : 0;
   constexpr int STAGES = (int)std::min<size_t>(10, (kSmemBudget - STAGING) / STAGE);
-  const size_t smem = (size_t)STAGES * STAGE + 1024 + kProjBarBytes + STAGING;
-  auto kern = k_project_tc<BN, STAGES, SPLIT, SPLITA>;
+  const size_t smem = (size_t)STAGES * STAGE + 1024 + 256 + STAGING;
+  auto kern = k_project_tc<BN, STAGES, SPLIT>;
   static bool attr = false;
   if (!attr) {
     if (set_smem(kern, smem) != TT_OK) {
@@ -981,7 +887,7 @@ int run_project(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap&
   }
   const long long ntiles = (n + 127) / 128;
   const int grid = (int)std::min<long long>(ntiles, (long long)g_sms);
-  kern<<<grid, SPLITA ? 448 : 320, smem, s>>>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st);
+  kern<<<grid, 320, smem, s>>>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st);
   count_launch();
   TT_LAUNCH_CHECK();
   return TT_OK;
@@ -1036,13 +942,13 @@ int sketch_tc_plan(long long m, long long n, int N, int* MT, int* ngroups, int* 
 }
 
 
-template <int NB, bool SPLITA>
+template <int NB>
 int run_gram(const CUtensorMap& ma, long long ncols, int m, int grouped, long long kchunk, int nsplit,
              double* part, DevStatus* st, cudaStream_t s) {
-  constexpr uint32_t STAGE = 4 * 32 * 128 * (SPLITA ? 2 : 1);
-  constexpr int STAGES = SPLITA ? 4 : 8;  // 128 KB ring + the m x (m+1) Gram accumulator
+  constexpr uint32_t STAGE = 4 * 32 * 128;
+  constexpr int STAGES = 8;  // 128 KB ring + the m x (m+1) Gram accumulator
   const size_t smem = (size_t)STAGES * STAGE + 1024 + 256 + (size_t)m * (m + 1) * sizeof(float);
-  auto kern = k_gram_tc<NB, STAGES, SPLITA>;
+  auto kern = k_gram_tc<NB, STAGES>;
   static bool attr = false;
   if (!attr) {
     const size_t most = (size_t)STAGES * STAGE + 1024 + 256 + 128 * 129 * sizeof(float);
@@ -1053,7 +959,7 @@ int run_gram(const CUtensorMap& ma, long long ncols, int m, int grouped, long lo
     attr = true;
   }
   const int grid = std::min(nsplit, g_sms);
-  kern<<<grid, SPLITA ? 320 : 192, smem, s>>>(ma, ncols, m, grouped, kchunk, nsplit, part, st);
+  kern<<<grid, 192, smem, s>>>(ma, ncols, m, grouped, kchunk, nsplit, part, st);
   count_launch();
   TT_LAUNCH_CHECK();
   return TT_OK;
@@ -1086,7 +992,7 @@ size_t gram_tc_ws_bytes(long long m, long long n) {
 
 // W (m x m, FP64) = A A^T with the tensor cores; A column-major m x n, m <= 128.
 int launch_gram_tc(const float* a, long long m, long long n, double* w, Arena& ws, DevStatus* st,
-                   cudaStream_t s, bool split_a) {
+                   cudaStream_t s) {
   if (!init_tc()) return TT_ERR_UNSUPPORTED;
   if (m < 1 || m > 128 || (m & 3) || (reinterpret_cast<uintptr_t>(a) & 15) || n > (1LL << 31) - 256)
     return TT_ERR_UNSUPPORTED;
@@ -1102,28 +1008,19 @@ int launch_gram_tc(const float* a, long long m, long long n, double* w, Arena& w
   CUtensorMap ma;
   const unsigned long long rows = grouped ? 128ull : (unsigned long long)m;
   TT_TRY(make_map(&ma, a, rows, (unsigned long long)nc, rows * 4, 32, 32, CU_TENSOR_MAP_SWIZZLE_128B_ATOM_32B,
-                  split_a ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
+                  CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
   const int NB = grouped ? 128 : (int)((m + 15) / 16 * 16);
   int rc;
-#define TT_GRAM_CASE(nb)                                                              \
-  case nb:                                                                            \
-    rc = split_a ? run_gram<nb, true>(ma, nc, (int)m, grouped, kc, ns, part, st, s)   \
-                 : run_gram<nb, false>(ma, nc, (int)m, grouped, kc, ns, part, st, s); \
-    break;
   switch (NB) {
-    TT_GRAM_CASE(16)
-    TT_GRAM_CASE(32)
-    TT_GRAM_CASE(48)
-    TT_GRAM_CASE(64)
-    TT_GRAM_CASE(80)
-    TT_GRAM_CASE(96)
-    TT_GRAM_CASE(112)
-    default:
-      rc = split_a ? run_gram<128, true>(ma, nc, (int)m, grouped, kc, ns, part, st, s)
-                   : run_gram<128, false>(ma, nc, (int)m, grouped, kc, ns, part, st, s);
-      break;
+    case 16: rc = run_gram<16>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
+    case 32: rc = run_gram<32>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
+    case 48: rc = run_gram<48>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
+    case 64: rc = run_gram<64>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
+    case 80: rc = run_gram<80>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
+    case 96: rc = run_gram<96>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
+    case 112: rc = run_gram<112>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
+    default: rc = run_gram<128>(ma, nc, (int)m, grouped, kc, ns, part, st, s); break;
   }
-#undef TT_GRAM_CASE
   if (rc != TT_OK) return rc;
   TT_TRY(launch_reduce_splits(part, m * m, ns, w, s));
   ws.reset(mk);
@@ -1141,7 +1038,7 @@ size_t sketch_tc_ws_bytes(long long m, long long n, int N) {
 }
 
 int launch_project_tc(const float* a, long long m, long long n, const float* q, int N,
-                      long long ldq, float* out, long long ldo, int mode, int r0, int r1, bool split_a,
+                      long long ldq, float* out, long long ldo, int mode, int r0, int r1,
                       Arena& ws, DevStatus* st, cudaStream_t s) {
   if (!init_tc()) return TT_ERR_UNSUPPORTED;
   if (N > 128 || (m & 3) || (reinterpret_cast<uintptr_t>(a) & 15) || n > (1LL << 31) - 256 ||
@@ -1166,33 +1063,21 @@ int launch_project_tc(const float* a, long long m, long long n, const float* q, 
     TT_LAUNCH_CHECK();
   }
   CUtensorMap ma, mb, mb2;
-  // A through the TFLOAT32 tensor-map type (the TMA rounds to TF32), or as FP32 for the
-  // in-kernel hi / lo split of the 3xTF32 variant.
+  // A through the TFLOAT32 tensor-map type; the MMA then sees TMA-converted operands.
   TT_TRY(make_map(&ma, a, (unsigned long long)m, (unsigned long long)n, (unsigned long long)m * 4, 32, 128,
-                  CU_TENSOR_MAP_SWIZZLE_128B,
-                  split_a ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
+                  CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_DATA_TYPE_TFLOAT32));
   TT_TRY(make_map(&mb, qhi, (unsigned long long)m, (unsigned long long)N, (unsigned long long)ldh * 4, 32,
                   (unsigned)BN, CU_TENSOR_MAP_SWIZZLE_128B));
   TT_TRY(make_map(&mb2, qlo, (unsigned long long)m, (unsigned long long)N, (unsigned long long)ldh * 4, 32,
                   (unsigned)BN, CU_TENSOR_MAP_SWIZZLE_128B));
   const int KB = (int)((m + 31) / 32);
   int rc;
-  if (split_a) {
-    switch (BN) {
-      case 16: rc = run_project<16, true, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-      case 32: rc = run_project<32, true, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-      case 48: rc = run_project<48, true, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-      case 64: rc = run_project<64, true, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-      default: rc = run_project<128, true, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-    }
-  } else {
-    switch (BN) {
-      case 16: rc = run_project<16, true, false>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-      case 32: rc = run_project<32, true, false>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-      case 48: rc = run_project<48, true, false>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-      case 64: rc = run_project<64, true, false>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-      default: rc = run_project<128, true, false>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
-    }
+  switch (BN) {
+    case 16: rc = run_project<16, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+    case 32: rc = run_project<32, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+    case 48: rc = run_project<48, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+    case 64: rc = run_project<64, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
+    default: rc = run_project<128, true>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st, s); break;
   }
   ws.reset(mk);  // the split copies are consumed by the launch above (stream-ordered)
   return rc;

@@ -149,12 +149,11 @@ size_t sketch_tc_ws_bytes(long long m, long long n, int N);
 size_t gram_tc_ws_bytes(long long m, long long n);
 // W (m x m, FP64, ld = m) = A A^T on the tensor cores, A column-major m x n, m <= 128.
 int launch_gram_tc(const float* a, long long m, long long n, double* w, Arena& ws, DevStatus* st,
-                   cudaStream_t s,
-                   bool split_a = false);
+                   cudaStream_t s);
 int launch_sketch_tc(const float* a, long long m, long long n, const float* w, int N, long long wj,
                      long long wc, double* y, Arena& ws, DevStatus* st, cudaStream_t s);
 int launch_project_tc(const float* a, long long m, long long n, const float* q, int N,
-                      long long ldq, float* out, long long ldo, int mode, int r0, int r1, bool split_a,
+                      long long ldq, float* out, long long ldo, int mode, int r0, int r1,
                       Arena& ws, DevStatus* st, cudaStream_t s);
 
 }  // namespace ttr
