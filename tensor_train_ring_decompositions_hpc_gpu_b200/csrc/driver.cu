@@ -47,6 +47,8 @@ struct tt_ctx {
   size_t chunk_bytes = 256ull << 20;  // host-streaming chunk
   cudaStream_t copy_stream = nullptr;  // host-streaming copies
   cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_used[2] = {nullptr, nullptr};
+  cudaStream_t side_stream = nullptr;  // eigen-solve of a folded step, overlapped with the next step
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 extern "C" const char* tt_last_error(void) { return ttr::g_err; }
@@ -119,6 +121,9 @@ extern "C" int tt_ctx_destroy(tt_ctx* c) {
     if (c->ev_used[b]) cudaEventDestroy(c->ev_used[b]);
   }
   if (c->copy_stream) cudaStreamDestroy(c->copy_stream);
+  if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+  if (c->ev_join) cudaEventDestroy(c->ev_join);
+  if (c->side_stream) cudaStreamDestroy(c->side_stream);
   delete c;
   return TT_OK;
 }
@@ -371,6 +376,10 @@ struct Bufs {
   std::vector<float*> cores;  // device cores
   float* chunk[2] = {nullptr, nullptr};  // host streaming
   double* wacc = nullptr;
+  double* w2 = nullptr;       // folded step: Gram, eigenpairs and basis on the side stream
+  double* evals2 = nullptr;
+  double* evecs2 = nullptr;
+  float* ef2 = nullptr;
 };
 
 size_t plan_bytes(const Plan& P, bool host_io) {
@@ -394,6 +403,8 @@ size_t plan_bytes(const Plan& P, bool host_io) {
   add(S * sizeof(double) * 2);
   add(S * S * sizeof(double) * 2);
   add(256);
+  add(S * S * sizeof(double) * 2 + S * sizeof(double) + 1024);  // side-stream eigen-solve
+  add(P.max_ef * sizeof(float));
   if (host_io)
     for (int k = 0; k < P.d; ++k) add(core_elems(P, k) * sizeof(float));
   add(P.max_ws);
@@ -428,11 +439,15 @@ int carve(tt_ctx* c, const Plan& P, bool host_io, Bufs& B, Arena& ws) {
   B.evals = a.take<double>(S);
   B.colscale = a.take<double>(S);
   B.flag = a.take<int>(64);
+  B.w2 = a.take<double>(S * S);
+  B.evals2 = a.take<double>(S);
+  B.evecs2 = a.take<double>(S * S);
+  B.ef2 = a.take<float>(P.max_ef);
   if (host_io) {
     B.cores.resize(P.d);
     for (int k = 0; k < P.d; ++k) B.cores[k] = a.take<float>(core_elems(P, k));
   }
-  if (!B.data[1] || !B.flag || (host_io && !B.cores[P.d - 1])) {
+  if (!B.data[1] || !B.flag || !B.ef2 || (host_io && !B.cores[P.d - 1])) {
     set_error(TT_ERR_NOMEM, "workspace carve");
     return TT_ERR_NOMEM;
   }
@@ -512,6 +527,8 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
               tt_stats* stats) {
   const bool host_io = (o.flags & TT_FLAG_HOST_IO) != 0;
   TT_CUDA(cudaSetDevice(c->device));
+  // a side-stream job of an earlier call that failed midway must not outlive its buffers
+  if (c->side_stream) TT_CUDA(cudaStreamSynchronize(c->side_stream));
   TT_TRY(tt_ctx_reserve(c, plan_bytes(P, host_io)));
   Bufs B;
   Arena ws;
@@ -614,6 +631,17 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
   const double* pend = nullptr;  // pending rotation (rows_in x rows_in), or null
   int pend_slot = 0;
   const int nsteps = (int)P.steps.size();
+  // A folded exact step (full rank, rotation kept pending) does not change the data the next
+  // step reads, so its eigen-solve, core and pending rotation run on a side stream while the
+  // next step's bulk passes proceed; join_side() makes s wait before the rotation is used.
+  bool side_pending = false;
+  auto join_side = [&]() -> int {
+    if (side_pending) {
+      TT_CUDA(cudaStreamWaitEvent(s, c->ev_join, 0));
+      side_pending = false;
+    }
+    return TT_OK;
+  };
   int npasses = 0, natt = 0, nfall = 0;  // bulk passes, EDrSVD attempts, learned fallbacks
   std::vector<int> step_ks((size_t)nsteps, 0), step_pw((size_t)nsteps, 0), step_att((size_t)nsteps, 0);
   for (int k = 0; k < nsteps; ++k) {
@@ -665,6 +693,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       TT_LAUNCH_CHECK();
       if (pend) {
         TT_TRY(launch_f64_to_f32_cols(B.w, m, m, (int)m, B.corebuf, m, (int)m, s));
+        TT_TRY(join_side());
         TT_TRY(launch_fold_rows(B.corebuf, core_dst, pend, rin, ni, (int)m, s));
       } else {
         TT_TRY(launch_f64_to_f32_cols(B.w, m, m, (int)m, core_dst, m, (int)m, s));
@@ -699,6 +728,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       count_launch();
       TT_TRY(launch_f64_to_f32_cols(B.evecs, m, m, re, B.ef, m, rq, s));
       TT_TRY(launch_canon_cols(B.ef, m, re, m, B.evecs, (int)m, m, s));
+      TT_TRY(join_side());
       TT_TRY(emit_core(B.ef, core_dst, pend, rin, rcore, ni, rq, s));
       TT_TRY(pass.run(TT_PASS_PROJECT, 2.0 * m * cols * nout, 4.0 * m * cols + 4.0 * nout * cols, [&]() -> int {
         return stream_pass([&](const float* a, long long c0, long long nc) -> int {
@@ -706,6 +736,38 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
                                 engine_for(o, m, nc), ws, c->dstat, s);
         });
       }));
+    } else if (st.path == PATH_EXACT_ROWS && st.fold && !adaptive && m <= 64) {
+      // folded step: Gram on s, the rest on the side stream (see join_side)
+      npasses += 1;
+      TT_TRY(join_side());  // one side job at a time: its buffers are reused here
+      TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols, [&] {
+        if (engine == TT_GEMM_TC) {
+          const int rc = launch_gram_tc(cur, m, cols, B.w2, ws, c->dstat, s);
+          if (rc != TT_ERR_UNSUPPORTED) return rc;
+        }
+        return launch_gram(cur, cols, (int)m, m, 1, B.w2, false, ws, s);
+      }));
+      if (!c->side_stream) {
+        TT_CUDA(cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking));
+        TT_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
+        TT_CUDA(cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming));
+      }
+      cudaStream_t ss = c->side_stream;
+      TT_CUDA(cudaEventRecord(c->ev_fork, s));
+      TT_CUDA(cudaStreamWaitEvent(ss, c->ev_fork, 0));
+      TT_TRY(launch_syev(B.w2, (int)m, B.evals2, B.evecs2, max_sweeps, ws, c->dstat, ss));
+      k_store_sigma<<<1, 64, 0, ss>>>(B.evals2, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
+      count_launch();
+      TT_TRY(launch_f64_to_f32_cols(B.evecs2, m, m, re, B.ef2, m, rq, ss));
+      TT_TRY(launch_canon_cols(B.ef2, m, re, m, B.evecs2, (int)m, m, ss));
+      TT_TRY(emit_core(B.ef2, core_dst, pend, rin, rcore, ni, rq, ss));
+      double* pnew = B.pend[pend_slot ^ 1];
+      TT_CUDA(cudaMemcpyAsync(pnew, B.evecs2, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, ss));
+      TT_CUDA(cudaEventRecord(c->ev_join, ss));
+      side_pending = true;
+      pend = pnew;
+      pend_slot ^= 1;
+      continue;
     } else if (st.path == PATH_EXACT_ROWS) {
       npasses += st.fold ? 1 : 2;
       TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols, [&] {
@@ -730,6 +792,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       if (ring1) {
         TT_TRY(launch_ring_core1(B.ef, (int)m, P.r[0], P.r[1], cores[0], s));
       } else {
+        TT_TRY(join_side());
         TT_TRY(emit_core(B.ef, core_dst, pend, rin, rcore, ni, rq, s));
       }
       if (st.fold) {
@@ -763,6 +826,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       if (ring1) {
         TT_TRY(launch_ring_core1(ubuf, (int)m, P.r[0], P.r[1], cores[0], s));
       } else {
+        TT_TRY(join_side());
         TT_TRY(emit_core(ubuf, core_dst, pend, rin, rcore, ni, rq, s));
       }
       if (st.perm231) {
@@ -919,6 +983,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       if (ring1) {
         TT_TRY(launch_ring_core1(ubuf, (int)m, P.r[0], P.r[1], cores[0], s));
       } else {
+        TT_TRY(join_side());
         TT_TRY(emit_core(ubuf, core_dst, pend, rin, rcore, ni, rq, s));
       }
     }
@@ -931,8 +996,10 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
   {
     const int k = P.d - 1;
     const long long ni = P.n[k] * (long long)P.r[P.d];
+    TT_TRY(join_side());
     TT_TRY(emit_core(cur, cores[k], pend, P.last_rows, P.r[k], ni, 1, s));
   }
+  TT_TRY(join_side());
   TT_CUDA(cudaEventRecord(c->ev1, s));
   if (host_io) {
     for (int k = 0; k < P.d; ++k)
