@@ -15,7 +15,10 @@ __device__ __forceinline__ bool jacobi_rotation(double app, double aqq, double a
   const double ps = app * inv_s, qs = aqq * inv_s, as = apq * inv_s;
   c = 1.0;
   s = 0.0;
-  if (!(fabs(as) > 1e-15 && as * as > 1e-28 * fabs(ps * qs))) return false;
+  // skip below 1e-12 of sqrt(a_pp a_qq) (and 1e-14 of the largest diagonal): eigenvalues then
+  // carry (1e-12)^2 relative error, residuals 1e-12 of the norm, and the final quiet sweep
+  // comes about one sweep earlier than with a 1e-14 cut
+  if (!(fabs(as) > 1e-14 && as * as > 1e-24 * fabs(ps * qs))) return false;
   const float d = (float)(qs - ps), e = 2.0f * (float)as;
   const float h = sqrtf(fmaf(d, d, e * e));
   const float tf = (d >= 0.0f ? e : -e) * __frcp_rn(fabsf(d) + h);

@@ -1409,9 +1409,8 @@ __global__ void __launch_bounds__(256) k_syev_jacobi(const double* __restrict__ 
 // Rotation angle: t from an FP32 evaluation of theta on the matrix scaled by its largest
 // diagonal entry, then c = 1/sqrt(1 + t^2), s = t c in FP64, so every applied rotation is
 // orthogonal to FP64 precision (an inexact t leaves a tiny a_pq for a later sweep).  Pairs
-// with a_pq^2 <= 1e-28 |a_pp a_qq| (relative accuracy) or |a_pq| <= 1e-15 max|diag| (FP64
-// rounding floor) are not rotated; the solve ends after Np - 1 consecutive rounds without a
-// rotation.  Eigenvalues are ordered by a parallel rank count.
+// with a_pq^2 <= 1e-24 |a_pp a_qq| or |a_pq| <= 1e-14 max|diag| are not rotated
+// (jacobi_rotation); the solve ends after Np - 1 consecutive rounds without a rotation.  Eigenvalues are ordered by a parallel rank count.
 // Slot of index i in round-robin round r (slot 0 fixed, slots 1..NR cycle), and its position.
 __device__ __forceinline__ int bl_slot(int i, int r, int NR) {
   if (i == 0) return 0;
