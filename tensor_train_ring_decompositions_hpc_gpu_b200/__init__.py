@@ -277,13 +277,20 @@ def gram_rows(a, gemm="fp32"):
     return w
 
 
-def gram_tall(z):
-    """Z^T Z (FP64) of a column-major tall matrix Z (n x N)."""
+def gram_tall(z, rowmajor=False):
+    """Z^T Z (FP64) of a tall matrix Z (n x N), column-major, or row-major (rows contiguous,
+    the layout of a projected factor B^T) with rowmajor=True."""
     torch = _torch()
-    z = _as_colmajor(z.float())
-    n, N = z.shape
+    if rowmajor:
+        z = z.float().contiguous()
+        n, N = z.shape
+        rs, cs = N, 1
+    else:
+        z = _as_colmajor(z.float())
+        n, N = z.shape
+        rs, cs = 1, n
     w = _colmajor(N, N, torch.float64, z.device)
-    check(lib().tt_k_gram_tall(_ctx_for(z.device.index), _ptr(z), n, N, 1, n, _ptr(w)))
+    check(lib().tt_k_gram_tall(_ctx_for(z.device.index), _ptr(z), n, N, rs, cs, _ptr(w)))
     return w
 
 

@@ -197,6 +197,10 @@ namespace {
 
 enum Path { PATH_EXACT_ROWS = 0, PATH_EXACT_COLS = 1, PATH_RAND = 2, PATH_IDENTITY = 3 };
 
+// Internal option bit (above the public TT_FLAG_* range): adaptive ranks may fold a step whose
+// chosen rank keeps every row.
+constexpr int kFlagAdaptiveFold = 1 << 30;
+
 struct Step {
   long long m = 0, cols = 0;
   int r_req = 0, r_eff = 0, ks = 0;
@@ -605,7 +609,11 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
   // the eigenvalues back to the host, and the rest of the plan is rebuilt with the chosen rank.
   const bool adaptive = o.eps > 0.0;
   double delta2 = 0.0, energy = 0.0, xnorm2 = 0.0, tail_sum = 0.0;
-  if (adaptive) {
+  // A first step with an exact Gram of the whole tensor gives ||X||^2 as its eigenvalue sum
+  // (the trace); otherwise one FP64 norm pass runs first.
+  const bool norm_from_gram = adaptive && !P.steps.empty() && !stream &&
+                              (P.steps[0].path == PATH_EXACT_ROWS || P.steps[0].path == PATH_EXACT_COLS);
+  if (adaptive && !norm_from_gram) {
     const size_t mk = ws.mark();
     double* acc = ws.take<double>(2);
     if (!acc) {
@@ -658,6 +666,12 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       std::vector<double> lam((size_t)nev);
       TT_CUDA(cudaMemcpyAsync(lam.data(), B.evals, sizeof(double) * nev, cudaMemcpyDeviceToHost, s));
       TT_CUDA(cudaStreamSynchronize(s));
+      if (norm_from_gram && k == 0) {
+        xnorm2 = 0.0;
+        for (double v : lam) xnorm2 += std::max(v, 0.0);
+        energy = xnorm2;
+        delta2 = o.eps * o.eps * xnorm2 / (double)(P.d - 1);
+      }
       const int cap = std::min(rmax[k + 1], std::min(nev, re));
       int r = 0;
       double tail = energy;
@@ -786,6 +800,10 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
       TT_TRY(decide((int)m));
+      // An adaptive rank that keeps every row makes the step a rotation: fold it like a
+      // planned full-rank step (the next step's geometry is the same either way).
+      const bool fold = st.fold || (adaptive && !ring1 && !st.perm231 && rq == m && re == m && rin == rcore &&
+                                    (o.flags & kFlagAdaptiveFold));
       // basis (m x r_req, zero-padded beyond r_eff), FP32, canonical column signs
       TT_TRY(launch_f64_to_f32_cols(B.evecs, m, m, re, B.ef, m, rq, s));
       TT_TRY(launch_canon_cols(B.ef, m, re, m, B.evecs, (int)m, m, s));
@@ -795,7 +813,8 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         TT_TRY(join_side());
         TT_TRY(emit_core(B.ef, core_dst, pend, rin, rcore, ni, rq, s));
       }
-      if (st.fold) {
+      if (fold) {
+        if (!st.fold) --npasses;
         // next data = raw data; pending rotation = eigenvectors of the raw Gram
         double* pnew = B.pend[pend_slot ^ 1];
         TT_CUDA(cudaMemcpyAsync(pnew, B.evecs, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, s));
@@ -855,11 +874,9 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
                                   s);
           }));
           // Adaptive ranks need the basis beyond the FP32 Gram's resolution (graded spectra
-          // down to delta / ||A|| ~ 1e-4): full CholeskyQR2 with FP64 Grams there; one
-          // FP32-Gram pass otherwise.
-          TT_TRY(pass.run(TT_PASS_OTHER, 6.0 * cols * ksa * ksa, 24.0 * cols * ksa, [&] {
-            return adaptive ? launch_cholqr2(B.bt, cols, ksa, 1, cols, nullptr, ws, c->dstat, s)
-                            : launch_orth_power(B.bt, cols, ksa, 1, cols, ws, c->dstat, s);
+          // down to delta / ||A|| ~ 1e-4): the pass forms its Gram with FP64 products there.
+          TT_TRY(pass.run(TT_PASS_OTHER, 4.0 * cols * ksa * ksa, 12.0 * cols * ksa, [&] {
+            return launch_orth_power(B.bt, cols, ksa, 1, cols, ws, c->dstat, s, adaptive);
           }));
           TT_TRY(pass.run(TT_PASS_SKETCH, fl_pass, by_pass, [&] {
             return launch_sketch(cur, m, cols, B.bt, ksa, 1, cols, B.yd, engine, ws, c->dstat, s);
@@ -1098,7 +1115,10 @@ int run_entry(tt_ctx* c, const float* x, int d, const int* n, const int* r, cons
       set_error(TT_ERR_UNSUPPORTED, "adaptive ranks (eps > 0) are implemented for TT-SVD only");
       return TT_ERR_UNSUPPORTED;
     }
-    o.flags |= TT_FLAG_NO_FOLD;  // the rank of a full-rank step is not known in advance
+    // The rank of a full-rank step is not known in advance: no step is planned as a fold, and
+    // run_chain folds a step whose chosen rank keeps every row unless the caller said no.
+    if (!(o.flags & TT_FLAG_NO_FOLD)) o.flags |= kFlagAdaptiveFold;
+    o.flags |= TT_FLAG_NO_FOLD;
   }
   Plan P;
   TT_TRY(make_plan(d, n, r, ring, o, P));

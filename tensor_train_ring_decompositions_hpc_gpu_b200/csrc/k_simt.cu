@@ -24,6 +24,7 @@ static int num_sms() {
   }
   return g_num_sms;
 }
+static int max_optin_smem();
 
 // ---------------------------------------------------------------------------------------
 // Philox4x32-10 Gaussian generator (replaces curandGenerateNormal, TT3O:585-587)
@@ -92,15 +93,21 @@ int launch_gaussian(float* out, long long rows, int cols, long long ld, unsigned
 // ---------------------------------------------------------------------------------------
 // Plain-FP32 sketch  Y = A * W  (split over the long dimension n, FP64 reduction of splits)
 // ---------------------------------------------------------------------------------------
+// 256 rows of A per block (8 per thread) x NT sketch columns (NT / 8 per thread), the long
+// dimension in chunks of 32 columns of A: the next chunk is loaded into registers while the
+// current one is multiplied out of shared memory (two buffers, one barrier per chunk).
 template <int NT>
-__global__ void __launch_bounds__(256) k_sketch_simt(const float* __restrict__ a, long long m,
-                                                     long long n, const float* __restrict__ w,
-                                                     int N, long long wj, long long wc,
-                                                     long long jchunk, int cblk,
-                                                     double* __restrict__ part) {
+__global__ void __launch_bounds__(256, NT >= 40 ? 1 : 2) k_sketch_simt(const float* __restrict__ a, long long m,
+                                                                       long long n, const float* __restrict__ w,
+                                                                       int N, long long wj, long long wc,
+                                                                       long long jchunk, int cblk,
+                                                                       double* __restrict__ part) {
   constexpr int TI = 256, JC = 32, RI = 8, RC = NT / 8;
-  __shared__ __align__(16) float as[JC][TI];
-  __shared__ __align__(16) float wsm[JC][NT];
+  constexpr int AV = (TI * JC / 4) / 256;     // float4 loads of A per thread per chunk
+  constexpr int WV = (JC * NT + 255) / 256;   // W values per thread per chunk
+  extern __shared__ __align__(16) float sm_sk[];
+  float* as_base = sm_sk;                // [2][JC][TI]
+  float* ws_base = sm_sk + 2 * JC * TI;  // [2][JC][NT]
   const int tid = threadIdx.x;
   const long long i0 = (long long)blockIdx.x * TI;
   const int split = blockIdx.y;
@@ -114,9 +121,11 @@ __global__ void __launch_bounds__(256) k_sketch_simt(const float* __restrict__ a
 #pragma unroll
     for (int c = 0; c < RC; ++c) acc[e][c] = 0.f;
   const bool vec = ((m & 3) == 0) && ((((uintptr_t)a) & 15) == 0);
-  for (long long j0 = jb; j0 < je; j0 += JC) {
+  float4 ra[AV];
+  float rw[WV];
+  auto fetch = [&](long long j0) {
 #pragma unroll
-    for (int q = 0; q < (TI * JC / 4) / 256; ++q) {
+    for (int q = 0; q < AV; ++q) {
       const int f = tid + 256 * q;
       const int jj = f / (TI / 4), i4 = f % (TI / 4);
       const long long j = j0 + jj, i = i0 + 4 * i4;
@@ -132,36 +141,70 @@ __global__ void __launch_bounds__(256) k_sketch_simt(const float* __restrict__ a
           if (i + 3 < m) v.w = p[3];
         }
       }
-      *reinterpret_cast<float4*>(&as[jj][4 * i4]) = v;
+      ra[q] = v;
     }
-    if (wc == 1) {
-      for (int f = tid; f < JC * NT; f += 256) {
-        const int c = f % NT, jj = f / NT;
-        const long long j = j0 + jj;
-        wsm[jj][c] = (j < je && c0 + c < N) ? w[j * wj + (long long)(c0 + c)] : 0.f;
+#pragma unroll
+    for (int u = 0; u < WV; ++u) {
+      const int f = tid + 256 * u;
+      int jj, c;
+      if (wc == 1) {
+        c = f % NT;
+        jj = f / NT;
+      } else {
+        jj = f % JC;
+        c = f / JC;
       }
-    } else {
-      for (int f = tid; f < JC * NT; f += 256) {
-        const int jj = f % JC, c = f / JC;
-        const long long j = j0 + jj;
-        wsm[jj][c] = (j < je && c0 + c < N) ? w[j * wj + (long long)(c0 + c) * wc] : 0.f;
+      const long long j = j0 + jj;
+      rw[u] = (f < JC * NT && j < je && c0 + c < N) ? w[j * wj + (long long)(c0 + c) * wc] : 0.f;
+    }
+  };
+  auto stash = [&](int b) {
+    float* as = as_base + b * JC * TI;
+    float* wsm = ws_base + b * JC * NT;
+#pragma unroll
+    for (int q = 0; q < AV; ++q) {
+      const int f = tid + 256 * q;
+      const int jj = f / (TI / 4), i4 = f % (TI / 4);
+      *reinterpret_cast<float4*>(&as[jj * TI + 4 * i4]) = ra[q];
+    }
+#pragma unroll
+    for (int u = 0; u < WV; ++u) {
+      const int f = tid + 256 * u;
+      if (f < JC * NT) {
+        if (wc == 1)
+          wsm[(f / NT) * NT + f % NT] = rw[u];
+        else
+          wsm[(f % JC) * NT + f / JC] = rw[u];
       }
     }
-    __syncthreads();
+  };
+  if (jb < je) {
+    fetch(jb);
+    stash(0);
+  }
+  __syncthreads();
+  int b = 0;
+  for (long long j0 = jb; j0 < je; j0 += JC) {
+    const bool more = j0 + JC < je;
+    if (more) fetch(j0 + JC);
+    const float* as = as_base + b * JC * TI;
+    const float* wsm = ws_base + b * JC * NT;
 #pragma unroll 4
     for (int jj = 0; jj < JC; ++jj) {
-      const float4 x0 = *reinterpret_cast<const float4*>(&as[jj][ti * RI]);
-      const float4 x1 = *reinterpret_cast<const float4*>(&as[jj][ti * RI + 4]);
+      const float4 x0 = *reinterpret_cast<const float4*>(&as[jj * TI + ti * RI]);
+      const float4 x1 = *reinterpret_cast<const float4*>(&as[jj * TI + ti * RI + 4]);
       const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
       float wv[RC];
 #pragma unroll
-      for (int c = 0; c < RC; ++c) wv[c] = wsm[jj][tc * RC + c];
+      for (int c = 0; c < RC; ++c) wv[c] = wsm[jj * NT + tc * RC + c];
 #pragma unroll
       for (int e = 0; e < RI; ++e)
 #pragma unroll
         for (int c = 0; c < RC; ++c) acc[e][c] = fmaf(xv[e], wv[c], acc[e][c]);
     }
+    if (more) stash(b ^ 1);
     __syncthreads();
+    b ^= 1;
   }
 #pragma unroll
   for (int e = 0; e < RI; ++e) {
@@ -173,6 +216,35 @@ __global__ void __launch_bounds__(256) k_sketch_simt(const float* __restrict__ a
     }
   }
   (void)cblk;
+}
+
+// Launch of k_sketch_simt with the tile width covering N (multiples of 8 up to 64; wider N
+// takes several column blocks of 64).
+static void launch_sketch_simt_kernel(const float* a, long long m, long long n, const float* w, int N, long long wj,
+                                      long long wc, long long jchunk, int nsplit, double* part, cudaStream_t s) {
+  const int NT = N <= 16 ? 16 : N <= 24 ? 24 : N <= 32 ? 32 : N <= 40 ? 40 : N <= 48 ? 48 : 64;
+  const int cblk = ceil_div(N, NT);
+  dim3 grid(ceil_div(m, 256), nsplit, cblk);
+  static bool attr = false;
+  if (!attr) {
+#define SK_ATTR(V) \
+  cudaFuncSetAttribute(k_sketch_simt<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * 32 * (256 + V) * 4))
+    SK_ATTR(16); SK_ATTR(24); SK_ATTR(32); SK_ATTR(40); SK_ATTR(48); SK_ATTR(64);
+#undef SK_ATTR
+    attr = true;
+  }
+  const size_t shm = (size_t)2 * 32 * (256 + NT) * sizeof(float);
+#define SK_CASE(V) \
+  case V: k_sketch_simt<V><<<grid, 256, shm, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
+  switch (NT) {
+    SK_CASE(16)
+    SK_CASE(24)
+    SK_CASE(32)
+    SK_CASE(40)
+    SK_CASE(48)
+    default: k_sketch_simt<64><<<grid, 256, shm, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
+  }
+#undef SK_CASE
 }
 
 // Sum of nsplit partial blocks: each 256-thread block owns 32 consecutive outputs, its 8 warps
@@ -249,15 +321,7 @@ int launch_sketch(const float* a, long long m, long long n, const float* w, int 
     set_error(TT_ERR_NOMEM, "sketch workspace");
     return TT_ERR_NOMEM;
   }
-  const int NT = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : 64;
-  const int cblk = ceil_div(N, NT);
-  dim3 grid(ceil_div(m, 256), nsplit, cblk);
-  switch (NT) {
-    case 16: k_sketch_simt<16><<<grid, 256, 0, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
-    case 32: k_sketch_simt<32><<<grid, 256, 0, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
-    case 48: k_sketch_simt<48><<<grid, 256, 0, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
-    default: k_sketch_simt<64><<<grid, 256, 0, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
-  }
+  launch_sketch_simt_kernel(a, m, n, w, N, wj, wc, jchunk, nsplit, part, s);
   count_launch();
   TT_LAUNCH_CHECK();
   TT_TRY(launch_reduce_splits(part, (long long)N * m, nsplit, y, s));
@@ -285,15 +349,7 @@ int launch_sketch_simt_static(const float* a, long long m, long long n, const fl
     jchunk = (jchunk + 31) / 32 * 32;
     nsplit = (int)((n + jchunk - 1) / jchunk);
   }
-  const int NT = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : 64;
-  const int cblk = ceil_div(N, NT);
-  dim3 grid(ceil_div(m, 256), nsplit, cblk);
-  switch (NT) {
-    case 16: k_sketch_simt<16><<<grid, 256, 0, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
-    case 32: k_sketch_simt<32><<<grid, 256, 0, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
-    case 48: k_sketch_simt<48><<<grid, 256, 0, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
-    default: k_sketch_simt<64><<<grid, 256, 0, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
-  }
+  launch_sketch_simt_kernel(a, m, n, w, N, wj, wc, jchunk, nsplit, part, s);
   count_launch();
   TT_LAUNCH_CHECK();
   return launch_reduce_splits(part, (long long)N * m, nsplit, y, s);
@@ -304,15 +360,21 @@ int launch_sketch_simt_static(const float* a, long long m, long long n, const fl
 // ---------------------------------------------------------------------------------------
 __device__ __forceinline__ int swz(int row, int col) { return col ^ (((row >> 2) & 7) << 2); }
 
+// 256 columns of A per block (8 per thread) x NT outputs (NT / 8 per thread), K in chunks of
+// 32: the next chunk is loaded into registers while the current one is multiplied out of
+// shared memory (two buffers, one barrier per chunk).
 template <int NT>
-__global__ void __launch_bounds__(256) k_project_simt(const float* __restrict__ a, long long m,
-                                                      long long n, const float* __restrict__ q,
-                                                      int N, long long ldq, float* __restrict__ out,
-                                                      long long ldo, int mode, int r0, int r1,
-                                                      long long kchunk) {
+__global__ void __launch_bounds__(256, NT >= 64 ? 1 : 2) k_project_simt(const float* __restrict__ a, long long m,
+                                                                        long long n, const float* __restrict__ q,
+                                                                        int N, long long ldq, float* __restrict__ out,
+                                                                        long long ldo, int mode, int r0, int r1,
+                                                                        long long kchunk) {
   constexpr int TJ = 256, KC = 32, RJ = 8, RC = NT / 8;
-  __shared__ __align__(16) float as[KC][TJ];
-  __shared__ __align__(16) float qs[KC][NT];
+  constexpr int AV = (TJ * KC / 4) / 256;    // float4 loads of A per thread per chunk
+  constexpr int QV = (KC * NT + 255) / 256;  // Q values per thread per chunk
+  extern __shared__ __align__(16) float sm_ps[];
+  float* as_base = sm_ps;                // [2][KC][TJ]
+  float* qs_base = sm_ps + 2 * KC * TJ;  // [2][KC][NT]
   const int tid = threadIdx.x;
   const long long j0 = (long long)blockIdx.x * TJ;
   const int c0 = blockIdx.y * NT;
@@ -327,9 +389,11 @@ __global__ void __launch_bounds__(256) k_project_simt(const float* __restrict__ 
   const long long kb = (long long)blockIdx.z * kchunk;
   const long long ke = (kb + kchunk < m) ? kb + kchunk : m;
   out += (long long)blockIdx.z * n * ldo;
-  for (long long k0 = kb; k0 < ke; k0 += KC) {
+  float4 ra[AV];
+  float rq[QV];
+  auto fetch = [&](long long k0) {
 #pragma unroll
-    for (int qq = 0; qq < (TJ * KC / 4) / 256; ++qq) {
+    for (int qq = 0; qq < AV; ++qq) {
       const int f = tid + 256 * qq;
       const int jj = f >> 3, k4 = f & 7;
       const long long j = j0 + jj, k = k0 + 4 * k4;
@@ -345,32 +409,61 @@ __global__ void __launch_bounds__(256) k_project_simt(const float* __restrict__ 
           if (k + 3 < ke) v.w = p[3];
         }
       }
-      const int kk = 4 * k4;
-      as[kk + 0][swz(kk + 0, jj)] = v.x;
-      as[kk + 1][swz(kk + 1, jj)] = v.y;
-      as[kk + 2][swz(kk + 2, jj)] = v.z;
-      as[kk + 3][swz(kk + 3, jj)] = v.w;
+      ra[qq] = v;
     }
-    for (int f = tid; f < KC * NT; f += 256) {
+#pragma unroll
+    for (int u = 0; u < QV; ++u) {
+      const int f = tid + 256 * u;
       const int kk = f % KC, c = f / KC;
       const long long k = k0 + kk;
-      qs[kk][c] = (k < ke && c0 + c < N) ? q[k + ldq * (long long)(c0 + c)] : 0.f;
+      rq[u] = (f < KC * NT && k < ke && c0 + c < N) ? q[k + ldq * (long long)(c0 + c)] : 0.f;
     }
-    __syncthreads();
+  };
+  auto stash = [&](int b) {
+    float* as = as_base + b * KC * TJ;
+    float* qs = qs_base + b * KC * NT;
+#pragma unroll
+    for (int qq = 0; qq < AV; ++qq) {
+      const int f = tid + 256 * qq;
+      const int jj = f >> 3, kk = 4 * (f & 7);
+      as[(kk + 0) * TJ + swz(kk + 0, jj)] = ra[qq].x;
+      as[(kk + 1) * TJ + swz(kk + 1, jj)] = ra[qq].y;
+      as[(kk + 2) * TJ + swz(kk + 2, jj)] = ra[qq].z;
+      as[(kk + 3) * TJ + swz(kk + 3, jj)] = ra[qq].w;
+    }
+#pragma unroll
+    for (int u = 0; u < QV; ++u) {
+      const int f = tid + 256 * u;
+      if (f < KC * NT) qs[(f % KC) * NT + f / KC] = rq[u];
+    }
+  };
+  if (kb < ke) {
+    fetch(kb);
+    stash(0);
+  }
+  __syncthreads();
+  int b = 0;
+  for (long long k0 = kb; k0 < ke; k0 += KC) {
+    const bool more = k0 + KC < ke;
+    if (more) fetch(k0 + KC);
+    const float* as = as_base + b * KC * TJ;
+    const float* qs = qs_base + b * KC * NT;
 #pragma unroll 4
     for (int kk = 0; kk < KC; ++kk) {
-      const float4 x0 = *reinterpret_cast<const float4*>(&as[kk][swz(kk, tj * RJ)]);
-      const float4 x1 = *reinterpret_cast<const float4*>(&as[kk][swz(kk, tj * RJ + 4)]);
+      const float4 x0 = *reinterpret_cast<const float4*>(&as[kk * TJ + swz(kk, tj * RJ)]);
+      const float4 x1 = *reinterpret_cast<const float4*>(&as[kk * TJ + swz(kk, tj * RJ + 4)]);
       const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
       float qv[RC];
 #pragma unroll
-      for (int c = 0; c < RC; ++c) qv[c] = qs[kk][tc * RC + c];
+      for (int c = 0; c < RC; ++c) qv[c] = qs[kk * NT + tc * RC + c];
 #pragma unroll
       for (int e = 0; e < RJ; ++e)
 #pragma unroll
         for (int c = 0; c < RC; ++c) acc[e][c] = fmaf(xv[e], qv[c], acc[e][c]);
     }
+    if (more) stash(b ^ 1);
     __syncthreads();
+    b ^= 1;
   }
 #pragma unroll
   for (int e = 0; e < RJ; ++e) {
@@ -601,16 +694,34 @@ int launch_project(const float* a, long long m, long long n, const float* q, int
   } else {
     kc = m;
   }
-  dim3 grid(ceil_div(n, 256), ceil_div(N, NT), ks);
+  // output tile width: the smallest multiple of 8 in {16, 24, 32, 40, 48, 64} covering N
+  const int NTs = N <= 16 ? 16 : N <= 24 ? 24 : N <= 32 ? 32 : N <= 40 ? 40 : N <= 48 ? 48 : 64;
+  dim3 grid(ceil_div(n, 256), ceil_div(N, NTs), ks);
   float* dst = ks > 1 ? part : out;
   const long long ldd = ks > 1 ? N : ldo;
   const int md = ks > 1 ? OUT_ROWMAJOR : mode;
-  switch (NT) {
-    case 16: k_project_simt<16><<<grid, 256, 0, s>>>(a, m, n, q, N, ldq, dst, ldd, md, r0, r1, kc); break;
-    case 32: k_project_simt<32><<<grid, 256, 0, s>>>(a, m, n, q, N, ldq, dst, ldd, md, r0, r1, kc); break;
-    case 48: k_project_simt<48><<<grid, 256, 0, s>>>(a, m, n, q, N, ldq, dst, ldd, md, r0, r1, kc); break;
-    default: k_project_simt<64><<<grid, 256, 0, s>>>(a, m, n, q, N, ldq, dst, ldd, md, r0, r1, kc); break;
+  {
+    static bool attr = false;
+    if (!attr) {
+#define PS_ATTR(V) \
+  cudaFuncSetAttribute(k_project_simt<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * 32 * (256 + V) * 4))
+      PS_ATTR(16); PS_ATTR(24); PS_ATTR(32); PS_ATTR(40); PS_ATTR(48); PS_ATTR(64);
+#undef PS_ATTR
+      attr = true;
+    }
   }
+  const size_t pshm = (size_t)2 * 32 * (256 + NTs) * sizeof(float);
+#define PS_CASE(V) \
+  case V: k_project_simt<V><<<grid, 256, pshm, s>>>(a, m, n, q, N, ldq, dst, ldd, md, r0, r1, kc); break;
+  switch (NTs) {
+    PS_CASE(16)
+    PS_CASE(24)
+    PS_CASE(32)
+    PS_CASE(40)
+    PS_CASE(48)
+    default: k_project_simt<64><<<grid, 256, pshm, s>>>(a, m, n, q, N, ldq, dst, ldd, md, r0, r1, kc); break;
+  }
+#undef PS_CASE
   count_launch();
   TT_LAUNCH_CHECK();
   if (ks > 1) {
@@ -757,15 +868,192 @@ __global__ void __launch_bounds__(256) k_gram(const float* __restrict__ x, long 
   }
 }
 
-__global__ void k_gram_reduce(const double* __restrict__ part, int nblk, int MP, int M,
+// W = sum over the per-block partials (upper tiles of size T stored, the lower half mirrored):
+// one warp per entry, lanes stride over the blocks, fixed-order shuffle tree (deterministic).
+__global__ void k_gram_reduce(const double* __restrict__ part, int nblk, int MP, int M, int T,
                               double* __restrict__ w) {
-  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int idx = (int)((blockIdx.x * (long long)blockDim.x + threadIdx.x) >> 5);
+  const int lane = threadIdx.x & 31;
   if (idx >= M * M) return;
   const int aI = idx % M, bI = idx / M;
-  const int src = (aI / 4 <= bI / 4) ? aI * MP + bI : bI * MP + aI;
+  const int src = (aI / T <= bI / T) ? aI * MP + bI : bI * MP + aI;
   double sacc = 0.0;
-  for (int k = 0; k < nblk; ++k) sacc += part[(long long)k * MP * MP + src];
-  w[aI + (long long)M * bI] = sacc;
+  for (int k = lane; k < nblk; k += 32) sacc += part[(long long)k * MP * MP + src];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) sacc += __shfl_xor_sync(0xffffffffu, sacc, o);
+  if (lane == 0) w[aI + (long long)M * bI] = sacc;
+}
+
+static void launch_gram_reduce(const double* part, int nblk, int MP, int M, int T, double* w, cudaStream_t s) {
+  const long long threads = 32LL * M * M;
+  k_gram_reduce<<<(int)ceil_div_ll(threads, 256), 256, 0, s>>>(part, nblk, MP, M, T, w);
+}
+
+// ---------------------------------------------------------------------------------------
+// Gram of many short vectors  W = sum_j x_j x_j^T  (17 <= M <= 64 components), two layouts:
+//  * contiguous (COL = false): x_j = x + j M, M % 4 == 0, x 16-byte aligned -- the Gram of a
+//    long unfolding with few rows (columns contiguous) and of a row-major factor B^T.  A stage
+//    of VC vectors is one contiguous block, copied with 16-byte cp.async;
+//  * column-major (COL = true): component c of x_j at x[j + c ld] -- a tall n x M matrix (the
+//    power-iteration basis Z).  Each component's VC values are copied with coalesced 4-byte
+//    cp.async into a row of stride VC + 1 (conflict-free column reads).
+// Stages are NS deep.  Each warp computes a 32 x 32 block of W: lane (p, q) = (lane / 8,
+// lane % 8) holds rows 8p..8p+7 x columns 4q..4q+3, 12 loaded values per vector for 32 FMAs.
+// MP = 32 has one such block (12 warps split the vectors), MP = 64 the three upper blocks
+// (4 warps each); one block of 384 threads per SM.  Rows and columns >= M read neighbouring
+// words; those entries are never written out.  FP32 products accumulate over VFLUSH vectors
+// per lane (round-to-nearest FMA, unbiased) and are then added into FP64; ACC64 accumulates
+// every product in FP64 instead.
+// ---------------------------------------------------------------------------------------
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
+}
+
+constexpr int GV_VC = 192;  // vectors per stage
+constexpr int GV_NS = 4;    // stages in flight
+constexpr int GV_VFLUSH = 64;
+
+template <int MP>
+struct GramVecShape {
+  static constexpr int WB = MP == 32 ? 1 : 3;    // 32 x 32 warp blocks (upper triangle)
+  static constexpr int WPB = MP == 32 ? 12 : 4;  // warps per warp block
+  static constexpr int NT = 32 * WB * WPB;       // 384
+};
+
+static size_t gram_vec_smem(int MP, int M, bool col) {
+  const size_t stage = col ? (size_t)MP * (GV_VC + 1) : (size_t)GV_VC * M + MP;
+  const size_t red = (size_t)12 * 1024 * 2;  // per-warp 32 x 32 FP64 blocks, in floats
+  return std::max(stage * GV_NS, red) * sizeof(float);
+}
+
+template <int MP, bool ACC64, bool COL>
+__global__ void __launch_bounds__(GramVecShape<MP>::NT, 1) k_gram_vec(const float* __restrict__ x, long long nvec,
+                                                                    int M, long long ld, long long vchunk,
+                                                                    double* __restrict__ part) {
+  using S = GramVecShape<MP>;
+  extern __shared__ __align__(16) float sm_gv[];
+  constexpr int LDC = GV_VC + 1;  // COL: row stride of a component
+  // floats per stage buffer: COL, MP component rows; otherwise VC vectors + MP words of slack
+  const int stage_f = COL ? MP * LDC : GV_VC * M + MP;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int wb = warp % S::WB, ph = warp / S::WB;
+  const int r0 = (wb == 2 ? 32 : 0) + 8 * (lane >> 3);
+  const int c0 = (wb == 0 ? 0 : 32) + 4 * (lane & 7);
+  const long long vb = (long long)blockIdx.x * vchunk;
+  const long long ve = (vb + vchunk < nvec) ? vb + vchunk : nvec;
+  const long long nst = vb < ve ? (ve - vb + GV_VC - 1) / GV_VC : 0;
+
+  auto load = [&](long long st) {
+    const long long v0 = vb + st * GV_VC;
+    const int nv = (int)((ve - v0 < GV_VC) ? ve - v0 : GV_VC);
+    float* dst = sm_gv + (int)(st % GV_NS) * stage_f;
+    if (COL) {
+      const int tot = nv * M;
+      for (int f = tid; f < tot; f += S::NT) {
+        const int c = f / nv, v = f - c * nv;
+        cp_async4(dst + c * LDC + v, x + (v0 + v) + (long long)c * ld);
+      }
+    } else {
+      const int n16 = nv * M / 4;
+      const float* src = x + v0 * M;
+      for (int f = tid; f < n16; f += S::NT) cp_async16(dst + 4 * f, src + 4 * f);
+    }
+  };
+
+  float acc[8][4];
+  double accd[8][4];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      acc[i][j] = 0.f;
+      accd[i][j] = 0.0;
+    }
+  int since = 0;
+#pragma unroll
+  for (int st = 0; st < GV_NS - 1; ++st) {
+    if (st < nst) load(st);
+    cp_async_commit();
+  }
+  for (long long it = 0; it < nst; ++it) {
+    cp_async_wait<GV_NS - 2>();
+    __syncthreads();  // stage `it` landed for every thread; stage it - 1 fully consumed
+    if (it + GV_NS - 1 < nst) load(it + GV_NS - 1);
+    cp_async_commit();
+    const float* buf = sm_gv + (int)(it % GV_NS) * stage_f;
+    const long long v0 = vb + it * GV_VC;
+    const int nv = (int)((ve - v0 < GV_VC) ? ve - v0 : GV_VC);
+    for (int v = ph; v < nv; v += S::WPB) {
+      float av[8], bv[4];
+      if (COL) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i) av[i] = buf[(r0 + i) * LDC + v];
+#pragma unroll
+        for (int j = 0; j < 4; ++j) bv[j] = buf[(c0 + j) * LDC + v];
+      } else {
+        const float* col = buf + v * M;
+        const float4 a0 = *reinterpret_cast<const float4*>(col + r0);
+        const float4 a1 = *reinterpret_cast<const float4*>(col + r0 + 4);
+        const float4 b = *reinterpret_cast<const float4*>(col + c0);
+        av[0] = a0.x; av[1] = a0.y; av[2] = a0.z; av[3] = a0.w;
+        av[4] = a1.x; av[5] = a1.y; av[6] = a1.z; av[7] = a1.w;
+        bv[0] = b.x; bv[1] = b.y; bv[2] = b.z; bv[3] = b.w;
+      }
+      if (ACC64) {
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) accd[i][j] = fma((double)av[i], (double)bv[j], accd[i][j]);
+      } else {
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 4; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+        if (++since == GV_VFLUSH) {
+          since = 0;
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              accd[i][j] += (double)acc[i][j];
+              acc[i][j] = 0.f;
+            }
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();  // stage buffers free: reused for the cross-warp sum
+  if (!ACC64) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) accd[i][j] += (double)acc[i][j];
+  }
+  double* red = reinterpret_cast<double*>(sm_gv);  // [warp][32][32]
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 4; ++j) red[warp * 1024 + (8 * (lane >> 3) + i) * 32 + 4 * (lane & 7) + j] = accd[i][j];
+  __syncthreads();
+  double* dst = part + (long long)blockIdx.x * MP * MP;
+  for (int e = tid; e < S::WB * 1024; e += S::NT) {
+    const int b = e >> 10, rr = (e >> 5) & 31, cc = e & 31;
+    double t = 0.0;
+    for (int p = 0; p < S::WPB; ++p) t += red[(p * S::WB + b) * 1024 + rr * 32 + cc];
+    const int R = (b == 2 ? 32 : 0) + rr, Cc = (b == 0 ? 0 : 32) + cc;
+    dst[R * MP + Cc] = t;
+  }
 }
 
 static int gram_mp(int M) { return M <= 16 ? 16 : M <= 32 ? 32 : M <= 48 ? 48 : M <= 64 ? 64 : 128; }
@@ -779,12 +1067,41 @@ static void gram_plan(long long nvec, int* nblk, long long* vchunk) {
   *nblk = (int)std::max<long long>(1, ceil_div_ll(nvec, vc));
 }
 
+// Vector Gram (k_gram_vec): taken for 17 <= M <= 64 and enough vectors to fill the GPU, with
+// x_j = x + j M (M % 4 == 0, 16-byte aligned base) or the column-major layout x[j + c es]
+// (vs = 1, es >= nvec).  Returns the block size MP (0: not taken), the grid and the vectors
+// per block.
+static int gram_vec_plan(const float* x, long long nvec, int M, long long vs, long long es, int* grid,
+                         long long* vchunk, bool* col) {
+  if (M < 17 || M > 64 || nvec < 8192) return 0;
+  *col = (vs == 1 && es >= nvec);
+  if (!*col) {
+    if (es != 1 || vs != M || (M & 3) != 0) return 0;
+    if (x && (reinterpret_cast<uintptr_t>(x) & 15) != 0) return 0;
+  }
+  const int MP = M <= 32 ? 32 : 64;
+  if (gram_vec_smem(MP, M, *col) > (size_t)max_optin_smem()) return 0;
+  const long long g = std::min<long long>((long long)num_sms(), ceil_div_ll(nvec, 4 * GV_VC));
+  long long vc = ceil_div_ll(nvec, g);
+  vc = ceil_div_ll(vc, GV_VC) * GV_VC;
+  *vchunk = vc;
+  *grid = (int)ceil_div_ll(nvec, vc);
+  return MP;
+}
+
 size_t gram_ws_bytes(long long nvec, int M) {
   int nblk;
   long long vc;
   gram_plan(nvec, &nblk, &vc);
   const int MP = gram_mp(M);
-  return (size_t)nblk * MP * MP * sizeof(double) + 4096;
+  size_t b = (size_t)nblk * MP * MP * sizeof(double);
+  int g = 0;
+  bool col = false;
+  int MPv = gram_vec_plan(nullptr, nvec, M, M, 1, &g, &vc, &col);
+  if (MPv) b = std::max(b, (size_t)g * MPv * MPv * sizeof(double));
+  MPv = gram_vec_plan(nullptr, nvec, M, 1, nvec, &g, &vc, &col);
+  if (MPv) b = std::max(b, (size_t)g * MPv * MPv * sizeof(double));
+  return b + 4096;
 }
 
 int launch_gram(const float* x, long long nvec, int M, long long vs, long long es, double* w,
@@ -796,6 +1113,52 @@ int launch_gram(const float* x, long long nvec, int M, long long vs, long long e
   }
   int nblk;
   long long vchunk;
+  {
+    bool col = false;
+    const int MPv = gram_vec_plan(x, nvec, M, vs, es, &nblk, &vchunk, &col);
+    if (MPv) {
+      const size_t mk = ws.mark();
+      double* part = ws.take<double>((size_t)nblk * MPv * MPv);
+      if (!part) {
+        set_error(TT_ERR_NOMEM, "gram workspace");
+        return TT_ERR_NOMEM;
+      }
+      const size_t shm = gram_vec_smem(MPv, M, col);
+      static bool attr = false;
+      if (!attr) {
+        const int mx = max_optin_smem();
+#define GV_ATTR(MPV, A, C) cudaFuncSetAttribute(k_gram_vec<MPV, A, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)
+        GV_ATTR(32, false, false); GV_ATTR(32, true, false); GV_ATTR(64, false, false); GV_ATTR(64, true, false);
+        GV_ATTR(32, false, true); GV_ATTR(32, true, true); GV_ATTR(64, false, true); GV_ATTR(64, true, true);
+#undef GV_ATTR
+        attr = true;
+      }
+      const long long ld = col ? es : M;
+#define GV_LAUNCH(MPV, A, C) \
+  k_gram_vec<MPV, A, C><<<nblk, GramVecShape<MPV>::NT, shm, s>>>(x, nvec, M, ld, vchunk, part)
+      if (MPv == 32) {
+        if (col) {
+          if (acc64) GV_LAUNCH(32, true, true); else GV_LAUNCH(32, false, true);
+        } else {
+          if (acc64) GV_LAUNCH(32, true, false); else GV_LAUNCH(32, false, false);
+        }
+      } else {
+        if (col) {
+          if (acc64) GV_LAUNCH(64, true, true); else GV_LAUNCH(64, false, true);
+        } else {
+          if (acc64) GV_LAUNCH(64, true, false); else GV_LAUNCH(64, false, false);
+        }
+      }
+#undef GV_LAUNCH
+      count_launch();
+      TT_LAUNCH_CHECK();
+      launch_gram_reduce(part, nblk, MPv, M, 32, w, s);
+      count_launch();
+      TT_LAUNCH_CHECK();
+      ws.reset(mk);
+      return TT_OK;
+    }
+  }
   gram_plan(std::max<long long>(nvec, 1), &nblk, &vchunk);
   const int MP = gram_mp(M);
   const size_t mk = ws.mark();
@@ -821,7 +1184,7 @@ int launch_gram(const float* x, long long nvec, int M, long long vs, long long e
 #undef GRAM_CASE
   count_launch();
   TT_LAUNCH_CHECK();
-  k_gram_reduce<<<ceil_div(M * M, 256), 256, 0, s>>>(part, nblk, MP, M, w);
+  launch_gram_reduce(part, nblk, MP, M, 4, w, s);
   count_launch();
   TT_LAUNCH_CHECK();
   ws.reset(mk);
@@ -915,64 +1278,70 @@ __global__ void __launch_bounds__(256) k_chol_inv(const double* __restrict__ w, 
   (void)st;
 }
 
-// Y (n x N) <- Y * T, T = R^-1 upper (FP64 in global, staged as FP32).  128 rows per block,
-// one row per thread, outputs produced 32 columns at a time.
+// Y (n x N) <- Y * T, T = R^-1 upper (FP64 in global, staged as FP32 once per block).  Blocks
+// loop over tiles of 128 rows, one row per thread, outputs produced 32 columns at a time and
+// written over the tile in shared memory.
 template <int NP>
 __global__ void __launch_bounds__(128) k_apply_rinv(float* __restrict__ y, long long n, int N,
                                                     long long vs, long long es,
                                                     const double* __restrict__ t) {
   extern __shared__ float sm_apply[];
   float* ts = sm_apply;                 // NP x NP, ts[k*NP + c]
-  float* ys = ts + NP * NP;             // 128 x (NP+1)
-  float* yo = ys + 128 * (NP + 1);      // 128 x (NP+1)
+  float* ys = ts + NP * NP;             // 128 x (NP+1): the tile, overwritten by the result
   constexpr int LD = NP + 1;
   const int tid = threadIdx.x;
   for (int idx = tid; idx < NP * NP; idx += 128) {
     const int k = idx % NP, c = idx / NP;
     ts[k * NP + c] = (k < N && c < N) ? (float)t[k + (long long)N * c] : 0.f;
   }
-  const long long j0 = (long long)blockIdx.x * 128;
-  if (es == 1) {
-    for (int f = tid; f < 128 * NP; f += 128) {
-      const int c = f % NP, r = f / NP;
-      const long long j = j0 + r;
-      ys[r * LD + c] = (j < n && c < N) ? y[j * vs + c] : 0.f;
-    }
-  } else {
-    for (int f = tid; f < 128 * NP; f += 128) {
-      const int r = f % 128, c = f / 128;
-      const long long j = j0 + r;
-      ys[r * LD + c] = (j < n && c < N) ? y[j * vs + (long long)c * es] : 0.f;
-    }
-  }
-  __syncthreads();
   // Output chunk width divides NP (NP is a multiple of 16), so cb + c < NP always.
   constexpr int CB = (NP % 32 == 0) ? 32 : 16;
   static_assert(NP % CB == 0, "chunk width must divide the padded width");
-  for (int cb = 0; cb < NP; cb += CB) {
-    float outv[CB];
-#pragma unroll
-    for (int c = 0; c < CB; ++c) outv[c] = 0.f;
-    for (int k = 0; k < cb + CB && k < NP; ++k) {
-      const float yk = ys[tid * LD + k];
-#pragma unroll
-      for (int c = 0; c < CB; ++c) outv[c] = fmaf(yk, ts[k * NP + cb + c], outv[c]);
+  const long long ntile = (n + 127) / 128;
+  for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
+    const long long j0 = tile * 128;
+    __syncthreads();  // ts ready / the previous tile's stores done
+    if (es == 1) {
+      for (int f = tid; f < 128 * NP; f += 128) {
+        const int c = f % NP, r = f / NP;
+        const long long j = j0 + r;
+        ys[r * LD + c] = (j < n && c < N) ? y[j * vs + c] : 0.f;
+      }
+    } else {
+      for (int f = tid; f < 128 * NP; f += 128) {
+        const int r = f % 128, c = f / 128;
+        const long long j = j0 + r;
+        ys[r * LD + c] = (j < n && c < N) ? y[j * vs + (long long)c * es] : 0.f;
+      }
     }
+    __syncthreads();
+    // Row tid in place: T is upper triangular, so output columns cb.. need inputs k < cb + CB
+    // only; chunks run from the last one down and overwrite inputs no later chunk reads.
+    for (int cb = NP - CB; cb >= 0; cb -= CB) {
+      float outv[CB];
 #pragma unroll
-    for (int c = 0; c < CB; ++c) yo[tid * LD + cb + c] = outv[c];
-  }
-  __syncthreads();
-  if (es == 1) {
-    for (int f = tid; f < 128 * NP; f += 128) {
-      const int c = f % NP, r = f / NP;
-      const long long j = j0 + r;
-      if (j < n && c < N) y[j * vs + c] = yo[r * LD + c];
+      for (int c = 0; c < CB; ++c) outv[c] = 0.f;
+      for (int k = 0; k < cb + CB; ++k) {
+        const float yk = ys[tid * LD + k];
+#pragma unroll
+        for (int c = 0; c < CB; ++c) outv[c] = fmaf(yk, ts[k * NP + cb + c], outv[c]);
+      }
+#pragma unroll
+      for (int c = 0; c < CB; ++c) ys[tid * LD + cb + c] = outv[c];
     }
-  } else {
-    for (int f = tid; f < 128 * NP; f += 128) {
-      const int r = f % 128, c = f / 128;
-      const long long j = j0 + r;
-      if (j < n && c < N) y[j * vs + (long long)c * es] = yo[r * LD + c];
+    __syncthreads();
+    if (es == 1) {
+      for (int f = tid; f < 128 * NP; f += 128) {
+        const int c = f % NP, r = f / NP;
+        const long long j = j0 + r;
+        if (j < n && c < N) y[j * vs + c] = ys[r * LD + c];
+      }
+    } else {
+      for (int f = tid; f < 128 * NP; f += 128) {
+        const int r = f % 128, c = f / 128;
+        const long long j = j0 + r;
+        if (j < n && c < N) y[j * vs + (long long)c * es] = ys[r * LD + c];
+      }
     }
   }
 }
@@ -1186,12 +1555,15 @@ int launch_cholqr2(float* y, long long n, int N, long long vs, long long es, dou
   return cholqr_passes(y, n, N, vs, es, r, ws, st, s, 2, true);
 }
 
-// One CholeskyQR pass with the FP32-accumulated Gram (FP64 across chunks of vectors): the
-// orthonormalisation between power iterations, which only has to keep the basis well
-// conditioned (the sketch that follows is orthonormalised by CholeskyQR2).
+// One CholeskyQR pass: the orthonormalisation between power iterations, which only has to keep
+// the basis well conditioned (the sketch that follows is orthonormalised by CholeskyQR2).  The
+// Gram is FP32-accumulated (FP64 across chunks of vectors), or FP64 per product with acc64: a
+// basis whose columns span a graded spectrum (condition kappa) then comes out with
+// orthogonality ~kappa * 2^-24, still well conditioned, where the FP32 Gram (condition
+// kappa^2) would lose the small directions.
 int launch_orth_power(float* y, long long n, int N, long long vs, long long es, Arena& ws, DevStatus* st,
-                      cudaStream_t s) {
-  return cholqr_passes(y, n, N, vs, es, nullptr, ws, st, s, 1, false);
+                      cudaStream_t s, bool acc64) {
+  return cholqr_passes(y, n, N, vs, es, nullptr, ws, st, s, 1, acc64);
 }
 
 static int cholqr_passes(float* y, long long n, int N, long long vs, long long es, double* r, Arena& ws,
@@ -1253,8 +1625,10 @@ static int cholqr_passes(float* y, long long n, int N, long long vs, long long e
     k_chol_inv<<<1, 256, shm, s>>>(w, N, pass == 0 ? r1 : r2, rinv, 1e-12, ri_smem, st);
     count_launch();
     TT_LAUNCH_CHECK();
-    const int grid = ceil_div(n, 128);
-    const size_t ashm = ((size_t)NP * NP + 2 * 128 * (size_t)(NP + 1)) * sizeof(float);
+    const size_t ashm = ((size_t)NP * NP + 128 * (size_t)(NP + 1)) * sizeof(float);
+    // persistent blocks (R^-1 staged once per block), as many as fit on the SMs
+    const int per_sm = std::max(1, std::min(8, (int)((200u * 1024u) / (ashm + 1024))));
+    const int grid = (int)std::min<long long>(ceil_div_ll(n, 128), (long long)per_sm * num_sms());
     switch (NP) {
       case 16: k_apply_rinv<16><<<grid, 128, ashm, s>>>(y, n, N, vs, es, rinv); break;
       case 32: k_apply_rinv<32><<<grid, 128, ashm, s>>>(y, n, N, vs, es, rinv); break;

@@ -60,9 +60,10 @@ int launch_gram(const float* x, long long nvec, int M, long long vs, long long e
 // Writes R (N x N, FP64, upper) when r != nullptr.
 int launch_cholqr2(float* y, long long n, int N, long long vs, long long es, double* r,
                    Arena& ws, DevStatus* st, cudaStream_t s);
-// One CholeskyQR pass with an FP32-accumulated Gram (between power iterations).
+// One CholeskyQR pass (between power iterations): FP32-accumulated Gram, or FP64 products with
+// acc64 (graded spectra, whose small directions lie below the FP32 Gram's resolution).
 int launch_orth_power(float* y, long long n, int N, long long vs, long long es, Arena& ws, DevStatus* st,
-                      cudaStream_t s);
+                      cudaStream_t s, bool acc64 = false);
 
 // Symmetric eigen-decomposition by parallel cyclic Jacobi (FP64, N <= 128).
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps,
