@@ -1067,6 +1067,131 @@ static void gram_plan(long long nvec, int* nblk, long long* vchunk) {
   *nblk = (int)std::max<long long>(1, ceil_div_ll(nvec, vc));
 }
 
+// Symmetric variant for contiguous vectors with 17 <= M <= 32 (the exact step's Gram of a long
+// unfolding with few rows): the upper triangle of 8 x 8 tiles of the 32 x 32 result (10 tiles)
+// times 3 vectors is 30 lanes of a warp, so a vector costs 640 FMAs instead of 1024 and a lane
+// loads 16 values per 64 FMAs.  8 warps of 3 vectors take 24 vectors per step of a stage.
+// FP32 products: the per-lane FP64 sums live in shared memory (row stride 65 doubles) next to
+// the stages, which keeps the registers to the FP32 tile; FP64 products: in registers.
+constexpr int GS_NT = 256;
+constexpr int GS_LD = 65;
+static size_t gram_sym_smem(int M, bool acc64) {
+  const size_t stages = ((size_t)GV_VC * M + 32) * GV_NS * sizeof(float);
+  const size_t red = (size_t)GS_NT * GS_LD * sizeof(double);
+  return acc64 ? std::max(stages, red) : stages + red;
+}
+
+template <bool ACC64>
+__global__ void __launch_bounds__(GS_NT, 1) k_gram_sym32(const float* __restrict__ x, long long nvec, int M,
+                                                        long long vchunk, double* __restrict__ part) {
+  extern __shared__ __align__(16) float sm_gs[];
+  const int stage_f = GV_VC * M + 32;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int t = lane % 10, u = lane / 10;  // tile, vector of the triple (u == 3: idle lanes)
+  const int p = t < 4 ? 0 : t < 7 ? 1 : t < 9 ? 2 : 3;
+  const int q = t < 4 ? t : t < 7 ? t - 3 : t < 9 ? t - 5 : 3;
+  const long long vb = (long long)blockIdx.x * vchunk;
+  const long long ve = (vb + vchunk < nvec) ? vb + vchunk : nvec;
+  const long long nst = vb < ve ? (ve - vb + GV_VC - 1) / GV_VC : 0;
+  auto load = [&](long long st) {
+    const long long v0 = vb + st * GV_VC;
+    const int nv = (int)((ve - v0 < GV_VC) ? ve - v0 : GV_VC);
+    float* dst = sm_gs + (int)(st % GV_NS) * stage_f;
+    const int n16 = nv * M / 4;
+    const float* src = x + v0 * M;
+    for (int f = tid; f < n16; f += GS_NT) cp_async16(dst + 4 * f, src + 4 * f);
+  };
+  // FP64 sums: registers (ACC64) or this thread's row of the shared block after the stages
+  double* sacc = reinterpret_cast<double*>(sm_gs + GV_NS * stage_f + ((GV_NS * stage_f) & 1)) + tid * GS_LD;
+  float acc[8][8];
+  double accd[ACC64 ? 8 : 1][ACC64 ? 8 : 1];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      acc[i][j] = 0.f;
+      if (ACC64) accd[ACC64 ? i : 0][ACC64 ? j : 0] = 0.0;
+    }
+  if (!ACC64)
+    for (int e = 0; e < 64; ++e) sacc[e] = 0.0;
+  auto flush = [&]() {
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        sacc[i * 8 + j] += (double)acc[i][j];
+        acc[i][j] = 0.f;
+      }
+  };
+  int since = 0;
+#pragma unroll
+  for (int st = 0; st < GV_NS - 1; ++st) {
+    if (st < nst) load(st);
+    cp_async_commit();
+  }
+  for (long long it = 0; it < nst; ++it) {
+    cp_async_wait<GV_NS - 2>();
+    __syncthreads();
+    if (it + GV_NS - 1 < nst) load(it + GV_NS - 1);
+    cp_async_commit();
+    const float* buf = sm_gs + (int)(it % GV_NS) * stage_f;
+    const long long v0 = vb + it * GV_VC;
+    const int nv = (int)((ve - v0 < GV_VC) ? ve - v0 : GV_VC);
+    if (u < 3) {
+      for (int v = 3 * warp + u; v < nv; v += 24) {
+        const float* col = buf + v * M;
+        const float4 a0 = *reinterpret_cast<const float4*>(col + 8 * p);
+        const float4 a1 = *reinterpret_cast<const float4*>(col + 8 * p + 4);
+        const float4 b0 = *reinterpret_cast<const float4*>(col + 8 * q);
+        const float4 b1 = *reinterpret_cast<const float4*>(col + 8 * q + 4);
+        const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+        const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        if (ACC64) {
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+              accd[ACC64 ? i : 0][ACC64 ? j : 0] = fma((double)av[i], (double)bv[j], accd[ACC64 ? i : 0][ACC64 ? j : 0]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 8; ++i)
+#pragma unroll
+            for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+          if (++since == GV_VFLUSH) {
+            since = 0;
+            flush();
+          }
+        }
+      }
+    }
+  }
+  cp_async_wait<0>();
+  if (!ACC64) flush();
+  __syncthreads();  // stage buffers free (ACC64 writes its sums over them)
+  const double* red;  // [thread][GS_LD]
+  if (ACC64) {
+    double* r = reinterpret_cast<double*>(sm_gs);
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) r[tid * GS_LD + i * 8 + j] = accd[ACC64 ? i : 0][ACC64 ? j : 0];
+    red = r;
+  } else {
+    red = sacc - tid * GS_LD;
+  }
+  __syncthreads();
+  double* dst = part + (long long)blockIdx.x * 32 * 32;
+  for (int e = tid; e < 10 * 64; e += GS_NT) {
+    const int tt = e >> 6, ij = e & 63;
+    double sum = 0.0;
+    for (int w = 0; w < GS_NT / 32; ++w)
+      for (int uu = 0; uu < 3; ++uu) sum += red[(w * 32 + uu * 10 + tt) * GS_LD + ij];
+    const int pp = tt < 4 ? 0 : tt < 7 ? 1 : tt < 9 ? 2 : 3;
+    const int qq = tt < 4 ? tt : tt < 7 ? tt - 3 : tt < 9 ? tt - 5 : 3;
+    dst[(8 * pp + (ij >> 3)) * 32 + 8 * qq + (ij & 7)] = sum;
+  }
+}
+
 // Vector Gram (k_gram_vec): taken for 17 <= M <= 64 and enough vectors to fill the GPU, with
 // x_j = x + j M (M % 4 == 0, 16-byte aligned base) or the column-major layout x[j + c es]
 // (vs = 1, es >= nvec).  Returns the block size MP (0: not taken), the grid and the vectors
@@ -1132,6 +1257,26 @@ int launch_gram(const float* x, long long nvec, int M, long long vs, long long e
         GV_ATTR(32, false, true); GV_ATTR(32, true, true); GV_ATTR(64, false, true); GV_ATTR(64, true, true);
 #undef GV_ATTR
         attr = true;
+      }
+      if (MPv == 32 && !col && gram_sym_smem(M, acc64) <= (size_t)max_optin_smem()) {
+        static bool sattr = false;
+        if (!sattr) {
+          cudaFuncSetAttribute(k_gram_sym32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin_smem());
+          cudaFuncSetAttribute(k_gram_sym32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin_smem());
+          sattr = true;
+        }
+        const size_t sshm = gram_sym_smem(M, acc64);
+        if (acc64)
+          k_gram_sym32<true><<<nblk, GS_NT, sshm, s>>>(x, nvec, M, vchunk, part);
+        else
+          k_gram_sym32<false><<<nblk, GS_NT, sshm, s>>>(x, nvec, M, vchunk, part);
+        count_launch();
+        TT_LAUNCH_CHECK();
+        launch_gram_reduce(part, nblk, 32, M, 8, w, s);
+        count_launch();
+        TT_LAUNCH_CHECK();
+        ws.reset(mk);
+        return TT_OK;
       }
       const long long ld = col ? es : M;
 #define GV_LAUNCH(MPV, A, C) \
