@@ -189,7 +189,7 @@ __global__ void __launch_bounds__(256, NT >= 40 ? 1 : 2) k_sketch_simt(const flo
     if (more) fetch(j0 + JC);
     const float* as = as_base + b * JC * TI;
     const float* wsm = ws_base + b * JC * NT;
-#pragma unroll 4
+#pragma unroll
     for (int jj = 0; jj < JC; ++jj) {
       const float4 x0 = *reinterpret_cast<const float4*>(&as[jj * TI + ti * RI]);
       const float4 x1 = *reinterpret_cast<const float4*>(&as[jj * TI + ti * RI + 4]);
@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(256, NT >= 64 ? 1 : 2) k_project_simt(const fl
     if (more) fetch(k0 + KC);
     const float* as = as_base + b * KC * TJ;
     const float* qs = qs_base + b * KC * NT;
-#pragma unroll 4
+#pragma unroll
     for (int kk = 0; kk < KC; ++kk) {
       const float4 x0 = *reinterpret_cast<const float4*>(&as[kk * TJ + swz(kk, tj * RJ)]);
       const float4 x1 = *reinterpret_cast<const float4*>(&as[kk * TJ + swz(kk, tj * RJ + 4)]);
@@ -1061,7 +1061,9 @@ static int gram_mp(int M) { return M <= 16 ? 16 : M <= 32 ? 32 : M <= 48 ? 48 : 
 static void gram_plan(long long nvec, int* nblk, long long* vchunk) {
   const int target = 4 * num_sms();
   long long vc = ceil_div_ll(nvec, target);
-  if (vc < 1024) vc = 1024;
+  // at least 64 vectors per block: a few thousand vectors (the last unfoldings' Grams) still
+  // spread over tens of blocks instead of one
+  if (vc < 64) vc = 64;
   vc = ceil_div_ll(vc, 32) * 32;
   *vchunk = vc;
   *nblk = (int)std::max<long long>(1, ceil_div_ll(nvec, vc));
