@@ -1194,6 +1194,120 @@ __global__ void __launch_bounds__(GS_NT, 1) k_gram_sym32(const float* __restrict
   }
 }
 
+// Symmetric variant with FP64 products for 33 <= M <= 48 components (the Grams of B^T and of the
+// power basis Z at sketch widths 33..48), either layout: the upper triangle of TPM x TPM tiles
+// of 8 x 8 (15 tiles at TPM = 5, 21 at 6) times VPW = 32 / tiles vectors per warp, FP64 sums in
+// registers (a 40-wide vector costs 960 FMAs instead of the 3072 of three 32 x 32 warp blocks).
+template <int TPM, bool COL>
+__global__ void __launch_bounds__(GS_NT, 1) k_gram_symt(const float* __restrict__ x, long long nvec, int M,
+                                                       long long ld, long long vchunk, double* __restrict__ part) {
+  constexpr int MP = 8 * TPM;
+  constexpr int NTILE = TPM * (TPM + 1) / 2;
+  constexpr int VPW = 32 / NTILE;
+  constexpr int LDC = GV_VC + 1;
+  extern __shared__ __align__(16) float sm_gt[];
+  const int stage_f = COL ? MP * LDC : GV_VC * M + MP;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const int t = lane % NTILE, u = lane / NTILE;  // u >= VPW: idle lane
+  int p = 0, rem = t;
+  while (rem >= TPM - p) {
+    rem -= TPM - p;
+    ++p;
+  }
+  const int q = p + rem;
+  const long long vb = (long long)blockIdx.x * vchunk;
+  const long long ve = (vb + vchunk < nvec) ? vb + vchunk : nvec;
+  const long long nst = vb < ve ? (ve - vb + GV_VC - 1) / GV_VC : 0;
+  auto load = [&](long long st) {
+    const long long v0 = vb + st * GV_VC;
+    const int nv = (int)((ve - v0 < GV_VC) ? ve - v0 : GV_VC);
+    float* dst = sm_gt + (int)(st % GV_NS) * stage_f;
+    if (COL) {
+      const int tot = nv * M;
+      for (int f = tid; f < tot; f += GS_NT) {
+        const int c = f / nv, v = f - c * nv;
+        cp_async4(dst + c * LDC + v, x + (v0 + v) + (long long)c * ld);
+      }
+    } else {
+      const int n16 = nv * M / 4;
+      const float* src = x + v0 * M;
+      for (int f = tid; f < n16; f += GS_NT) cp_async16(dst + 4 * f, src + 4 * f);
+    }
+  };
+  double accd[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) accd[i][j] = 0.0;
+#pragma unroll
+  for (int st = 0; st < GV_NS - 1; ++st) {
+    if (st < nst) load(st);
+    cp_async_commit();
+  }
+  for (long long it = 0; it < nst; ++it) {
+    cp_async_wait<GV_NS - 2>();
+    __syncthreads();
+    if (it + GV_NS - 1 < nst) load(it + GV_NS - 1);
+    cp_async_commit();
+    const float* buf = sm_gt + (int)(it % GV_NS) * stage_f;
+    const long long v0 = vb + it * GV_VC;
+    const int nv = (int)((ve - v0 < GV_VC) ? ve - v0 : GV_VC);
+    if (u < VPW) {
+      for (int v = VPW * warp + u; v < nv; v += VPW * (GS_NT / 32)) {
+        float av[8], bv[8];
+        if (COL) {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            av[i] = buf[(8 * p + i) * LDC + v];
+            bv[i] = buf[(8 * q + i) * LDC + v];
+          }
+        } else {
+          const float* col = buf + v * M;
+          const float4 a0 = *reinterpret_cast<const float4*>(col + 8 * p);
+          const float4 a1 = *reinterpret_cast<const float4*>(col + 8 * p + 4);
+          const float4 b0 = *reinterpret_cast<const float4*>(col + 8 * q);
+          const float4 b1 = *reinterpret_cast<const float4*>(col + 8 * q + 4);
+          av[0] = a0.x; av[1] = a0.y; av[2] = a0.z; av[3] = a0.w;
+          av[4] = a1.x; av[5] = a1.y; av[6] = a1.z; av[7] = a1.w;
+          bv[0] = b0.x; bv[1] = b0.y; bv[2] = b0.z; bv[3] = b0.w;
+          bv[4] = b1.x; bv[5] = b1.y; bv[6] = b1.z; bv[7] = b1.w;
+        }
+#pragma unroll
+        for (int i = 0; i < 8; ++i)
+#pragma unroll
+          for (int j = 0; j < 8; ++j) accd[i][j] = fma((double)av[i], (double)bv[j], accd[i][j]);
+      }
+    }
+  }
+  cp_async_wait<0>();
+  __syncthreads();  // stage buffers free: the per-lane sums go over them
+  double* red = reinterpret_cast<double*>(sm_gt);  // [thread][GS_LD]
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) red[tid * GS_LD + i * 8 + j] = accd[i][j];
+  __syncthreads();
+  double* dst = part + (long long)blockIdx.x * MP * MP;
+  for (int e = tid; e < NTILE * 64; e += GS_NT) {
+    const int tt = e >> 6, ij = e & 63;
+    double sum = 0.0;
+    for (int w = 0; w < GS_NT / 32; ++w)
+      for (int uu = 0; uu < VPW; ++uu) sum += red[(w * 32 + uu * NTILE + tt) * GS_LD + ij];
+    int pp = 0, rr = tt;
+    while (rr >= TPM - pp) {
+      rr -= TPM - pp;
+      ++pp;
+    }
+    const int qq = pp + rr;
+    dst[(8 * pp + (ij >> 3)) * MP + 8 * qq + (ij & 7)] = sum;
+  }
+}
+
+static size_t gram_symt_smem(int MP, int M, bool col) {
+  const size_t stages = (col ? (size_t)MP * (GV_VC + 1) : (size_t)GV_VC * M + MP) * GV_NS * sizeof(float);
+  return std::max(stages, (size_t)GS_NT * GS_LD * sizeof(double));
+}
+
 // Vector Gram (k_gram_vec): taken for 17 <= M <= 64 and enough vectors to fill the GPU, with
 // x_j = x + j M (M % 4 == 0, 16-byte aligned base) or the column-major layout x[j + c es]
 // (vs = 1, es >= nvec).  Returns the block size MP (0: not taken), the grid and the vectors
@@ -1281,6 +1395,39 @@ int launch_gram(const float* x, long long nvec, int M, long long vs, long long e
         return TT_OK;
       }
       const long long ld = col ? es : M;
+      if (acc64 && M > 32 && M <= 48) {
+        const int MPs = M <= 40 ? 40 : 48;
+        const size_t tshm = gram_symt_smem(MPs, M, col);
+        if (tshm <= (size_t)max_optin_smem()) {
+          static bool tattr = false;
+          if (!tattr) {
+            const int mx = max_optin_smem();
+            cudaFuncSetAttribute(k_gram_symt<5, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+            cudaFuncSetAttribute(k_gram_symt<5, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+            cudaFuncSetAttribute(k_gram_symt<6, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+            cudaFuncSetAttribute(k_gram_symt<6, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+            tattr = true;
+          }
+          if (MPs == 40) {
+            if (col)
+              k_gram_symt<5, true><<<nblk, GS_NT, tshm, s>>>(x, nvec, M, ld, vchunk, part);
+            else
+              k_gram_symt<5, false><<<nblk, GS_NT, tshm, s>>>(x, nvec, M, ld, vchunk, part);
+          } else {
+            if (col)
+              k_gram_symt<6, true><<<nblk, GS_NT, tshm, s>>>(x, nvec, M, ld, vchunk, part);
+            else
+              k_gram_symt<6, false><<<nblk, GS_NT, tshm, s>>>(x, nvec, M, ld, vchunk, part);
+          }
+          count_launch();
+          TT_LAUNCH_CHECK();
+          launch_gram_reduce(part, nblk, MPs, M, 8, w, s);
+          count_launch();
+          TT_LAUNCH_CHECK();
+          ws.reset(mk);
+          return TT_OK;
+        }
+      }
 #define GV_LAUNCH(MPV, A, C) \
   k_gram_vec<MPV, A, C><<<nblk, GramVecShape<MPV>::NT, shm, s>>>(x, nvec, M, ld, vchunk, part)
       if (MPv == 32) {
