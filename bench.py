@@ -510,7 +510,7 @@ def run_ours(args, wl):
     peak, peak_src = peaks()
     key = f"{kinds[top_kind]}:{top_step}"
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-            "traffic": committed_traffic(args.workload, key),
+            "traffic": None if (args.shape or args.ranks) else committed_traffic(args.workload, key),
             "kernel": f"{kinds[top_kind]} pass of unfolding {top_step + 1}", "peak_source": peak_src,
             "algorithmic_bytes_per_launch": top_bytes,
             "avg_launch_ms": top_ms,

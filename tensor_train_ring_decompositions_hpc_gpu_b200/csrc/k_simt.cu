@@ -2071,6 +2071,8 @@ __global__ void __launch_bounds__(256) k_syev_jacobi(const double* __restrict__ 
 // W from itself and the two rotations of its row and column pairs) and V' = V J (each row's
 // 1 x 2 blocks), written straight to the positions the indices take next round (a fixed map
 // `mv`: the round-robin tournament shifts every index but index 0 by one slot per round).
+// W is kept in its upper triangle only (each entry stored once, at its upper position), which
+// halves the scattered stores; a block row is read as one 16-byte load.
 // The last warp computes the next round's rotations meanwhile, from the current blocks and
 // rotations, so a round needs one barrier.  W is symmetrised on input ((W + W^T) / 2), and
 // only the upper blocks are computed (mirrored on store).
@@ -2197,8 +2199,12 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
           if (!(dd >> 16)) {
             const int a = dd & 255, b = (dd >> 8) & 255;
             const double ca = c_[a], sa = s_[a], cbv = c_[b], sb = s_[b];
-            const double w00 = W[(2 * a) * Np + 2 * b], w01 = W[(2 * a) * Np + 2 * b + 1];
-            const double w10 = W[(2 * a + 1) * Np + 2 * b], w11 = W[(2 * a + 1) * Np + 2 * b + 1];
+            // Only the upper triangle (row <= column) of W is kept.  Block (a, b), a < b, lies
+            // wholly above the diagonal; a diagonal block's lower entry is its upper one.
+            const double2 r0v = *reinterpret_cast<const double2*>(&W[(2 * a) * Np + 2 * b]);
+            const double2 r1v = *reinterpret_cast<const double2*>(&W[(2 * a + 1) * Np + 2 * b]);
+            const double w00 = r0v.x, w01 = r0v.y, w11 = r1v.y;
+            const double w10 = (a == b) ? w01 : r1v.x;
             // X = J_a^T B: rows (c, -s), (s, c)
             const double x00 = ca * w00 - sa * w10, x01 = ca * w01 - sa * w11;
             const double x10 = sa * w00 + ca * w10, x11 = sa * w01 + ca * w11;
@@ -2206,22 +2212,18 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
             const double y00 = x00 * cbv - x01 * sb, y01 = x00 * sb + x01 * cbv;
             const double y10 = x10 * cbv - x11 * sb, y11 = x10 * sb + x11 * cbv;
             const int r0 = mv[2 * a], r1 = mv[2 * a + 1], q0 = mv[2 * b], q1 = mv[2 * b + 1];
-            Wn[r0 * Np + q0] = y00;
-            Wn[r0 * Np + q1] = y01;
-            Wn[r1 * Np + q0] = y10;
-            Wn[r1 * Np + q1] = y11;
-            if (a != b) {
-              Wn[q0 * Np + r0] = y00;
-              Wn[q1 * Np + r0] = y01;
-              Wn[q0 * Np + r1] = y10;
-              Wn[q1 * Np + r1] = y11;
-            }
+            // each entry to its upper position (a diagonal block's two off-diagonal entries
+            // are the same entry)
+            Wn[min(r0, q0) * Np + max(r0, q0)] = y00;
+            Wn[min(r0, q1) * Np + max(r0, q1)] = y01;
+            if (a != b) Wn[min(r1, q0) * Np + max(r1, q0)] = y10;
+            Wn[min(r1, q1) * Np + max(r1, q1)] = y11;
           } else {
             const int i = dd & 255, b = (dd >> 8) & 255;
             const double cbv = c_[b], sb = s_[b];
-            const double v0 = V[i * Np + 2 * b], v1 = V[i * Np + 2 * b + 1];
-            Vn[i * Np + mv[2 * b]] = v0 * cbv - v1 * sb;
-            Vn[i * Np + mv[2 * b + 1]] = v0 * sb + v1 * cbv;
+            const double2 vv = *reinterpret_cast<const double2*>(&V[i * Np + 2 * b]);
+            Vn[i * Np + mv[2 * b]] = vv.x * cbv - vv.y * sb;
+            Vn[i * Np + mv[2 * b + 1]] = vv.x * sb + vv.y * cbv;
           }
         }
       } else if (lane < H) {
@@ -2240,12 +2242,15 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
           const double cP = c_[aP], sP = s_[aP], cQ = c_[aQ], sQ = s_[aQ];
           const double tP0 = xP ? sP : cP, tP1 = xP ? cP : -sP;
           const double tQ0 = xQ ? sQ : cQ, tQ1 = xQ ? cQ : -sQ;
-          const double* Bpp = W + (2 * aP) * Np + 2 * aP;
-          const double* Bqq = W + (2 * aQ) * Np + 2 * aQ;
-          const double* Bpq = W + (2 * aP) * Np + 2 * aQ;
-          const double p0 = tP0 * Bpp[0] + tP1 * Bpp[Np], p1 = tP0 * Bpp[1] + tP1 * Bpp[Np + 1];
-          const double q0 = tQ0 * Bqq[0] + tQ1 * Bqq[Np], q1 = tQ0 * Bqq[1] + tQ1 * Bqq[Np + 1];
-          const double m0 = tP0 * Bpq[0] + tP1 * Bpq[Np], m1 = tP0 * Bpq[1] + tP1 * Bpq[Np + 1];
+          // entries through the upper triangle (W is kept there only)
+          auto wu = [&](int r, int c2) { return r <= c2 ? W[r * Np + c2] : W[c2 * Np + r]; };
+          const int P0 = 2 * aP, Q0 = 2 * aQ;
+          const double p0 = tP0 * wu(P0, P0) + tP1 * wu(P0, P0 + 1);
+          const double p1 = tP0 * wu(P0, P0 + 1) + tP1 * wu(P0 + 1, P0 + 1);
+          const double q0 = tQ0 * wu(Q0, Q0) + tQ1 * wu(Q0, Q0 + 1);
+          const double q1 = tQ0 * wu(Q0, Q0 + 1) + tQ1 * wu(Q0 + 1, Q0 + 1);
+          const double m0 = tP0 * wu(P0, Q0) + tP1 * wu(P0 + 1, Q0);
+          const double m1 = tP0 * wu(P0, Q0 + 1) + tP1 * wu(P0 + 1, Q0 + 1);
           const double app = p0 * tP0 + p1 * tP1;
           const double aqq = q0 * tQ0 + q1 * tQ1;
           const double apq = m0 * tQ0 + m1 * tQ1;
