@@ -2105,8 +2105,9 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
   double* Wb1 = Wb0 + NN;
   double* Vb0 = Wb1 + NN;
   double* Vb1 = Vb0 + NN;
-  __shared__ double pc[2][32], ps[2][32];
+  __shared__ double2 pcs[2][32];  // (c, s) of each pair, current and next round
   __shared__ int mv[64], imv[64];
+  __shared__ int2 mv2[32];         // (mv[2k], mv[2k + 1])
   __shared__ double dg[64];
   __shared__ int rk[64];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -2124,8 +2125,10 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
     double v = 0.0;
     if (i < N && j < N) v = 0.5 * (w_in[i + (long long)N * j] + w_in[j + (long long)N * i]);
     Wb0[Pi * Np + Pj] = v;
-    Vb0[i * Np + Pj] = (i == j) ? 1.0 : 0.0;  // V rows: original index; columns: position
+    Vb0[Pj * Np + i] = (i == j) ? 1.0 : 0.0;  // V by (position, original index): V^T
   }
+  __syncthreads();  // mv complete
+  for (int q = tid; q < Np / 2; q += blockDim.x) mv2[q] = make_int2(mv[2 * q], mv[2 * q + 1]);
   double dm = 0.0;
   for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(w_in[i + (long long)N * i]));
   const double inv_s = dm > 0.0 ? 1.0 / dm : 1.0;
@@ -2138,8 +2141,7 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
       const int i0 = k, i1 = Np - 1 - k;  // indices in slots k and Np-1-k at round 0
       if (i0 < N && i1 < N) jacobi_rotation(Wb0[(2 * k) * Np + 2 * k], Wb0[(2 * k + 1) * Np + 2 * k + 1],
                                             Wb0[(2 * k) * Np + 2 * k + 1], inv_s, c, sn);
-      pc[0][k] = c;
-      ps[0][k] = sn;
+      pcs[0][k] = make_double2(c, sn);
     }
   }
   __syncthreads();
@@ -2163,8 +2165,8 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
       }
       dsc[u] = a | ((a + rem) << 8);
     } else {
-      const int e = it - NWB;
-      dsc[u] = (e / H) | ((e % H) << 8) | (1 << 16);
+      const int e = it - NWB;  // V items: index i fastest, so a warp's accesses are contiguous
+      dsc[u] = (e % N) | ((e / N) << 8) | (1 << 16);
     }
   }
   // Param-warp constants: positions (this round) of the indices that form pair `lane` next
@@ -2189,8 +2191,7 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
       double* Wn = cb ? Wb0 : Wb1;
       const double* V = cb ? Vb1 : Vb0;
       double* Vn = cb ? Vb0 : Vb1;
-      const double* c_ = pc[cb];
-      const double* s_ = ps[cb];
+      const double2* cs_ = pcs[cb];
       if (warp != PW) {
 #pragma unroll
         for (int u = 0; u < MAXIT; ++u) {
@@ -2198,7 +2199,8 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
           if (dd < 0) continue;
           if (!(dd >> 16)) {
             const int a = dd & 255, b = (dd >> 8) & 255;
-            const double ca = c_[a], sa = s_[a], cbv = c_[b], sb = s_[b];
+            const double2 csa = cs_[a], csb = cs_[b];
+            const double ca = csa.x, sa = csa.y, cbv = csb.x, sb = csb.y;
             // Only the upper triangle (row <= column) of W is kept.  Block (a, b), a < b, lies
             // wholly above the diagonal; a diagonal block's lower entry is its upper one.
             const double2 r0v = *reinterpret_cast<const double2*>(&W[(2 * a) * Np + 2 * b]);
@@ -2211,7 +2213,8 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
             // X J_b: columns (c, -s)^T, (s, c)^T
             const double y00 = x00 * cbv - x01 * sb, y01 = x00 * sb + x01 * cbv;
             const double y10 = x10 * cbv - x11 * sb, y11 = x10 * sb + x11 * cbv;
-            const int r0 = mv[2 * a], r1 = mv[2 * a + 1], q0 = mv[2 * b], q1 = mv[2 * b + 1];
+            const int2 ma = mv2[a], mb = mv2[b];
+            const int r0 = ma.x, r1 = ma.y, q0 = mb.x, q1 = mb.y;
             // each entry to its upper position (a diagonal block's two off-diagonal entries
             // are the same entry)
             Wn[min(r0, q0) * Np + max(r0, q0)] = y00;
@@ -2220,10 +2223,12 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
             Wn[min(r1, q1) * Np + max(r1, q1)] = y11;
           } else {
             const int i = dd & 255, b = (dd >> 8) & 255;
-            const double cbv = c_[b], sb = s_[b];
-            const double2 vv = *reinterpret_cast<const double2*>(&V[i * Np + 2 * b]);
-            Vn[i * Np + mv[2 * b]] = vv.x * cbv - vv.y * sb;
-            Vn[i * Np + mv[2 * b + 1]] = vv.x * sb + vv.y * cbv;
+            const double2 csb = cs_[b];
+            const double cbv = csb.x, sb = csb.y;
+            const int2 mb = mv2[b];
+            const double v0 = V[(2 * b) * Np + i], v1 = V[(2 * b + 1) * Np + i];
+            Vn[mb.x * Np + i] = v0 * cbv - v1 * sb;
+            Vn[mb.y * Np + i] = v0 * sb + v1 * cbv;
           }
         }
       } else if (lane < H) {
@@ -2239,7 +2244,7 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
         }
         double c = 1.0, sn = 0.0;
         if (live) {
-          const double cP = c_[aP], sP = s_[aP], cQ = c_[aQ], sQ = s_[aQ];
+          const double cP = cs_[aP].x, sP = cs_[aP].y, cQ = cs_[aQ].x, sQ = cs_[aQ].y;
           const double tP0 = xP ? sP : cP, tP1 = xP ? cP : -sP;
           const double tQ0 = xQ ? sQ : cQ, tQ1 = xQ ? cQ : -sQ;
           // entries through the upper triangle (W is kept there only)
@@ -2256,8 +2261,7 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
           const double apq = m0 * tQ0 + m1 * tQ1;
           if (jacobi_rotation(app, aqq, apq, inv_s, c, sn)) rotated = 1;
         }
-        pc[cb ^ 1][lane] = c;
-        ps[cb ^ 1][lane] = sn;
+        pcs[cb ^ 1][lane] = make_double2(c, sn);
       }
       if (rnd + 1 < NR) {
         __syncthreads();
@@ -2300,7 +2304,7 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
   for (int idx = tid; idx < N * N; idx += blockDim.x) {
     const int i = idx % N, a = idx / N;  // eigenvector of index a, component i
     const int P = bl_pos(bl_slot(a, R, NR), Np);
-    evecs[i + (long long)N * rk[a]] = Vf[i * Np + P];
+    evecs[i + (long long)N * rk[a]] = Vf[P * Np + i];
   }
 }
 
