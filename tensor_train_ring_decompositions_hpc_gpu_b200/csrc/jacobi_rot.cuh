@@ -10,15 +10,21 @@ namespace ttr {
 // t^2 + 2 (d / e) t - 1 = 0, formed without the quotient d / e; FP32 suffices for t.
 // c = 1 / sqrt(1 + t^2) to FP64 precision: FP32 estimate, then two Newton steps
 // y <- y (3 - x y^2) / 2, each squaring the relative error.
+// Whether the pair (p, q) is rotated: |a_pq| above 1e-12 of sqrt(a_pp a_qq) and above 1e-14 of
+// the largest diagonal (values scaled by inv_s = 1 / that diagonal).  Eigenvalues then carry
+// (1e-12)^2 relative error, residuals 1e-12 of the norm, and the solve ends about one sweep
+// earlier than with a 1e-14 cut.
+__device__ __forceinline__ bool jacobi_needed(double app, double aqq, double apq, double inv_s) {
+  const double ps = app * inv_s, qs = aqq * inv_s, as = apq * inv_s;
+  return fabs(as) > 1e-14 && as * as > 1e-24 * fabs(ps * qs);
+}
+
 __device__ __forceinline__ bool jacobi_rotation(double app, double aqq, double apq, double inv_s, double& c,
                                                 double& s) {
   const double ps = app * inv_s, qs = aqq * inv_s, as = apq * inv_s;
   c = 1.0;
   s = 0.0;
-  // skip below 1e-12 of sqrt(a_pp a_qq) (and 1e-14 of the largest diagonal): eigenvalues then
-  // carry (1e-12)^2 relative error, residuals 1e-12 of the norm, and the final quiet sweep
-  // comes about one sweep earlier than with a 1e-14 cut
-  if (!(fabs(as) > 1e-14 && as * as > 1e-24 * fabs(ps * qs))) return false;
+  if (!jacobi_needed(app, aqq, apq, inv_s)) return false;
   const float d = (float)(qs - ps), e = 2.0f * (float)as;
   const float h = sqrtf(fmaf(d, d, e * e));
   const float tf = (d >= 0.0f ? e : -e) * __frcp_rn(fabsf(d) + h);

@@ -2080,7 +2080,7 @@ __global__ void __launch_bounds__(256) k_syev_jacobi(const double* __restrict__ 
 // diagonal entry, then c = 1/sqrt(1 + t^2), s = t c in FP64, so every applied rotation is
 // orthogonal to FP64 precision (an inexact t leaves a tiny a_pq for a later sweep).  Pairs
 // with a_pq^2 <= 1e-24 |a_pp a_qq| or |a_pq| <= 1e-14 max|diag| are not rotated
-// (jacobi_rotation); the solve ends after Np - 1 consecutive rounds without a rotation.  Eigenvalues are ordered by a parallel rank count.
+// (jacobi_needed); the solve ends after the first sweep that leaves no pair to rotate.  Eigenvalues are ordered by a parallel rank count.
 // Slot of index i in round-robin round r (slot 0 fixed, slots 1..NR cycle), and its position.
 __device__ __forceinline__ int bl_slot(int i, int r, int NR) {
   if (i == 0) return 0;
@@ -2183,7 +2183,6 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
   int sweep = 0;
   bool converged = false;
   for (; sweep < max_sweeps; ++sweep) {
-    int rotated = 0;
     bool stop = false;
     for (int rnd = 0; rnd < NR; ++rnd, ++R) {
       const int cb = R & 1;
@@ -2259,14 +2258,22 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
           const double app = p0 * tP0 + p1 * tP1;
           const double aqq = q0 * tQ0 + q1 * tQ1;
           const double apq = m0 * tQ0 + m1 * tQ1;
-          if (jacobi_rotation(app, aqq, apq, inv_s, c, sn)) rotated = 1;
+          jacobi_rotation(app, aqq, apq, inv_s, c, sn);
         }
         pcs[cb ^ 1][lane] = make_double2(c, sn);
       }
       if (rnd + 1 < NR) {
         __syncthreads();
-      } else if (!__syncthreads_or(rotated)) {
-        stop = true;
+      } else {
+        // End of a sweep: stop when no pair of the updated matrix would be rotated (the
+        // following sweep would change nothing), which saves that quiet sweep.
+        __syncthreads();
+        int need = 0;
+        for (int idx = tid; idx < NN; idx += blockDim.x) {
+          const int P = idx / Np, Q = idx - (idx / Np) * Np;
+          if (P < Q && jacobi_needed(Wn[P * Np + P], Wn[Q * Np + Q], Wn[P * Np + Q], inv_s)) need = 1;
+        }
+        if (!__syncthreads_or(need)) stop = true;
       }
     }
     if (stop) {
