@@ -129,7 +129,8 @@ __device__ void cta_gram(const float* __restrict__ base, long long ps, long long
 // Eigen-decomposition of the symmetric W (N x N row-major, N <= BSMALL) by cyclic Jacobi with
 // the round-robin pairing, all rotations of a round applied together as W' = J^T W J, V' = V J
 // (double-buffered).  Output: evals[N] descending, evecs (N x N column-major, stride N).
-// Returns the sweep count (max_sweeps + 1 when not converged).
+// The solve ends after the first sweep that leaves no pair to rotate.  Returns the sweep count
+// (max_sweeps + 1 when not converged).
 __device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, double* evecs, int max_sweeps,
                           double* red) {
   const int tid = threadIdx.x;
@@ -151,10 +152,18 @@ __device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, do
   for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(W[i * N + i]));
   const double inv_s = dm > 0.0 ? 1.0 / dm : 1.0;
   __syncthreads();
+  // this thread's entries (NN <= 1024 = JU * BT), row and column fixed for the whole solve
+  constexpr int JU = (BSMALL * BSMALL + BT - 1) / BT;
+  int ji[JU], jj[JU];
+#pragma unroll
+  for (int u = 0; u < JU; ++u) {
+    const int idx = tid + u * BT;
+    ji[u] = idx / Np;
+    jj[u] = idx - ji[u] * Np;
+  }
   int cur = 0, sweep = 0;
   bool conv = false;
   for (; sweep < max_sweeps; ++sweep) {
-    int rot = 0;
     for (int rnd = 0; rnd < NR; ++rnd) {
       const double* Wc = Wb[cur];
       if (tid < Np / 2) {
@@ -167,7 +176,7 @@ __device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, do
           q = tt;
         }
         double c = 1.0, s = 0.0;
-        if (q < N && jacobi_rotation(Wc[p * Np + p], Wc[q * Np + q], Wc[p * Np + q], inv_s, c, s)) rot = 1;
+        if (q < N) jacobi_rotation(Wc[p * Np + p], Wc[q * Np + q], Wc[p * Np + q], inv_s, c, s);
         cs[k] = c;
         sn[k] = s;
         pr[p] = q;
@@ -181,8 +190,11 @@ __device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, do
       double* Wn = Wb[cur ^ 1];
       const double* Vc = Vb[cur];
       double* Vn = Vb[cur ^ 1];
-      for (int idx = tid; idx < NN; idx += BT) {
-        const int i = idx / Np, j = idx - (idx / Np) * Np;
+#pragma unroll
+      for (int u = 0; u < JU; ++u) {
+        const int idx = tid + u * BT;
+        if (idx >= NN) break;
+        const int i = ji[u], j = jj[u];
         const int pi = pr[i], pj = pr[j];
         const double ci = cs[pr[Np + i]], si = sn[pr[Np + i]];
         const double cj = cs[pr[Np + j]], sj = sn[pr[Np + j]];
@@ -193,7 +205,16 @@ __device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, do
       __syncthreads();
       cur ^= 1;
     }
-    if (!__syncthreads_or(rot)) {
+    // stop when no pair of the updated matrix would be rotated (saves the quiet sweep)
+    int need = 0;
+    {
+      const double* Wc = Wb[cur];
+      for (int idx = tid; idx < NN; idx += BT) {
+        const int i = idx / Np, j = idx - (idx / Np) * Np;
+        if (i < j && jacobi_needed(Wc[i * Np + i], Wc[j * Np + j], Wc[i * Np + j], inv_s)) need = 1;
+      }
+    }
+    if (!__syncthreads_or(need)) {
       conv = true;
       ++sweep;
       break;
