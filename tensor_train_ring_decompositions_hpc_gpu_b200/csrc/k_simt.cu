@@ -33,6 +33,23 @@ static int max_optin_smem();
 __global__ void k_gaussian(float* __restrict__ out, long long rows, long long total, long long ld,
                            unsigned long long seed, unsigned stream_id) {
   const long long ncall = (total + 3) / 4;
+  if (ld == rows) {
+    // contiguous matrix: element e sits at out[e]; whole float4 stores when aligned
+    const bool v4 = (total & 3) == 0 && (reinterpret_cast<uintptr_t>(out) & 15) == 0;
+    for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncall;
+         c += (long long)gridDim.x * blockDim.x) {
+      const float4 gv = philox_normal4((unsigned long long)c, stream_id, seed);
+      if (v4) {
+        reinterpret_cast<float4*>(out)[c] = gv;
+      } else {
+        const float g[4] = {gv.x, gv.y, gv.z, gv.w};
+#pragma unroll
+        for (int l = 0; l < 4; ++l)
+          if (4 * c + l < total) out[4 * c + l] = g[l];
+      }
+    }
+    return;
+  }
   for (long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x; c < ncall;
        c += (long long)gridDim.x * blockDim.x) {
     const float4 gv = philox_normal4((unsigned long long)c, stream_id, seed);
@@ -515,6 +532,10 @@ __global__ void __launch_bounds__(256) k_proj_smallk(const float* __restrict__ a
   // Row-major outputs with ldo == N form one contiguous block per tile; bond-permuted outputs
   // (r0, r1, n) -> (r1, n, r0) form r0 contiguous runs of r1 * nj values per tile.
   const bool staged_out = (mode == OUT_ROWMAJOR && ldo == N) || (mode == OUT_PERM231 && r0 * r1 == N);
+  // Quotients of tile-local indices (< 2^15) by m, N or r1 (<= 128) through a float reciprocal:
+  // the rounding error is far below the 0.5 / divisor margin, so the floor is exact.
+  const float inv_m = 1.0f / (float)m, inv_n = 1.0f / (float)N, inv_r1 = 1.0f / (float)(r1 > 0 ? r1 : 1);
+  auto qdiv = [](int e, float inv) { return (int)(((float)e + 0.5f) * inv); };
   for (long long tile = blockIdx.x; tile * TJ < n; tile += gridDim.x) {
     const long long j0 = tile * TJ;
     const int nj = (int)((n - j0 < TJ) ? n - j0 : TJ);
@@ -524,7 +545,7 @@ __global__ void __launch_bounds__(256) k_proj_smallk(const float* __restrict__ a
     if (vec) {
       for (int f4 = tid; f4 < (cnt >> 2); f4 += 256) {
         const float4 v = __ldg(reinterpret_cast<const float4*>(src) + f4);
-        const int e = 4 * f4, col = e / m, k = e - col * m;
+        const int e = 4 * f4, col = qdiv(e, inv_m), k = e - col * m;
         float* d = Xs + col * S + k;
         d[0] = v.x;
         d[1] = v.y;
@@ -533,7 +554,7 @@ __global__ void __launch_bounds__(256) k_proj_smallk(const float* __restrict__ a
       }
     } else {
       for (int f = tid; f < cnt; f += 256) {
-        const int col = f / m, k = f - col * m;
+        const int col = qdiv(f, inv_m), k = f - col * m;
         Xs[col * S + k] = __ldg(src + f);
       }
     }
@@ -567,7 +588,7 @@ __global__ void __launch_bounds__(256) k_proj_smallk(const float* __restrict__ a
       if (mode == OUT_ROWMAJOR) {
         float* dst = out + j0 * N;
         for (int f = tid; f < nj * N; f += 256) {
-          const int col = f / N, c = f - col * N;
+          const int col = qdiv(f, inv_n), c = f - col * N;
           dst[f] = Xs[col * OS + c];
         }
       } else {
@@ -575,7 +596,7 @@ __global__ void __launch_bounds__(256) k_proj_smallk(const float* __restrict__ a
         for (int ai = 0; ai < r0; ++ai) {
           float* dst = out + (long long)r1 * (j0 + n * (long long)ai);
           for (int f = tid; f < run; f += 256) {
-            const int col = f / r1, bi = f - col * r1;
+            const int col = qdiv(f, inv_r1), bi = f - col * r1;
             dst[f] = Xs[col * OS + ai + r0 * bi];
           }
         }
