@@ -128,7 +128,8 @@ __device__ void cta_gram(const float* __restrict__ base, long long ps, long long
 
 // Eigen-decomposition of the symmetric W (N x N row-major, N <= BSMALL) by cyclic Jacobi with
 // the round-robin pairing, all rotations of a round applied together as W' = J^T W J, V' = V J
-// (double-buffered).  Output: evals[N] descending, evecs (N x N column-major, stride N).
+// (double-buffered), the next round's rotations computed meanwhile by the last warp.  Output:
+// evals[N] descending, evecs (N x N column-major, stride N).
 // The solve ends after the first sweep that leaves no pair to rotate.  Returns the sweep count
 // (max_sweeps + 1 when not converged).
 __device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, double* evecs, int max_sweeps,
@@ -140,9 +141,9 @@ __device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, do
   const int NN = Np * Np;
   double* Wb[2] = {jac, jac + NN};
   double* Vb[2] = {jac + 2 * NN, jac + 3 * NN};
-  double* cs = red;             // Np/2
-  double* sn = red + 32;        // Np/2
-  int* pr = reinterpret_cast<int*>(red + 64);  // partner, pair, first (3 x Np)
+  // per round parity b: cosines red[32 b ..], sines red[64 + 32 b ..], and as ints from red + 128:
+  // partner, pair, first flag (3 x Np each parity)
+  int* prb = reinterpret_cast<int*>(red + 128);
   for (int idx = tid; idx < NN; idx += BT) {
     const int i = idx / Np, j = idx - (idx / Np) * Np;
     Wb[0][idx] = (i < N && j < N) ? W[i * N + j] : 0.0;
@@ -151,56 +152,95 @@ __device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, do
   double dm = 0.0;
   for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(W[i * N + i]));
   const double inv_s = dm > 0.0 ? 1.0 / dm : 1.0;
+  // The last warp computes the rotations of the next round while the others apply the current
+  // one (one barrier per round); it takes the three entries of J^T W J it needs from the
+  // current W and the current rotations.
+  constexpr int PWARP = BT / 32 - 1;
+  const bool pthread = (tid >> 5) == PWARP;
+  const int k = tid & 31;  // pair computed by a lane of the parameter warp
+  auto pair_of = [&](int rnd, int& p, int& q) {
+    const int x = k, y = Np - 1 - k;
+    p = x == 0 ? 0 : 1 + (x - 1 + rnd) % NR;
+    q = y == 0 ? 0 : 1 + (y - 1 + rnd) % NR;
+    if (p > q) {
+      const int tt = p;
+      p = q;
+      q = tt;
+    }
+  };
+  auto publish = [&](int b, int p, int q, double c, double sn) {
+    red[32 * b + k] = c;
+    red[64 + 32 * b + k] = sn;
+    int* pr = prb + 3 * Np * b;
+    pr[p] = q;
+    pr[q] = p;
+    pr[Np + p] = k;
+    pr[Np + q] = k;
+    pr[2 * Np + p] = 1;
+    pr[2 * Np + q] = 0;
+  };
   __syncthreads();
-  // this thread's entries (NN <= 1024 = JU * BT), row and column fixed for the whole solve
-  constexpr int JU = (BSMALL * BSMALL + BT - 1) / BT;
+  if (pthread && k < Np / 2) {  // rotations of round 0 straight from W
+    int p, q;
+    pair_of(0, p, q);
+    double c = 1.0, sn = 0.0;
+    if (q < N) jacobi_rotation(Wb[0][p * Np + p], Wb[0][q * Np + q], Wb[0][p * Np + q], inv_s, c, sn);
+    publish(0, p, q, c, sn);
+  }
+  // this thread's entries (the parameter warp takes none), fixed for the whole solve
+  constexpr int NU = BT - 32;
+  constexpr int JU = (BSMALL * BSMALL + NU - 1) / NU;
   int ji[JU], jj[JU];
 #pragma unroll
   for (int u = 0; u < JU; ++u) {
-    const int idx = tid + u * BT;
+    const int idx = tid + u * NU;
     ji[u] = idx / Np;
     jj[u] = idx - ji[u] * Np;
   }
-  int cur = 0, sweep = 0;
+  __syncthreads();
+  int cur = 0, sweep = 0, R = 0;
   bool conv = false;
   for (; sweep < max_sweeps; ++sweep) {
-    for (int rnd = 0; rnd < NR; ++rnd) {
+    for (int rnd = 0; rnd < NR; ++rnd, ++R) {
+      const int b = R & 1;
       const double* Wc = Wb[cur];
-      if (tid < Np / 2) {
-        const int k = tid, x = k, y = Np - 1 - k;
-        int p = x == 0 ? 0 : 1 + (x - 1 + rnd) % NR;
-        int q = y == 0 ? 0 : 1 + (y - 1 + rnd) % NR;
-        if (p > q) {
-          const int tt = p;
-          p = q;
-          q = tt;
-        }
-        double c = 1.0, s = 0.0;
-        if (q < N) jacobi_rotation(Wc[p * Np + p], Wc[q * Np + q], Wc[p * Np + q], inv_s, c, s);
-        cs[k] = c;
-        sn[k] = s;
-        pr[p] = q;
-        pr[q] = p;
-        pr[Np + p] = k;
-        pr[Np + q] = k;
-        pr[2 * Np + p] = 1;
-        pr[2 * Np + q] = 0;
-      }
-      __syncthreads();
-      double* Wn = Wb[cur ^ 1];
-      const double* Vc = Vb[cur];
-      double* Vn = Vb[cur ^ 1];
+      const double* cs = red + 32 * b;
+      const double* sn = red + 64 + 32 * b;
+      const int* pr = prb + 3 * Np * b;
+      if (!pthread) {
+        double* Wn = Wb[cur ^ 1];
+        const double* Vc = Vb[cur];
+        double* Vn = Vb[cur ^ 1];
 #pragma unroll
-      for (int u = 0; u < JU; ++u) {
-        const int idx = tid + u * BT;
-        if (idx >= NN) break;
-        const int i = ji[u], j = jj[u];
-        const int pi = pr[i], pj = pr[j];
-        const double ci = cs[pr[Np + i]], si = sn[pr[Np + i]];
-        const double cj = cs[pr[Np + j]], sj = sn[pr[Np + j]];
-        const double jpi = pr[2 * Np + i] ? -si : si, jpj = pr[2 * Np + j] ? -sj : sj;
-        Wn[idx] = ci * (Wc[i * Np + j] * cj + Wc[i * Np + pj] * jpj) + jpi * (Wc[pi * Np + j] * cj + Wc[pi * Np + pj] * jpj);
-        Vn[idx] = Vc[i * Np + j] * cj + Vc[i * Np + pj] * jpj;
+        for (int u = 0; u < JU; ++u) {
+          const int idx = tid + u * NU;
+          if (idx >= NN) break;
+          const int i = ji[u], j = jj[u];
+          const int pi = pr[i], pj = pr[j];
+          const double ci = cs[pr[Np + i]], si = sn[pr[Np + i]];
+          const double cj = cs[pr[Np + j]], sj = sn[pr[Np + j]];
+          const double jpi = pr[2 * Np + i] ? -si : si, jpj = pr[2 * Np + j] ? -sj : sj;
+          Wn[idx] = ci * (Wc[i * Np + j] * cj + Wc[i * Np + pj] * jpj) +
+                    jpi * (Wc[pi * Np + j] * cj + Wc[pi * Np + pj] * jpj);
+          Vn[idx] = Vc[i * Np + j] * cj + Vc[i * Np + pj] * jpj;
+        }
+      } else if (k < Np / 2) {
+        // next round's pair (p, q) and the entries (p, p), (q, q), (p, q) of J^T W J
+        int p, q;
+        pair_of(rnd + 1 == NR ? 0 : rnd + 1, p, q);
+        double c = 1.0, s2 = 0.0;
+        if (q < N) {
+          auto wj = [&](int a, int bb) {
+            const int pa = pr[a], pb = pr[bb];
+            const double ca = cs[pr[Np + a]], sa = sn[pr[Np + a]];
+            const double cb2 = cs[pr[Np + bb]], sb = sn[pr[Np + bb]];
+            const double ja = pr[2 * Np + a] ? -sa : sa, jb = pr[2 * Np + bb] ? -sb : sb;
+            return ca * (Wc[a * Np + bb] * cb2 + Wc[a * Np + pb] * jb) +
+                   ja * (Wc[pa * Np + bb] * cb2 + Wc[pa * Np + pb] * jb);
+          };
+          jacobi_rotation(wj(p, p), wj(q, q), wj(p, q), inv_s, c, s2);
+        }
+        publish(b ^ 1, p, q, c, s2);
       }
       __syncthreads();
       cur ^= 1;
@@ -220,6 +260,7 @@ __device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, do
       break;
     }
   }
+  int* pr = prb;
   const double* Wf = Wb[cur];
   const double* Vf = Vb[cur];
   int* rk = pr;  // reuse
