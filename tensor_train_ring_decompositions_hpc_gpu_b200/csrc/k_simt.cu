@@ -1811,16 +1811,17 @@ __global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, in
       }
 #pragma unroll
       for (int c = 0; c < NP; ++c) {
-        float a = q[c];
+        // four independent partial sums (one per float4 lane) shorten the dependency chain
+        float a0 = q[c], a1 = 0.f, a2 = 0.f, a3 = 0.f;
 #pragma unroll
         for (int k4 = 0; k4 < (c + 3) / 4; ++k4) {
           const float4 rr = *reinterpret_cast<const float4*>(&Rf[c * NP + 4 * k4]);
-          a = fmaf(-q[4 * k4], rr.x, a);
-          a = fmaf(-q[4 * k4 + 1], rr.y, a);
-          a = fmaf(-q[4 * k4 + 2], rr.z, a);
-          a = fmaf(-q[4 * k4 + 3], rr.w, a);
+          a0 = fmaf(-q[4 * k4], rr.x, a0);
+          a1 = fmaf(-q[4 * k4 + 1], rr.y, a1);
+          a2 = fmaf(-q[4 * k4 + 2], rr.z, a2);
+          a3 = fmaf(-q[4 * k4 + 3], rr.w, a3);
         }
-        q[c] = a * invd[c];
+        q[c] = ((a0 + a1) + (a2 + a3)) * invd[c];
       }
       if (pass == 0) {
 #pragma unroll
