@@ -980,8 +980,11 @@ __global__ void __launch_bounds__(GramVecShape<MP>::NT, 1) k_gram_vec(const floa
     float* dst = sm_gv + (int)(st % GV_NS) * stage_f;
     if (COL) {
       const int tot = nv * M;
+      // f / nv with f < 64 * 192 through a float reciprocal (exact: the error is far below the
+      // 0.5 / nv margin)
+      const float inv_nv = 1.0f / (float)nv;
       for (int f = tid; f < tot; f += S::NT) {
-        const int c = f / nv, v = f - c * nv;
+        const int c = (int)(((float)f + 0.5f) * inv_nv), v = f - c * nv;
         cp_async4(dst + c * LDC + v, x + (v0 + v) + (long long)c * ld);
       }
     } else {
@@ -1245,8 +1248,9 @@ __global__ void __launch_bounds__(GS_NT, 1) k_gram_symt(const float* __restrict_
     float* dst = sm_gt + (int)(st % GV_NS) * stage_f;
     if (COL) {
       const int tot = nv * M;
+      const float inv_nv = 1.0f / (float)nv;  // exact quotient as in k_gram_vec
       for (int f = tid; f < tot; f += GS_NT) {
-        const int c = f / nv, v = f - c * nv;
+        const int c = (int)(((float)f + 0.5f) * inv_nv), v = f - c * nv;
         cp_async4(dst + c * LDC + v, x + (v0 + v) + (long long)c * ld);
       }
     } else {
