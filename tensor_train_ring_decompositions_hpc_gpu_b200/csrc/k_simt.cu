@@ -916,8 +916,8 @@ static void launch_gram_reduce(const double* part, int nblk, int MP, int M, int 
 //    long unfolding with few rows (columns contiguous) and of a row-major factor B^T.  A stage
 //    of VC vectors is one contiguous block, copied with 16-byte cp.async;
 //  * column-major (COL = true): component c of x_j at x[j + c ld] -- a tall n x M matrix (the
-//    power-iteration basis Z).  Each component's VC values are copied with coalesced 4-byte
-//    cp.async into a row of stride VC + 1 (conflict-free column reads).
+//    power-iteration basis Z).  Each component's VC values are copied with 16-byte cp.async
+//    into a row of the stage, chunks swizzled for conflict-free column reads (gv_col_at).
 // Stages are NS deep.  Each warp computes a 32 x 32 block of W: lane (p, q) = (lane / 8,
 // lane % 8) holds rows 8p..8p+7 x columns 4q..4q+3, 12 loaded values per vector for 32 FMAs.
 // MP = 32 has one such block (12 warps split the vectors), MP = 64 the three upper blocks
@@ -944,6 +944,40 @@ constexpr int GV_VC = 192;  // vectors per stage
 constexpr int GV_NS = 4;    // stages in flight
 constexpr int GV_VFLUSH = 64;
 
+// Column-major stages: component c's values of the stage's vectors occupy row c (stride
+// GV_VC floats) with 4-vector chunks XOR-swizzled by the key (c >> 2) & 7, so the 16-byte copies
+// stay aligned and the reads of the rows 8p + i (i fixed) and 4q + j (j fixed) of one vector hit
+// distinct banks.  Element (c, v) of the stage sits at gv_col_at(c, v).
+__device__ __forceinline__ int gv_col_key(int c) { return ((c >> 2) & 7) << 2; }
+__device__ __forceinline__ int gv_col_at(int c, int v) { return c * GV_VC + (v ^ gv_col_key(c)); }
+
+// Copy vectors [v0, v0 + nv) of the column-major n x M matrix x (column stride ld) into a
+// column-major stage: 16-byte copies of 4 vectors when the layout allows them, 4-byte ones
+// otherwise.
+template <int NT>
+__device__ __forceinline__ void gv_load_col(float* dst, const float* __restrict__ x, long long v0, int nv, int M,
+                                            long long ld, int tid) {
+  const bool v16 = ((ld & 3) == 0) && ((v0 & 3) == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+  const int n4 = v16 ? nv >> 2 : 0;  // whole 4-vector chunks per component
+  if (n4 > 0) {
+    const int tot = n4 * M;
+    const float inv = 1.0f / (float)n4;  // exact quotients: c < 64, far inside the 0.5 / n4 margin
+    for (int f = tid; f < tot; f += NT) {
+      const int c = (int)(((float)f + 0.5f) * inv), g = f - c * n4;
+      cp_async16(dst + gv_col_at(c, 4 * g), x + (v0 + 4 * g) + (long long)c * ld);
+    }
+  }
+  const int rest = nv - 4 * n4;  // remaining vectors, 4-byte copies
+  if (rest > 0) {
+    const int tot = rest * M;
+    const float inv = 1.0f / (float)rest;
+    for (int f = tid; f < tot; f += NT) {
+      const int c = (int)(((float)f + 0.5f) * inv), v = 4 * n4 + (f - c * rest);
+      cp_async4(dst + gv_col_at(c, v), x + (v0 + v) + (long long)c * ld);
+    }
+  }
+}
+
 template <int MP>
 struct GramVecShape {
   static constexpr int WB = MP == 32 ? 1 : 3;    // 32 x 32 warp blocks (upper triangle)
@@ -952,7 +986,7 @@ struct GramVecShape {
 };
 
 static size_t gram_vec_smem(int MP, int M, bool col) {
-  const size_t stage = col ? (size_t)MP * (GV_VC + 1) : (size_t)GV_VC * M + MP;
+  const size_t stage = col ? (size_t)MP * GV_VC : (size_t)GV_VC * M + MP;
   const size_t red = (size_t)12 * 1024 * 2;  // per-warp 32 x 32 FP64 blocks, in floats
   return std::max(stage * GV_NS, red) * sizeof(float);
 }
@@ -963,9 +997,8 @@ __global__ void __launch_bounds__(GramVecShape<MP>::NT, 1) k_gram_vec(const floa
                                                                     double* __restrict__ part) {
   using S = GramVecShape<MP>;
   extern __shared__ __align__(16) float sm_gv[];
-  constexpr int LDC = GV_VC + 1;  // COL: row stride of a component
   // floats per stage buffer: COL, MP component rows; otherwise VC vectors + MP words of slack
-  const int stage_f = COL ? MP * LDC : GV_VC * M + MP;
+  const int stage_f = COL ? MP * GV_VC : GV_VC * M + MP;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wb = warp % S::WB, ph = warp / S::WB;
   const int r0 = (wb == 2 ? 32 : 0) + 8 * (lane >> 3);
@@ -979,14 +1012,7 @@ __global__ void __launch_bounds__(GramVecShape<MP>::NT, 1) k_gram_vec(const floa
     const int nv = (int)((ve - v0 < GV_VC) ? ve - v0 : GV_VC);
     float* dst = sm_gv + (int)(st % GV_NS) * stage_f;
     if (COL) {
-      const int tot = nv * M;
-      // f / nv with f < 64 * 192 through a float reciprocal (exact: the error is far below the
-      // 0.5 / nv margin)
-      const float inv_nv = 1.0f / (float)nv;
-      for (int f = tid; f < tot; f += S::NT) {
-        const int c = (int)(((float)f + 0.5f) * inv_nv), v = f - c * nv;
-        cp_async4(dst + c * LDC + v, x + (v0 + v) + (long long)c * ld);
-      }
+      gv_load_col<S::NT>(dst, x, v0, nv, M, ld, tid);
     } else {
       const int n16 = nv * M / 4;
       const float* src = x + v0 * M;
@@ -1021,9 +1047,9 @@ __global__ void __launch_bounds__(GramVecShape<MP>::NT, 1) k_gram_vec(const floa
       float av[8], bv[4];
       if (COL) {
 #pragma unroll
-        for (int i = 0; i < 8; ++i) av[i] = buf[(r0 + i) * LDC + v];
+        for (int i = 0; i < 8; ++i) av[i] = buf[gv_col_at(r0 + i, v)];
 #pragma unroll
-        for (int j = 0; j < 4; ++j) bv[j] = buf[(c0 + j) * LDC + v];
+        for (int j = 0; j < 4; ++j) bv[j] = buf[gv_col_at(c0 + j, v)];
       } else {
         const float* col = buf + v * M;
         const float4 a0 = *reinterpret_cast<const float4*>(col + r0);
@@ -1228,9 +1254,8 @@ __global__ void __launch_bounds__(GS_NT, 1) k_gram_symt(const float* __restrict_
   constexpr int MP = 8 * TPM;
   constexpr int NTILE = TPM * (TPM + 1) / 2;
   constexpr int VPW = 32 / NTILE;
-  constexpr int LDC = GV_VC + 1;
   extern __shared__ __align__(16) float sm_gt[];
-  const int stage_f = COL ? MP * LDC : GV_VC * M + MP;
+  const int stage_f = COL ? MP * GV_VC : GV_VC * M + MP;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int t = lane % NTILE, u = lane / NTILE;  // u >= VPW: idle lane
   int p = 0, rem = t;
@@ -1247,12 +1272,7 @@ __global__ void __launch_bounds__(GS_NT, 1) k_gram_symt(const float* __restrict_
     const int nv = (int)((ve - v0 < GV_VC) ? ve - v0 : GV_VC);
     float* dst = sm_gt + (int)(st % GV_NS) * stage_f;
     if (COL) {
-      const int tot = nv * M;
-      const float inv_nv = 1.0f / (float)nv;  // exact quotient as in k_gram_vec
-      for (int f = tid; f < tot; f += GS_NT) {
-        const int c = (int)(((float)f + 0.5f) * inv_nv), v = f - c * nv;
-        cp_async4(dst + c * LDC + v, x + (v0 + v) + (long long)c * ld);
-      }
+      gv_load_col<GS_NT>(dst, x, v0, nv, M, ld, tid);
     } else {
       const int n16 = nv * M / 4;
       const float* src = x + v0 * M;
@@ -1283,8 +1303,8 @@ __global__ void __launch_bounds__(GS_NT, 1) k_gram_symt(const float* __restrict_
         if (COL) {
 #pragma unroll
           for (int i = 0; i < 8; ++i) {
-            av[i] = buf[(8 * p + i) * LDC + v];
-            bv[i] = buf[(8 * q + i) * LDC + v];
+            av[i] = buf[gv_col_at(8 * p + i, v)];
+            bv[i] = buf[gv_col_at(8 * q + i, v)];
           }
         } else {
           const float* col = buf + v * M;
@@ -1329,7 +1349,7 @@ __global__ void __launch_bounds__(GS_NT, 1) k_gram_symt(const float* __restrict_
 }
 
 static size_t gram_symt_smem(int MP, int M, bool col) {
-  const size_t stages = (col ? (size_t)MP * (GV_VC + 1) : (size_t)GV_VC * M + MP) * GV_NS * sizeof(float);
+  const size_t stages = (col ? (size_t)MP * GV_VC : (size_t)GV_VC * M + MP) * GV_NS * sizeof(float);
   return std::max(stages, (size_t)GS_NT * GS_LD * sizeof(double));
 }
 
@@ -1617,6 +1637,8 @@ __global__ void __launch_bounds__(128) k_apply_rinv(float* __restrict__ y, long 
   constexpr int CB = (NP % 32 == 0) ? 32 : 16;
   static_assert(NP % CB == 0, "chunk width must divide the padded width");
   const long long ntile = (n + 127) / 128;
+  // column-major rows read / written as 16-byte runs of 4 rows
+  const bool v4 = vs == 1 && es != 1 && (es & 3) == 0 && ((reinterpret_cast<uintptr_t>(y) & 15) == 0);
   for (long long tile = blockIdx.x; tile < ntile; tile += gridDim.x) {
     const long long j0 = tile * 128;
     __syncthreads();  // ts ready / the previous tile's stores done
@@ -1625,6 +1647,27 @@ __global__ void __launch_bounds__(128) k_apply_rinv(float* __restrict__ y, long 
         const int c = f % NP, r = f / NP;
         const long long j = j0 + r;
         ys[r * LD + c] = (j < n && c < N) ? y[j * vs + c] : 0.f;
+      }
+    } else if (v4) {
+      // 4 consecutive rows of a column per 16-byte load; a warp covers 8 row groups x 4 columns
+      for (int f = tid; f < 32 * NP; f += 128) {
+        const int r4 = (f & 7) + 8 * ((f >> 5) & 3), c = ((f >> 3) & 3) + 4 * (f >> 7);
+        const long long j = j0 + 4 * r4;
+        float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (c < N) {
+          if (j + 3 < n) {
+            v = *reinterpret_cast<const float4*>(y + j + (long long)c * es);
+          } else {
+            const float* src = y + (long long)c * es;
+            if (j < n) v.x = src[j];
+            if (j + 1 < n) v.y = src[j + 1];
+            if (j + 2 < n) v.z = src[j + 2];
+          }
+        }
+        ys[(4 * r4) * LD + c] = v.x;
+        ys[(4 * r4 + 1) * LD + c] = v.y;
+        ys[(4 * r4 + 2) * LD + c] = v.z;
+        ys[(4 * r4 + 3) * LD + c] = v.w;
       }
     } else {
       for (int f = tid; f < 128 * NP; f += 128) {
@@ -1654,6 +1697,22 @@ __global__ void __launch_bounds__(128) k_apply_rinv(float* __restrict__ y, long 
         const int c = f % NP, r = f / NP;
         const long long j = j0 + r;
         if (j < n && c < N) y[j * vs + c] = ys[r * LD + c];
+      }
+    } else if (v4) {
+      for (int f = tid; f < 32 * NP; f += 128) {
+        const int r4 = (f & 7) + 8 * ((f >> 5) & 3), c = ((f >> 3) & 3) + 4 * (f >> 7);
+        const long long j = j0 + 4 * r4;
+        if (c >= N || j >= n) continue;
+        const float4 v = make_float4(ys[(4 * r4) * LD + c], ys[(4 * r4 + 1) * LD + c], ys[(4 * r4 + 2) * LD + c],
+                                     ys[(4 * r4 + 3) * LD + c]);
+        float* dst = y + (long long)c * es;
+        if (j + 3 < n) {
+          *reinterpret_cast<float4*>(dst + j) = v;
+        } else {
+          dst[j] = v.x;
+          if (j + 1 < n) dst[j + 1] = v.y;
+          if (j + 2 < n) dst[j + 2] = v.z;
+        }
       }
     } else {
       for (int f = tid; f < 128 * NP; f += 128) {
