@@ -1119,25 +1119,26 @@ static void gram_plan(long long nvec, int* nblk, long long* vchunk) {
   *nblk = (int)std::max<long long>(1, ceil_div_ll(nvec, vc));
 }
 
-// Symmetric variant for contiguous vectors with 17 <= M <= 32 (the exact step's Gram of a long
-// unfolding with few rows): the upper triangle of 8 x 8 tiles of the 32 x 32 result (10 tiles)
+// Symmetric variant for 17 <= M <= 32 components, either layout (the exact step's Gram of a long
+// unfolding with few rows; the power basis Z at widths up to 32): the upper triangle of 8 x 8
+// tiles of the 32 x 32 result (10 tiles)
 // times 3 vectors is 30 lanes of a warp, so a vector costs 640 FMAs instead of 1024 and a lane
 // loads 16 values per 64 FMAs.  8 warps of 3 vectors take 24 vectors per step of a stage.
 // FP32 products: the per-lane FP64 sums live in shared memory (row stride 65 doubles) next to
 // the stages, which keeps the registers to the FP32 tile; FP64 products: in registers.
 constexpr int GS_NT = 256;
 constexpr int GS_LD = 65;
-static size_t gram_sym_smem(int M, bool acc64) {
-  const size_t stages = ((size_t)GV_VC * M + 32) * GV_NS * sizeof(float);
+static size_t gram_sym_smem(int M, bool acc64, bool col) {
+  const size_t stages = (col ? (size_t)32 * GV_VC : (size_t)GV_VC * M + 32) * GV_NS * sizeof(float);
   const size_t red = (size_t)GS_NT * GS_LD * sizeof(double);
   return acc64 ? std::max(stages, red) : stages + red;
 }
 
-template <bool ACC64>
+template <bool ACC64, bool COL>
 __global__ void __launch_bounds__(GS_NT, 1) k_gram_sym32(const float* __restrict__ x, long long nvec, int M,
-                                                        long long vchunk, double* __restrict__ part) {
+                                                        long long ld, long long vchunk, double* __restrict__ part) {
   extern __shared__ __align__(16) float sm_gs[];
-  const int stage_f = GV_VC * M + 32;
+  const int stage_f = COL ? 32 * GV_VC : GV_VC * M + 32;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int t = lane % 10, u = lane / 10;  // tile, vector of the triple (u == 3: idle lanes)
   const int p = t < 4 ? 0 : t < 7 ? 1 : t < 9 ? 2 : 3;
@@ -1149,9 +1150,13 @@ __global__ void __launch_bounds__(GS_NT, 1) k_gram_sym32(const float* __restrict
     const long long v0 = vb + st * GV_VC;
     const int nv = (int)((ve - v0 < GV_VC) ? ve - v0 : GV_VC);
     float* dst = sm_gs + (int)(st % GV_NS) * stage_f;
-    const int n16 = nv * M / 4;
-    const float* src = x + v0 * M;
-    for (int f = tid; f < n16; f += GS_NT) cp_async16(dst + 4 * f, src + 4 * f);
+    if (COL) {
+      gv_load_col<GS_NT>(dst, x, v0, nv, M, ld, tid);
+    } else {
+      const int n16 = nv * M / 4;
+      const float* src = x + v0 * M;
+      for (int f = tid; f < n16; f += GS_NT) cp_async16(dst + 4 * f, src + 4 * f);
+    }
   };
   // FP64 sums: registers (ACC64) or this thread's row of the shared block after the stages
   double* sacc = reinterpret_cast<double*>(sm_gs + GV_NS * stage_f + ((GV_NS * stage_f) & 1)) + tid * GS_LD;
@@ -1191,13 +1196,24 @@ __global__ void __launch_bounds__(GS_NT, 1) k_gram_sym32(const float* __restrict
     const int nv = (int)((ve - v0 < GV_VC) ? ve - v0 : GV_VC);
     if (u < 3) {
       for (int v = 3 * warp + u; v < nv; v += 24) {
-        const float* col = buf + v * M;
-        const float4 a0 = *reinterpret_cast<const float4*>(col + 8 * p);
-        const float4 a1 = *reinterpret_cast<const float4*>(col + 8 * p + 4);
-        const float4 b0 = *reinterpret_cast<const float4*>(col + 8 * q);
-        const float4 b1 = *reinterpret_cast<const float4*>(col + 8 * q + 4);
-        const float av[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
-        const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+        float av[8], bv[8];
+        if (COL) {
+#pragma unroll
+          for (int i = 0; i < 8; ++i) {
+            av[i] = buf[gv_col_at(8 * p + i, v)];
+            bv[i] = buf[gv_col_at(8 * q + i, v)];
+          }
+        } else {
+          const float* col = buf + v * M;
+          const float4 a0 = *reinterpret_cast<const float4*>(col + 8 * p);
+          const float4 a1 = *reinterpret_cast<const float4*>(col + 8 * p + 4);
+          const float4 b0 = *reinterpret_cast<const float4*>(col + 8 * q);
+          const float4 b1 = *reinterpret_cast<const float4*>(col + 8 * q + 4);
+          av[0] = a0.x; av[1] = a0.y; av[2] = a0.z; av[3] = a0.w;
+          av[4] = a1.x; av[5] = a1.y; av[6] = a1.z; av[7] = a1.w;
+          bv[0] = b0.x; bv[1] = b0.y; bv[2] = b0.z; bv[3] = b0.w;
+          bv[4] = b1.x; bv[5] = b1.y; bv[6] = b1.z; bv[7] = b1.w;
+        }
         if (ACC64) {
 #pragma unroll
           for (int i = 0; i < 8; ++i)
@@ -1419,18 +1435,29 @@ int launch_gram(const float* x, long long nvec, int M, long long vs, long long e
 #undef GV_ATTR
         attr = true;
       }
-      if (MPv == 32 && !col && gram_sym_smem(M, acc64) <= (size_t)max_optin_smem()) {
+      if (MPv == 32 && gram_sym_smem(M, acc64, col) <= (size_t)max_optin_smem()) {
         static bool sattr = false;
         if (!sattr) {
-          cudaFuncSetAttribute(k_gram_sym32<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin_smem());
-          cudaFuncSetAttribute(k_gram_sym32<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, max_optin_smem());
+          const int mx = max_optin_smem();
+          cudaFuncSetAttribute(k_gram_sym32<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+          cudaFuncSetAttribute(k_gram_sym32<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+          cudaFuncSetAttribute(k_gram_sym32<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
+          cudaFuncSetAttribute(k_gram_sym32<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
           sattr = true;
         }
-        const size_t sshm = gram_sym_smem(M, acc64);
-        if (acc64)
-          k_gram_sym32<true><<<nblk, GS_NT, sshm, s>>>(x, nvec, M, vchunk, part);
-        else
-          k_gram_sym32<false><<<nblk, GS_NT, sshm, s>>>(x, nvec, M, vchunk, part);
+        const size_t sshm = gram_sym_smem(M, acc64, col);
+        const long long lds = col ? es : M;
+        if (col) {
+          if (acc64)
+            k_gram_sym32<true, true><<<nblk, GS_NT, sshm, s>>>(x, nvec, M, lds, vchunk, part);
+          else
+            k_gram_sym32<false, true><<<nblk, GS_NT, sshm, s>>>(x, nvec, M, lds, vchunk, part);
+        } else {
+          if (acc64)
+            k_gram_sym32<true, false><<<nblk, GS_NT, sshm, s>>>(x, nvec, M, lds, vchunk, part);
+          else
+            k_gram_sym32<false, false><<<nblk, GS_NT, sshm, s>>>(x, nvec, M, lds, vchunk, part);
+        }
         count_launch();
         TT_LAUNCH_CHECK();
         launch_gram_reduce(part, nblk, 32, M, 8, w, s);
