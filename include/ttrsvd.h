@@ -222,8 +222,9 @@ int tt_k_syev(tt_ctx* ctx, const double* w, int N, double* evals, double* evecs,
  * the library until exit); m * N above 2^21 - 32 is rejected with TT_ERR_SHAPE.  All calls
  * share that array: calls that overlap on the GPU race and must be serialised.  The first
  * call on a device looks up the array's address (with that device current) and should come
- * before any stream capture.  Runs on `stream` (NULL = legacy default stream) and returns
- * after the result is complete.  This entry point has no counterpart in the reference. */
+ * before any stream capture.  Runs on `stream` (NULL = legacy default stream), which must
+ * belong to the current device (TT_ERR_ARG otherwise), and returns after the result is
+ * complete.  gemm outside TT_GEMM_AUTO..TT_GEMM_FP32 is rejected with TT_ERR_ARG.  This entry point has no counterpart in the reference. */
 int tt_k_sketch_noalloc(const float* a, long long m, long long n, const float* w, int N,
                         long long ldw, double* y, int gemm, void* stream);
 

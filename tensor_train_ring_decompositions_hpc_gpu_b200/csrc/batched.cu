@@ -667,16 +667,7 @@ int check_batch_args(int count, int d, int rmax, double eps, int oversample) {
 
 template <int BCH>
 int set_smem_attr() {
-  static bool done = false;
-  if (!done) {
-    if (cudaFuncSetAttribute(k_tt_batched<BCH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm_total<BCH>()) !=
-        cudaSuccess) {
-      set_error(TT_ERR_CUDA, "batched kernel shared-memory attribute");
-      return TT_ERR_CUDA;
-    }
-    done = true;
-  }
-  return TT_OK;
+  return smem_optin_k(k_tt_batched<BCH>, sm_total<BCH>());
 }
 
 struct BatchArgs {
@@ -718,12 +709,7 @@ int launch_batched(int bch, int grid, cudaStream_t s, const BatchArgs& a) {
   }
 }
 
-int persistent_grid(int count) {
-  int dev = 0, sms = 148;
-  TT_CUDA(cudaGetDevice(&dev));
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-  return std::max(1, std::min(count, sms));
-}
+int persistent_grid(int count) { return std::max(1, std::min(count, dev_sms())); }
 
 }  // namespace
 }  // namespace ttr

@@ -54,6 +54,18 @@ __device__ __forceinline__ void dev_fail(DevStatus* st, int code, int detail) {
 inline int ceil_div(long long a, long long b) { return (int)((a + b - 1) / b); }
 inline long long ceil_div_ll(long long a, long long b) { return (a + b - 1) / b; }
 
+// Current device, its multiprocessor count (cached per device), and a once-per-device raise
+// of a kernel's dynamic shared-memory limit (cudaFuncSetAttribute acts on the current device
+// only).  smem_optin returns TT_OK or TT_ERR_CUDA with the error message set.
+int cur_device();
+int dev_sms();
+int dev_smem_max();  // opt-in shared memory per block of the current device
+int smem_optin(const void* fn, size_t bytes);
+template <typename K>
+inline int smem_optin_k(K* kernel, size_t bytes) {
+  return smem_optin(reinterpret_cast<const void*>(kernel), bytes);
+}
+
 // Launch-count accounting (kernels launched by the current library call).
 extern thread_local int g_kernel_launches;
 inline void count_launch(int n = 1) { g_kernel_launches += n; }

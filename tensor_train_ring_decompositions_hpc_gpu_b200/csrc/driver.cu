@@ -1265,6 +1265,10 @@ extern "C" int tt_k_sketch(tt_ctx* c, const float* a, long long m, long long n, 
   TT_NEED(a);
   TT_NEED(w);
   TT_NEED(y);
+  if (gemm < TT_GEMM_AUTO || gemm > TT_GEMM_FP32) {
+    set_error(TT_ERR_ARG, "gemm option %d (expected TT_GEMM_AUTO, TT_GEMM_TC or TT_GEMM_FP32)", gemm);
+    return TT_ERR_ARG;
+  }
   if (m < 1 || n < 1 || N < 1 || ldw < n) {
     set_error(TT_ERR_SHAPE, "sketch shape");
     return TT_ERR_SHAPE;

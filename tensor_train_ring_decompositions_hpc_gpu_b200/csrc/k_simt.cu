@@ -14,16 +14,7 @@ namespace ttr {
 
 thread_local int g_kernel_launches = 0;
 
-static int g_num_sms = 0;
-static int num_sms() {
-  if (g_num_sms == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&g_num_sms, cudaDevAttrMultiProcessorCount, dev);
-    if (g_num_sms <= 0) g_num_sms = 148;
-  }
-  return g_num_sms;
-}
+static int num_sms() { return dev_sms(); }
 static int max_optin_smem();
 
 // ---------------------------------------------------------------------------------------
@@ -242,15 +233,10 @@ static void launch_sketch_simt_kernel(const float* a, long long m, long long n, 
   const int NT = N <= 16 ? 16 : N <= 24 ? 24 : N <= 32 ? 32 : N <= 40 ? 40 : N <= 48 ? 48 : 64;
   const int cblk = ceil_div(N, NT);
   dim3 grid(ceil_div(m, 256), nsplit, cblk);
-  static bool attr = false;
-  if (!attr) {
-#define SK_ATTR(V) \
-  cudaFuncSetAttribute(k_sketch_simt<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * 32 * (256 + V) * 4))
-    SK_ATTR(16); SK_ATTR(24); SK_ATTR(32); SK_ATTR(40); SK_ATTR(48); SK_ATTR(64);
-#undef SK_ATTR
-    attr = true;
-  }
   const size_t shm = (size_t)2 * 32 * (256 + NT) * sizeof(float);
+#define SK_ATTR(V) smem_optin_k(k_sketch_simt<V>, (size_t)2 * 32 * (256 + V) * 4)
+  SK_ATTR(16); SK_ATTR(24); SK_ATTR(32); SK_ATTR(40); SK_ATTR(48); SK_ATTR(64);
+#undef SK_ATTR
 #define SK_CASE(V) \
   case V: k_sketch_simt<V><<<grid, 256, shm, s>>>(a, m, n, w, N, wj, wc, jchunk, cblk, part); break;
   switch (NT) {
@@ -682,14 +668,10 @@ int launch_project(const float* a, long long m, long long n, const float* q, int
     const int split = NT <= 16 ? 1 : NT <= 48 ? 2 : 4;
     const int tj = 256 / split;
     const size_t shm = (64 * (size_t)NT + (size_t)tj * std::max<long long>(m + 1, NT + 1)) * sizeof(float);
-    static bool attr = false;
-    if (!attr) {
-      cudaFuncSetAttribute(k_proj_smallk<16, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-      cudaFuncSetAttribute(k_proj_smallk<32, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-      cudaFuncSetAttribute(k_proj_smallk<48, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-      cudaFuncSetAttribute(k_proj_smallk<64, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-      attr = true;
-    }
+    smem_optin_k(k_proj_smallk<16, 1>, 100 * 1024);
+    smem_optin_k(k_proj_smallk<32, 2>, 100 * 1024);
+    smem_optin_k(k_proj_smallk<48, 2>, 100 * 1024);
+    smem_optin_k(k_proj_smallk<64, 4>, 100 * 1024);
     const int grid = (int)std::min<long long>(ceil_div_ll(n, tj), 64LL * num_sms());
     const int mi = (int)m;
     switch (NT) {
@@ -721,16 +703,9 @@ int launch_project(const float* a, long long m, long long n, const float* q, int
   float* dst = ks > 1 ? part : out;
   const long long ldd = ks > 1 ? N : ldo;
   const int md = ks > 1 ? OUT_ROWMAJOR : mode;
-  {
-    static bool attr = false;
-    if (!attr) {
-#define PS_ATTR(V) \
-  cudaFuncSetAttribute(k_project_simt<V>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)(2 * 32 * (256 + V) * 4))
-      PS_ATTR(16); PS_ATTR(24); PS_ATTR(32); PS_ATTR(40); PS_ATTR(48); PS_ATTR(64);
+#define PS_ATTR(V) smem_optin_k(k_project_simt<V>, (size_t)2 * 32 * (256 + V) * 4)
+  PS_ATTR(16); PS_ATTR(24); PS_ATTR(32); PS_ATTR(40); PS_ATTR(48); PS_ATTR(64);
 #undef PS_ATTR
-      attr = true;
-    }
-  }
   const size_t pshm = (size_t)2 * 32 * (256 + NTs) * sizeof(float);
 #define PS_CASE(V) \
   case V: k_project_simt<V><<<grid, 256, pshm, s>>>(a, m, n, q, N, ldq, dst, ldd, md, r0, r1, kc); break;
@@ -1426,24 +1401,20 @@ int launch_gram(const float* x, long long nvec, int M, long long vs, long long e
         return TT_ERR_NOMEM;
       }
       const size_t shm = gram_vec_smem(MPv, M, col);
-      static bool attr = false;
-      if (!attr) {
+      {
         const int mx = max_optin_smem();
-#define GV_ATTR(MPV, A, C) cudaFuncSetAttribute(k_gram_vec<MPV, A, C>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx)
+#define GV_ATTR(MPV, A, C) smem_optin_k(k_gram_vec<MPV, A, C>, mx)
         GV_ATTR(32, false, false); GV_ATTR(32, true, false); GV_ATTR(64, false, false); GV_ATTR(64, true, false);
         GV_ATTR(32, false, true); GV_ATTR(32, true, true); GV_ATTR(64, false, true); GV_ATTR(64, true, true);
 #undef GV_ATTR
-        attr = true;
       }
       if (MPv == 32 && gram_sym_smem(M, acc64, col) <= (size_t)max_optin_smem()) {
-        static bool sattr = false;
-        if (!sattr) {
+        {
           const int mx = max_optin_smem();
-          cudaFuncSetAttribute(k_gram_sym32<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-          cudaFuncSetAttribute(k_gram_sym32<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-          cudaFuncSetAttribute(k_gram_sym32<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-          cudaFuncSetAttribute(k_gram_sym32<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-          sattr = true;
+          smem_optin_k(k_gram_sym32<false, false>, mx);
+          smem_optin_k(k_gram_sym32<true, false>, mx);
+          smem_optin_k(k_gram_sym32<false, true>, mx);
+          smem_optin_k(k_gram_sym32<true, true>, mx);
         }
         const size_t sshm = gram_sym_smem(M, acc64, col);
         const long long lds = col ? es : M;
@@ -1471,14 +1442,12 @@ int launch_gram(const float* x, long long nvec, int M, long long vs, long long e
         const int MPs = M <= 40 ? 40 : 48;
         const size_t tshm = gram_symt_smem(MPs, M, col);
         if (tshm <= (size_t)max_optin_smem()) {
-          static bool tattr = false;
-          if (!tattr) {
+          {
             const int mx = max_optin_smem();
-            cudaFuncSetAttribute(k_gram_symt<5, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-            cudaFuncSetAttribute(k_gram_symt<5, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-            cudaFuncSetAttribute(k_gram_symt<6, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-            cudaFuncSetAttribute(k_gram_symt<6, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-            tattr = true;
+            smem_optin_k(k_gram_symt<5, false>, mx);
+            smem_optin_k(k_gram_symt<5, true>, mx);
+            smem_optin_k(k_gram_symt<6, false>, mx);
+            smem_optin_k(k_gram_symt<6, true>, mx);
           }
           if (MPs == 40) {
             if (col)
@@ -1928,16 +1897,7 @@ __global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, in
   }
 }
 
-static int max_optin_smem() {
-  static int v = 0;
-  if (v == 0) {
-    int dev = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    if (v <= 0) v = 48 * 1024;
-  }
-  return v;
-}
+static int max_optin_smem() { return dev_smem_max(); }
 
 // Shared-memory bytes of k_cholqr2_small, or 0 when the sketch does not fit.
 static size_t cholqr2_small_smem(long long n, int N, bool want_r, int* S_out) {
@@ -1982,14 +1942,12 @@ static int cholqr_passes(float* y, long long n, int N, long long vs, long long e
   int S = 0;
   const size_t sshm = cholqr2_small_smem(n, N, r != nullptr, &S);
   if (sshm > 0) {
-    static bool attr_small = false;
-    if (!attr_small) {
+    {
       const int mx = max_optin_smem();
-      cudaFuncSetAttribute(k_cholqr2_small<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-      cudaFuncSetAttribute(k_cholqr2_small<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-      cudaFuncSetAttribute(k_cholqr2_small<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-      cudaFuncSetAttribute(k_cholqr2_small<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx);
-      attr_small = true;
+      smem_optin_k(k_cholqr2_small<16>, mx);
+      smem_optin_k(k_cholqr2_small<32>, mx);
+      smem_optin_k(k_cholqr2_small<48>, mx);
+      smem_optin_k(k_cholqr2_small<64>, mx);
     }
     const int nn = (int)n;
     if (N <= 16)
@@ -2016,16 +1974,12 @@ static int cholqr_passes(float* y, long long n, int N, long long vs, long long e
   const int NP = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : N <= 64 ? 64 : 128;
   const int ri_smem = 2 * (size_t)N * N * sizeof(double) + N * sizeof(int) + 16 <= 200 * 1024;
   const size_t shm = (size_t)(ri_smem ? 2 : 1) * N * N * sizeof(double) + N * sizeof(int) + 16;
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_chol_inv, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_apply_rinv<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_apply_rinv<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_apply_rinv<48>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_apply_rinv<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_apply_rinv<128>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
+  smem_optin_k(k_chol_inv, 200 * 1024);
+  smem_optin_k(k_apply_rinv<16>, 200 * 1024);
+  smem_optin_k(k_apply_rinv<32>, 200 * 1024);
+  smem_optin_k(k_apply_rinv<48>, 200 * 1024);
+  smem_optin_k(k_apply_rinv<64>, 200 * 1024);
+  smem_optin_k(k_apply_rinv<128>, 200 * 1024);
   for (int pass = 0; pass < passes; ++pass) {
     TT_TRY(launch_gram(y, n, N, vs, es, w, acc64, ws, s));
     k_chol_inv<<<1, 256, shm, s>>>(w, N, pass == 0 ? r1 : r2, rinv, 1e-12, ri_smem, st);
@@ -2437,11 +2391,7 @@ int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sw
   if (N <= 64) {
     const int Nps = N + (N & 1);
     const size_t shm_bl = 4 * (size_t)Nps * Nps * sizeof(double);
-    static bool attr_bl = false;
-    if (!attr_bl) {
-      cudaFuncSetAttribute(k_syev_bl, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-      attr_bl = true;
-    }
+    smem_optin_k(k_syev_bl, 160 * 1024);
     k_syev_bl<<<1, 1024, shm_bl, s>>>(w, N, evals, evecs, max_sweeps, st);
     count_launch();
     TT_LAUNCH_CHECK();
@@ -2460,12 +2410,8 @@ int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sw
       return TT_ERR_NOMEM;
     }
   }
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_syev_jacobi<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    cudaFuncSetAttribute(k_syev_jacobi<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
+  smem_optin_k(k_syev_jacobi<true>, 200 * 1024);
+  smem_optin_k(k_syev_jacobi<false>, 200 * 1024);
   if (vsm)
     k_syev_jacobi<true><<<1, 256, shm, s>>>(w, N, evals, evecs, vg, max_sweeps, st);
   else
@@ -2879,11 +2825,7 @@ int launch_recon_err(const float* x, int n1, long long N, const float* g1, int r
     set_error(TT_ERR_UNSUPPORTED, "reconstruction check: first core too large");
     return TT_ERR_UNSUPPORTED;
   }
-  static bool attr_set = false;
-  if (!attr_set) {
-    cudaFuncSetAttribute(k_recon_err, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-    attr_set = true;
-  }
+  TT_TRY(smem_optin_k(k_recon_err, 200 * 1024));
   const int grid = (int)std::min<long long>(ceil_div_ll(N, 32), 8LL * num_sms());
   k_recon_err<<<grid, 256, shm, s>>>(x, n1, N, g1, r0, r1, mrg, acc);
   count_launch();

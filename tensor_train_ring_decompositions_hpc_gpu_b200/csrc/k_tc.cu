@@ -776,30 +776,36 @@ __global__ void __launch_bounds__(192, 1)
 // ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
-PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;
-int g_tc_state = -1;  // -1 unknown, 0 unavailable, 1 available
-int g_sms = 0;
+PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;  // process-wide driver entry point
+constexpr int kMaxTcDev = 64;
+int g_tc_state[kMaxTcDev];  // per device: 0 unknown, 1 unavailable, 2 available
 
+// Tensor-core engine availability of the current device (its compute capability decides).
 bool init_tc() {
-  if (g_tc_state >= 0) return g_tc_state == 1;
-  g_tc_state = 0;
-  const char* dis = getenv("TTR_DISABLE_TC");
-  if (dis && dis[0] == '1') return false;
-  int dev = 0, major = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) return false;
-  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
-  cudaDeviceGetAttribute(&g_sms, cudaDevAttrMultiProcessorCount, dev);
-  if (major != 10) return false;
-  void* fn = nullptr;
-  cudaDriverEntryPointQueryResult q;
-  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
-      q != cudaDriverEntryPointSuccess || !fn) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
-  g_tc_state = 1;
-  return true;
+  int* state = (dev >= 0 && dev < kMaxTcDev) ? &g_tc_state[dev] : nullptr;
+  if (state && *state) return *state == 2;
+  bool ok = false;
+  const char* dis = getenv("TTR_DISABLE_TC");
+  int major = 0;
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (!(dis && dis[0] == '1') && major == 10) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess && fn) {
+      g_encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+      ok = true;
+    } else {
+      cudaGetLastError();
+    }
+  }
+  if (state) *state = ok ? 2 : 1;
+  return ok;
 }
 
 int make_map(CUtensorMap* map, const void* base, unsigned long long d0, unsigned long long d1,
@@ -837,9 +843,7 @@ int make_map_blocks(CUtensorMap* map, const float* base, unsigned long long m, u
 
 template <typename K>
 int set_smem(K kernel, size_t bytes) {
-  return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) == cudaSuccess
-             ? TT_OK
-             : TT_ERR_CUDA;
+  return smem_optin(reinterpret_cast<const void*>(kernel), bytes);
 }
 
 constexpr size_t kSmemBudget = 200 * 1024;
@@ -877,16 +881,9 @@ int run_project(const CUtensorMap& ma, const CUtensorMap& mb, const CUtensorMap&
   constexpr int STAGES = (int)std::min<size_t>(10, (kSmemBudget - STAGING) / STAGE);
   const size_t smem = (size_t)STAGES * STAGE + 1024 + 256 + STAGING;
   auto kern = k_project_tc<BN, STAGES, SPLIT>;
-  static bool attr = false;
-  if (!attr) {
-    if (set_smem(kern, smem) != TT_OK) {
-      set_error(TT_ERR_CUDA, "project_tc smem attribute");
-      return TT_ERR_CUDA;
-    }
-    attr = true;
-  }
+  if (set_smem(kern, smem) != TT_OK) return TT_ERR_CUDA;
   const long long ntiles = (n + 127) / 128;
-  const int grid = (int)std::min<long long>(ntiles, (long long)g_sms);
+  const int grid = (int)std::min<long long>(ntiles, (long long)dev_sms());
   kern<<<grid, 320, smem, s>>>(ma, mb, mb2, n, N, KB, out, ldo, mode, r0, r1, st);
   count_launch();
   TT_LAUNCH_CHECK();
@@ -902,16 +899,9 @@ int run_sketch(const CUtensorMap& ma, const CUtensorMap& mb, long long m, long l
   constexpr int STAGES = (int)std::min<size_t>(8, kSmemBudget / STAGE);
   const size_t smem = (size_t)STAGES * STAGE + 1024 + 256;
   auto kern = k_sketch_tc<BN, MT, BK, STAGES>;
-  static bool attr = false;
-  if (!attr) {
-    if (set_smem(kern, smem) != TT_OK) {
-      set_error(TT_ERR_CUDA, "sketch_tc smem attribute");
-      return TT_ERR_CUDA;
-    }
-    attr = true;
-  }
+  if (set_smem(kern, smem) != TT_OK) return TT_ERR_CUDA;
   const int units = ngroups * nsplit;
-  const int grid = std::min(units, g_sms);
+  const int grid = std::min(units, dev_sms());
   kern<<<grid, 192, smem, s>>>(ma, mb, m, n, N, kchunk, nsplit, ngroups, part, st, a3d);
   count_launch();
   TT_LAUNCH_CHECK();
@@ -928,7 +918,7 @@ int sketch_tc_plan(long long m, long long n, int N, int* MT, int* ngroups, int* 
   while (mt > 1 && mt * BNP > 512) mt /= 2;
   const int bk = mt >= 8 ? 8 : mt == 4 ? 16 : 32;
   const int ng = (int)((m + mt * 128 - 1) / (mt * 128));
-  const int sms = g_sms > 0 ? g_sms : 148;
+  const int sms = dev_sms();
   int ns = std::max(1, sms / ng);
   long long kc = (n + ns - 1) / ns;
   kc = std::max<long long>(kc, 4LL * bk);
@@ -949,16 +939,11 @@ int run_gram(const CUtensorMap& ma, long long ncols, int m, int grouped, long lo
   constexpr int STAGES = 8;  // 128 KB ring + the m x (m+1) Gram accumulator
   const size_t smem = (size_t)STAGES * STAGE + 1024 + 256 + (size_t)m * (m + 1) * sizeof(float);
   auto kern = k_gram_tc<NB, STAGES>;
-  static bool attr = false;
-  if (!attr) {
+  {
     const size_t most = (size_t)STAGES * STAGE + 1024 + 256 + 128 * 129 * sizeof(float);
-    if (set_smem(kern, most) != TT_OK) {
-      set_error(TT_ERR_CUDA, "gram_tc smem attribute");
-      return TT_ERR_CUDA;
-    }
-    attr = true;
+    if (set_smem(kern, most) != TT_OK) return TT_ERR_CUDA;
   }
-  const int grid = std::min(nsplit, g_sms);
+  const int grid = std::min(nsplit, dev_sms());
   kern<<<grid, 192, smem, s>>>(ma, ncols, m, grouped, kchunk, nsplit, part, st);
   count_launch();
   TT_LAUNCH_CHECK();
@@ -972,7 +957,7 @@ void gram_tc_plan(long long m, long long n, int* grouped, long long* ncols, int*
   *ncols = g ? (n * m) / 128 : n;
   // Each unit's MMA accumulation runs in FP32 (TMEM); units of at most 2048 columns keep its
   // rounding small before the FP64 sum of the unit partials.
-  const int sms = g_sms > 0 ? g_sms : 148;
+  const int sms = dev_sms();
   long long kc = (*ncols + sms - 1) / sms;
   kc = std::min<long long>(std::max<long long>(kc, 128), 2048);
   kc = (kc + 31) / 32 * 32;
@@ -1057,7 +1042,7 @@ int launch_project_tc(const float* a, long long m, long long n, const float* q, 
   }
   {
     const long long total = m * (long long)N;
-    const int grid = (int)std::min<long long>((total + 255) / 256, 4LL * (g_sms > 0 ? g_sms : 148));
+    const int grid = (int)std::min<long long>((total + 255) / 256, 4LL * dev_sms());
     k_split_tf32<<<grid, 256, 0, s>>>(q, m, N, ldq, qhi, qlo, ldh);
     count_launch();
     TT_LAUNCH_CHECK();

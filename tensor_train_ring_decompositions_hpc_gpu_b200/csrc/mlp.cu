@@ -277,18 +277,7 @@ __global__ void k_probe_features(const double* __restrict__ mu, double energy, d
   out[7] = (float)(log10(fmax(tol, 1e-30)) / 4.0);
 }
 
-int train_attr() {
-  static bool done = false;
-  if (!done) {
-    if (cudaFuncSetAttribute(k_mlp_train, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TRAIN_SMEM) !=
-        cudaSuccess) {
-      set_error(TT_ERR_CUDA, "predictor training kernel shared-memory attribute");
-      return TT_ERR_CUDA;
-    }
-    done = true;
-  }
-  return TT_OK;
-}
+int train_attr() { return smem_optin_k(k_mlp_train, TRAIN_SMEM); }
 
 }  // namespace
 

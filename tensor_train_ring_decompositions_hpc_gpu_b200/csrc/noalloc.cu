@@ -65,6 +65,10 @@ extern "C" int tt_k_sketch_noalloc(const float* a, long long m, long long n, con
     ttr::set_error(TT_ERR_ARG, "null argument");
     return TT_ERR_ARG;
   }
+  if (gemm < TT_GEMM_AUTO || gemm > TT_GEMM_FP32) {
+    ttr::set_error(TT_ERR_ARG, "gemm option %d (expected TT_GEMM_AUTO, TT_GEMM_TC or TT_GEMM_FP32)", gemm);
+    return TT_ERR_ARG;
+  }
   if (m < 1 || n < 1 || N < 1 || N > TT_MAX_SMALL || ldw < n) {
     ttr::set_error(TT_ERR_SHAPE, "sketch shape m=%lld n=%lld N=%d ldw=%lld", m, n, N, ldw);
     return TT_ERR_SHAPE;
@@ -72,12 +76,23 @@ extern "C" int tt_k_sketch_noalloc(const float* a, long long m, long long n, con
   const long long cap = kScratchDoubles - kStatusDoubles;
   if ((double)m * (double)N > (double)cap) {
     ttr::set_error(TT_ERR_SHAPE,
-                   "m * N = %lld exceeds the %lld-double static scratch of tt_k_sketch_noalloc", m * N, cap);
+                   "m * N = %lld * %d exceeds the %lld-double static scratch of tt_k_sketch_noalloc", m, N, cap);
     return TT_ERR_SHAPE;
+  }
+  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
+  if (s) {
+    // The scratch address below belongs to the current device; a stream of another device
+    // would hand its kernels a pointer they cannot use.
+    int cur = 0, sdev = 0;
+    TT_CUDA(cudaGetDevice(&cur));
+    TT_CUDA(cudaStreamGetDevice(s, &sdev));
+    if (sdev != cur) {
+      ttr::set_error(TT_ERR_ARG, "stream belongs to device %d but device %d is current", sdev, cur);
+      return TT_ERR_ARG;
+    }
   }
   double* base = nullptr;
   TT_TRY(scratch_address(&base));
-  cudaStream_t s = reinterpret_cast<cudaStream_t>(stream);
   ttr::DevStatus* st = reinterpret_cast<ttr::DevStatus*>(base);
   double* part = base + kStatusDoubles;
   TT_CUDA(cudaMemsetAsync(st, 0, sizeof(ttr::DevStatus), s));

@@ -67,3 +67,13 @@ def test_ctx_create_reports_missing_device():
     p = C.c_void_p()
     st = lib.tt_ctx_create(C.byref(p), 0, None)
     assert st != 0 and not p.value
+
+
+def test_noalloc_rejects_bad_gemm_option_without_gpu():
+    """An unknown gemm value is an argument error, checked before any device work."""
+    from tensor_train_ring_decompositions_hpc_gpu_b200 import _lib
+    lib = _lib.load()
+    fake = C.c_void_p(256)  # never dereferenced: the option check comes first
+    for bad in (-1, 3, 7):
+        assert lib.tt_k_sketch_noalloc(fake, 64, 64, fake, 8, 64, fake, bad, None) == 1  # TT_ERR_ARG
+        assert b"gemm option" in lib.tt_last_error()
