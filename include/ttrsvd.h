@@ -195,7 +195,9 @@ int tt_k_project(tt_ctx* ctx, const float* a, long long m, long long n, const fl
 
 /* Gram of the rows W = A * A^T (m x m, FP64), A (m x n, lda = m), m <= TT_MAX_SMALL.
  * gemm = TT_GEMM_TC uses tcgen05 TF32 tiles (operands rounded to nearest by the TMA unit,
- * FP32 accumulation, FP64 across blocks); TT_GEMM_FP32 the FP32 FMA kernel.
+ * FP32 accumulation, FP64 across blocks); TT_GEMM_FP32 the FP32 FMA kernel.  With
+ * TT_GEMM_AUTO or TT_GEMM_FP32, m <= 32 (m % 4 == 0) takes the exact CUDA-core kernel (FP32
+ * products, FP64 sums), the one every decomposition uses for such unfoldings.
  * Replaces largeMatrixSelfMulti_once_device (ttdec6_singleGPU.cu:388-401). */
 int tt_k_gram_rows(tt_ctx* ctx, const float* a, long long m, long long n, double* w, int gemm);
 

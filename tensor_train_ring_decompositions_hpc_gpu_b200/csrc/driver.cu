@@ -346,6 +346,7 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
         P.max_ws = std::max(P.max_ws, gram_ws_bytes(st.cols, w));
         P.max_ws = std::max(P.max_ws, gram_ws_bytes(st.m, w));
         P.max_ws = std::max(P.max_ws, gram_tc_ws_bytes(w, st.cols));
+        P.max_ws = std::max(P.max_ws, gram32x_ws_bytes());
         P.max_ws = std::max(P.max_ws, project_ws_bytes(st.m, st.cols, w));
         P.max_ws = std::max(P.max_ws, project_ws_bytes(w, st.cols, std::min(w, st.r_req)));
       }
@@ -354,6 +355,7 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
       P.max_ws = std::max(P.max_ws, project_ws_bytes(st.m, st.cols, st.r_req));
       P.max_ws = std::max(P.max_ws, gram_ws_bytes(std::max(st.m, st.cols), (int)mn));
       P.max_ws = std::max(P.max_ws, gram_tc_ws_bytes(st.m, st.cols));
+      P.max_ws = std::max(P.max_ws, gram32x_ws_bytes());
     }
   }
   P.max_ws += (size_t)TT_MAX_SMALL * TT_MAX_SMALL * sizeof(double) * 8;
@@ -650,6 +652,24 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
     }
     return TT_OK;
   };
+  // Gram of the rows of an unfolding with m <= 128 rows (the exact step).  Up to 32 rows: the
+  // exact CUDA-core kernel in every form (FP32 products, FP64 sums), whose result resolves
+  // eigenvalues down to ~1e-9 of the largest; the tensor cores' truncating FP32 accumulation
+  // would bias the small ones.  Wider: tensor cores when allowed, else the FP32 engine.
+  // `precise` (adaptive ranks: energies to ~1e-8 relative) keeps short unfoldings, whose few
+  // partial sums do not average the FP32 rounding out, on FP64 products.
+  auto gram_rows = [&](const float* a, long long mm, long long nc, double* w, int eng, bool precise) -> int {
+    const bool long_unf = nc >= (1LL << 16);
+    if (mm <= 32 && (!precise || long_unf)) {
+      const int rc = launch_gram32x(a, nc, (int)mm, w, ws, c->dstat, s);
+      if (rc != TT_ERR_UNSUPPORTED) return rc;
+    }
+    if (eng == TT_GEMM_TC && !precise) {
+      const int rc = launch_gram_tc(a, mm, nc, w, ws, c->dstat, s);
+      if (rc != TT_ERR_UNSUPPORTED) return rc;
+    }
+    return launch_gram(a, nc, (int)mm, mm, 1, w, precise && nc < (1LL << 22), ws, s);
+  };
   int npasses = 0, natt = 0, nfall = 0;  // bulk passes, EDrSVD attempts, learned fallbacks
   std::vector<int> step_ks((size_t)nsteps, 0), step_pw((size_t)nsteps, 0), step_att((size_t)nsteps, 0);
   for (int k = 0; k < nsteps; ++k) {
@@ -724,11 +744,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols, [&]() -> int {
         TT_CUDA(cudaMemsetAsync(B.wacc, 0, sizeof(double) * m * m, s));
         TT_TRY(stream_pass([&](const float* a, long long, long long nc) -> int {
-          const int eng = engine_for(o, m, nc);
-          int rc = TT_ERR_UNSUPPORTED;
-          if (eng == TT_GEMM_TC) rc = launch_gram_tc(a, m, nc, B.w, ws, c->dstat, s);
-          if (rc == TT_ERR_UNSUPPORTED) rc = launch_gram(a, nc, (int)m, m, 1, B.w, false, ws, s);
-          TT_TRY(rc);
+          TT_TRY(gram_rows(a, m, nc, B.w, engine_for(o, m, nc), false));
           k_add_f64<<<ceil_div(m * m, 256), 256, 0, s>>>(B.w, B.wacc, (int)(m * m));
           count_launch();
           TT_LAUNCH_CHECK();
@@ -754,13 +770,8 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       // folded step: Gram on s, the rest on the side stream (see join_side)
       npasses += 1;
       TT_TRY(join_side());  // one side job at a time: its buffers are reused here
-      TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols, [&] {
-        if (engine == TT_GEMM_TC) {
-          const int rc = launch_gram_tc(cur, m, cols, B.w2, ws, c->dstat, s);
-          if (rc != TT_ERR_UNSUPPORTED) return rc;
-        }
-        return launch_gram(cur, cols, (int)m, m, 1, B.w2, false, ws, s);
-      }));
+      TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols,
+                      [&] { return gram_rows(cur, m, cols, B.w2, engine, false); }));
       if (!c->side_stream) {
         TT_CUDA(cudaStreamCreateWithFlags(&c->side_stream, cudaStreamNonBlocking));
         TT_CUDA(cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming));
@@ -784,18 +795,8 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       continue;
     } else if (st.path == PATH_EXACT_ROWS) {
       npasses += st.fold ? 1 : 2;
-      TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols, [&] {
-        // Adaptive ranks read energies to ~1e-8 relative: the FP32 engine (round-to-nearest
-        // products, FP64 accumulation per product for short unfoldings, per 1024 columns for
-        // long ones whose many partial sums average the FP32 rounding out).  Tensor-core
-        // accumulation truncates, a bias above delta^2.
-        const bool long_unf = cols >= (1LL << 22);
-        if (engine == TT_GEMM_TC && !adaptive) {
-          const int rc = launch_gram_tc(cur, m, cols, B.w, ws, c->dstat, s);
-          if (rc != TT_ERR_UNSUPPORTED) return rc;
-        }
-        return launch_gram(cur, cols, (int)m, m, 1, B.w, adaptive && !long_unf, ws, s);
-      }));
+      TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols,
+                      [&] { return gram_rows(cur, m, cols, B.w, engine, adaptive); }));
       TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
@@ -1133,6 +1134,7 @@ int run_entry(tt_ctx* c, const float* x, int d, const int* n, const int* r, cons
     // the Gram and projection kernels see one chunk at a time
     P.max_ws = std::max(P.max_ws, gram_ws_bytes(P.stream_cols, (int)s0.m));
     P.max_ws = std::max(P.max_ws, gram_tc_ws_bytes(s0.m, P.stream_cols));
+    P.max_ws = std::max(P.max_ws, gram32x_ws_bytes());
     P.max_ws = std::max(P.max_ws, project_ws_bytes(s0.m, P.stream_cols, s0.r_req));
   }
   for (int k = 0; k < d; ++k)
@@ -1425,10 +1427,13 @@ extern "C" int tt_k_gram_rows(tt_ctx* c, const float* a, long long m, long long 
   }
   TT_CUDA(cudaSetDevice(c->device));
   Arena ws;
-  TT_TRY(ws_for(c, std::max(gram_ws_bytes(n, (int)m), gram_tc_ws_bytes(m, n)), ws));
+  TT_TRY(ws_for(c, std::max(std::max(gram_ws_bytes(n, (int)m), gram_tc_ws_bytes(m, n)), gram32x_ws_bytes()), ws));
   TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
   int rc = TT_ERR_UNSUPPORTED;
-  if (gemm != TT_GEMM_FP32 && tc_available()) rc = launch_gram_tc(a, m, n, w, ws, c->dstat, c->stream);
+  // up to 32 rows, AUTO and FP32 take the exact CUDA-core kernel; TC forces the tensor cores
+  if (gemm != TT_GEMM_TC && m <= 32) rc = launch_gram32x(a, n, (int)m, w, ws, c->dstat, c->stream);
+  if (rc == TT_ERR_UNSUPPORTED && gemm != TT_GEMM_FP32 && tc_available())
+    rc = launch_gram_tc(a, m, n, w, ws, c->dstat, c->stream);
   if (rc == TT_ERR_UNSUPPORTED) rc = launch_gram(a, n, (int)m, m, 1, w, false, ws, c->stream);
   TT_TRY(rc);
   return check_status(c);

@@ -774,6 +774,177 @@ __global__ void __launch_bounds__(192, 1)
 }
 
 // ---------------------------------------------------------------------------------------
+// Exact Gram of short vectors on the CUDA cores: W = sum_j x_j x_j^T, x_j = M <= 32
+// contiguous floats (the exact step's Gram of an unfolding with at most 32 rows, e.g. the
+// 32 x 33,554,432 first unfolding of a 32^6 tensor; largeMatrixSelfMulti_once_device,
+// ttdec6_singleGPU.cu:388-401, which the reference runs on FP16 tensor cores).
+//
+// The tensor cores cannot serve this Gram: their FP32 accumulator truncates, which biases a
+// long sum by ~1e-7 of its leading entries, while the smallest kept eigenvalue of such an
+// unfolding can sit at 1e-5 of the largest.  Here the products are FP32 (round to nearest)
+// and go through FP32 partial sums of 64 vectors into FP64 sums, so every rounding error is
+// unbiased and the result is accurate to ~1e-9 relative.
+//
+// Each warp runs its own TMA pipeline: 48-vector boxes (6 KB, 128B-swizzled rows) through 4
+// stages, the warp's lane 0 refilling a stage as soon as the warp has consumed it; no block-wide
+// barrier exists until the final reduction.  Within a warp, lane = 10 u + t computes the 8 x 8
+// tile t of the upper triangle of 32 x 32 tiles (10 tiles) for vector 3 it + u of the box
+// (lanes 30, 31 idle), with paired FP32 FMAs (fma.rn.f32x2): 32 issue slots per 64 FMAs.
+// ---------------------------------------------------------------------------------------
+constexpr int G32_VPS = 48;     // vectors per TMA box (one stage)
+constexpr int G32_STAGES = 4;   // stages per warp
+constexpr int G32_WARPS = 8;
+constexpr int G32_FLUSH = 4;    // stages (64 vectors per lane) between FP64 flushes
+constexpr uint32_t G32_STAGE_BYTES = G32_VPS * 128;
+constexpr size_t G32_RING = (size_t)G32_WARPS * G32_STAGES * G32_STAGE_BYTES;
+constexpr size_t G32_SMEM = 1024 + G32_RING + (size_t)G32_WARPS * G32_STAGES * 8;
+static_assert(G32_RING >= 256 * 65 * sizeof(double), "reduction area fits in the stage ring");
+
+__device__ __forceinline__ uint64_t f2_dup(float a) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(a));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(uint64_t v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ void ffma2(uint64_t& d, uint64_t a, uint64_t b) {
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
+}
+__device__ __forceinline__ float4 lds_f4(uint32_t addr) {
+  float4 v;
+  asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr));
+  return v;
+}
+__device__ __forceinline__ void lds_u2(uint32_t addr, uint64_t& a, uint64_t& b) {
+  asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "r"(addr));
+}
+
+__global__ void __launch_bounds__(256, 1)
+    k_gram32x(const __grid_constant__ CUtensorMap tm, long long nvec, double* __restrict__ part, DevStatus* st) {
+  extern __shared__ uint8_t smem_raw[];
+  uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const uint32_t wbase = smem_u32(smem) + (uint32_t)(warp * G32_STAGES) * G32_STAGE_BYTES;
+  const Bars bars{smem_u32(smem + G32_RING) + 8u * G32_STAGES * warp, G32_STAGES};
+  if (lane == 0) {
+    for (int s = 0; s < G32_STAGES; ++s) mbar_init(bars.full(s), 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    asm volatile("prefetch.tensormap [%0];" ::"l"((unsigned long long)&tm) : "memory");
+  }
+  __syncwarp();
+  const long long nchunk = (nvec + G32_VPS - 1) / G32_VPS;
+  const long long gw = (long long)blockIdx.x * G32_WARPS + warp;
+  const long long GW = (long long)gridDim.x * G32_WARPS;
+  const long long my = gw < nchunk ? (nchunk - 1 - gw) / GW + 1 : 0;  // boxes of this warp
+  if (lane == 0) {
+    for (int s = 0; s < G32_STAGES && s < my; ++s) {
+      mbar_expect_tx(bars.full(s), G32_STAGE_BYTES);
+      tma_load_2d(wbase + s * G32_STAGE_BYTES, &tm, bars.full(s), 0, (int)((gw + s * GW) * G32_VPS));
+    }
+  }
+  const int t = lane % 10, u = lane / 10;
+  const int p = t < 4 ? 0 : t < 7 ? 1 : t < 9 ? 2 : 3;
+  const int q = t < 4 ? t : t < 7 ? t - 3 : t < 9 ? t - 5 : 3;
+  uint64_t acc[8][4];  // (W[8p+i][8q+2j], W[8p+i][8q+2j+1])
+  double accd[8][8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+#pragma unroll
+    for (int j = 0; j < 4; ++j) acc[i][j] = 0ull;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) accd[i][j] = 0.0;
+  }
+  auto flush = [&]() {
+#pragma unroll
+    for (int i = 0; i < 8; ++i)
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        float lo, hi;
+        f2_unpack(acc[i][j], lo, hi);
+        accd[i][2 * j] += (double)lo;
+        accd[i][2 * j + 1] += (double)hi;
+        acc[i][j] = 0ull;
+      }
+  };
+  long long k = 0;
+  bool ok = true;
+  for (; k < my; ++k) {
+    const int s = (int)(k % G32_STAGES);
+    ok = mbar_wait_bounded(bars.full(s), (uint32_t)((k / G32_STAGES) & 1));
+    ok = __all_sync(0xffffffffu, ok);
+    if (!ok) break;
+    const uint32_t sb = wbase + (uint32_t)s * G32_STAGE_BYTES;
+    if (u < 3) {
+#pragma unroll 2
+      for (int it = 0; it < G32_VPS / 3; ++it) {
+        const int v = 3 * it + u;
+        const uint32_t row = sb + (uint32_t)v * 128u;
+        const int sw = v & 7;
+        const float4 a0 = lds_f4(row + ((uint32_t)((2 * p) ^ sw) << 4));
+        const float4 a1 = lds_f4(row + ((uint32_t)((2 * p + 1) ^ sw) << 4));
+        uint64_t b[4];
+        lds_u2(row + ((uint32_t)((2 * q) ^ sw) << 4), b[0], b[1]);
+        lds_u2(row + ((uint32_t)((2 * q + 1) ^ sw) << 4), b[2], b[3]);
+        const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+          const uint64_t ad = f2_dup(a[i]);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) ffma2(acc[i][j], ad, b[j]);
+        }
+      }
+    }
+    __syncwarp();
+    if (lane == 0 && k + G32_STAGES < my) {
+      // the warp's reads of this stage are done; order them before the async-proxy refill
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      mbar_expect_tx(bars.full(s), G32_STAGE_BYTES);
+      tma_load_2d(sb, &tm, bars.full(s), 0, (int)((gw + (k + G32_STAGES) * GW) * G32_VPS));
+    }
+    if ((k % G32_FLUSH) == G32_FLUSH - 1) flush();
+  }
+  flush();
+  if (!ok) {
+    if (lane == 0) {
+      dev_fail(st, TT_ERR_TIMEOUT, 4);
+      // every issued fill must land before the CTA leaves (fills issued: min(my, k + STAGES))
+      drain_fills(bars, G32_STAGES, my < k + G32_STAGES ? my : k + G32_STAGES);
+    }
+    __syncwarp();
+  }
+  __syncthreads();  // every warp is done with its ring: reuse it for the block reduction
+  double* red = reinterpret_cast<double*>(smem);
+  const int tid = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) red[tid * 65 + i * 8 + j] = accd[i][j];
+  __syncthreads();
+  double* dst = part + (long long)blockIdx.x * 1024;
+  for (int e = tid; e < 10 * 64; e += blockDim.x) {
+    const int tt = e >> 6, ij = e & 63;
+    double sum = 0.0;
+    for (int w = 0; w < G32_WARPS; ++w)
+      for (int uu = 0; uu < 3; ++uu) sum += red[(w * 32 + uu * 10 + tt) * 65 + ij];
+    const int pp = tt < 4 ? 0 : tt < 7 ? 1 : tt < 9 ? 2 : 3;
+    const int qq = tt < 4 ? tt : tt < 7 ? tt - 3 : tt < 9 ? tt - 5 : 3;
+    dst[(8 * pp + (ij >> 3)) * 32 + 8 * qq + (ij & 7)] = sum;
+  }
+}
+
+// W (M x M, column-major) = sum over blocks of the upper-tile partials (fixed order).
+__global__ void k_gram32x_finish(const double* __restrict__ part, int nblk, int M, double* __restrict__ w) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < M * M; e += gridDim.x * blockDim.x) {
+    const int i = e % M, j = e / M;
+    const int r = i < j ? i : j, c = i < j ? j : i;
+    double sum = 0.0;
+    for (int b = 0; b < nblk; ++b) sum += part[(long long)b * 1024 + r * 32 + c];
+    w[e] = sum;
+  }
+}
+
+// ---------------------------------------------------------------------------------------
 // host side
 // ---------------------------------------------------------------------------------------
 PFN_cuTensorMapEncodeTiled_v12000 g_encode = nullptr;  // process-wide driver entry point
@@ -1013,6 +1184,46 @@ int launch_gram_tc(const float* a, long long m, long long n, double* w, Arena& w
 }
 
 bool tc_available() { return init_tc(); }
+
+size_t gram32x_ws_bytes() { return (size_t)dev_sms() * 1024 * sizeof(double) + 4096; }
+
+// Exact Gram of nvec contiguous M-float vectors (M <= 32, M % 4 == 0, 16-byte aligned) on the
+// CUDA cores; TT_ERR_UNSUPPORTED (nothing launched) when the shape or the device does not fit.
+int launch_gram32x(const float* x, long long nvec, int M, double* w, Arena& ws, DevStatus* st, cudaStream_t s) {
+  if (!init_tc()) return TT_ERR_UNSUPPORTED;
+  if (M < 1 || M > 32 || (M & 3) || nvec < 1 || (reinterpret_cast<uintptr_t>(x) & 15) ||
+      nvec > (1LL << 31) - 2 * G32_VPS)
+    return TT_ERR_UNSUPPORTED;
+  CUtensorMap map;
+  {
+    cuuint64_t dims[2] = {(cuuint64_t)M, (cuuint64_t)nvec};
+    cuuint64_t strides[1] = {(cuuint64_t)M * 4};
+    cuuint32_t box[2] = {32, (cuuint32_t)G32_VPS};
+    cuuint32_t es[2] = {1, 1};
+    const CUresult r = g_encode(&map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, const_cast<float*>(x), dims, strides,
+                                box, es, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                                CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return TT_ERR_UNSUPPORTED;
+  }
+  const long long nchunk = (nvec + G32_VPS - 1) / G32_VPS;
+  const int grid = (int)std::max<long long>(1, std::min<long long>(dev_sms(), ceil_div_ll(nchunk, G32_WARPS)));
+  const size_t mk = ws.mark();
+  double* part = ws.take<double>((size_t)grid * 1024);
+  if (!part) {
+    set_error(TT_ERR_NOMEM, "gram32x workspace");
+    return TT_ERR_NOMEM;
+  }
+  TT_TRY(set_smem(k_gram32x, G32_SMEM));
+  k_gram32x<<<grid, 256, G32_SMEM, s>>>(map, nvec, part, st);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  k_gram32x_finish<<<ceil_div(M * M, 256), 256, 0, s>>>(part, grid, M, w);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  ws.reset(mk);
+  return TT_OK;
+}
+
 
 size_t sketch_tc_ws_bytes(long long m, long long n, int N) {
   if (!init_tc()) return 0;

@@ -136,6 +136,12 @@ DevStatus* ctx_status(tt_ctx* c);
 // out (Rout x cols) from in (Rin x cols), rows Rin..Rout-1 zero; column-major.
 int launch_expand_rows(const float* in, int Rin, float* out, int Rout, long long cols, cudaStream_t s);
 
+// Exact Gram W (M x M, FP64, ld = M) = sum_j x_j x_j^T of nvec contiguous M-float vectors
+// (M <= 32, M % 4 == 0, 16-byte aligned base) on the CUDA cores: FP32 products, FP64 sums.
+// TT_ERR_UNSUPPORTED (nothing launched) when the shape or device does not fit.
+size_t gram32x_ws_bytes();
+int launch_gram32x(const float* x, long long nvec, int M, double* w, Arena& ws, DevStatus* st, cudaStream_t s);
+
 // Sketch variants that take their split-K scratch from the caller (no allocation).
 int launch_sketch_tc_static(const float* a, long long m, long long n, const float* w, int N,
                             long long wj, long long wc, double* y, double* part, size_t part_cap,

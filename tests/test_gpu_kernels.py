@@ -292,3 +292,49 @@ def test_gram_rows_tc_resolves_graded_spectrum(gpu, n):
     lead = ref >= 1e-2 * ref[0]
     np.testing.assert_allclose(got[lead], ref[lead], rtol=1e-4)
     np.testing.assert_allclose(got, ref, rtol=1e-4, atol=2e-6 * ref[0])
+
+
+@pytest.mark.parametrize("gemm", ["fp32", "auto"])
+@pytest.mark.parametrize("m,n", [(32, 1), (32, 47), (32, 48 * 8 * 148 + 5), (32, 1 << 20), (16, 100003),
+                                 (8, 333333), (28, 70000), (4, 5000), (12, 48), (24, 4096 * 37 + 12)])
+def test_gram_rows_exact_short_vectors(gpu, gemm, m, n):
+    """Up to 32 rows the exact CUDA-core Gram runs (FP32 products, FP64 sums): ~1e-9 relative."""
+    ttr = _ttr()
+    a = _randn_cm(m, n, 15, gpu)
+    w = ttr.gram_rows(a, gemm).cpu().numpy()
+    ad = a.double().cpu().numpy()
+    ref = ad @ ad.T
+    # a handful of vectors leaves one FP32-rounded partial sum per entry (~6e-8); long inputs
+    # average many of them
+    assert _rel(w, ref) < (2e-7 if n < 65536 else 5e-8)
+    np.testing.assert_array_equal(w, w.T)
+
+
+@pytest.mark.parametrize("n", [1 << 21, 3 << 20])
+def test_gram_rows_exact_resolves_graded_spectrum(gpu, n):
+    """The same graded 32-row unfolding as above (eigenvalues over 5 decades, like unfolding 1
+    of the 32^6 TT): the exact kernel gives every eigenvalue, the smallest at 1e-5 of the
+    largest included, within 1e-4 relative (singular values within 5e-5)."""
+    import torch
+    ttr = _ttr()
+    m = 32
+    g = torch.Generator(device="cpu").manual_seed(9)
+    u, _ = torch.linalg.qr(torch.randn(m, m, generator=g, dtype=torch.float64))
+    sig = torch.logspace(0, -2.5, m, dtype=torch.float64)
+    z = torch.randn(n, m, generator=g, dtype=torch.float32).to(gpu)
+    z = z / torch.linalg.vector_norm(z, dim=0, keepdim=True)
+    a_t = (z.double() @ (u * sig).T.to(gpu)).float()
+    a = a_t.t()
+    w = ttr.gram_rows(a, "auto").cpu().numpy()
+    ad = a_t.double().cpu().numpy()
+    ref = np.sort(np.linalg.eigvalsh(ad.T @ ad))[::-1]
+    got = np.sort(np.linalg.eigvalsh(0.5 * (w + w.T)))[::-1]
+    np.testing.assert_allclose(got, ref, rtol=1e-4)
+
+
+def test_gram_rows_exact_is_deterministic(gpu):
+    ttr = _ttr()
+    a = _randn_cm(32, 3 << 18, 21, gpu)
+    w1 = ttr.gram_rows(a, "auto").cpu().numpy()
+    w2 = ttr.gram_rows(a, "auto").cpu().numpy()
+    np.testing.assert_array_equal(w1, w2)
