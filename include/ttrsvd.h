@@ -19,13 +19,14 @@
 extern "C" {
 #endif
 
-#define TTRSVD_ABI_VERSION 3
+#define TTRSVD_ABI_VERSION 4
 #define TT_MAX_ORDER 16
 #define TT_MAX_SMALL 128 /* largest Gram / Jacobi size handled on chip */
 #define TT_MLP_INPUTS 8    /* probe features per unfolding (tt_probe_features) */
 #define TT_MLP_OUTPUTS 3   /* predicted log2 rank / 10, log2 oversampling / 5, power iterations / 2 */
 #define TT_MLP_PARAMS 4931 /* 8 -> 64 -> 64 -> 3 ReLU network, packed W1 b1 W2 b2 W3 b3 */
 #define TT_PROBE_COLS 16   /* Gaussian probe columns behind the features */
+#define TT_LEARNED_MAX_S 32 /* largest oversampling the learned predictor may choose */
 
 /* Status codes.  The reference aborts through assert() on every library status
  * (e.g. ttdecomposition/high_order_GPUs/ttdec6_singleGPU.cu:826-831); here every failure
@@ -84,7 +85,10 @@ enum {
    * pointers unless TT_FLAG_HOST_IO is also set.  Replaces ttdec_half_lu_host_6
    * (ttdecomposition/high_order_GPUs/ttdec6_singleGPU.cu:656-796; its per-slice Gram at :567
    * restarts the accumulation with beta = 0 on every slice, here the slices are summed). */
-  TT_FLAG_HOST_STREAM = 256
+  TT_FLAG_HOST_STREAM = 256,
+  /* eps > 0: fail with TT_ERR_RANK when a rank bound keeps the error above eps
+   * (tt_stats.eps_unmet > 0) instead of returning TT_OK with est_rel_err > eps. */
+  TT_FLAG_STRICT_EPS = 512
 };
 
 typedef struct tt_opts {
@@ -126,6 +130,12 @@ typedef struct tt_stats {
   int step_ks[TT_MAX_ORDER];       /* sketch width finally used per unfolding (0: exact step) */
   int step_power[TT_MAX_ORDER];    /* power iterations finally used per unfolding */
   int step_attempts[TT_MAX_ORDER]; /* EDrSVD attempts per unfolding */
+  /* eps > 0: unfoldings whose rank bound (the caller's rank, or the sketch-width limit
+   * TT_MAX_SMALL of a randomized step) stopped the truncation with more than the step's
+   * budget delta^2 = eps^2 ||X||^2 / (d - 1) discarded.  Nonzero means est_rel_err > eps: the
+   * tolerance was not met (the call still returns TT_OK with the best decomposition within
+   * the bounds; TT_FLAG_STRICT_EPS turns this into TT_ERR_RANK). */
+  int eps_unmet;
 } tt_stats;
 
 /* Bulk pass kinds reported in tt_stats.pass_*. */

@@ -21,7 +21,7 @@ import numpy as np
 from . import _lib
 from ._lib import (TT_FLAG_ADAPTIVE_KS, TT_FLAG_CHECK_FINITE, TT_FLAG_HOST_IO, TT_FLAG_HOST_STREAM,
                    TT_FLAG_IDENTITY_GAUGE,
-                   TT_FLAG_KEEP_SIGMA, TT_FLAG_LEARNED, TT_FLAG_NO_FOLD, TT_GEMM_AUTO, TT_GEMM_FP32, TT_GEMM_TC,
+                   TT_FLAG_KEEP_SIGMA, TT_FLAG_LEARNED, TT_FLAG_NO_FOLD, TT_FLAG_STRICT_EPS, TT_GEMM_AUTO, TT_GEMM_FP32, TT_GEMM_TC,
                    TT_METHOD_EDRSVD, TT_METHOD_EXACT, TTError, check)
 
 __all__ = [
@@ -110,6 +110,7 @@ class Result:
     step_ks: list = field(default_factory=list)
     step_power: list = field(default_factory=list)
     step_attempts: list = field(default_factory=list)
+    eps_unmet: int = 0  # eps > 0: unfoldings whose rank bound kept the discarded energy above budget
 
 
 def _opts(gemm, method, oversample, power_iters, seed, flags, max_sweeps):
@@ -184,7 +185,8 @@ def _run(ring: bool, x, ranks, gemm="auto", method="edrsvd", oversample=8, power
     return Result(cores=cores, ms=st.ms, sigmas=sig, ranks=list(st.ranks[: len(ranks)]),
                   kernels=st.kernels, jacobi_sweeps=st.jacobi_sweeps, est_rel_err=st.est_rel_err,
                   passes=st.passes, fallbacks=st.fallbacks, step_ks=list(st.step_ks[:ns]),
-                  step_power=list(st.step_power[:ns]), step_attempts=list(st.step_attempts[:ns]))
+                  step_power=list(st.step_power[:ns]), step_attempts=list(st.step_attempts[:ns]),
+                  eps_unmet=int(st.eps_unmet))
 
 
 def tt_svd(x, ranks, **kw) -> Result:
@@ -193,7 +195,9 @@ def tt_svd(x, ranks, **kw) -> Result:
     method ('edrsvd' | 'exact'), oversample, power_iters, seed, flags, max_sweeps, eps.
     With eps > 0 the ranks are upper bounds and every unfolding is truncated to the smallest
     rank whose discarded energy is <= eps^2 ||X||^2 / (d - 1) (TT-SVD delta-truncation);
-    Result.ranks holds the ranks chosen and Result.est_rel_err the implied error bound.
+    Result.ranks holds the ranks chosen and Result.est_rel_err the implied error bound;
+    Result.eps_unmet > 0 says a rank bound (the caller's, or the 128-column sketch limit) kept the
+    bound above eps (flags |= TT_FLAG_STRICT_EPS makes that an error instead).
     stream=True (NumPy input, fixed ranks): the first unfolding is streamed from host memory in
     chunks (set_stream_chunk) instead of being copied to the device whole."""
     return _run(False, x, ranks, **kw)

@@ -17,7 +17,7 @@ TT_GEMM_AUTO, TT_GEMM_TC, TT_GEMM_FP32 = 0, 1, 2
 TT_METHOD_EDRSVD, TT_METHOD_EXACT = 0, 1
 TT_FLAG_HOST_IO, TT_FLAG_CHECK_FINITE, TT_FLAG_NO_FOLD, TT_FLAG_IDENTITY_GAUGE, TT_FLAG_KEEP_SIGMA = 1, 2, 4, 8, 16
 TT_FLAG_PROFILE = 32
-TT_FLAG_ADAPTIVE_KS, TT_FLAG_LEARNED, TT_FLAG_HOST_STREAM = 64, 128, 256
+TT_FLAG_ADAPTIVE_KS, TT_FLAG_LEARNED, TT_FLAG_HOST_STREAM, TT_FLAG_STRICT_EPS = 64, 128, 256, 512
 TT_MLP_INPUTS, TT_MLP_OUTPUTS, TT_MLP_PARAMS, TT_PROBE_COLS = 8, 3, 4931, 16
 TT_PASS_GRAM, TT_PASS_SKETCH, TT_PASS_PROJECT, TT_PASS_OTHER = 0, 1, 2, 3
 PASS_NAMES = ["gram", "sketch", "project", "other"]
@@ -59,6 +59,7 @@ class TTStats(C.Structure):
         ("top_kind", C.c_int), ("top_step", C.c_int), ("top_ms", C.c_double), ("top_bytes", C.c_double),
         ("passes", C.c_int), ("fallbacks", C.c_int), ("step_ks", C.c_int * TT_MAX_ORDER),
         ("step_power", C.c_int * TT_MAX_ORDER), ("step_attempts", C.c_int * TT_MAX_ORDER),
+        ("eps_unmet", C.c_int),
     ]
 
 

@@ -223,7 +223,7 @@ struct Plan {
   std::vector<int> r;
   std::vector<Step> steps;
   long long total = 0;
-  size_t max_data = 0, max_omega = 0, max_y = 0, max_bt = 0, max_core = 0, max_ws = 0;
+  size_t max_data = 0, max_omega = 0, max_y = 0, max_y0 = 0, max_bt = 0, max_core = 0, max_ws = 0;
   size_t max_ef = (size_t)TT_MAX_SMALL * TT_MAX_SMALL;  // FP32 basis (m x r or ks x r)
   int max_small = 0;
   int last_rows = 1;  // rows per mode index of the data left for the last core
@@ -306,7 +306,10 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
       st.ks = (int)mn;
     } else {
       st.path = PATH_RAND;
-      st.ks = (int)std::min<long long>({(long long)st.r_eff + s, mn, (long long)TT_MAX_SMALL});
+      // The learned form may pick oversampling up to TT_LEARNED_MAX_S: its sketch width limit
+      // makes room for that.
+      const int s_cap = (o.flags & TT_FLAG_LEARNED) ? std::max(s, TT_LEARNED_MAX_S) : s;
+      st.ks = (int)std::min<long long>({(long long)st.r_eff + s_cap, mn, (long long)TT_MAX_SMALL});
       if (st.ks < st.r_eff) {
         set_error(TT_ERR_UNSUPPORTED, "step %d: rank %d above the sketch limit %d", k, st.r_eff, TT_MAX_SMALL);
         return TT_ERR_UNSUPPORTED;
@@ -337,7 +340,8 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
     P.max_small = std::max(P.max_small, std::max(st.ks, (int)std::min<long long>(mn, TT_MAX_SMALL)));
     if (st.path == PATH_RAND) {
       P.max_omega = std::max<size_t>(P.max_omega, (size_t)st.cols * st.ks);
-      P.max_y = std::max<size_t>(P.max_y, (size_t)st.m * st.ks);
+      P.max_y = std::max<size_t>(P.max_y, (size_t)st.m * std::max(st.ks, TT_PROBE_COLS));
+      if (o.flags & TT_FLAG_LEARNED) P.max_y0 = std::max<size_t>(P.max_y0, (size_t)st.m * TT_PROBE_COLS);
       P.max_bt = std::max<size_t>(P.max_bt, (size_t)st.cols * st.ks);
       // the adaptive modes run narrower sketches (and the probe) within the same buffers
       const bool narrow = (o.flags & (TT_FLAG_ADAPTIVE_KS | TT_FLAG_LEARNED)) != 0;
@@ -370,6 +374,8 @@ struct Bufs {
   float* omega = nullptr;
   double* yd = nullptr;
   float* yf = nullptr;
+  double* y0 = nullptr;     // learned probe Y0 (m x TT_PROBE_COLS, FP64)
+  double* resid = nullptr;  // per probe column ||(I - QQ^T) y0_j||^2
   float* bt = nullptr;
   float* corebuf = nullptr;
   float* ef = nullptr;
@@ -402,6 +408,8 @@ size_t plan_bytes(const Plan& P, bool host_io) {
   add(P.max_omega * sizeof(float));
   add(P.max_y * sizeof(double));
   add(P.max_y * sizeof(float));
+  add(P.max_y0 * sizeof(double));
+  add(TT_PROBE_COLS * sizeof(double));
   add(P.max_bt * sizeof(float));
   add(P.max_core * sizeof(float));
   add(P.max_ef * sizeof(float));
@@ -435,6 +443,8 @@ int carve(tt_ctx* c, const Plan& P, bool host_io, Bufs& B, Arena& ws) {
   B.omega = a.take<float>(std::max<size_t>(P.max_omega, 1));
   B.yd = a.take<double>(std::max<size_t>(P.max_y, 1));
   B.yf = a.take<float>(std::max<size_t>(P.max_y, 1));
+  B.y0 = a.take<double>(std::max<size_t>(P.max_y0, 1));
+  B.resid = a.take<double>(TT_PROBE_COLS);
   B.bt = a.take<float>(std::max<size_t>(P.max_bt, 1));
   B.corebuf = a.take<float>(std::max<size_t>(P.max_core, 1));
   B.ef = a.take<float>(P.max_ef);
@@ -611,6 +621,8 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
   // the eigenvalues back to the host, and the rest of the plan is rebuilt with the chosen rank.
   const bool adaptive = o.eps > 0.0;
   double delta2 = 0.0, energy = 0.0, xnorm2 = 0.0, tail_sum = 0.0;
+  int eps_unmet = 0;  // steps whose rank bound left more than delta^2 discarded
+  bool energy_exact = true;  // `energy` is exact (false after a step judged on the probe estimate)
   // A first step with an exact Gram of the whole tensor gives ||X||^2 as its eigenvalue sum
   // (the trace); otherwise one FP64 norm pass runs first.
   const bool norm_from_gram = adaptive && !P.steps.empty() && !stream &&
@@ -680,25 +692,34 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
     int rq = st.r_req, re = st.r_eff;
     int nout = st.n_out;                            // rows of the next data (compacted)
     // Adaptive rank of this step from the first `nev` eigenvalues in B.evals: the smallest r
-    // whose discarded energy (energy of the unfolding minus the kept eigenvalues) is <= delta^2.
-    auto decide = [&](int nev) -> int {
+    // whose discarded energy, outside + sum_{i >= r} lambda_i, is <= delta^2.  `outside` is the
+    // energy outside the eigen-decomposed subspace: 0 for an exact step (its Gram holds the whole
+    // unfolding), the carried energy minus every eigenvalue for a plain EDrSVD attempt, and the
+    // probe estimate for a learned attempt.
+    auto decide = [&](int nev, double outside) -> int {
       if (!adaptive) return TT_OK;
       std::vector<double> lam((size_t)nev);
       TT_CUDA(cudaMemcpyAsync(lam.data(), B.evals, sizeof(double) * nev, cudaMemcpyDeviceToHost, s));
       TT_CUDA(cudaStreamSynchronize(s));
+      double inside = 0.0;
+      for (double v : lam) inside += std::max(v, 0.0);
       if (norm_from_gram && k == 0) {
-        xnorm2 = 0.0;
-        for (double v : lam) xnorm2 += std::max(v, 0.0);
+        xnorm2 = inside;
         energy = xnorm2;
         delta2 = o.eps * o.eps * xnorm2 / (double)(P.d - 1);
       }
       const int cap = std::min(rmax[k + 1], std::min(nev, re));
       int r = 0;
-      double tail = energy;
-      while (r < cap && (r == 0 || tail > delta2)) tail -= std::max(lam[(size_t)r++], 0.0);
+      double tail = std::max(outside, 0.0) + inside, kept = 0.0;
+      while (r < cap && (r == 0 || tail > delta2)) {
+        const double l = std::max(lam[(size_t)r++], 0.0);
+        tail -= l;
+        kept += l;
+      }
       tail = std::max(tail, 0.0);
+      if (tail > delta2 * (1.0 + 1e-12)) ++eps_unmet;  // the bound stopped the truncation above delta
       tail_sum += tail;
-      energy = std::max(energy - tail, 0.0);
+      energy = kept;  // energy of the next data
       rq = re = nout = r;
       st.r_req = st.r_eff = st.n_out = r;
       st.next_elems = (long long)r * cols;
@@ -800,7 +821,8 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
-      TT_TRY(decide((int)m));
+      TT_TRY(decide((int)m, 0.0));
+      energy_exact = true;
       // An adaptive rank that keeps every row makes the step a rotation: fold it like a
       // planned full-rank step (the next step's geometry is the same either way).
       const bool fold = st.fold || (adaptive && !ring1 && !st.perm231 && rq == m && re == m && rin == rcore &&
@@ -836,7 +858,8 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       TT_TRY(launch_syev(B.w, (int)cols, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(cols, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
-      TT_TRY(decide((int)cols));
+      TT_TRY(decide((int)cols, 0.0));
+      energy_exact = true;
       TT_TRY(launch_inv_sigma(B.evals, re, B.colscale, 1e-30, s));
       float* ubuf = B.corebuf;
       TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * m * cols * rq, 4.0 * m * cols + 4.0 * m * rq, [&] {
@@ -859,7 +882,9 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
     } else {  // PATH_RAND
       // One EDrSVD attempt with sketch width ksa and pwa power iterations: Q (B.yf), B^T
       // (B.bt), the eigen-decomposition of B B^T (B.evals / B.evecs), sigma stored.
-      auto attempt = [&](int ksa, int pwa, unsigned sid) -> int {
+      // tc_b: form B on the tensor cores even with adaptive ranks (a learned attempt judged by
+      // the probe estimate, which does not read B's energy).
+      auto attempt = [&](int ksa, int pwa, unsigned sid, bool tc_b) -> int {
         TT_TRY(launch_gaussian(B.omega, cols, ksa, cols, o.seed, sid, s));
         const double fl_pass = 2.0 * m * cols * ksa;
         const double by_pass = 4.0 * m * cols + 4.0 * cols * ksa;
@@ -892,7 +917,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         // engine (round-to-nearest FMA).
         TT_TRY(pass.run(TT_PASS_PROJECT, fl_pass, by_pass, [&] {
           return launch_project(cur, m, cols, B.yf, ksa, m, B.bt, ksa, OUT_ROWMAJOR, 1, 1,
-                                adaptive ? TT_GEMM_FP32 : engine, ws, c->dstat, s);
+                                (adaptive && !tc_b) ? TT_GEMM_FP32 : engine, ws, c->dstat, s);
         }));
         // Gram of the small factor B (ksa x cols, column-major = B^T row-major): the input of
         // the eigen-based small SVD (TT3O:717), on the tensor cores for long B.
@@ -913,21 +938,45 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         ++natt;
         return TT_OK;
       };
-      // Energy outside the attempt's subspace plus nothing discarded yet: ||A||^2 - ||B||^2.
+      double step_outside = 0.0;  // energy outside the accepted attempt's subspace
+      bool learned_step = false;   // accepted on the probe estimate (B and its energy from TF32 tiles)
+      // Energy outside the attempt's subspace: ||A||^2 - ||B||^2, with ||A||^2 the exact carried
+      // energy (recomputed by one FP64 norm pass when a learned step left an estimate).
       auto outside = [&](int ksa, double* out) -> int {
+        if (!energy_exact) {
+          const size_t mk = ws.mark();
+          double* acc = ws.take<double>(2);
+          if (!acc) {
+            set_error(TT_ERR_NOMEM, "norm accumulator");
+            return TT_ERR_NOMEM;
+          }
+          TT_CUDA(cudaMemsetAsync(acc, 0, 2 * sizeof(double), s));
+          TT_TRY(launch_diff_norm(cur, nullptr, m * cols, acc, s));
+          double h[2];
+          TT_CUDA(cudaMemcpyAsync(h, acc, sizeof(h), cudaMemcpyDeviceToHost, s));
+          TT_CUDA(cudaStreamSynchronize(s));
+          ws.reset(mk);
+          energy = h[1];
+          energy_exact = true;
+        }
         std::vector<double> lam((size_t)ksa);
         TT_CUDA(cudaMemcpyAsync(lam.data(), B.evals, sizeof(double) * ksa, cudaMemcpyDeviceToHost, s));
         TT_CUDA(cudaStreamSynchronize(s));
         double kept = 0.0;
         for (double v : lam) kept += std::max(v, 0.0);
         *out = energy - kept;
+        step_outside = *out;
         return TT_OK;
       };
       const int ks_cap = st.ks;
       int ks = ks_cap, pw = o.power_iters;
       const bool adapt_ks = adaptive && (o.flags & (TT_FLAG_ADAPTIVE_KS | TT_FLAG_LEARNED));
       if (!adapt_ks) {
-        TT_TRY(attempt(ks, pw, (unsigned)k));
+        TT_TRY(attempt(ks, pw, (unsigned)k, false));
+        if (adaptive) {
+          double out = 0.0;
+          TT_TRY(outside(ks, &out));
+        }
       } else {
         bool done = false;
         int ks_next = std::min(ks_cap, 16 + std::max(0, o.oversample));
@@ -937,17 +986,19 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
             set_error(TT_ERR_ARG, "TT_FLAG_LEARNED without a predictor (tt_ctx_set_predictor)");
             return TT_ERR_ARG;
           }
-          // probe: Y0 = A Omega0 (TT_PROBE_COLS columns), eigenvalues of Y0^T Y0, features
+          // probe: Y0 = A Omega0 (TT_PROBE_COLS columns) on the FP32 engine (exact products, FP64
+          // sums), eigenvalues of Y0^T Y0, features.  Y0 is kept: it also measures the energy the
+          // attempt leaves outside its subspace (the a-posteriori estimate below).
           float* feat = c->pred + TT_MLP_PARAMS;
           float* yout = feat + TT_MLP_INPUTS;
           TT_TRY(launch_gaussian(B.omega, cols, TT_PROBE_COLS, cols, o.seed, 0x40000000u + (unsigned)k, s));
           TT_TRY(pass.run(TT_PASS_SKETCH, 2.0 * m * cols * TT_PROBE_COLS, 4.0 * m * cols + 4.0 * cols * TT_PROBE_COLS,
                           [&] {
-                            return launch_sketch(cur, m, cols, B.omega, TT_PROBE_COLS, 1, cols, B.yd, engine, ws,
-                                                 c->dstat, s);
+                            return launch_sketch(cur, m, cols, B.omega, TT_PROBE_COLS, 1, cols, B.y0, TT_GEMM_FP32,
+                                                 ws, c->dstat, s);
                           }));
           ++npasses;
-          TT_TRY(launch_f64_to_f32_cols(B.yd, m, m, TT_PROBE_COLS, B.yf, m, TT_PROBE_COLS, s));
+          TT_TRY(launch_f64_to_f32_cols(B.y0, m, m, TT_PROBE_COLS, B.yf, m, TT_PROBE_COLS, s));
           TT_TRY(launch_gram(B.yf, m, TT_PROBE_COLS, 1, m, B.w, true, ws, s));
           TT_TRY(launch_syev(B.w, TT_PROBE_COLS, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
           const double tol = energy > 0.0 ? std::sqrt(delta2 / energy) : 1.0;
@@ -962,11 +1013,27 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
           pw = (int)std::lround(std::min(std::max(2.0 * (double)hy[2], 0.0), 3.0));
           ks = (int)std::min<double>((double)ks_cap, std::max(1.0, rh + sh));
           if (10 * ks >= 9 * ks_cap) ks = ks_cap;  // within 10 % of the width limit: use the limit
-          TT_TRY(attempt(ks, pw, sid));
-          double out = 0.0;
-          TT_TRY(outside(ks, &out));
-          if (out <= delta2 || ks >= ks_cap) {
+          // B on the tensor cores unless their rounding noise in B (TF32 operands: relative RMS
+          // ~2e-4 per element, of which the fraction ks/m lands in B) could reach 5 % of the budget.
+          const bool tc_b = engine == TT_GEMM_TC && (double)ks / (double)m * 4e-8 * energy <= 0.05 * delta2;
+          TT_TRY(attempt(ks, pw, sid, tc_b));
+          // A-posteriori estimate of the energy outside range(Q) (Halko, Martinsson & Tropp 2011,
+          // sec. 4.3): for Gaussian omega, E||(I - QQ^T) A omega||^2 = ||(I - QQ^T) A||_F^2, so the
+          // mean over the probe columns is unbiased; two standard errors of the mean are added.
+          TT_TRY(launch_probe_resid(B.yf, m, ks, m, B.y0, m, TT_PROBE_COLS, B.resid, s));
+          double hr[TT_PROBE_COLS];
+          TT_CUDA(cudaMemcpyAsync(hr, B.resid, sizeof(hr), cudaMemcpyDeviceToHost, s));
+          TT_CUDA(cudaStreamSynchronize(s));
+          double mean = 0.0, var = 0.0;
+          for (double v : hr) mean += v;
+          mean /= TT_PROBE_COLS;
+          for (double v : hr) var += (v - mean) * (v - mean);
+          var /= (TT_PROBE_COLS - 1);
+          const double est = mean + 2.0 * std::sqrt(var / TT_PROBE_COLS);
+          if (est <= delta2 || ks >= ks_cap) {
             done = true;
+            step_outside = est;
+            learned_step = tc_b;
           } else {
             ++nfall;
             ks_next = std::min(ks_cap, std::max(2 * ks, ks_next));
@@ -976,7 +1043,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         while (!done) {
           ks = ks_next;
           pw = o.power_iters;
-          TT_TRY(attempt(ks, pw, sid + 0x1000u * (unsigned)natt));
+          TT_TRY(attempt(ks, pw, sid + 0x1000u * (unsigned)natt, false));
           double out = 0.0;
           TT_TRY(outside(ks, &out));
           if (out <= delta2 || ks >= ks_cap) done = true;
@@ -986,7 +1053,8 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       step_ks[k] = ks;
       step_pw[k] = pw;
       step_att[k] = natt - natt0;
-      TT_TRY(decide(ks));
+      TT_TRY(decide(ks, step_outside));
+      energy_exact = !learned_step;
       // core = Q E_r with canonical column signs (E's columns follow)
       float* ubuf = B.corebuf;
       TT_TRY(launch_small_nn(B.yf, m, ks, m, B.evecs, rq, ks, nullptr, re, ubuf, m, s));
@@ -1038,6 +1106,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
     stats->est_rel_err = adaptive && xnorm2 > 0.0 ? std::sqrt(tail_sum / xnorm2) : 0.0;
     stats->passes = npasses;
     stats->fallbacks = nfall;
+    stats->eps_unmet = eps_unmet;
     for (int k = 0; k < nsteps && k < TT_MAX_ORDER; ++k) {
       stats->step_ks[k] = step_ks[(size_t)k];
       stats->step_power[k] = step_pw[(size_t)k];
@@ -1076,6 +1145,12 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
   if (c->hstat->code != 0) {
     set_error(c->hstat->code, "device status %d (detail %d)", c->hstat->code, c->hstat->detail);
     return c->hstat->code;
+  }
+  if (eps_unmet > 0 && (o.flags & TT_FLAG_STRICT_EPS)) {
+    set_error(TT_ERR_RANK, "eps = %g not met: %d unfolding(s) reached their rank bound with more than delta^2 "
+              "discarded (est. rel. error %.3e)", o.eps, eps_unmet,
+              xnorm2 > 0.0 ? std::sqrt(tail_sum / xnorm2) : 0.0);
+    return TT_ERR_RANK;
   }
   return TT_OK;
 }

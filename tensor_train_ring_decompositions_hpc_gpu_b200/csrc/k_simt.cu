@@ -2668,6 +2668,54 @@ int launch_canon_cols(float* u, long long m, int r, long long ldu, double* comp,
   return TT_OK;
 }
 
+// Residual energies of the probe columns outside range(Q): out[j] = ||y_j - Q (Q^T y_j)||^2,
+// Q (m x ks, FP32, ldq, orthonormal columns), Y0 (m x q, FP64, ldy).  One block per probe
+// column; FP64 throughout, so the difference of two nearly equal energies is not formed.
+__global__ void __launch_bounds__(256) k_probe_resid(const float* __restrict__ q, long long m, int ks, long long ldq,
+                                                     const double* __restrict__ y0, long long ldy,
+                                                     double* __restrict__ out) {
+  extern __shared__ double sh_pr[];  // c[ks] + 8 warp partials
+  double* c = sh_pr;
+  double* red = sh_pr + ks;
+  const int j = blockIdx.x, tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const double* y = y0 + (long long)j * ldy;
+  // c = Q^T y: warp w takes columns w, w + 8, ...
+  for (int a = warp; a < ks; a += 8) {
+    const float* qa = q + (long long)a * ldq;
+    double t = 0.0;
+    for (long long i = lane; i < m; i += 32) t = fma((double)qa[i], y[i], t);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t += __shfl_xor_sync(0xffffffffu, t, o);
+    if (lane == 0) c[a] = t;
+  }
+  __syncthreads();
+  double acc = 0.0;
+  for (long long i = tid; i < m; i += blockDim.x) {
+    double r = y[i];
+    for (int a = 0; a < ks; ++a) r = fma(-(double)q[i + (long long)a * ldq], c[a], r);
+    acc = fma(r, r, acc);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+  if (lane == 0) red[warp] = acc;
+  __syncthreads();
+  if (tid == 0) {
+    double t = 0.0;
+    for (int w = 0; w < 8; ++w) t += red[w];
+    out[j] = t;
+  }
+}
+
+int launch_probe_resid(const float* q, long long m, int ks, long long ldq, const double* y0, long long ldy, int nq,
+                       double* out, cudaStream_t s) {
+  if (nq <= 0) return TT_OK;
+  const size_t shm = (size_t)(ks + 8) * sizeof(double);
+  k_probe_resid<<<nq, 256, shm, s>>>(q, m, ks, ldq, y0, ldy, out);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  return TT_OK;
+}
+
 __global__ void k_check_finite(const float* __restrict__ x, long long count, int* flag) {
   int bad = 0;
   for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < count;

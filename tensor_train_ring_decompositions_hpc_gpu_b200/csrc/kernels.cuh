@@ -102,6 +102,11 @@ int launch_ring_core1(const float* u, int n1, int r0, int r1, float* core, cudaS
 int launch_canon_cols(float* u, long long m, int r, long long ldu, double* comp, int K,
                       long long ldc, cudaStream_t s);
 
+// out[j] = ||y_j - Q Q^T y_j||^2 (FP64) for the nq columns of Y0 (m x nq, FP64, ldy);
+// Q (m x ks, FP32, ldq) with orthonormal columns.
+int launch_probe_resid(const float* q, long long m, int ks, long long ldq, const double* y0, long long ldy, int nq,
+                       double* out, cudaStream_t s);
+
 // NaN/Inf scan; *flag set to 1 when found.
 int launch_check_finite(const float* x, long long count, int* flag, cudaStream_t s);
 

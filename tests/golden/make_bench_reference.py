@@ -86,7 +86,7 @@ def chain_error(x: np.ndarray, wl: dict):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("workload", choices=["tt6", "tr6"])
+    ap.add_argument("workload", choices=["tt6", "tr6", "tt3"])
     ap.add_argument("--seed", type=int, default=20261203)
     args = ap.parse_args()
     t0 = time.time()

@@ -303,3 +303,21 @@ def test_host_stream_rejects_unsupported(gpu):
     big = np.ones((200, 4, 4), dtype=np.float32)  # first unfolding 200 x 16: randomized step
     with pytest.raises(ttr.TTError):
         ttr.tt_svd(big, [1, 4, 4, 1], stream=True)
+
+
+@pytest.mark.parametrize("gemm", ["fp32", "auto"])
+def test_adaptive_eps_reports_unmet_tolerance(gpu, gemm):
+    """A rank bound below the eps-rank: the call says so (eps_unmet, est_rel_err > eps) instead
+    of a silent success, and TT_FLAG_STRICT_EPS turns it into TT_ERR_RANK."""
+    ttr = _ttr()
+    import torch
+    shape = [16, 12, 10, 14]
+    x = oracle.make_tt_tensor(shape, [1, 6, 8, 5, 1], 1e-5, seed=23)
+    xt = torch.from_numpy(np.ascontiguousarray(x.ravel(order="F"))).to(gpu)
+    ok = ttr.tt_svd(xt, [1, 16, 16, 16, 1], gemm=gemm, eps=1e-3, shape=shape)
+    assert ok.eps_unmet == 0 and ok.est_rel_err <= 1e-3 * 1.001
+    low = ttr.tt_svd(xt, [1, 3, 3, 3, 1], gemm=gemm, eps=1e-3, shape=shape)
+    assert low.eps_unmet > 0 and low.est_rel_err > 1e-3
+    with pytest.raises(ttr.TTError) as ei:
+        ttr.tt_svd(xt, [1, 3, 3, 3, 1], gemm=gemm, eps=1e-3, shape=shape, flags=ttr.TT_FLAG_STRICT_EPS)
+    assert ei.value.code == 3  # TT_ERR_RANK

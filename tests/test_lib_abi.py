@@ -41,7 +41,7 @@ def test_reference_cpp_symbols_exported():
 def test_abi_version_and_defaults():
     from tensor_train_ring_decompositions_hpc_gpu_b200 import _lib
     lib = _lib.load()
-    assert lib.tt_abi_version() == 3
+    assert lib.tt_abi_version() == 4
     o = _lib.TTOpts()
     lib.tt_default_opts(C.byref(o))
     assert o.oversample == 8 and o.gemm == 0 and o.max_sweeps == 40
