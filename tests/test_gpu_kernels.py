@@ -145,13 +145,14 @@ def test_cholqr2_rank_deficient_zeroes_dependent_columns(gpu):
 
 
 @pytest.mark.parametrize("N", [1, 2, 5, 24, 32, 33, 40, 63, 64, 65, 96, 128])
-def test_syev(gpu, N):
+@pytest.mark.parametrize("gram", [False, True])
+def test_syev(gpu, N, gram):
     import torch
     ttr = _ttr()
     rng = np.random.default_rng(N)
     b = rng.standard_normal((N, N + 7))
     w = b @ b.T
-    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu))
+    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu), gram=gram)
     ev = ev.cpu().numpy()
     vec = vec.cpu().numpy()
     ref = np.sort(np.linalg.eigvalsh(w))[::-1]
@@ -162,7 +163,8 @@ def test_syev(gpu, N):
 
 
 @pytest.mark.parametrize("N,rank", [(40, 12), (64, 1), (32, 0), (96, 30)])
-def test_syev_rank_deficient_terminates(gpu, N, rank):
+@pytest.mark.parametrize("gram", [False, True])
+def test_syev_rank_deficient_terminates(gpu, N, rank, gram):
     """Gram matrices of rank-deficient sketches have eigenvalues at the FP64 rounding floor;
     the sweep loop must still converge (rotations below that floor are skipped)."""
     import torch
@@ -170,7 +172,7 @@ def test_syev_rank_deficient_terminates(gpu, N, rank):
     rng = np.random.default_rng(N + rank)
     b = rng.standard_normal((N, rank))
     w = b @ b.T
-    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu))
+    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu), gram=gram)
     ev = ev.cpu().numpy()
     vec = vec.cpu().numpy()
     ref = np.sort(np.linalg.eigvalsh(w))[::-1]
@@ -181,7 +183,8 @@ def test_syev_rank_deficient_terminates(gpu, N, rank):
 
 
 @pytest.mark.parametrize("N", [16, 40, 96])
-def test_syev_asymmetric_rounding_converges(gpu, N):
+@pytest.mark.parametrize("gram", [False, True])
+def test_syev_asymmetric_rounding_converges(gpu, N, gram):
     """Tensor-core Grams are symmetric only to FP32 rounding; the solver symmetrises its input
     and must converge to the eigen-decomposition of (W + W^T) / 2."""
     import torch
@@ -190,7 +193,7 @@ def test_syev_asymmetric_rounding_converges(gpu, N):
     b = rng.standard_normal((N, 3 * N))
     w = b @ b.T
     w_in = w + 1e-7 * np.abs(w).max() * np.triu(rng.standard_normal((N, N)), 1)
-    ev, vec, sweeps = ttr.syev(torch.from_numpy(w_in).to(gpu))
+    ev, vec, sweeps = ttr.syev(torch.from_numpy(w_in).to(gpu), gram=gram)
     ev = ev.cpu().numpy()
     vec = vec.cpu().numpy()
     ws = 0.5 * (w_in + w_in.T)
@@ -201,7 +204,8 @@ def test_syev_asymmetric_rounding_converges(gpu, N):
 
 
 @pytest.mark.parametrize("N", [3, 16, 31])
-def test_syev_warp_sizes_and_clusters(gpu, N):
+@pytest.mark.parametrize("gram", [False, True])
+def test_syev_warp_sizes_and_clusters(gpu, N, gram):
     """N <= 32 runs the one-warp register-resident solver; clustered (repeated) eigenvalues."""
     import torch
     ttr = _ttr()
@@ -209,7 +213,7 @@ def test_syev_warp_sizes_and_clusters(gpu, N):
     q, _ = np.linalg.qr(rng.standard_normal((N, N)))
     lam = np.repeat(np.array([3.0, 1.0, 1e-3, 0.0]), (N + 3) // 4)[:N]
     w = (q * lam) @ q.T
-    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu))
+    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu), gram=gram)
     ev = ev.cpu().numpy()
     vec = vec.cpu().numpy()
     np.testing.assert_allclose(ev, np.sort(lam)[::-1], atol=1e-12)
@@ -219,14 +223,15 @@ def test_syev_warp_sizes_and_clusters(gpu, N):
 
 
 @pytest.mark.parametrize("N", [20, 32, 40])
-def test_syev_graded_spectrum_relative_accuracy(gpu, N):
+@pytest.mark.parametrize("gram", [False, True])
+def test_syev_graded_spectrum_relative_accuracy(gpu, N, gram):
     import torch
     ttr = _ttr()
     rng = np.random.default_rng(1)
     q, _ = np.linalg.qr(rng.standard_normal((N, N)))
     lam = np.logspace(0, -10, N)
     w = (q * lam) @ q.T
-    ev, _, _ = ttr.syev(torch.from_numpy(w).to(gpu))
+    ev, _, _ = ttr.syev(torch.from_numpy(w).to(gpu), gram=gram)
     keep = lam >= 1e-6  # FP64 rounding of W (1e-16 absolute) leaves 1e-10 relative there
     np.testing.assert_allclose(ev.cpu().numpy()[keep], lam[keep], rtol=1e-8)
 
