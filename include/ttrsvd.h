@@ -334,6 +334,9 @@ float tt_ref_ttdec_half_lu_device_6(float* h_a, const int* tt_ranks, const int* 
                                     int calculate_times, int p, int cal_error);
 float tt_ref_trdec_half_lu_device_6(float* h_a, const int* tt_ranks, const int* tt_demns,
                                     int calculate_times, int p, int cal_error);
+/* ttdec_half_lu_host_6 (ttdec6_singleGPU.cu:656): host-streamed first unfolding in p slices. */
+float tt_ref_ttdec_half_lu_host_6(float* h_a, const int* tt_ranks, const int* tt_demns,
+                                  int calculate_times, int p, int cal_error);
 
 #ifdef __cplusplus
 }

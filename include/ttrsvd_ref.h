@@ -28,6 +28,14 @@ float trdec_gpu_float(float* h_tensor, int* h_n_array, int* h_r_array, double* e
 float ttdec_half_lu_device_6(float* h_A, const int* ttRanks, const int* ttDemns,
                              const int& calculateTimes, const int& p, bool calError);
 
+/* ttdecomposition/high_order_GPUs/ttdec6_singleGPU.cu:656: the tensor stays in (ideally pinned)
+ * host memory and its first unfolding is streamed in p column slices, copies overlapped with
+ * the kernels (TT_FLAG_HOST_STREAM; first unfolding of at most TT_MAX_SMALL rows).  The
+ * reference restarts its Gram accumulation on every slice (beta = 0, ttdec6_singleGPU.cu:567);
+ * here the slices are summed.  calError prints the "MSE:" line. */
+float ttdec_half_lu_host_6(float* h_A, int* ttRanks, const int* ttDemns, const int& calculateTimes, const int& p,
+                           const bool calError);
+
 /* trdecomposition/high_order_GPUs/trdec6_singleGPU.cu:827, where the TR program reuses the
  * name ttdec_half_lu_device_6; exported here as trdec_half_lu_device_6 so both can share one
  * library.  ttRanks = {r0, r1, ..., r5, r0}. */

@@ -579,6 +579,18 @@ def ttdec_half_lu_device_6(h_A, ttRanks, ttDemns, calculateTimes=1, p=64, calErr
     return float(t)
 
 
+def ttdec_half_lu_host_6(h_A, ttRanks, ttDemns, calculateTimes=1, p=8, calError=False):
+    """Order-6 TT-SVD with the tensor left in host memory and its first unfolding streamed in
+    p slices; mirrors ttdec_half_lu_host_6 (ttdec6_singleGPU.cu:656)."""
+    a = _host_f32(h_A)
+    t = lib().tt_ref_ttdec_half_lu_host_6(C.c_void_p(a.ctypes.data), _lib.int_array(ttRanks),
+                                          _lib.int_array(ttDemns), int(calculateTimes), int(p),
+                                          1 if calError else 0)
+    if t < 0:
+        raise TTError(int(-t), lib().tt_last_error().decode())
+    return float(t)
+
+
 def trdec_half_lu_device_6(h_A, ttRanks, ttDemns, calculateTimes=1, p=64, calError=False):
     """Order-6 TR-SVD; mirrors the TR ttdec_half_lu_device_6 (trdec6_singleGPU.cu:827)."""
     a = _host_f32(h_A)

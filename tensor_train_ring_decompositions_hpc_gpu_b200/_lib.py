@@ -37,7 +37,7 @@ EXPORTED = [
     "tt_cores_save", "tt_cores_header", "tt_cores_load",
     "tt_ctx_set_predictor", "tt_probe_features", "tt_mlp_forward", "tt_mlp_grad", "tt_mlp_train",
     "tt_k_permute231", "tt_ref_ttdec_gpu_float", "tt_ref_trdec_gpu_float",
-    "tt_ref_ttdec_half_lu_device_6", "tt_ref_trdec_half_lu_device_6",
+    "tt_ref_ttdec_half_lu_device_6", "tt_ref_trdec_half_lu_device_6", "tt_ref_ttdec_half_lu_host_6",
 ]
 
 
@@ -125,6 +125,7 @@ def load():
         "tt_ref_trdec_gpu_float": (C.c_float, [vp, P(i), P(i), P(d), P(C.c_float), P(C.c_float)]),
         "tt_ref_ttdec_half_lu_device_6": (C.c_float, [vp, P(i), P(i), i, i, i]),
         "tt_ref_trdec_half_lu_device_6": (C.c_float, [vp, P(i), P(i), i, i, i]),
+        "tt_ref_ttdec_half_lu_host_6": (C.c_float, [vp, P(i), P(i), i, i, i]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

@@ -64,6 +64,50 @@ double run_host(float* h_x, int d, const int* n, const int* r, bool ring, int ov
   return secs;
 }
 
+// Host-streamed TT-SVD (the tensor stays in host memory; its first unfolding is read in
+// `slices` column chunks, copies overlapped with the kernels).  Seconds or a negative status.
+double run_host_stream(float* h_x, int d, const int* n, const int* r, int slices, double* rel_err) {
+  tt_ctx* ctx = shim_ctx();
+  if (!ctx) return -1.0;
+  long long total = 1;
+  for (int k = 0; k < d; ++k) total *= n[k];
+  const long long cols = total / n[0];
+  const long long per = (cols + (slices > 0 ? slices : 1) - 1) / (slices > 0 ? slices : 1);
+  int st = tt_ctx_set_stream_chunk(ctx, (size_t)per * n[0] * sizeof(float));
+  std::vector<float*> dcores(d, nullptr);
+  for (int k = 0; k < d && st == TT_OK; ++k)
+    if (cudaMalloc(&dcores[k], sizeof(float) * (size_t)r[k] * n[k] * r[k + 1]) != cudaSuccess)
+      st = TT_ERR_NOMEM;
+  const auto t0 = std::chrono::steady_clock::now();
+  if (st == TT_OK) {
+    tt_opts o;
+    tt_default_opts(&o);
+    o.power_iters = 0;
+    o.flags |= TT_FLAG_HOST_STREAM;
+    st = tt_svd(ctx, h_x, d, n, r, &o, dcores.data(), nullptr);
+  }
+  const double secs =
+      std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+  if (st == TT_OK && rel_err) {
+    // the error check needs the tensor on the device once (outside the timed part)
+    float* dx = nullptr;
+    if (cudaMalloc(&dx, sizeof(float) * total) != cudaSuccess) {
+      st = TT_ERR_NOMEM;
+    } else {
+      if (cudaMemcpy(dx, h_x, sizeof(float) * total, cudaMemcpyHostToDevice) != cudaSuccess) st = TT_ERR_CUDA;
+      if (st == TT_OK) st = tt_rel_error(ctx, dx, d, n, r, 0, dcores.data(), rel_err);
+      cudaFree(dx);
+    }
+  }
+  for (int k = 0; k < d; ++k)
+    if (dcores[k]) cudaFree(dcores[k]);
+  if (st != TT_OK) {
+    fprintf(stderr, "ttrsvd: %s\n", tt_last_error());
+    return -(double)st;
+  }
+  return secs;
+}
+
 }  // namespace
 
 // ---- C ABI versions (pointer arguments) ----
@@ -133,6 +177,23 @@ extern "C" float tt_ref_trdec_half_lu_device_6(float* h_a, const int* tt_ranks, 
   return order6(h_a, tt_ranks, tt_demns, calculate_times, cal_error != 0, true);
 }
 
+extern "C" float tt_ref_ttdec_half_lu_host_6(float* h_a, const int* tt_ranks, const int* tt_demns,
+                                             int calculate_times, int p, int cal_error) {
+  if (calculate_times < 1) calculate_times = 1;
+  double total = 0.0;
+  for (int i = 0; i < calculate_times; ++i) {
+    double err = 0.0;
+    const double t = run_host_stream(h_a, 6, tt_demns, tt_ranks, p, cal_error ? &err : nullptr);
+    if (t < 0) return (float)t;
+    total += t;
+    if (cal_error) {
+      printf("\n*********************** MSE: %f ******************\n", err);
+      fflush(stdout);
+    }
+  }
+  return (float)(total / calculate_times);
+}
+
 // ---- C++ overloads with the reference's exact signatures ----
 float ttdec_gpu_float(float* h_tensor, int* h_n_array, int* h_r_array, double* eps,
                       float* singleError, float* singleComRatio) {
@@ -152,4 +213,9 @@ float ttdec_half_lu_device_6(float* h_A, const int* ttRanks, const int* ttDemns,
 float trdec_half_lu_device_6(float* h_A, const int* ttRanks, const int* ttDemns,
                              const int& calculateTimes, const int& p, bool calError) {
   return tt_ref_trdec_half_lu_device_6(h_A, ttRanks, ttDemns, calculateTimes, p, calError ? 1 : 0);
+}
+
+float ttdec_half_lu_host_6(float* h_A, int* ttRanks, const int* ttDemns, const int& calculateTimes, const int& p,
+                           const bool calError) {
+  return tt_ref_ttdec_half_lu_host_6(h_A, ttRanks, ttDemns, calculateTimes, p, calError ? 1 : 0);
 }

@@ -208,6 +208,11 @@ def test_reference_entry_points(gpu, capfd):
     assert t6 > 0
     out = capfd.readouterr().out
     assert "MSE:" in out
+    th = ttr.ttdec_half_lu_host_6(x6, [1, 3, 3, 3, 3, 3, 1], [6] * 6, 1, 7, True)
+    assert th > 0
+    mse = [float(line.split("MSE:")[1].split()[0]) for line in capfd.readouterr().out.splitlines()
+           if "MSE:" in line]
+    assert mse and mse[-1] < 1e-3
     xr = oracle.make_tr_tensor([6] * 6, 2, 1e-4, seed=37)
     tr = ttr.trdec_half_lu_device_6(xr, [2, 2, 4, 4, 4, 4, 2], [6] * 6, 1, 64, False)
     assert tr > 0

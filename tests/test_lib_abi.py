@@ -34,7 +34,8 @@ def test_reference_cpp_symbols_exported():
     for sig in ["ttdec_gpu_float(float*, int*, int*, double*, float*, float*)",
                 "trdec_gpu_float(float*, int*, int*, double*, float*, float*)",
                 "ttdec_half_lu_device_6(float*, int const*, int const*, int const&, int const&, bool)",
-                "trdec_half_lu_device_6(float*, int const*, int const*, int const&, int const&, bool)"]:
+                "trdec_half_lu_device_6(float*, int const*, int const*, int const&, int const&, bool)",
+                "ttdec_half_lu_host_6(float*, int*, int const*, int const&, int const&, bool)"]:
         assert sig in out, sig
 
 
