@@ -150,6 +150,17 @@ int tt_ctx_create(tt_ctx** out, int device, void* stream);
 int tt_ctx_destroy(tt_ctx* ctx);
 int tt_ctx_set_stream(tt_ctx* ctx, void* stream);
 int tt_ctx_reserve(tt_ctx* ctx, size_t bytes);
+/* Fault injection and limits (no counterpart in the reference, which asserts on every CUDA
+ * status).  tt_ctx_set_alloc_limit: workspace growth above `bytes` fails with TT_ERR_NOMEM as
+ * if cudaMalloc had failed (0 removes the limit).  tt_ctx_set_wait_limit: wall-clock limit of
+ * every pipeline wait of the TMA kernels on the context's device (ns; 0 = the default 2 s); a
+ * wait that runs out ends its kernel with TT_ERR_TIMEOUT after the CTA has drained its own
+ * copies (the drain always gets 2 s).  tt_k_wait_selftest: a kernel waiting on a barrier that
+ * nothing completes, under the same limit; returns TT_ERR_TIMEOUT. */
+int tt_ctx_set_alloc_limit(tt_ctx* ctx, size_t bytes);
+int tt_ctx_set_wait_limit(tt_ctx* ctx, unsigned long long ns);
+int tt_k_wait_selftest(tt_ctx* ctx);
+
 /* Bytes of one host-streaming chunk (TT_FLAG_HOST_STREAM; default 256 MiB, minimum one column). */
 int tt_ctx_set_stream_chunk(tt_ctx* ctx, size_t bytes);
 const char* tt_last_error(void);

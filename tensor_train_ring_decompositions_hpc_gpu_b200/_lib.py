@@ -27,7 +27,7 @@ TT_STATS_MAX_SIGMA = 64
 
 # Every extern "C" symbol declared in include/ttrsvd.h.
 EXPORTED = [
-    "tt_ctx_create", "tt_ctx_destroy", "tt_ctx_set_stream", "tt_ctx_reserve", "tt_ctx_set_stream_chunk",
+    "tt_ctx_create", "tt_ctx_destroy", "tt_ctx_set_stream", "tt_ctx_reserve", "tt_ctx_set_stream_chunk", "tt_ctx_set_alloc_limit", "tt_ctx_set_wait_limit", "tt_k_wait_selftest",
     "tt_last_error",
     "tt_default_opts", "tt_abi_version", "tt_svd", "tr_svd", "tt_rel_error", "tt_k_gaussian", "tt_k_gaussian_rows",
     "tt_k_sketch", "tt_k_project", "tt_k_gram_rows", "tt_k_gram_tall", "tt_k_cholqr2",
@@ -89,6 +89,9 @@ def load():
         "tt_ctx_set_stream": (i, [vp, vp]),
         "tt_ctx_reserve": (i, [vp, C.c_size_t]),
         "tt_ctx_set_stream_chunk": (i, [vp, C.c_size_t]),
+        "tt_ctx_set_alloc_limit": (i, [vp, C.c_size_t]),
+        "tt_ctx_set_wait_limit": (i, [vp, C.c_ulonglong]),
+        "tt_k_wait_selftest": (i, [vp]),
         "tt_last_error": (C.c_char_p, []),
         "tt_default_opts": (None, [P(TTOpts)]),
         "tt_abi_version": (i, []),

@@ -49,6 +49,7 @@ struct tt_ctx {
   cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_used[2] = {nullptr, nullptr};
   cudaStream_t side_stream = nullptr;  // eigen-solve of a folded step, overlapped with the next step
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  size_t alloc_limit = 0;  // workspace bytes above which growth fails with TT_ERR_NOMEM (0: none)
 };
 
 extern "C" const char* tt_last_error(void) { return ttr::g_err; }
@@ -170,12 +171,26 @@ extern "C" int tt_ctx_set_stream_chunk(tt_ctx* c, size_t bytes) {
   return TT_OK;
 }
 
+extern "C" int tt_ctx_set_alloc_limit(tt_ctx* c, size_t bytes) {
+  if (!c) {
+    set_error(TT_ERR_ARG, "null ctx");
+    return TT_ERR_ARG;
+  }
+  c->alloc_limit = bytes;
+  return TT_OK;
+}
+
 extern "C" int tt_ctx_reserve(tt_ctx* c, size_t bytes) {
   if (!c) {
     set_error(TT_ERR_ARG, "null ctx");
     return TT_ERR_ARG;
   }
   if (bytes <= c->cap) return TT_OK;
+  if (c->alloc_limit && bytes > c->alloc_limit) {
+    set_error(TT_ERR_NOMEM, "workspace of %zu bytes above the context's allocation limit of %zu bytes", bytes,
+              c->alloc_limit);
+    return TT_ERR_NOMEM;
+  }
   TT_CUDA(cudaSetDevice(c->device));
   if (c->arena) {
     TT_CUDA(cudaStreamSynchronize(c->stream));
@@ -1321,6 +1336,26 @@ int check_status(tt_ctx* c) {
       return TT_ERR_ARG;                          \
     }                                             \
   } while (0)
+
+extern "C" int tt_ctx_set_wait_limit(tt_ctx* c, unsigned long long ns) {
+  if (!c) {
+    set_error(TT_ERR_ARG, "null ctx");
+    return TT_ERR_ARG;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  return set_wait_limit_ns(ns);
+}
+
+extern "C" int tt_k_wait_selftest(tt_ctx* c) {
+  if (!c) {
+    set_error(TT_ERR_ARG, "null ctx");
+    return TT_ERR_ARG;
+  }
+  TT_CUDA(cudaSetDevice(c->device));
+  TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
+  TT_TRY(launch_wait_selftest(c->dstat, c->stream));
+  return check_status(c);
+}
 
 extern "C" int tt_k_gaussian(tt_ctx* c, float* out, long long rows, int cols, long long ld,
                              unsigned long long seed, unsigned stream_id) {

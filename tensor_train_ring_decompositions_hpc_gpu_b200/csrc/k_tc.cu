@@ -25,7 +25,11 @@
 namespace ttr {
 namespace {
 
-constexpr unsigned long long kWaitLimitNs = 2000000000ull;  // 2 s per wait
+// Wall-clock limit of every pipeline wait (settable per device, tt_ctx_set_wait_limit), and the
+// fixed limit of the waits that drain a CTA's own copies after a failure: those always get the
+// full 2 s, so lowering the pipeline limit never lets a CTA leave with copies in flight.
+constexpr unsigned long long kWaitLimitNs = 2000000000ull;
+__device__ unsigned long long g_wait_limit_ns = kWaitLimitNs;
 
 // ---------------------------------------------------------------------------------------
 // PTX wrappers
@@ -68,8 +72,16 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatil
     for (int i = 0; i < 32; ++i)
       if (mbar_try_wait(bar, parity)) return true;
     if (*abort_flag) return false;
-    if (globaltimer() - t0 > kWaitLimitNs) return false;
+    if (globaltimer() - t0 > g_wait_limit_ns) return false;
   }
+}
+// Bounded pipeline wait without an abort flag (the per-warp pipelines of the exact Gram).
+__device__ __forceinline__ bool mbar_wait_limit(uint32_t bar, uint32_t parity) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = globaltimer(), lim = g_wait_limit_ns;
+  while (!mbar_try_wait(bar, parity))
+    if (globaltimer() - t0 > lim) return false;
+  return true;
 }
 __device__ __forceinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
   const unsigned long long t0 = globaltimer();
@@ -893,7 +905,7 @@ __global__ void __launch_bounds__(G32_WARPS * 32, 1)
   bool ok = true;
   for (; k < my; ++k) {
     const int s = (int)(k % G32_STAGES);
-    ok = mbar_wait_bounded(bars.full(s), (uint32_t)((k / G32_STAGES) & 1));
+    ok = mbar_wait_limit(bars.full(s), (uint32_t)((k / G32_STAGES) & 1));
     ok = __all_sync(0xffffffffu, ok);
     if (!ok) break;
     const uint32_t sb = wbase + (uint32_t)s * G32_STAGE_BYTES;
@@ -957,6 +969,24 @@ __global__ void k_gram32x_finish(const double* __restrict__ part, int nblk, int 
     double sum = 0.0;
     for (int b = 0; b < nblk; ++b) sum += part[(long long)b * 1024 + r * 32 + c];
     w[e] = sum;
+  }
+}
+
+// Self-test of the bounded wait: one warp waits (with the pipeline limit and the abort-flag
+// path of the tensor-core kernels) on an mbarrier that nothing ever arrives at, and reports
+// TT_ERR_TIMEOUT through the status word when the limit runs out.  No copy or MMA is in flight,
+// so the CTA can leave at once.
+__global__ void k_wait_selftest(DevStatus* st) {
+  __shared__ __align__(8) uint64_t bar;
+  __shared__ int abort_flag;
+  if (threadIdx.x == 0) {
+    mbar_init(smem_u32(&bar), 1);
+    abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (!mbar_wait(smem_u32(&bar), 0, &abort_flag)) dev_fail(st, TT_ERR_TIMEOUT, 99);
   }
 }
 
@@ -1200,6 +1230,19 @@ int launch_gram_tc(const float* a, long long m, long long n, double* w, Arena& w
 }
 
 bool tc_available() { return init_tc(); }
+
+int set_wait_limit_ns(unsigned long long ns) {
+  const unsigned long long v = ns ? ns : kWaitLimitNs;
+  TT_CUDA(cudaMemcpyToSymbol(g_wait_limit_ns, &v, sizeof(v)));
+  return TT_OK;
+}
+
+int launch_wait_selftest(DevStatus* st, cudaStream_t s) {
+  k_wait_selftest<<<1, 32, 0, s>>>(st);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  return TT_OK;
+}
 
 size_t gram32x_ws_bytes() { return (size_t)dev_sms() * 1024 * sizeof(double) + 4096; }
 

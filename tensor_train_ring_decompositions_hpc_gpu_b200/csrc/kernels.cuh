@@ -157,6 +157,11 @@ int launch_sketch_simt_static(const float* a, long long m, long long n, const fl
                               long long wj, long long wc, double* y, double* part, size_t part_cap,
                               cudaStream_t s);
 
+// Wall-clock limit (ns, 0 = default 2 s) of the pipeline waits of the TMA kernels on the
+// current device, and a self-test kernel whose wait can only run out (TT_ERR_TIMEOUT).
+int set_wait_limit_ns(unsigned long long ns);
+int launch_wait_selftest(DevStatus* st, cudaStream_t s);
+
 // Tensor-core engine availability (sm_100 device, TMA encoder found, TTR_DISABLE_TC unset).
 bool tc_available();
 size_t sketch_tc_ws_bytes(long long m, long long n, int N);
