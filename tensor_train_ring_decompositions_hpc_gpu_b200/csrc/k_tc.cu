@@ -797,23 +797,24 @@ __global__ void __launch_bounds__(192, 1)
 // and go through FP32 partial sums of 64 vectors into FP64 sums, so every rounding error is
 // unbiased and the result is accurate to ~1e-9 relative.
 //
-// Each warp runs its own TMA pipeline: 48-vector boxes (6 KB, 128B-swizzled rows) through 4
-// stages, the warp's lane 0 refilling a stage as soon as the warp has consumed it; no block-wide
-// barrier exists until the final reduction.  Within a warp, lane = 10 u + t computes the 8 x 8
-// tile t of the upper triangle of 32 x 32 tiles (10 tiles) for vector 3 it + u of the box
-// (lanes 30, 31 idle), with paired FP32 FMAs (fma.rn.f32x2): 32 issue slots per 64 FMAs, the
-// next vector's operands loaded while the current one is multiplied.  Every 128 vectors per
-// lane the three lanes of a tile add their FP32 partial sums (two shuffles per entry) and each
-// keeps a third of the tile's 64 FP64 sums, so the registers hold 64 FP32 + 22 FP64 sums.
+// Each warp runs its own TMA pipeline: 24-vector boxes (3 KB, 128B-swizzled rows) through 2
+// stages, the warp's lane 0 refilling a stage as soon as the warp has consumed it; 16 warps per
+// SM hide the shared-memory and FMA latencies, and no block-wide barrier exists until the final
+// reduction.  Within a warp, lane = 10 u + t computes the 8 x 8 tile t of the upper triangle of
+// 32 x 32 tiles (10 tiles) for vector 3 it + u of the box (lanes 30, 31 idle), with paired FP32
+// FMAs (fma.rn.f32x2): 32 issue slots per 64 FMAs.  Every 64 vectors per lane the three lanes
+// of a tile add their FP32 partial sums (two shuffles per entry) and each adds a third of the
+// tile's entries into the warp's FP64 sums in shared memory.
 // ---------------------------------------------------------------------------------------
-constexpr int G32_VPS = 48;     // vectors per TMA box (one stage)
-constexpr int G32_STAGES = 4;   // stages per warp
-constexpr int G32_WARPS = 8;
-constexpr int G32_FLUSH = 8;    // stages (128 vectors per lane) between FP64 flushes
-constexpr uint32_t G32_STAGE_BYTES = G32_VPS * 128;
+constexpr int G32_VPS = 24;     // vectors per TMA box (one stage)
+constexpr int G32_STAGES = 2;   // stages per warp
+constexpr int G32_WARPS = 16;
+constexpr int G32_FLUSH = 8;    // stages (64 vectors per lane) between FP64 flushes
+constexpr uint32_t G32_STAGE_BYTES = G32_VPS * 128;  // 3 KB: stages stay 1024-byte aligned
 constexpr size_t G32_RING = (size_t)G32_WARPS * G32_STAGES * G32_STAGE_BYTES;
-constexpr size_t G32_SMEM = 1024 + G32_RING + (size_t)G32_WARPS * G32_STAGES * 8;
-static_assert(G32_RING >= (size_t)G32_WARPS * 32 * 22 * sizeof(double), "reduction area fits in the stage ring");
+constexpr size_t G32_ACC = (size_t)G32_WARPS * 640 * sizeof(double);  // FP64 sums per warp
+constexpr size_t G32_SMEM = 1024 + G32_RING + G32_ACC + (size_t)G32_WARPS * G32_STAGES * 8;
+static_assert(G32_STAGE_BYTES % 1024 == 0, "128B-swizzled stages need 1024-byte alignment");
 
 __device__ __forceinline__ uint64_t f2_dup(float a) {
   uint64_t r;
@@ -855,7 +856,8 @@ __global__ void __launch_bounds__(G32_WARPS * 32, 1)
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t wbase = smem_u32(smem) + (uint32_t)(warp * G32_STAGES) * G32_STAGE_BYTES;
-  const Bars bars{smem_u32(smem + G32_RING) + 8u * G32_STAGES * warp, G32_STAGES};
+  double* wacc = reinterpret_cast<double*>(smem + G32_RING) + warp * 640;  // [tile][64]
+  const Bars bars{smem_u32(smem + G32_RING + G32_ACC) + 8u * G32_STAGES * warp, G32_STAGES};
   if (lane == 0) {
     for (int s = 0; s < G32_STAGES; ++s) mbar_init(bars.full(s), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -879,13 +881,12 @@ __global__ void __launch_bounds__(G32_WARPS * 32, 1)
   const int l1 = u < 3 ? ((u + 1) % 3) * 10 + t : lane;
   const int l2 = u < 3 ? ((u + 2) % 3) * 10 + t : lane;
   uint64_t acc[8][4];  // (W[8p+i][8q+2j], W[8p+i][8q+2j+1])
-  double accd[22];     // tile entries e = 8 i + j with e % 3 == u, at e / 3
 #pragma unroll
   for (int i = 0; i < 8; ++i)
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0ull;
-#pragma unroll
-  for (int e = 0; e < 22; ++e) accd[e] = 0.0;
+  for (int e = lane; e < 640; e += 32) wacc[e] = 0.0;
+  __syncwarp();
   auto flush = [&]() {
 #pragma unroll
     for (int i = 0; i < 8; ++i)
@@ -897,8 +898,8 @@ __global__ void __launch_bounds__(G32_WARPS * 32, 1)
         const float slo = lo + __shfl_sync(0xffffffffu, lo, l1) + __shfl_sync(0xffffffffu, lo, l2);
         const float shi = hi + __shfl_sync(0xffffffffu, hi, l1) + __shfl_sync(0xffffffffu, hi, l2);
         const int e0 = 8 * i + 2 * j, e1 = e0 + 1;
-        if (e0 % 3 == u) accd[e0 / 3] += (double)slo;
-        if (e1 % 3 == u) accd[e1 / 3] += (double)shi;
+        if (e0 % 3 == u) wacc[t * 64 + e0] += (double)slo;
+        if (e1 % 3 == u) wacc[t * 64 + e1] += (double)shi;
       }
   };
   long long k = 0;
@@ -910,12 +911,10 @@ __global__ void __launch_bounds__(G32_WARPS * 32, 1)
     if (!ok) break;
     const uint32_t sb = wbase + (uint32_t)s * G32_STAGE_BYTES;
     if (u < 3) {
-      G32Ops cur, nxt;
-      g32_load(nxt, sb, u, p, q);
 #pragma unroll 1
       for (int it = 0; it < G32_VPS / 3; ++it) {
-        cur = nxt;
-        if (it + 1 < G32_VPS / 3) g32_load(nxt, sb, 3 * (it + 1) + u, p, q);
+        G32Ops cur;
+        g32_load(cur, sb, 3 * it + u, p, q);
         const float a[8] = {cur.a0.x, cur.a0.y, cur.a0.z, cur.a0.w, cur.a1.x, cur.a1.y, cur.a1.z, cur.a1.w};
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
@@ -943,18 +942,14 @@ __global__ void __launch_bounds__(G32_WARPS * 32, 1)
     }
     __syncwarp();
   }
-  __syncthreads();  // every warp is done with its ring: reuse it for the block reduction
-  double* red = reinterpret_cast<double*>(smem);  // [warp][lane][22]
+  __syncthreads();  // every warp's FP64 sums are final
+  const double* red = reinterpret_cast<const double*>(smem + G32_RING);  // [warp][tile][64]
   const int tid = threadIdx.x;
-#pragma unroll
-  for (int e = 0; e < 22; ++e) red[tid * 22 + e] = accd[e];
-  __syncthreads();
   double* dst = part + (long long)blockIdx.x * 1024;
   for (int e = tid; e < 10 * 64; e += blockDim.x) {
     const int tt = e >> 6, ij = e & 63;
-    const int owner = (ij % 3) * 10 + tt, slot = ij / 3;
     double sum = 0.0;
-    for (int w = 0; w < G32_WARPS; ++w) sum += red[(w * 32 + owner) * 22 + slot];
+    for (int w = 0; w < G32_WARPS; ++w) sum += red[w * 640 + e];
     const int pp = tt < 4 ? 0 : tt < 7 ? 1 : tt < 9 ? 2 : 3;
     const int qq = tt < 4 ? tt : tt < 7 ? tt - 3 : tt < 9 ? tt - 5 : 3;
     dst[(8 * pp + (ij >> 3)) * 32 + 8 * qq + (ij & 7)] = sum;

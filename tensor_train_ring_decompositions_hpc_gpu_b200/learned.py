@@ -4,25 +4,28 @@ The predictor (kernels in ``csrc/mlp.cu``) maps 8 Gaussian-probe features of an 
 (``tt_probe_features``) to its truncation rank, oversampling and power-iteration count.  This
 module builds its training set and trains it with the library's own GPU kernels:
 
-* Unfoldings: spectra sigma_i = i^-alpha (i = 1..k) with alpha ~ U[0.5, 2], k = min(m, n)
-  log-uniform in [129, 2048] (sizes where a TT step of an order-6 tensor with modes 24..40
-  takes the randomized path), and a step tolerance tol log-uniform in [2e-4, 3e-3] (the
-  per-unfolding share eps / sqrt(d - 1) of eps = 1e-3 for orders 2..6, with margin).
+* Unfoldings: spectra of a low-rank tensor with noise, sigma_i = i^-alpha for i <= R (the bond
+  dimension, R ~ U{8..112}, alpha ~ U[0.5, 2]) and a flat noise floor holding a share eta^2 of
+  the energy beyond R (eta log-uniform in [1e-6, tol / 4]), k = min(m, n) log-uniform in
+  [129, 2048] (sizes where a TT step of an order-6 tensor with modes 24..40 takes the randomized
+  path), and a step tolerance tol log-uniform in [2e-4, 3e-3] (the per-unfolding share
+  eps / sqrt(d - 1) of eps = 1e-3 for orders 2..6, with margin).  The eps-rank is then at most
+  R + a few, within the 128-column sketch limit, so every label is a reachable target.
 * Features: ``tt_probe_features`` on the k x k matrix diag(sigma).  For A = U diag(sigma) V^T
   with orthonormal U, V and a Gaussian probe Omega, V^T Omega is Gaussian again, so the probe
   statistics (and every EDrSVD quantity) of A and of diag(sigma) have the same distribution.
 * Labels (the plain method in FP64): the rank r* of the exact truncated SVD at tolerance tol
   (smallest r with sum_{i>r} sigma_i^2 <= tol^2 sum sigma_i^2), and the cheapest (power
   iterations p, oversampling s) for which the FP64 EDrSVD with r* + s columns leaves at most
-  tol^2 of the energy outside its subspace in every trial: fewer passes over A first
-  (2 + 2p), then the narrower sketch.  Ranks above RANK_CAP (most spectra with alpha < 1.8 at
-  these tolerances) cannot be met within the sketch-width limit of 128; they are labelled
-  with the widest sketch (see ``label``).
+  half of tol^2 of the energy outside its subspace in every trial (the half leaves room for the
+  noise of the probe-based a-posteriori estimate that judges a learned attempt): fewer passes
+  over A first (2 + 2p), then the narrower sketch.
 * Training: ``tt_mlp_train`` (Adam, one persistent launch), on 90 % of the samples; the rest
   measure the validation loss.
 
-``python -m tensor_train_ring_decompositions_hpc_gpu_b200.learned train --out FILE`` runs it on a
-GPU and writes the parameters (``TT_MLP_PARAMS`` float32 values in a .npy file);
+``python -m tensor_train_ring_decompositions_hpc_gpu_b200.learned labels --out FILE.npz`` computes
+the specifications and labels on the CPU; ``... learned train --data FILE.npz --out FILE.npy``
+adds the probe features and trains on a GPU (without --data it labels first);
 ``... learned evaluate`` compares the shipped predictor with the plain adaptive method.
 """
 from __future__ import annotations
@@ -42,17 +45,27 @@ POWER = (0, 1, 2)
 WEIGHTS = os.path.join(os.path.dirname(os.path.abspath(__file__)), "predictor_weights.npy")
 
 
-def sample_specs(count, seed, kmin=129, kmax=2048, amin=0.5, amax=2.0, tmin=2e-4, tmax=3e-3):
-    """(k, alpha, tol) of `count` training unfoldings."""
+def sample_specs(count, seed, kmin=129, kmax=2048, amin=0.5, amax=2.0, tmin=2e-4, tmax=3e-3, rmin=8, rmax=112):
+    """(k, alpha, tol, R, eta) of `count` training unfoldings."""
     rng = np.random.default_rng(seed)
     k = np.exp(rng.uniform(np.log(kmin), np.log(kmax + 1), count)).astype(np.int64)
     alpha = rng.uniform(amin, amax, count)
     tol = np.exp(rng.uniform(np.log(tmin), np.log(tmax), count))
-    return k, alpha, tol
+    bond = np.minimum(rng.integers(rmin, rmax + 1, count), k - 1)
+    eta = np.exp(rng.uniform(np.log(1e-6), np.log(tol / 4.0)))
+    return k, alpha, tol, bond, eta
 
 
-def spectrum(k, alpha):
-    return np.arange(1, int(k) + 1, dtype=np.float64) ** (-float(alpha))
+def spectrum(k, alpha, bond=None, eta=0.0):
+    """sigma_i = i^-alpha for i <= bond, then a flat floor carrying a share eta^2 of the energy."""
+    k = int(k)
+    bond = k if bond is None else int(bond)
+    sig = np.zeros(k, dtype=np.float64)
+    sig[:bond] = np.arange(1, bond + 1, dtype=np.float64) ** (-float(alpha))
+    if bond < k and eta > 0.0:
+        e = float(np.sum(sig[:bond] ** 2))
+        sig[bond:] = np.sqrt(eta * eta * e / (1.0 - eta * eta) / (k - bond))
+    return sig
 
 
 def exact_rank(sig, tol, cap=RANK_CAP):
@@ -81,12 +94,11 @@ def edrsvd_outside(sig, ks, p, rng):
     return max(e.sum() - captured, 0.0) / e.sum()
 
 
-def label(k, alpha, tol, seed, trials=2):
-    """(r*, s*, p*, feasible) of one unfolding.  When the exact rank exceeds RANK_CAP no sketch
-    within the width limit meets tol; the label is then the widest sketch with the plain
-    method's power count (s = 8, p = 1: r* + s reaches the limit), so that the step ends where
-    the plain adaptive method's doubling would."""
-    sig = spectrum(k, alpha)
+def label(k, alpha, tol, seed, bond=None, eta=0.0, trials=2):
+    """(r*, s*, p*, feasible) of one unfolding: the eps-rank and the cheapest (p, s) whose FP64
+    EDrSVD leaves at most tol^2 / 2 outside its subspace in every trial.  A rank above RANK_CAP
+    (not reached by this distribution) is labelled with the widest sketch and p = 1."""
+    sig = spectrum(k, alpha, bond, eta)
     r = exact_rank(sig, tol, cap=int(k))
     if r > RANK_CAP:
         return RANK_CAP, 8, 1, False
@@ -94,26 +106,30 @@ def label(k, alpha, tol, seed, trials=2):
     for p in POWER:
         for s in OVERSAMPLE:
             ks = min(r + s, _lib.TT_MAX_SMALL, int(k))
-            if all(edrsvd_outside(sig, ks, p, rng) <= tol * tol for _ in range(trials)):
+            if all(edrsvd_outside(sig, ks, p, rng) <= 0.5 * tol * tol for _ in range(trials)):
                 return r, s, p, True
     return r, OVERSAMPLE[-1], POWER[-1], False
 
 
 def _label_chunk(args):
-    k, alpha, tol, seeds, one_thread = args
+    k, alpha, tol, bond, eta, seeds, one_thread = args
+    rows = list(zip(k, alpha, tol, bond, eta, seeds))
+
+    def run():
+        return [label(int(a), float(b), float(c), int(f), int(d), float(e)) for a, b, c, d, e, f in rows]
     if one_thread:  # one BLAS thread per pool worker: the pool already fills the cores
         from threadpoolctl import threadpool_limits
         with threadpool_limits(1):
-            return [label(int(a), float(b), float(c), int(d)) for a, b, c, d in zip(k, alpha, tol, seeds)]
-    return [label(int(a), float(b), float(c), int(d)) for a, b, c, d in zip(k, alpha, tol, seeds)]
+            return run()
+    return run()
 
 
-def labels(k, alpha, tol, seed, workers=None):
+def labels(k, alpha, tol, bond, eta, seed, workers=None):
     """Labels of all samples, over a spawn process pool (started before any GPU call)."""
     seeds = np.random.default_rng(seed + 1).integers(1 << 31, size=k.size)
     workers = workers or max(1, min(32, len(os.sched_getaffinity(0))))
     chunks = np.array_split(np.arange(k.size), workers * 4)
-    jobs = [(k[c], alpha[c], tol[c], seeds[c], workers > 1) for c in chunks]
+    jobs = [(k[c], alpha[c], tol[c], bond[c], eta[c], seeds[c], workers > 1) for c in chunks]
     if workers == 1:
         res = [_label_chunk(j) for j in jobs]
     else:
@@ -130,7 +146,7 @@ def targets(r, s, p):
     return np.stack([np.log2(r) / 10.0, np.log2(s) / 5.0, p / 2.0], axis=1).astype(np.float32)
 
 
-def features(k, alpha, tol, seed, device=None, log=None):
+def features(k, alpha, tol, seed, bond, eta, device=None, log=None):
     """Probe features of diag(sigma) for every sample, computed by tt_probe_features."""
     import torch
     from . import probe_features
@@ -138,7 +154,7 @@ def features(k, alpha, tol, seed, device=None, log=None):
     out = torch.empty((k.size, _lib.TT_MLP_INPUTS), dtype=torch.float32, device=dev)
     t0 = time.time()
     for i in range(k.size):
-        sig = spectrum(k[i], alpha[i])
+        sig = spectrum(k[i], alpha[i], bond[i], eta[i])
         a = torch.diag(torch.from_numpy(sig).float().to(dev))  # symmetric: its column-major view is itself
         e = float(np.sum(sig * sig))
         out[i] = probe_features(a, energy=e, tol=float(tol[i]), seed=int(seed) + i, stream_id=0)
@@ -199,23 +215,33 @@ def load_params(path=WEIGHTS):
     return p
 
 
-def build_dataset(count, seed, workers=None, log=None):
-    """Specs, labels (CPU) and features (GPU) of `count` training unfoldings."""
+def label_dataset(count, seed, workers=None, log=None):
+    """Specifications and labels (CPU only) of `count` training unfoldings."""
     log = log or (lambda msg: print(msg, flush=True))
     t0 = time.time()
-    k, alpha, tol = sample_specs(count, seed)
-    r, s, p, feas = labels(k, alpha, tol, seed, workers)
+    k, alpha, tol, bond, eta = sample_specs(count, seed)
+    r, s, p, feas = labels(k, alpha, tol, bond, eta, seed, workers)
     log(f"labels of {count} unfoldings: {time.time() - t0:.1f} s, feasible {feas.mean():.3f}")
+    return dict(k=k, alpha=alpha, tol=tol, bond=bond, eta=eta, r=r, s=s, p=p, feasible=feas, seed=seed)
+
+
+def add_features(data, log=None):
+    """The probe features (GPU) and network targets of a labelled set."""
+    log = log or (lambda msg: print(msg, flush=True))
     t0 = time.time()
-    x = features(k, alpha, tol, seed, log=log)
+    data = dict(data)
+    data["x"] = features(data["k"], data["alpha"], data["tol"], int(data["seed"]), data["bond"], data["eta"],
+                         log=log)
+    data["t"] = targets(data["r"], data["s"], data["p"])
     log(f"features: {time.time() - t0:.1f} s")
-    return dict(k=k, alpha=alpha, tol=tol, r=r, s=s, p=p, feasible=feas, x=x, t=targets(r, s, p))
+    return data
 
 
 def evaluate(weights=WEIGHTS, count=24, n=32768, tol=1e-3, seed=5, reps=3, log=None):
-    """Learned against plain adaptive EDrSVD on `count` held-out unfoldings U diag(i^-alpha) V^T
-    (m ~ U{200..1024}, alpha ~ U[0.5, 2], orthonormal U, V drawn on the GPU): passes over A,
-    device time (median of `reps` after a warm-up), achieved error and its estimate."""
+    """Learned against plain adaptive EDrSVD on `count` held-out unfoldings U diag(sigma) V^T
+    with the training distribution's spectra (m ~ U{200..1024}, bond R ~ U{8..112}, alpha ~
+    U[0.5, 2], noise floor eta ~ logU[1e-6, tol / 4]; orthonormal U, V drawn on the GPU): passes
+    over A, device time (median of `reps` after a warm-up), achieved error and its estimate."""
     import torch
     from . import TT_FLAG_ADAPTIVE_KS, TT_FLAG_LEARNED, set_predictor, tt_svd
     dev = torch.device("cuda", 0)
@@ -226,12 +252,14 @@ def evaluate(weights=WEIGHTS, count=24, n=32768, tol=1e-3, seed=5, reps=3, log=N
         for i in range(count):
             m = int(rng.integers(200, 1025))
             alpha = float(rng.uniform(0.5, 2.0))
+            bond = int(rng.integers(8, 113))
+            eta = float(np.exp(rng.uniform(np.log(1e-6), np.log(tol / 4.0))))
             g = torch.Generator(device=dev).manual_seed(i)
             u, _ = torch.linalg.qr(torch.randn(m, m, generator=g, device=dev))
             v, _ = torch.linalg.qr(torch.randn(n, m, generator=g, device=dev))
-            sig = torch.arange(1, m + 1, device=dev, dtype=torch.float32) ** (-alpha)
+            sig = torch.from_numpy(spectrum(m, alpha, bond, eta)).float().to(dev)
             a = (u * sig) @ v.T
-            out = {"m": m, "n": n, "alpha": alpha}
+            out = {"m": m, "n": n, "alpha": alpha, "bond": bond, "eta": eta}
             for name, flags in (("plain", TT_FLAG_ADAPTIVE_KS), ("learned", TT_FLAG_LEARNED)):
                 tt_svd(a, [1, 120, 1], eps=tol, power_iters=1, flags=flags)
                 ms = []
@@ -243,7 +271,7 @@ def evaluate(weights=WEIGHTS, count=24, n=32768, tol=1e-3, seed=5, reps=3, log=N
                 err = float(torch.linalg.matrix_norm(a.double() - uu @ ww) / torch.linalg.matrix_norm(a.double()))
                 out[name] = dict(ms=float(np.median(ms)), passes=res.passes, ks=res.step_ks[0], p=res.step_power[0],
                                  attempts=res.step_attempts[0], fallbacks=res.fallbacks, rank=res.ranks[1],
-                                 est=res.est_rel_err, err=err)
+                                 est=res.est_rel_err, err=err, eps_unmet=res.eps_unmet)
             rows.append(out)
             if log:
                 log(json.dumps(out))
@@ -262,7 +290,13 @@ def evaluate(weights=WEIGHTS, count=24, n=32768, tol=1e-3, seed=5, reps=3, log=N
 def main(argv=None):
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
+    lb = sub.add_parser("labels")
+    lb.add_argument("--count", type=int, default=20000)
+    lb.add_argument("--seed", type=int, default=20261203)
+    lb.add_argument("--workers", type=int, default=None)
+    lb.add_argument("--out", required=True, help="labelled set (.npz)")
     tr = sub.add_parser("train")
+    tr.add_argument("--data", default=None, help="labelled set from `labels` (default: label here first)")
     tr.add_argument("--count", type=int, default=20000)
     tr.add_argument("--steps", type=int, default=8000)
     tr.add_argument("--batch", type=int, default=256)
@@ -271,7 +305,6 @@ def main(argv=None):
     tr.add_argument("--workers", type=int, default=None)
     tr.add_argument("--out", required=True)
     tr.add_argument("--report", default=None, help="JSON summary of the run")
-    tr.add_argument("--save-data", default=None, help="write the training set (.npz)")
     ev = sub.add_parser("evaluate")
     ev.add_argument("--weights", default=WEIGHTS)
     ev.add_argument("--count", type=int, default=24)
@@ -281,9 +314,16 @@ def main(argv=None):
         summ, _ = evaluate(args.weights, args.count, tol=args.tol, log=lambda msg: print(msg, flush=True))
         print(json.dumps({"summary": summ}))
         return 0
-    data = build_dataset(args.count, args.seed, args.workers)  # the pool runs before the first GPU call
-    if args.save_data:
-        np.savez_compressed(args.save_data, **data)
+    if args.cmd == "labels":
+        data = label_dataset(args.count, args.seed, args.workers)
+        np.savez_compressed(args.out, **data)
+        return 0
+    if args.data:
+        data = {key: val for key, val in np.load(args.data).items()}
+    else:
+        data = label_dataset(args.count, args.seed, args.workers)  # the pool runs before the first GPU call
+    data = add_features(data)
+    args.count = int(data["k"].size)
     n = args.count
     ntr = int(0.9 * n)
     t0 = time.time()

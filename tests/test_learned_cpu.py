@@ -42,10 +42,24 @@ def test_exact_rank_and_labels():
     for tol in (1e-3, 3e-3):
         r = learned.exact_rank(sig, tol, cap=300)
         assert e[r:].sum() <= tol * tol * e.sum() < e[r - 1:].sum()
-    # fast decay: a feasible label; slow decay: the width-limit label
+    # fast decay: a feasible label; a pure slow power law over 400 values: the width-limit label
     r, s, p, ok = learned.label(400, 2.0, 2e-3, seed=3)
     assert ok and r <= learned.RANK_CAP and s in learned.OVERSAMPLE and p in learned.POWER
     assert learned.label(400, 0.6, 1e-3, seed=3) == (learned.RANK_CAP, 8, 1, False)
+
+
+def test_training_spectra_have_reachable_ranks():
+    """Bond-limited spectra with a noise floor below tol / 4: the eps-rank stays within the bond
+    (plus the floor's share), so the labels are reachable targets."""
+    k, alpha, tol, bond, eta = learned.sample_specs(200, seed=11)
+    assert np.all(eta <= tol / 4 * (1 + 1e-12)) and np.all(bond < k)
+    for i in range(0, 200, 10):
+        sig = learned.spectrum(k[i], alpha[i], bond[i], eta[i])
+        e = sig ** 2
+        assert abs(e[bond[i]:].sum() / e.sum() - eta[i] ** 2) < 1e-9
+        assert learned.exact_rank(sig, tol[i], cap=int(k[i])) <= bond[i]
+    r, s, p, ok = learned.label(int(k[0]), float(alpha[0]), float(tol[0]), 5, int(bond[0]), float(eta[0]))
+    assert ok and r <= bond[0]
 
 
 def test_targets_decode_round_trip():
