@@ -237,12 +237,6 @@ int tt_k_cholqr2(tt_ctx* ctx, float* y, long long n, int N, long long ld, double
  * cusolverDnSsyevd + matrixInvertColumn (ttdec6_singleGPU.cu:274-290,334-385). */
 int tt_k_syev(tt_ctx* ctx, const double* w, int N, double* evals, double* evecs, int* sweeps);
 
-/* As tt_k_syev for a symmetric positive semidefinite W (a Gram matrix, the only kind the
- * decompositions factorise): N <= 64 runs the one-sided Jacobi SVD of W (one warp per column
- * pair, columns in registers), N > 64 the two-sided solver.  For an indefinite W it returns the
- * magnitudes of the eigenvalues.  Replaces cusolverDnSsyevd on the Grams of TT6:334-385 and
- * gesvd of basicSvd (ttdec_gpu_float_edrsvd.cu:90-173). */
-int tt_k_syev_gram(tt_ctx* ctx, const double* w, int N, double* evals, double* evecs, int* sweeps);
 
 /* Allocation-free sketch Y = A * W (same operands and result as tt_k_sketch), for callers
  * that cannot call cudaMalloc: a process whose device memory belongs to another allocator or

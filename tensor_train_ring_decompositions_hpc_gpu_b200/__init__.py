@@ -308,17 +308,15 @@ def cholqr2(y):
     return q, r
 
 
-def syev(w, gram=False):
-    """Eigen-decomposition of a symmetric FP64 matrix (descending); returns (evals, evecs, sweeps).
-    gram=True: W is positive semidefinite (tt_k_syev_gram, the one-sided solver for N <= 64)."""
+def syev(w):
+    """Eigen-decomposition of a symmetric FP64 matrix (descending); returns (evals, evecs, sweeps)."""
     torch = _torch()
     w = _as_colmajor(w.double())
     N = w.shape[0]
     ev = torch.empty(N, dtype=torch.float64, device=w.device)
     vec = _colmajor(N, N, torch.float64, w.device)
     sw = C.c_int()
-    fn = lib().tt_k_syev_gram if gram else lib().tt_k_syev
-    check(fn(_ctx_for(w.device.index), _ptr(w), N, _ptr(ev), _ptr(vec), C.byref(sw)))
+    check(lib().tt_k_syev(_ctx_for(w.device.index), _ptr(w), N, _ptr(ev), _ptr(vec), C.byref(sw)))
     return ev, vec, sw.value
 
 

@@ -31,7 +31,7 @@ EXPORTED = [
     "tt_last_error",
     "tt_default_opts", "tt_abi_version", "tt_svd", "tr_svd", "tt_rel_error", "tt_k_gaussian", "tt_k_gaussian_rows",
     "tt_k_sketch", "tt_k_project", "tt_k_gram_rows", "tt_k_gram_tall", "tt_k_cholqr2",
-    "tt_k_syev", "tt_k_syev_gram", "tt_k_sketch_noalloc", "tt_svd_batched", "tt_batch_core_capacity",
+    "tt_k_syev", "tt_k_sketch_noalloc", "tt_svd_batched", "tt_batch_core_capacity",
     "tt_batch_plan_create", "tt_batch_plan_tune", "tt_batch_plan_variant", "tt_batch_plan_run",
     "tt_batch_plan_destroy",
     "tt_cores_save", "tt_cores_header", "tt_cores_load",
@@ -105,7 +105,6 @@ def load():
         "tt_k_gram_tall": (i, [vp, vp, ll, i, ll, ll, vp]),
         "tt_k_cholqr2": (i, [vp, vp, ll, i, ll, vp]),
         "tt_k_syev": (i, [vp, vp, i, vp, vp, P(i)]),
-        "tt_k_syev_gram": (i, [vp, vp, i, vp, vp, P(i)]),
         "tt_k_permute231": (i, [vp, vp, vp, i, i, ll]),
         "tt_k_sketch_noalloc": (i, [vp, ll, ll, vp, i, ll, vp, i, vp]),
         "tt_k_gaussian_rows": (i, [vp, vp, ll, ll, ll, i, ll, ull, C.c_uint]),

@@ -789,7 +789,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
         TT_CUDA(cudaMemcpyAsync(B.w, B.wacc, sizeof(double) * m * m, cudaMemcpyDeviceToDevice, s));
         return TT_OK;
       }));
-      TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s, true));
+      TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
       TT_TRY(launch_f64_to_f32_cols(B.evecs, m, m, re, B.ef, m, rq, s));
@@ -816,7 +816,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       cudaStream_t ss = c->side_stream;
       TT_CUDA(cudaEventRecord(c->ev_fork, s));
       TT_CUDA(cudaStreamWaitEvent(ss, c->ev_fork, 0));
-      TT_TRY(launch_syev(B.w2, (int)m, B.evals2, B.evecs2, max_sweeps, ws, c->dstat, ss, true));
+      TT_TRY(launch_syev(B.w2, (int)m, B.evals2, B.evecs2, max_sweeps, ws, c->dstat, ss));
       k_store_sigma<<<1, 64, 0, ss>>>(B.evals2, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
       TT_TRY(launch_f64_to_f32_cols(B.evecs2, m, m, re, B.ef2, m, rq, ss));
@@ -833,7 +833,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       npasses += st.fold ? 1 : 2;
       TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols,
                       [&] { return gram_rows(cur, m, cols, B.w, engine, adaptive); }));
-      TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s, true));
+      TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
       TT_TRY(decide((int)m, 0.0));
@@ -870,7 +870,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       // W = A^T A over the rows of A (vectors = rows i, components = columns)
       TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * cols * cols, 4.0 * m * cols,
                       [&] { return launch_gram(cur, m, (int)cols, 1, m, B.w, true, ws, s); }));
-      TT_TRY(launch_syev(B.w, (int)cols, B.evals, B.evecs, max_sweeps, ws, c->dstat, s, true));
+      TT_TRY(launch_syev(B.w, (int)cols, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(cols, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
       TT_TRY(decide((int)cols, 0.0));
@@ -946,7 +946,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
           }
           return launch_gram(B.bt, cols, ksa, ksa, 1, B.w, true, ws, s);
         }));
-        TT_TRY(launch_syev(B.w, ksa, B.evals, B.evecs, max_sweeps, ws, c->dstat, s, true));
+        TT_TRY(launch_syev(B.w, ksa, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
         k_store_sigma<<<1, 64, 0, s>>>(B.evals, std::min(ksa, TT_STATS_MAX_SIGMA), sigdst);
         count_launch();
         npasses += 2 + 2 * pwa;
@@ -1015,7 +1015,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
           ++npasses;
           TT_TRY(launch_f64_to_f32_cols(B.y0, m, m, TT_PROBE_COLS, B.yf, m, TT_PROBE_COLS, s));
           TT_TRY(launch_gram(B.yf, m, TT_PROBE_COLS, 1, m, B.w, true, ws, s));
-          TT_TRY(launch_syev(B.w, TT_PROBE_COLS, B.evals, B.evecs, max_sweeps, ws, c->dstat, s, true));
+          TT_TRY(launch_syev(B.w, TT_PROBE_COLS, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
           const double tol = energy > 0.0 ? std::sqrt(delta2 / energy) : 1.0;
           TT_TRY(launch_probe_features(B.evals, energy, tol, m, cols, feat, s));
           TT_TRY(launch_mlp_forward(c->pred, feat, 1, yout, s));
@@ -1451,7 +1451,7 @@ extern "C" int tt_probe_features(tt_ctx* c, const float* a, long long m, long lo
   TT_TRY(launch_sketch(a, m, n, om, P, 1, n, yd, engine, ws, c->dstat, s));
   TT_TRY(launch_f64_to_f32_cols(yd, m, m, P, yf, m, P, s));
   TT_TRY(launch_gram(yf, m, P, 1, m, w, true, ws, s));
-  TT_TRY(launch_syev(w, P, ev, vec, 40, ws, c->dstat, s, true));
+  TT_TRY(launch_syev(w, P, ev, vec, 40, ws, c->dstat, s));
   TT_TRY(launch_probe_features(ev, energy, tol, m, n, features, s));
   return check_status(c);
 }
@@ -1596,26 +1596,6 @@ extern "C" int tt_k_syev(tt_ctx* c, const double* w, int N, double* evals, doubl
   TT_TRY(ws_for(c, 2 * TT_MAX_SMALL * TT_MAX_SMALL * sizeof(double), ws));
   TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
   TT_TRY(launch_syev(w, N, evals, evecs, 40, ws, c->dstat, c->stream));
-  int st = check_status(c);
-  if (sweeps) *sweeps = c->hstat->sweeps;
-  return st;
-}
-
-extern "C" int tt_k_syev_gram(tt_ctx* c, const double* w, int N, double* evals, double* evecs,
-                              int* sweeps) {
-  TT_NEED(c);
-  TT_NEED(w);
-  TT_NEED(evals);
-  TT_NEED(evecs);
-  if (N < 1 || N > TT_MAX_SMALL) {
-    set_error(TT_ERR_SHAPE, "syev_gram size %d", N);
-    return TT_ERR_SHAPE;
-  }
-  TT_CUDA(cudaSetDevice(c->device));
-  Arena ws;
-  TT_TRY(ws_for(c, 2 * TT_MAX_SMALL * TT_MAX_SMALL * sizeof(double), ws));
-  TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
-  TT_TRY(launch_syev(w, N, evals, evecs, 40, ws, c->dstat, c->stream, true));
   int st = check_status(c);
   if (sweeps) *sweeps = c->hstat->sweeps;
   return st;

@@ -38,33 +38,4 @@ __device__ __forceinline__ bool jacobi_rotation(double app, double aqq, double a
   return true;
 }
 
-// One-sided Jacobi: columns x, y with a = |x|^2, b = |y|^2, g = x . y are rotated when
-// g^2 > 1e-24 a b (their cosine above 1e-12); no absolute floor, so columns of tiny norm are
-// still orthogonalised.  The rotation is the two-sided one of [[a, g], [g, b]], its inputs
-// scaled by a power of two into [0.5, 1) before the FP32 angle (a, b, g span any FP64 range).
-__device__ __forceinline__ bool os_needed(double a, double b, double g) {
-  return g != 0.0 && g * g > 1e-24 * (a * b);
-}
-
-__device__ __forceinline__ bool os_rotation(double a, double b, double g, double& c, double& s) {
-  c = 1.0;
-  s = 0.0;
-  if (!os_needed(a, b, g)) return false;
-  const double d = b - a, e = 2.0 * g;
-  const double mx = fmax(fabs(d), fabs(e));
-  const int ex = ((__double2hiint(mx) >> 20) & 0x7ff) - 1022;  // mx in [2^(ex-1), 2^ex)
-  const double sc = __hiloint2double((1023 - ex) << 20, 0);    // 2^-ex (exact)
-  const float df = (float)(d * sc), ef = (float)(e * sc);
-  const float h = sqrtf(fmaf(df, df, ef * ef));
-  const float tf = (df >= 0.0f ? ef : -ef) * __frcp_rn(fabsf(df) + h);
-  const double t = (double)tf;
-  const double x = fma(t, t, 1.0);
-  double y = (double)rsqrtf((float)x);
-  y = y * fma(-0.5 * x, y * y, 1.5);
-  y = y * fma(-0.5 * x, y * y, 1.5);
-  c = y;
-  s = t * y;
-  return true;
-}
-
 }  // namespace ttr

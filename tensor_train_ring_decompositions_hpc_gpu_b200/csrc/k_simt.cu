@@ -2381,195 +2381,12 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
   }
 }
 
-// One-sided (Hestenes) Jacobi for a symmetric positive semidefinite W (a Gram matrix,
-// N <= 64): the k x k one-sided Jacobi SVD.  Plane rotations from the right (W <- W J,
-// V <- V J) orthogonalise the columns of W; at convergence W V = E Lambda, so every eigenvalue
-// is a column norm of W V and V holds the eigenvectors.  A rotation touches only its own two
-// columns, so one warp owns one column pair, both columns of W and V in registers (lane l holds
-// rows l and l + 32): a round is three dot products by butterfly shuffles, the rotation (FP32
-// angle, FP64 Newton normalisation, so it is orthogonal to FP64 precision), the update, and the
-// round-robin move of the columns through shared memory (double-buffered: one barrier per
-// round).  After each sweep every pair of the moved columns is tested from shared memory and
-// the solve stops as soon as none needs a rotation (no quiet sweep).
-template <int EPL>
-__global__ void __launch_bounds__(1024) k_syev_os(const double* __restrict__ w_in, int N,
-                                                   double* __restrict__ evals, double* __restrict__ evecs,
-                                                   int max_sweeps, DevStatus* st) {
-  extern __shared__ __align__(16) double sm_os[];
-  const int Np = N + (N & 1);
-  const int LD = 32 * EPL;  // rows per stored column (padded)
-  // exchange buffers [2][slot][W | V][LD] doubles, then the column index of each slot [2][Np]
-  double* xb = sm_os;
-  int* xi = reinterpret_cast<int*>(xb + 2 * (size_t)Np * 2 * LD);
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // slot k holds column k at round 0; warp k owns slots (k, Np - 1 - k)
-  const int sp0 = warp, sq0 = Np - 1 - warp;
-  double wp[EPL], wq[EPL], vp[EPL], vq[EPL];
-  int ip = sp0, iq = sq0;
-#pragma unroll
-  for (int e = 0; e < EPL; ++e) {
-    const int i = lane + 32 * e;
-    wp[e] = (i < N && ip < N) ? 0.5 * (w_in[i + (long long)N * ip] + w_in[ip + (long long)N * i]) : 0.0;
-    wq[e] = (i < N && iq < N) ? 0.5 * (w_in[i + (long long)N * iq] + w_in[iq + (long long)N * i]) : 0.0;
-    vp[e] = (i == ip) ? 1.0 : 0.0;
-    vq[e] = (i == iq) ? 1.0 : 0.0;
-  }
-  const int NR = Np - 1;
-  int sweep = 0;
-  bool converged = false;
-  int R = 0, wb = 0;  // rounds done; buffer written last
-  for (; sweep < max_sweeps && !converged; ++sweep) {
-    for (int rnd = 0; rnd < NR; ++rnd, ++R) {
-      double a = 0.0, b = 0.0, g = 0.0;
-#pragma unroll
-      for (int e = 0; e < EPL; ++e) {
-        a = fma(wp[e], wp[e], a);
-        b = fma(wq[e], wq[e], b);
-        g = fma(wp[e], wq[e], g);
-      }
-#pragma unroll
-      for (int o = 16; o > 0; o >>= 1) {
-        a += __shfl_xor_sync(0xffffffffu, a, o);
-        b += __shfl_xor_sync(0xffffffffu, b, o);
-        g += __shfl_xor_sync(0xffffffffu, g, o);
-      }
-      double c, sn;
-      if (ip < N && iq < N && os_rotation(a, b, g, c, sn)) {
-#pragma unroll
-        for (int e = 0; e < EPL; ++e) {
-          const double x = wp[e], y = wq[e];
-          wp[e] = c * x - sn * y;
-          wq[e] = sn * x + c * y;
-          const double u = vp[e], v = vq[e];
-          vp[e] = c * u - sn * v;
-          vq[e] = sn * u + c * v;
-        }
-      }
-      // round-robin move: slot x -> x - 1 (x >= 2), 1 -> Np - 1, 0 stays
-      const int sp = sp0 == 0 ? 0 : (sp0 == 1 ? Np - 1 : sp0 - 1);
-      const int tq = sq0 == 1 ? Np - 1 : sq0 - 1;  // sq0 >= Np / 2 >= 1
-      wb = R & 1;
-      double* buf = xb + (size_t)wb * Np * 2 * LD;
-      int* ibuf = xi + wb * Np;
-#pragma unroll
-      for (int e = 0; e < EPL; ++e) {
-        buf[((size_t)sp * 2) * LD + lane + 32 * e] = wp[e];
-        buf[((size_t)sp * 2 + 1) * LD + lane + 32 * e] = vp[e];
-        buf[((size_t)tq * 2) * LD + lane + 32 * e] = wq[e];
-        buf[((size_t)tq * 2 + 1) * LD + lane + 32 * e] = vq[e];
-      }
-      if (lane == 0) {
-        ibuf[sp] = ip;
-        ibuf[tq] = iq;
-      }
-      if (rnd + 1 < NR) {
-        __syncthreads();
-      } else {
-        // end of sweep: would any pair of the current columns still be rotated?
-        __syncthreads();
-        int need = 0;
-        const int npairs = Np * (Np - 1) / 2;
-        for (int t = warp; t < npairs; t += blockDim.x >> 5) {
-          int x = 0, rem = t;  // pair t -> slots (x, y), x < y, row by row
-          while (rem >= Np - 1 - x) {
-            rem -= Np - 1 - x;
-            ++x;
-          }
-          const int y = x + 1 + rem;
-          if (ibuf[x] >= N || ibuf[y] >= N) continue;
-          double aa = 0.0, bb = 0.0, gg = 0.0;
-          for (int i = lane; i < N; i += 32) {
-            const double u = buf[((size_t)x * 2) * LD + i], v = buf[((size_t)y * 2) * LD + i];
-            aa = fma(u, u, aa);
-            bb = fma(v, v, bb);
-            gg = fma(u, v, gg);
-          }
-#pragma unroll
-          for (int o = 16; o > 0; o >>= 1) {
-            aa += __shfl_xor_sync(0xffffffffu, aa, o);
-            bb += __shfl_xor_sync(0xffffffffu, bb, o);
-            gg += __shfl_xor_sync(0xffffffffu, gg, o);
-          }
-          if (os_needed(aa, bb, gg)) need = 1;
-        }
-        if (!__syncthreads_or(need)) converged = true;
-      }
-#pragma unroll
-      for (int e = 0; e < EPL; ++e) {
-        wp[e] = buf[((size_t)sp0 * 2) * LD + lane + 32 * e];
-        vp[e] = buf[((size_t)sp0 * 2 + 1) * LD + lane + 32 * e];
-        wq[e] = buf[((size_t)sq0 * 2) * LD + lane + 32 * e];
-        vq[e] = buf[((size_t)sq0 * 2 + 1) * LD + lane + 32 * e];
-      }
-      ip = ibuf[sp0];
-      iq = ibuf[sq0];
-      if (converged) break;
-    }
-  }
-  // eigenvalue of each slot = column norm of W V; rank them (descending) and write out
-  __syncthreads();
-  const double* buf = xb + (size_t)wb * Np * 2 * LD;  // last written buffer
-  const int* ibuf = xi + wb * Np;
-  double* lam = xb + (size_t)(wb ^ 1) * Np * 2 * LD;  // the other buffer is free
-  int* rk = reinterpret_cast<int*>(lam + Np);
-  for (int x = warp; x < Np; x += blockDim.x >> 5) {
-    double a = 0.0;
-    for (int i = lane; i < N; i += 32) a = fma(buf[((size_t)x * 2) * LD + i], buf[((size_t)x * 2) * LD + i], a);
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
-    if (lane == 0) lam[x] = (ibuf[x] < N) ? sqrt(a) : -1.0;
-  }
-  __syncthreads();
-  if (tid < Np) {
-    const double la = lam[tid];
-    int rank = 0;
-    for (int y = 0; y < Np; ++y) {
-      const double lb = lam[y];
-      rank += (lb > la || (lb == la && y < tid)) ? 1 : 0;
-    }
-    rk[tid] = rank;
-    if (rank < N) evals[rank] = la;
-  }
-  if (tid == 0 && st) {
-    atomicMax(&st->sweeps, sweep);
-    if (!converged) dev_fail(st, TT_ERR_NOCONV, sweep);
-  }
-  __syncthreads();
-  for (int idx = tid; idx < Np * N; idx += blockDim.x) {
-    const int x = idx / N, i = idx % N;
-    const int r = rk[x];
-    if (r < N) evecs[i + (long long)N * r] = buf[((size_t)x * 2 + 1) * LD + i];
-  }
-}
-
-static size_t syev_os_smem(int N) {
-  const int Np = N + (N & 1);
-  const int LD = Np <= 32 ? 32 : 64;
-  return 2 * (size_t)Np * 2 * LD * sizeof(double) + 2 * (size_t)Np * sizeof(int) + 64;
-}
-
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps, Arena& ws,
-                DevStatus* st, cudaStream_t s, bool psd) {
+                DevStatus* st, cudaStream_t s) {
   if (N <= 0) return TT_OK;
   if (N > TT_MAX_SMALL) {
     set_error(TT_ERR_UNSUPPORTED, "eigen-solver size %d > %d", N, TT_MAX_SMALL);
     return TT_ERR_UNSUPPORTED;
-  }
-  if (psd && N <= 64) {
-    // Gram matrices: one-sided Jacobi, one warp per column pair
-    const int Np = N + (N & 1);
-    const size_t shm = syev_os_smem(N);
-    const int threads = 32 * (Np / 2);
-    if (Np <= 32) {
-      TT_TRY(smem_optin_k(k_syev_os<1>, shm));
-      k_syev_os<1><<<1, threads, shm, s>>>(w, N, evals, evecs, max_sweeps, st);
-    } else {
-      TT_TRY(smem_optin_k(k_syev_os<2>, shm));
-      k_syev_os<2><<<1, threads, shm, s>>>(w, N, evals, evecs, max_sweeps, st);
-    }
-    count_launch();
-    TT_LAUNCH_CHECK();
-    return TT_OK;
   }
   if (N <= 64) {
     const int Nps = N + (N & 1);

@@ -797,24 +797,20 @@ __global__ void __launch_bounds__(192, 1)
 // and go through FP32 partial sums of 64 vectors into FP64 sums, so every rounding error is
 // unbiased and the result is accurate to ~1e-9 relative.
 //
-// Each warp runs its own TMA pipeline: 24-vector boxes (3 KB, 128B-swizzled rows) through 2
-// stages, the warp's lane 0 refilling a stage as soon as the warp has consumed it; 16 warps per
-// SM hide the shared-memory and FMA latencies, and no block-wide barrier exists until the final
-// reduction.  Within a warp, lane = 10 u + t computes the 8 x 8 tile t of the upper triangle of
-// 32 x 32 tiles (10 tiles) for vector 3 it + u of the box (lanes 30, 31 idle), with paired FP32
-// FMAs (fma.rn.f32x2): 32 issue slots per 64 FMAs.  Every 64 vectors per lane the three lanes
-// of a tile add their FP32 partial sums (two shuffles per entry) and each adds a third of the
-// tile's entries into the warp's FP64 sums in shared memory.
+// Each warp runs its own TMA pipeline: 48-vector boxes (6 KB, 128B-swizzled rows) through 4
+// stages, the warp's lane 0 refilling a stage as soon as the warp has consumed it; no block-wide
+// barrier exists until the final reduction.  Within a warp, lane = 10 u + t computes the 8 x 8
+// tile t of the upper triangle of 32 x 32 tiles (10 tiles) for vector 3 it + u of the box
+// (lanes 30, 31 idle), with paired FP32 FMAs (fma.rn.f32x2): 32 issue slots per 64 FMAs.
 // ---------------------------------------------------------------------------------------
-constexpr int G32_VPS = 24;     // vectors per TMA box (one stage)
-constexpr int G32_STAGES = 2;   // stages per warp
-constexpr int G32_WARPS = 16;
-constexpr int G32_FLUSH = 8;    // stages (64 vectors per lane) between FP64 flushes
-constexpr uint32_t G32_STAGE_BYTES = G32_VPS * 128;  // 3 KB: stages stay 1024-byte aligned
+constexpr int G32_VPS = 48;     // vectors per TMA box (one stage)
+constexpr int G32_STAGES = 4;   // stages per warp
+constexpr int G32_WARPS = 8;
+constexpr int G32_FLUSH = 4;    // stages (64 vectors per lane) between FP64 flushes
+constexpr uint32_t G32_STAGE_BYTES = G32_VPS * 128;
 constexpr size_t G32_RING = (size_t)G32_WARPS * G32_STAGES * G32_STAGE_BYTES;
-constexpr size_t G32_ACC = (size_t)G32_WARPS * 640 * sizeof(double);  // FP64 sums per warp
-constexpr size_t G32_SMEM = 1024 + G32_RING + G32_ACC + (size_t)G32_WARPS * G32_STAGES * 8;
-static_assert(G32_STAGE_BYTES % 1024 == 0, "128B-swizzled stages need 1024-byte alignment");
+constexpr size_t G32_SMEM = 1024 + G32_RING + (size_t)G32_WARPS * G32_STAGES * 8;
+static_assert(G32_RING >= 256 * 65 * sizeof(double), "reduction area fits in the stage ring");
 
 __device__ __forceinline__ uint64_t f2_dup(float a) {
   uint64_t r;
@@ -836,28 +832,13 @@ __device__ __forceinline__ void lds_u2(uint32_t addr, uint64_t& a, uint64_t& b) 
   asm volatile("ld.shared.v2.b64 {%0, %1}, [%2];" : "=l"(a), "=l"(b) : "r"(addr));
 }
 
-struct G32Ops {
-  float4 a0, a1;
-  uint64_t b[4];
-};
-// Operands of vector v of a stage: rows 8p..8p+7 and 8q..8q+7 (16-byte chunks XOR-swizzled by v).
-__device__ __forceinline__ void g32_load(G32Ops& o, uint32_t sb, int v, int p, int q) {
-  const uint32_t row = sb + (uint32_t)v * 128u;
-  const int sw = v & 7;
-  o.a0 = lds_f4(row + ((uint32_t)((2 * p) ^ sw) << 4));
-  o.a1 = lds_f4(row + ((uint32_t)((2 * p + 1) ^ sw) << 4));
-  lds_u2(row + ((uint32_t)((2 * q) ^ sw) << 4), o.b[0], o.b[1]);
-  lds_u2(row + ((uint32_t)((2 * q + 1) ^ sw) << 4), o.b[2], o.b[3]);
-}
-
-__global__ void __launch_bounds__(G32_WARPS * 32, 1)
+__global__ void __launch_bounds__(256, 1)
     k_gram32x(const __grid_constant__ CUtensorMap tm, long long nvec, double* __restrict__ part, DevStatus* st) {
   extern __shared__ uint8_t smem_raw[];
   uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const uint32_t wbase = smem_u32(smem) + (uint32_t)(warp * G32_STAGES) * G32_STAGE_BYTES;
-  double* wacc = reinterpret_cast<double*>(smem + G32_RING) + warp * 640;  // [tile][64]
-  const Bars bars{smem_u32(smem + G32_RING + G32_ACC) + 8u * G32_STAGES * warp, G32_STAGES};
+  const Bars bars{smem_u32(smem + G32_RING) + 8u * G32_STAGES * warp, G32_STAGES};
   if (lane == 0) {
     for (int s = 0; s < G32_STAGES; ++s) mbar_init(bars.full(s), 1);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -877,16 +858,15 @@ __global__ void __launch_bounds__(G32_WARPS * 32, 1)
   const int t = lane % 10, u = lane / 10;
   const int p = t < 4 ? 0 : t < 7 ? 1 : t < 9 ? 2 : 3;
   const int q = t < 4 ? t : t < 7 ? t - 3 : t < 9 ? t - 5 : 3;
-  // the other two lanes of this tile (lanes 30, 31 pair with themselves; their sums are dropped)
-  const int l1 = u < 3 ? ((u + 1) % 3) * 10 + t : lane;
-  const int l2 = u < 3 ? ((u + 2) % 3) * 10 + t : lane;
   uint64_t acc[8][4];  // (W[8p+i][8q+2j], W[8p+i][8q+2j+1])
+  double accd[8][8];
 #pragma unroll
-  for (int i = 0; i < 8; ++i)
+  for (int i = 0; i < 8; ++i) {
 #pragma unroll
     for (int j = 0; j < 4; ++j) acc[i][j] = 0ull;
-  for (int e = lane; e < 640; e += 32) wacc[e] = 0.0;
-  __syncwarp();
+#pragma unroll
+    for (int j = 0; j < 8; ++j) accd[i][j] = 0.0;
+  }
   auto flush = [&]() {
 #pragma unroll
     for (int i = 0; i < 8; ++i)
@@ -894,12 +874,9 @@ __global__ void __launch_bounds__(G32_WARPS * 32, 1)
       for (int j = 0; j < 4; ++j) {
         float lo, hi;
         f2_unpack(acc[i][j], lo, hi);
+        accd[i][2 * j] += (double)lo;
+        accd[i][2 * j + 1] += (double)hi;
         acc[i][j] = 0ull;
-        const float slo = lo + __shfl_sync(0xffffffffu, lo, l1) + __shfl_sync(0xffffffffu, lo, l2);
-        const float shi = hi + __shfl_sync(0xffffffffu, hi, l1) + __shfl_sync(0xffffffffu, hi, l2);
-        const int e0 = 8 * i + 2 * j, e1 = e0 + 1;
-        if (e0 % 3 == u) wacc[t * 64 + e0] += (double)slo;
-        if (e1 % 3 == u) wacc[t * 64 + e1] += (double)shi;
       }
   };
   long long k = 0;
@@ -911,16 +888,22 @@ __global__ void __launch_bounds__(G32_WARPS * 32, 1)
     if (!ok) break;
     const uint32_t sb = wbase + (uint32_t)s * G32_STAGE_BYTES;
     if (u < 3) {
-#pragma unroll 1
+#pragma unroll 2
       for (int it = 0; it < G32_VPS / 3; ++it) {
-        G32Ops cur;
-        g32_load(cur, sb, 3 * it + u, p, q);
-        const float a[8] = {cur.a0.x, cur.a0.y, cur.a0.z, cur.a0.w, cur.a1.x, cur.a1.y, cur.a1.z, cur.a1.w};
+        const int v = 3 * it + u;
+        const uint32_t row = sb + (uint32_t)v * 128u;
+        const int sw = v & 7;
+        const float4 a0 = lds_f4(row + ((uint32_t)((2 * p) ^ sw) << 4));
+        const float4 a1 = lds_f4(row + ((uint32_t)((2 * p + 1) ^ sw) << 4));
+        uint64_t b[4];
+        lds_u2(row + ((uint32_t)((2 * q) ^ sw) << 4), b[0], b[1]);
+        lds_u2(row + ((uint32_t)((2 * q + 1) ^ sw) << 4), b[2], b[3]);
+        const float a[8] = {a0.x, a0.y, a0.z, a0.w, a1.x, a1.y, a1.z, a1.w};
 #pragma unroll
         for (int i = 0; i < 8; ++i) {
           const uint64_t ad = f2_dup(a[i]);
 #pragma unroll
-          for (int j = 0; j < 4; ++j) ffma2(acc[i][j], ad, cur.b[j]);
+          for (int j = 0; j < 4; ++j) ffma2(acc[i][j], ad, b[j]);
         }
       }
     }
@@ -942,14 +925,20 @@ __global__ void __launch_bounds__(G32_WARPS * 32, 1)
     }
     __syncwarp();
   }
-  __syncthreads();  // every warp's FP64 sums are final
-  const double* red = reinterpret_cast<const double*>(smem + G32_RING);  // [warp][tile][64]
+  __syncthreads();  // every warp is done with its ring: reuse it for the block reduction
+  double* red = reinterpret_cast<double*>(smem);
   const int tid = threadIdx.x;
+#pragma unroll
+  for (int i = 0; i < 8; ++i)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) red[tid * 65 + i * 8 + j] = accd[i][j];
+  __syncthreads();
   double* dst = part + (long long)blockIdx.x * 1024;
   for (int e = tid; e < 10 * 64; e += blockDim.x) {
     const int tt = e >> 6, ij = e & 63;
     double sum = 0.0;
-    for (int w = 0; w < G32_WARPS; ++w) sum += red[w * 640 + e];
+    for (int w = 0; w < G32_WARPS; ++w)
+      for (int uu = 0; uu < 3; ++uu) sum += red[(w * 32 + uu * 10 + tt) * 65 + ij];
     const int pp = tt < 4 ? 0 : tt < 7 ? 1 : tt < 9 ? 2 : 3;
     const int qq = tt < 4 ? tt : tt < 7 ? tt - 3 : tt < 9 ? tt - 5 : 3;
     dst[(8 * pp + (ij >> 3)) * 32 + 8 * qq + (ij & 7)] = sum;
@@ -1268,7 +1257,7 @@ int launch_gram32x(const float* x, long long nvec, int M, double* w, Arena& ws, 
     return TT_ERR_NOMEM;
   }
   TT_TRY(set_smem(k_gram32x, G32_SMEM));
-  k_gram32x<<<grid, G32_WARPS * 32, G32_SMEM, s>>>(map, nvec, part, st);
+  k_gram32x<<<grid, 256, G32_SMEM, s>>>(map, nvec, part, st);
   count_launch();
   TT_LAUNCH_CHECK();
   k_gram32x_finish<<<ceil_div(M * M, 256), 256, 0, s>>>(part, grid, M, w);

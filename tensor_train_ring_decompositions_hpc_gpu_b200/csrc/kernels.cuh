@@ -65,11 +65,9 @@ int launch_cholqr2(float* y, long long n, int N, long long vs, long long es, dou
 int launch_orth_power(float* y, long long n, int N, long long vs, long long es, Arena& ws, DevStatus* st,
                       cudaStream_t s, bool acc64 = false);
 
-// Symmetric eigen-decomposition by parallel cyclic Jacobi (FP64, N <= 128), eigenvalues
-// descending.  psd: W is positive semidefinite (a Gram matrix), which lets N <= 64 take the
-// one-sided solver (it returns |eigenvalues|; an indefinite W needs psd = false).
+// Symmetric eigen-decomposition by parallel cyclic Jacobi (FP64, N <= 128), eigenvalues descending.
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps,
-                Arena& ws, DevStatus* st, cudaStream_t s, bool psd = false);
+                Arena& ws, DevStatus* st, cudaStream_t s);
 
 // out (r0, r1, n) -> (r1, n, r0) column-major.
 int launch_permute231(const float* in, float* out, int r0, int r1, long long n, cudaStream_t s);

@@ -104,7 +104,7 @@ class DeviceBackend:
         return q
 
     def syev(self, w):
-        ev, vec, _ = self.ttr.syev(w, gram=True)
+        ev, vec, _ = self.ttr.syev(w)
         return ev, vec
 
     def inv_sqrt_psd(self, w, rel_floor=1e-12):

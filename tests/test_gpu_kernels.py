@@ -145,14 +145,13 @@ def test_cholqr2_rank_deficient_zeroes_dependent_columns(gpu):
 
 
 @pytest.mark.parametrize("N", [1, 2, 5, 24, 32, 33, 40, 63, 64, 65, 96, 128])
-@pytest.mark.parametrize("gram", [False, True])
-def test_syev(gpu, N, gram):
+def test_syev(gpu, N):
     import torch
     ttr = _ttr()
     rng = np.random.default_rng(N)
     b = rng.standard_normal((N, N + 7))
     w = b @ b.T
-    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu), gram=gram)
+    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu))
     ev = ev.cpu().numpy()
     vec = vec.cpu().numpy()
     ref = np.sort(np.linalg.eigvalsh(w))[::-1]
@@ -163,8 +162,7 @@ def test_syev(gpu, N, gram):
 
 
 @pytest.mark.parametrize("N,rank", [(40, 12), (64, 1), (32, 0), (96, 30)])
-@pytest.mark.parametrize("gram", [False, True])
-def test_syev_rank_deficient_terminates(gpu, N, rank, gram):
+def test_syev_rank_deficient_terminates(gpu, N, rank):
     """Gram matrices of rank-deficient sketches have eigenvalues at the FP64 rounding floor;
     the sweep loop must still converge (rotations below that floor are skipped)."""
     import torch
@@ -172,7 +170,7 @@ def test_syev_rank_deficient_terminates(gpu, N, rank, gram):
     rng = np.random.default_rng(N + rank)
     b = rng.standard_normal((N, rank))
     w = b @ b.T
-    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu), gram=gram)
+    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu))
     ev = ev.cpu().numpy()
     vec = vec.cpu().numpy()
     ref = np.sort(np.linalg.eigvalsh(w))[::-1]
@@ -183,8 +181,7 @@ def test_syev_rank_deficient_terminates(gpu, N, rank, gram):
 
 
 @pytest.mark.parametrize("N", [16, 40, 96])
-@pytest.mark.parametrize("gram", [False, True])
-def test_syev_asymmetric_rounding_converges(gpu, N, gram):
+def test_syev_asymmetric_rounding_converges(gpu, N):
     """Tensor-core Grams are symmetric only to FP32 rounding; the solver symmetrises its input
     and must converge to the eigen-decomposition of (W + W^T) / 2."""
     import torch
@@ -193,7 +190,7 @@ def test_syev_asymmetric_rounding_converges(gpu, N, gram):
     b = rng.standard_normal((N, 3 * N))
     w = b @ b.T
     w_in = w + 1e-7 * np.abs(w).max() * np.triu(rng.standard_normal((N, N)), 1)
-    ev, vec, sweeps = ttr.syev(torch.from_numpy(w_in).to(gpu), gram=gram)
+    ev, vec, sweeps = ttr.syev(torch.from_numpy(w_in).to(gpu))
     ev = ev.cpu().numpy()
     vec = vec.cpu().numpy()
     ws = 0.5 * (w_in + w_in.T)
@@ -204,8 +201,7 @@ def test_syev_asymmetric_rounding_converges(gpu, N, gram):
 
 
 @pytest.mark.parametrize("N", [3, 16, 31])
-@pytest.mark.parametrize("gram", [False, True])
-def test_syev_warp_sizes_and_clusters(gpu, N, gram):
+def test_syev_warp_sizes_and_clusters(gpu, N):
     """N <= 32 runs the one-warp register-resident solver; clustered (repeated) eigenvalues."""
     import torch
     ttr = _ttr()
@@ -213,7 +209,7 @@ def test_syev_warp_sizes_and_clusters(gpu, N, gram):
     q, _ = np.linalg.qr(rng.standard_normal((N, N)))
     lam = np.repeat(np.array([3.0, 1.0, 1e-3, 0.0]), (N + 3) // 4)[:N]
     w = (q * lam) @ q.T
-    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu), gram=gram)
+    ev, vec, sweeps = ttr.syev(torch.from_numpy(w).to(gpu))
     ev = ev.cpu().numpy()
     vec = vec.cpu().numpy()
     np.testing.assert_allclose(ev, np.sort(lam)[::-1], atol=1e-12)
@@ -223,15 +219,14 @@ def test_syev_warp_sizes_and_clusters(gpu, N, gram):
 
 
 @pytest.mark.parametrize("N", [20, 32, 40])
-@pytest.mark.parametrize("gram", [False, True])
-def test_syev_graded_spectrum_relative_accuracy(gpu, N, gram):
+def test_syev_graded_spectrum_relative_accuracy(gpu, N):
     import torch
     ttr = _ttr()
     rng = np.random.default_rng(1)
     q, _ = np.linalg.qr(rng.standard_normal((N, N)))
     lam = np.logspace(0, -10, N)
     w = (q * lam) @ q.T
-    ev, _, _ = ttr.syev(torch.from_numpy(w).to(gpu), gram=gram)
+    ev, _, _ = ttr.syev(torch.from_numpy(w).to(gpu))
     keep = lam >= 1e-6  # FP64 rounding of W (1e-16 absolute) leaves 1e-10 relative there
     np.testing.assert_allclose(ev.cpu().numpy()[keep], lam[keep], rtol=1e-8)
 
