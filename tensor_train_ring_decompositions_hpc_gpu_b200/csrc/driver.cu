@@ -370,11 +370,13 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
         P.max_ws = std::max(P.max_ws, project_ws_bytes(w, st.cols, std::min(w, st.r_req)));
       }
       P.max_ws = std::max(P.max_ws, project_ws_bytes(st.ks, st.cols, st.r_req));
+      P.max_ws = std::max(P.max_ws, syev_ws_bytes(st.ks, o.max_sweeps));
     } else {
       P.max_ws = std::max(P.max_ws, project_ws_bytes(st.m, st.cols, st.r_req));
       P.max_ws = std::max(P.max_ws, gram_ws_bytes(std::max(st.m, st.cols), (int)mn));
       P.max_ws = std::max(P.max_ws, gram_tc_ws_bytes(st.m, st.cols));
       P.max_ws = std::max(P.max_ws, gram32x_ws_bytes());
+      P.max_ws = std::max(P.max_ws, syev_ws_bytes((int)mn, o.max_sweeps));
     }
   }
   P.max_ws += (size_t)TT_MAX_SMALL * TT_MAX_SMALL * sizeof(double) * 8;
@@ -1593,7 +1595,7 @@ extern "C" int tt_k_syev(tt_ctx* c, const double* w, int N, double* evals, doubl
   }
   TT_CUDA(cudaSetDevice(c->device));
   Arena ws;
-  TT_TRY(ws_for(c, 2 * TT_MAX_SMALL * TT_MAX_SMALL * sizeof(double), ws));
+  TT_TRY(ws_for(c, 2 * TT_MAX_SMALL * TT_MAX_SMALL * sizeof(double) + syev_ws_bytes(N, 40), ws));
   TT_CUDA(cudaMemsetAsync(c->dstat, 0, sizeof(DevStatus), c->stream));
   TT_TRY(launch_syev(w, N, evals, evecs, 40, ws, c->dstat, c->stream));
   int st = check_status(c);

@@ -19,15 +19,18 @@ __device__ __forceinline__ bool jacobi_needed(double app, double aqq, double apq
   return fabs(as) > 1e-14 && as * as > 1e-24 * fabs(ps * qs);
 }
 
-__device__ __forceinline__ bool jacobi_rotation(double app, double aqq, double apq, double inv_s, double& c,
-                                                double& s) {
+// The rotation in two halves: the FP32 tangent t (0 when the pair is not rotated), and (c, s)
+// from t in FP64.  The large-N solver logs t per pair and round and rebuilds (c, s) from it when it
+// replays the rotations on the eigenvectors: the same arithmetic gives the same bits.
+__device__ __forceinline__ float jacobi_tf(double app, double aqq, double apq, double inv_s) {
+  if (!jacobi_needed(app, aqq, apq, inv_s)) return 0.0f;
   const double ps = app * inv_s, qs = aqq * inv_s, as = apq * inv_s;
-  c = 1.0;
-  s = 0.0;
-  if (!jacobi_needed(app, aqq, apq, inv_s)) return false;
   const float d = (float)(qs - ps), e = 2.0f * (float)as;
   const float h = sqrtf(fmaf(d, d, e * e));
-  const float tf = (d >= 0.0f ? e : -e) * __frcp_rn(fabsf(d) + h);
+  return (d >= 0.0f ? e : -e) * __frcp_rn(fabsf(d) + h);
+}
+
+__device__ __forceinline__ void rot_from_tf(float tf, double& c, double& s) {
   const double t = (double)tf;
   const double x = fma(t, t, 1.0);
   double y = (double)rsqrtf((float)x);
@@ -35,6 +38,14 @@ __device__ __forceinline__ bool jacobi_rotation(double app, double aqq, double a
   y = y * fma(-0.5 * x, y * y, 1.5);
   c = y;
   s = t * y;
+}
+
+__device__ __forceinline__ bool jacobi_rotation(double app, double aqq, double apq, double inv_s, double& c,
+                                                double& s) {
+  c = 1.0;
+  s = 0.0;
+  if (!jacobi_needed(app, aqq, apq, inv_s)) return false;
+  rot_from_tf(jacobi_tf(app, aqq, apq, inv_s), c, s);
   return true;
 }
 

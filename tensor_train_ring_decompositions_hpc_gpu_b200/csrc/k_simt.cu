@@ -2,6 +2,7 @@
 // TT/TR-SVD chain (Gaussian test matrix, Gram matrices, CholeskyQR2, Jacobi eigen-solver,
 // bond permute, core folding, reconstruction error).
 #include <float.h>
+#include <stdlib.h>
 #include <math.h>
 
 #include <algorithm>
@@ -2381,6 +2382,251 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
   }
 }
 
+// Large-N variant (64 < N <= 128) of the Brent-Luk solver.  W alone stays in shared memory: its
+// upper triangle packed by rows (row P stored from column P & ~1, so every 2 x 2 block row is a
+// 16-byte load), double-buffered (2 x 66.5 KB for N = 128).  The eigenvectors are not updated
+// round by round: the rotation warps log each round's FP32 tangents to global memory, and
+// k_bl_replay applies them afterwards to the rows of V, one CTA per row (rows are independent),
+// with the same moves.  Two warps compute the next round's rotations during the update.
+__device__ __forceinline__ int blp_off(int P, int Np) {
+  // sum over rows p < P of (Np - (p & ~1)): pairs of rows (2a, 2a + 1) hold 2 (Np - 2a) entries
+  const int a = P >> 1;
+  return 2 * (a * Np - a * (a - 1)) + (P & 1) * (Np - 2 * a);
+}
+
+__global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_in, int N,
+                                                    double* __restrict__ evals, float* __restrict__ tlog,
+                                                    int* __restrict__ meta, int max_sweeps, DevStatus* st) {
+  constexpr int RW0 = 30;  // warps 30, 31 compute the next round's rotations
+  constexpr int NE = RW0 * 32;
+  extern __shared__ __align__(16) double sm_blw[];
+  const int Np = N + (N & 1);
+  const int NR = Np - 1;
+  const int H = Np / 2;
+  const int PS = blp_off(Np, Np);
+  double* Wb0 = sm_blw;
+  double* Wb1 = Wb0 + PS;
+  __shared__ double2 pcs[2][64];
+  __shared__ int mv[128], imv[128];
+  __shared__ int2 mv2[64];
+  __shared__ int roff[128];
+  __shared__ double dg[128];
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  auto at = [&](int P, int Q) { return roff[P] + (Q - (P & ~1)); };  // P <= Q
+  for (int P = tid; P < Np; P += blockDim.x) {
+    const int x = P % 2 == 0 ? P / 2 : Np - 1 - P / 2;
+    const int xn = x == 0 ? 0 : (x == 1 ? NR : x - 1);
+    const int Pn = bl_pos(xn, Np);
+    mv[P] = Pn;
+    imv[Pn] = P;
+    roff[P] = blp_off(P, Np);
+  }
+  __syncthreads();
+  for (int e = tid; e < 2 * PS; e += blockDim.x) Wb0[e] = 0.0;
+  __syncthreads();
+  for (int idx = tid; idx < Np * Np; idx += blockDim.x) {
+    const int i = idx / Np, j = idx - (idx / Np) * Np;
+    const int Pi = bl_pos(i, Np), Pj = bl_pos(j, Np);
+    if (Pi > Pj) continue;
+    double v = 0.0;
+    if (i < N && j < N) v = 0.5 * (w_in[i + (long long)N * j] + w_in[j + (long long)N * i]);
+    Wb0[at(Pi, Pj)] = v;
+  }
+  for (int q = tid; q < H; q += blockDim.x) mv2[q] = make_int2(mv[2 * q], mv[2 * q + 1]);
+  double dm = 0.0;
+  for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(w_in[i + (long long)N * i]));
+  const double inv_s = dm > 0.0 ? 1.0 / dm : 1.0;
+  __syncthreads();
+  const int rl = tid - NE;  // rotation lane (0..63) on the rotation warps
+  if (warp >= RW0 && rl < H) {
+    const int k = rl;
+    const int i0 = k, i1 = Np - 1 - k;
+    float tf = 0.0f;
+    if (i0 < N && i1 < N) tf = jacobi_tf(Wb0[at(2 * k, 2 * k)], Wb0[at(2 * k + 1, 2 * k + 1)], Wb0[at(2 * k, 2 * k + 1)],
+                                         inv_s);
+    double c, sn;
+    rot_from_tf(tf, c, sn);
+    pcs[0][k] = make_double2(c, sn);
+    tlog[k] = tf;
+  }
+  __syncthreads();
+  const int NWB = H * (H + 1) / 2;
+  constexpr int MAXIT = (64 * 65 / 2 + NE - 1) / NE;
+  int dsc[MAXIT];
+#pragma unroll
+  for (int u = 0; u < MAXIT; ++u) {
+    const int it = tid + u * NE;
+    if (warp >= RW0 || it >= NWB) {
+      dsc[u] = -1;
+    } else {
+      int a = 0, rem = it;
+      while (rem >= H - a) {
+        rem -= H - a;
+        ++a;
+      }
+      dsc[u] = a | ((a + rem) << 8);
+    }
+  }
+  int aP = 0, xP = 0, aQ = 0, xQ = 0;
+  if (warp >= RW0 && rl < H) {
+    const int P = imv[2 * rl], Q = imv[2 * rl + 1];
+    aP = P >> 1;
+    xP = P & 1;
+    aQ = Q >> 1;
+    xQ = Q & 1;
+  }
+  int R = 0;
+  int sweep = 0;
+  bool converged = false;
+  for (; sweep < max_sweeps; ++sweep) {
+    bool stop = false;
+    for (int rnd = 0; rnd < NR; ++rnd, ++R) {
+      const int cb = R & 1;
+      const double* W = cb ? Wb1 : Wb0;
+      double* Wn = cb ? Wb0 : Wb1;
+      const double2* cs_ = pcs[cb];
+      if (warp < RW0) {
+#pragma unroll
+        for (int u = 0; u < MAXIT; ++u) {
+          const int dd = dsc[u];
+          if (dd < 0) continue;
+          const int a = dd & 255, b = (dd >> 8) & 255;
+          const double2 csa = cs_[a], csb = cs_[b];
+          const double ca = csa.x, sa = csa.y, cbv = csb.x, sb = csb.y;
+          const double2 r0v = *reinterpret_cast<const double2*>(&W[at(2 * a, 2 * b)]);
+          const double2 r1v = *reinterpret_cast<const double2*>(&W[roff[2 * a + 1] + (2 * b - 2 * a)]);
+          const double w00 = r0v.x, w01 = r0v.y, w11 = r1v.y;
+          const double w10 = (a == b) ? w01 : r1v.x;
+          const double x00 = ca * w00 - sa * w10, x01 = ca * w01 - sa * w11;
+          const double x10 = sa * w00 + ca * w10, x11 = sa * w01 + ca * w11;
+          const double y00 = x00 * cbv - x01 * sb, y01 = x00 * sb + x01 * cbv;
+          const double y10 = x10 * cbv - x11 * sb, y11 = x10 * sb + x11 * cbv;
+          const int2 ma = mv2[a], mb = mv2[b];
+          const int r0 = ma.x, r1 = ma.y, q0 = mb.x, q1 = mb.y;
+          Wn[at(min(r0, q0), max(r0, q0))] = y00;
+          Wn[at(min(r0, q1), max(r0, q1))] = y01;
+          if (a != b) Wn[at(min(r1, q0), max(r1, q0))] = y10;
+          Wn[at(min(r1, q1), max(r1, q1))] = y11;
+        }
+      } else if (rl < H) {
+        const int rn = (rnd + 1 == NR) ? 0 : rnd + 1;
+        bool live = true;
+        if (Np != N) {
+          const int xs = bl_slot(Np - 1, rn, NR);
+          live = (xs != rl) && (xs != Np - 1 - rl);
+        }
+        float tf = 0.0f;
+        if (live) {
+          const double cP = cs_[aP].x, sP = cs_[aP].y, cQ = cs_[aQ].x, sQ = cs_[aQ].y;
+          const double tP0 = xP ? sP : cP, tP1 = xP ? cP : -sP;
+          const double tQ0 = xQ ? sQ : cQ, tQ1 = xQ ? cQ : -sQ;
+          auto wu = [&](int r, int c2) { return r <= c2 ? W[at(r, c2)] : W[at(c2, r)]; };
+          const int P0 = 2 * aP, Q0 = 2 * aQ;
+          const double p0 = tP0 * wu(P0, P0) + tP1 * wu(P0, P0 + 1);
+          const double p1 = tP0 * wu(P0, P0 + 1) + tP1 * wu(P0 + 1, P0 + 1);
+          const double q0 = tQ0 * wu(Q0, Q0) + tQ1 * wu(Q0, Q0 + 1);
+          const double q1 = tQ0 * wu(Q0, Q0 + 1) + tQ1 * wu(Q0 + 1, Q0 + 1);
+          const double m0 = tP0 * wu(P0, Q0) + tP1 * wu(P0 + 1, Q0);
+          const double m1 = tP0 * wu(P0, Q0 + 1) + tP1 * wu(P0 + 1, Q0 + 1);
+          tf = jacobi_tf(p0 * tP0 + p1 * tP1, q0 * tQ0 + q1 * tQ1, m0 * tQ0 + m1 * tQ1, inv_s);
+        }
+        double c, sn;
+        rot_from_tf(tf, c, sn);
+        pcs[cb ^ 1][rl] = make_double2(c, sn);
+        tlog[(size_t)(R + 1) * H + rl] = tf;  // rotations of round R + 1
+      }
+      __syncthreads();
+      if (rnd + 1 == NR) {
+        int need = 0;
+        for (int idx = tid; idx < Np * Np; idx += blockDim.x) {
+          const int P = idx / Np, Q = idx - (idx / Np) * Np;
+          if (P < Q && jacobi_needed(Wn[at(P, P)], Wn[at(Q, Q)], Wn[at(P, Q)], inv_s)) need = 1;
+        }
+        if (!__syncthreads_or(need)) stop = true;
+      }
+    }
+    if (stop) {
+      converged = true;
+      ++sweep;
+      break;
+    }
+  }
+  // eigenvalues by rank; meta = [rounds, rank of index 0..N-1, final position of index 0..N-1]
+  const double* Wf = (R & 1) ? Wb1 : Wb0;
+  if (tid < N) {
+    const int P = bl_pos(bl_slot(tid, R, NR), Np);
+    dg[tid] = Wf[at(P, P)];
+  }
+  __syncthreads();
+  if (tid < N) {
+    double la = dg[tid];
+    if (la != la) la = -INFINITY;
+    int rank = 0;
+    for (int b = 0; b < N; ++b) {
+      double lb = dg[b];
+      if (lb != lb) lb = -INFINITY;
+      rank += (lb > la || (lb == la && b < tid)) ? 1 : 0;
+    }
+    evals[rank] = dg[tid];
+    meta[1 + tid] = rank;
+    meta[1 + 128 + tid] = bl_pos(bl_slot(tid, R, NR), Np);
+  }
+  if (tid == 0) {
+    meta[0] = R;
+    if (st) {
+      atomicMax(&st->sweeps, sweep);
+      if (!converged) dev_fail(st, TT_ERR_NOCONV, sweep);
+    }
+  }
+}
+
+// Replays the logged rotations on row i of V (one CTA per row, one thread per pair; V starts as
+// the identity with index i at its round-0 position) and writes the eigenvectors by rank.
+__global__ void __launch_bounds__(64) k_bl_replay(const float* __restrict__ tlog, const int* __restrict__ meta,
+                                                  int N, double* __restrict__ evecs) {
+  __shared__ double vb[2][128];
+  __shared__ int mvs[128];
+  const int Np = N + (N & 1), H = Np / 2, NR = Np - 1;
+  const int i = blockIdx.x, k = threadIdx.x;
+  for (int P = k; P < Np; P += blockDim.x) {
+    const int x = P % 2 == 0 ? P / 2 : Np - 1 - P / 2;
+    const int xn = x == 0 ? 0 : (x == 1 ? NR : x - 1);
+    mvs[P] = bl_pos(xn, Np);
+    vb[0][P] = (P == bl_pos(i, Np)) ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  const int rounds = meta[0];
+  const int m0 = k < H ? mvs[2 * k] : 0, m1 = k < H ? mvs[2 * k + 1] : 0;
+  constexpr int U = 8;
+  for (int R0 = 0; R0 < rounds; R0 += U) {
+    float tf[U];
+#pragma unroll
+    for (int j = 0; j < U; ++j) tf[j] = (k < H && R0 + j < rounds) ? tlog[(size_t)(R0 + j) * H + k] : 0.0f;
+#pragma unroll
+    for (int j = 0; j < U; ++j) {
+      if (R0 + j >= rounds) break;
+      const int cb = (R0 + j) & 1;
+      if (k < H) {
+        double c, sn;
+        rot_from_tf(tf[j], c, sn);
+        const double v0 = vb[cb][2 * k], v1 = vb[cb][2 * k + 1];
+        vb[cb ^ 1][m0] = v0 * c - v1 * sn;
+        vb[cb ^ 1][m1] = v0 * sn + v1 * c;
+      }
+      __syncthreads();
+    }
+  }
+  const double* vf = vb[rounds & 1];
+  for (int a = k; a < N; a += blockDim.x) evecs[i + (long long)N * meta[1 + a]] = vf[meta[1 + 128 + a]];
+}
+
+size_t syev_ws_bytes(int N, int max_sweeps) {
+  if (N <= 64) return 0;
+  const int Np = N + (N & 1);
+  const int sw = max_sweeps > 0 ? max_sweeps : 40;
+  return ((size_t)sw * (Np - 1) + 2) * (Np / 2) * sizeof(float) + (1 + 2 * 128) * sizeof(int) + 1024;
+}
+
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps, Arena& ws,
                 DevStatus* st, cudaStream_t s) {
   if (N <= 0) return TT_OK;
@@ -2395,6 +2641,28 @@ int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sw
     k_syev_bl<<<1, 1024, shm_bl, s>>>(w, N, evals, evecs, max_sweeps, st);
     count_launch();
     TT_LAUNCH_CHECK();
+    return TT_OK;
+  }
+  if (!getenv("TTR_SYEV_JACOBI")) {
+    // 64 < N <= 128: packed Brent-Luk on W, eigenvectors by replaying the logged rotations
+    const int Np = N + (N & 1), H = Np / 2;
+    const int sw = max_sweeps > 0 ? max_sweeps : 40;
+    const size_t mk = ws.mark();
+    float* tlog = ws.take<float>(((size_t)sw * (Np - 1) + 2) * H);
+    int* meta = ws.take<int>(1 + 2 * 128);
+    if (!tlog || !meta) {
+      set_error(TT_ERR_NOMEM, "eigen-solver rotation log");
+      return TT_ERR_NOMEM;
+    }
+    const size_t shm = 2 * (size_t)(2 * (H * Np - H * (H - 1))) * sizeof(double);
+    TT_TRY(smem_optin_k(k_syev_blw, shm));
+    k_syev_blw<<<1, 1024, shm, s>>>(w, N, evals, tlog, meta, sw, st);
+    count_launch();
+    TT_LAUNCH_CHECK();
+    k_bl_replay<<<N, 64, 0, s>>>(tlog, meta, N, evecs);
+    count_launch();
+    TT_LAUNCH_CHECK();
+    ws.reset(mk);
     return TT_OK;
   }
   const int Np = N + (N & 1);

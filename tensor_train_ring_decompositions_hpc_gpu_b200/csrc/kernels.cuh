@@ -65,6 +65,8 @@ int launch_cholqr2(float* y, long long n, int N, long long vs, long long es, dou
 int launch_orth_power(float* y, long long n, int N, long long vs, long long es, Arena& ws, DevStatus* st,
                       cudaStream_t s, bool acc64 = false);
 
+// Arena bytes launch_syev takes for N > 64 (the rotation log); 0 for N <= 64.
+size_t syev_ws_bytes(int N, int max_sweeps);
 // Symmetric eigen-decomposition by parallel cyclic Jacobi (FP64, N <= 128), eigenvalues descending.
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps,
                 Arena& ws, DevStatus* st, cudaStream_t s);
