@@ -245,6 +245,14 @@ struct Plan {
   long long stream_cols = 0;  // host streaming: columns of the first unfolding per chunk (0: off)
 };
 
+// An exact step whose Gram comes from the tensor cores (more than 32 rows) and that truncates
+// gets its kept subspace refined by exact Rayleigh-Ritz (see run_chain); b = r + 16 columns.
+bool refine_exact(const Step& st, int engine, bool adaptive) {
+  return st.path == PATH_EXACT_ROWS && engine == TT_GEMM_TC && !adaptive && st.m > 32 && st.r_eff < st.m &&
+         !st.perm231;
+}
+int refine_width(const Step& st) { return (int)std::min<long long>(st.m, (long long)st.r_eff + 16); }
+
 int engine_of(const tt_opts& o) {
   if (o.gemm == TT_GEMM_FP32) return TT_GEMM_FP32;
   return tc_available() ? TT_GEMM_TC : TT_GEMM_FP32;
@@ -259,6 +267,10 @@ int engine_for(const tt_opts& o, long long m, long long cols) {
     return TT_GEMM_FP32;
   return e;
 }
+
+struct Step;
+bool refine_exact(const Step& st, int engine, bool adaptive);
+int refine_width(const Step& st);
 
 int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Plan& P) {
   if (d < 2 || d > TT_MAX_ORDER) {
@@ -350,6 +362,15 @@ int make_plan(int d, const int* n, const int* r, bool ring, const tt_opts& o, Pl
     if (st.perm231 && st.path == PATH_EXACT_COLS)
       P.max_bt = std::max<size_t>(P.max_bt, (size_t)st.next_elems);
     if (!st.fold) P.max_data = std::max<size_t>(P.max_data, (size_t)st.next_elems);
+    if (st.path == PATH_EXACT_ROWS && st.m > 32 && st.r_eff < st.m && !st.perm231) {
+      // room for a refined exact step (U0: m x b, Z: cols x b)
+      const int b = refine_width(st);
+      P.max_y = std::max<size_t>(P.max_y, (size_t)st.m * b);
+      P.max_bt = std::max<size_t>(P.max_bt, (size_t)st.cols * b);
+      P.max_ws = std::max(P.max_ws, project_ws_bytes(st.m, st.cols, b));
+      P.max_ws = std::max(P.max_ws, project_ws_bytes(b, st.cols, st.r_req));
+      P.max_ws = std::max(P.max_ws, gram_ws_bytes(st.cols, b));
+    }
     P.max_core = std::max<size_t>(P.max_core, (size_t)st.m * std::max(st.r_req, st.ks));
     P.max_ef = std::max<size_t>(P.max_ef, (size_t)std::max<long long>(st.m, st.ks) * st.r_req);
     P.max_small = std::max(P.max_small, std::max(st.ks, (int)std::min<long long>(mn, TT_MAX_SMALL)));
@@ -844,6 +865,43 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       // planned full-rank step (the next step's geometry is the same either way).
       const bool fold = st.fold || (adaptive && !ring1 && !st.perm231 && rq == m && re == m && rin == rcore &&
                                     (o.flags & kFlagAdaptiveFold));
+      if (refine_exact(st, engine, adaptive) && !fold) {
+        // Exact Rayleigh-Ritz on the span of the top b eigenvectors of the tensor-core Gram:
+        // that Gram's TF32 rounding tilts eigenvectors of close eigenvalues (a flat spectrum
+        // around the cut), which would change the kept subspace; the span of b = r + 16 of them
+        // holds the exact top-r subspace to ~1e-5, and Z = A^T U0 (FP32 FMA, FP64 Gram) gives
+        // the exact Ritz pairs.  The next data E_r^T Z^T replaces the projection pass.
+        const int b = refine_width(st);
+        npasses += 1;
+        TT_TRY(launch_f64_to_f32_cols(B.evecs, m, m, b, B.yf, m, b, s));
+        TT_TRY(pass.run(TT_PASS_PROJECT, 2.0 * m * cols * b, 4.0 * m * cols + 4.0 * b * cols, [&] {
+          return launch_project(cur, m, cols, B.yf, b, m, B.bt, b, OUT_ROWMAJOR, 1, 1, TT_GEMM_FP32, ws, c->dstat,
+                                s);
+        }));
+        TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * b * b, 4.0 * cols * b,
+                        [&] { return launch_gram(B.bt, cols, b, b, 1, B.w, true, ws, s); }));
+        TT_TRY(launch_syev(B.w, b, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
+        k_store_sigma<<<1, 64, 0, s>>>(B.evals, std::min(b, TT_STATS_MAX_SIGMA), sigdst);
+        count_launch();
+        float* ubuf = B.corebuf;
+        TT_TRY(launch_small_nn(B.yf, m, b, m, B.evecs, rq, b, nullptr, re, ubuf, m, s));  // U = U0 E_r
+        TT_TRY(launch_canon_cols(ubuf, m, re, m, B.evecs, b, b, s));
+        if (ring1) {
+          TT_TRY(launch_ring_core1(ubuf, (int)m, P.r[0], P.r[1], cores[0], s));
+        } else {
+          TT_TRY(join_side());
+          TT_TRY(emit_core(ubuf, core_dst, pend, rin, rcore, ni, rq, s));
+        }
+        TT_TRY(launch_f64_to_f32_cols(B.evecs, b, b, re, B.ef, b, rq, s));
+        TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * b * cols * nout, 4.0 * b * cols + 4.0 * nout * cols, [&] {
+          return launch_project(B.bt, b, cols, B.ef, nout, b, next, st.perm231 ? 0 : nout,
+                                st.perm231 ? OUT_PERM231 : OUT_ROWMAJOR, P.r[0], pr1, TT_GEMM_FP32, ws, c->dstat, s);
+        }));
+        pend = nullptr;
+        cur = next;
+        slot ^= 1;
+        continue;
+      }
       // basis (m x r_req, zero-padded beyond r_eff), FP32, canonical column signs
       TT_TRY(launch_f64_to_f32_cols(B.evecs, m, m, re, B.ef, m, rq, s));
       TT_TRY(launch_canon_cols(B.ef, m, re, m, B.evecs, (int)m, m, s));
@@ -937,17 +995,14 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
                                 (adaptive && !tc_b) ? TT_GEMM_FP32 : engine, ws, c->dstat, s);
         }));
         // Gram of the small factor B (ksa x cols, column-major = B^T row-major): the input of
-        // the eigen-based small SVD (TT3O:717), on the tensor cores for long B.
-        // Adaptive ranks read ||A||^2 - sum(lambda) down to delta^2 = eps^2 ||X||^2 / (d - 1): the
-        // eigenvalue sum must then hold ~1e-8 relative, which the tensor-core Gram (TF32
-        // operands, FP32 accumulation within 2048-column units) does not guarantee on short B.
-        TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ksa * ksa, 4.0 * cols * ksa, [&] {
-          if (engine == TT_GEMM_TC && !adaptive) {
-            const int rc = launch_gram_tc(B.bt, ksa, cols, B.w, ws, c->dstat, s);
-            if (rc != TT_ERR_UNSUPPORTED) return rc;
-          }
-          return launch_gram(B.bt, cols, ksa, ksa, 1, B.w, true, ws, s);
-        }));
+        // the eigen-based small SVD (TT3O:717), on the CUDA cores with FP64 products in every
+        // form.  Its eigenvectors choose the r kept directions out of ksa; the tensor cores'
+        // operand rounding and truncating accumulation tilt them by ~1e-4, which leaks ~1e-7 of
+        // the signal energy per step into the discarded directions (measured: rel. error 8.7e-4
+        // instead of 2.8e-4 on the 32^6 chain at p = 0).  B is ksa / m of the unfolding, so this
+        // pass is short.
+        TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ksa * ksa, 4.0 * cols * ksa,
+                        [&] { return launch_gram(B.bt, cols, ksa, ksa, 1, B.w, true, ws, s); }));
         TT_TRY(launch_syev(B.w, ksa, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
         k_store_sigma<<<1, 64, 0, s>>>(B.evals, std::min(ksa, TT_STATS_MAX_SIGMA), sigdst);
         count_launch();
