@@ -995,14 +995,17 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
                                 (adaptive && !tc_b) ? TT_GEMM_FP32 : engine, ws, c->dstat, s);
         }));
         // Gram of the small factor B (ksa x cols, column-major = B^T row-major): the input of
-        // the eigen-based small SVD (TT3O:717), on the CUDA cores with FP64 products in every
-        // form.  Its eigenvectors choose the r kept directions out of ksa; the tensor cores'
-        // operand rounding and truncating accumulation tilt them by ~1e-4, which leaks ~1e-7 of
-        // the signal energy per step into the discarded directions (measured: rel. error 8.7e-4
-        // instead of 2.8e-4 on the 32^6 chain at p = 0).  B is ksa / m of the unfolding, so this
-        // pass is short.
-        TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ksa * ksa, 4.0 * cols * ksa,
-                        [&] { return launch_gram(B.bt, cols, ksa, ksa, 1, B.w, true, ws, s); }));
+        // the eigen-based small SVD (TT3O:717), on the tensor cores for long B.
+        // Adaptive ranks read ||A||^2 - sum(lambda) down to delta^2 = eps^2 ||X||^2 / (d - 1): the
+        // eigenvalue sum must then hold ~1e-8 relative, which the tensor-core Gram (TF32
+        // operands, FP32 accumulation within 2048-column units) does not guarantee on short B.
+        TT_TRY(pass.run(TT_PASS_OTHER, 2.0 * cols * ksa * ksa, 4.0 * cols * ksa, [&] {
+          if (engine == TT_GEMM_TC && !adaptive) {
+            const int rc = launch_gram_tc(B.bt, ksa, cols, B.w, ws, c->dstat, s);
+            if (rc != TT_ERR_UNSUPPORTED) return rc;
+          }
+          return launch_gram(B.bt, cols, ksa, ksa, 1, B.w, true, ws, s);
+        }));
         TT_TRY(launch_syev(B.w, ksa, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
         k_store_sigma<<<1, 64, 0, s>>>(B.evals, std::min(ksa, TT_STATS_MAX_SIGMA), sigdst);
         count_launch();

@@ -16,10 +16,11 @@ module builds its training set and trains it with the library's own GPU kernels:
   statistics (and every EDrSVD quantity) of A and of diag(sigma) have the same distribution.
 * Labels (the plain method in FP64): the rank r* of the exact truncated SVD at tolerance tol
   (smallest r with sum_{i>r} sigma_i^2 <= tol^2 sum sigma_i^2), and the cheapest (power
-  iterations p, oversampling s) for which the FP64 EDrSVD with r* + s columns leaves at most
-  half of tol^2 of the energy outside its subspace in every trial (the half leaves room for the
-  noise of the probe-based a-posteriori estimate that judges a learned attempt): fewer passes
-  over A first (2 + 2p), then the narrower sketch.
+  iterations p, oversampling s) for which the EDrSVD with r* + s columns, its passes over A
+  perturbed by the tensor cores' TF32 operand rounding (the engine the learned form runs on),
+  leaves at most half of tol^2 of the energy outside its subspace in every trial (the half
+  leaves room for the noise of the probe-based a-posteriori estimate that judges a learned
+  attempt): fewer passes over A first (2 + 2p), then the narrower sketch.
 * Training: ``tt_mlp_train`` (Adam, one persistent launch), on 90 % of the samples; the rest
   measure the validation loss.
 
@@ -82,14 +83,29 @@ def _orth(y):
     return q
 
 
-def edrsvd_outside(sig, ks, p, rng):
-    """Energy share outside the EDrSVD subspace of diag(sig) (ks columns, p power iterations)."""
+# Relative RMS of the TF32 rounding of an FP32 operand (10 stored mantissa bits, round to
+# nearest): the learned form's sketch and power passes run on the tensor cores, and this white
+# noise, about as strong per direction as a 1e-4 noise floor, perturbs the captured range.
+TF32_NOISE = 2.5e-4
+
+
+def edrsvd_outside(sig, ks, p, rng, op_noise=TF32_NOISE):
+    """Energy share outside the EDrSVD subspace of A = diag(sig) (ks columns, p power
+    iterations), every pass over A seeing A plus fresh white noise of relative RMS op_noise per
+    element of a dense A of the same spectrum (the tensor cores' operand rounding)."""
     k = sig.size
-    q = _orth(sig[:, None] * rng.standard_normal((k, ks)))
-    for _ in range(p):
-        z = _orth(sig[:, None] * q)      # A^T Q (A = diag(sig) is symmetric)
-        q = _orth(sig[:, None] * z)      # A Z
     e = sig * sig
+    g_sd = op_noise * np.sqrt(e.sum()) / k  # per-entry sd: ||G||_F = op_noise ||A||_F
+
+    def mul(x):  # (A + G) x with a fresh G
+        out = sig[:, None] * x
+        if g_sd > 0.0:
+            out += g_sd * (rng.standard_normal((k, k)) @ x)
+        return out
+    q = _orth(mul(rng.standard_normal((k, ks))))
+    for _ in range(p):
+        z = _orth(mul(q))               # A^T Q (A = diag(sig) is symmetric)
+        q = _orth(mul(z))               # A Z
     captured = float(np.sum(e[:, None] * q * q))
     return max(e.sum() - captured, 0.0) / e.sum()
 
