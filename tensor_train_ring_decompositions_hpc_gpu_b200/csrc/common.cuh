@@ -66,6 +66,20 @@ inline int smem_optin_k(K* kernel, size_t bytes) {
   return smem_optin(reinterpret_cast<const void*>(kernel), bytes);
 }
 
+// Paired FP32 FMA (fma.rn.f32x2: two lanes of an FP32 pair per issue slot, each rounded like
+// fmaf) and the moves in and out of a pair.
+__device__ __forceinline__ uint64_t f2_dup(float a) {
+  uint64_t r;
+  asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(a));
+  return r;
+}
+__device__ __forceinline__ void f2_unpack(uint64_t v, float& lo, float& hi) {
+  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
+}
+__device__ __forceinline__ void ffma2(uint64_t& d, uint64_t a, uint64_t b) {
+  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
+}
+
 // Launch-count accounting (kernels launched by the current library call).
 extern thread_local int g_kernel_launches;
 inline void count_launch(int n = 1) { g_kernel_launches += n; }

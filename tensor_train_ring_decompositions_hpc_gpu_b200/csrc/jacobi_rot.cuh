@@ -4,12 +4,6 @@
 
 namespace ttr {
 
-// Rotation (c, s) annihilating a_pq of the 2 x 2 block [[a_pp, a_pq], [a_pq, a_qq]] (values
-// scaled by inv_s for the skip test).  Returns false (c = 1, s = 0) when a_pq is negligible.
-// t = sign(d) e / (|d| + sqrt(d^2 + e^2)) with d = a_qq - a_pp, e = 2 a_pq is the smaller root of
-// t^2 + 2 (d / e) t - 1 = 0, formed without the quotient d / e; FP32 suffices for t.
-// c = 1 / sqrt(1 + t^2) to FP64 precision: FP32 estimate, then two Newton steps
-// y <- y (3 - x y^2) / 2, each squaring the relative error.
 // Whether the pair (p, q) is rotated: |a_pq| above 1e-12 of sqrt(a_pp a_qq) and above 1e-14 of
 // the largest diagonal (values scaled by inv_s = 1 / that diagonal).  Eigenvalues then carry
 // (1e-12)^2 relative error, residuals 1e-12 of the norm, and the solve ends about one sweep
@@ -19,34 +13,45 @@ __device__ __forceinline__ bool jacobi_needed(double app, double aqq, double apq
   return fabs(as) > 1e-14 && as * as > 1e-24 * fabs(ps * qs);
 }
 
-// The rotation in two halves: the FP32 tangent t (0 when the pair is not rotated), and (c, s)
-// from t in FP64.  The large-N solver logs t per pair and round and rebuilds (c, s) from it when it
-// replays the rotations on the eigenvectors: the same arithmetic gives the same bits.
-__device__ __forceinline__ float jacobi_tf(double app, double aqq, double apq, double inv_s) {
-  if (!jacobi_needed(app, aqq, apq, inv_s)) return 0.0f;
+// The rotation annihilating a_pq of [[a_pp, a_pq], [a_pq, a_qq]] in two halves, so that the
+// latency-critical part is short: an FP32 (c, s) and an FP64 renormalisation.
+//
+// FP32 half: with d = a_qq - a_pp (formed in FP64, then rounded), e = 2 a_pq, h = sqrt(d^2 + e^2)
+// and u = h + |d|, the smaller-angle rotation has t = sign(d) e / u, and since
+// 1 + t^2 = 2 h u / u^2,
+//     c = u / sqrt(2 h u),   s = sign(d) e / sqrt(2 h u),
+// so two reciprocal square roots (h = x rsqrt(x)) give (c, s) with no division.  Both factors of s
+// carry small relative errors, so the rotation leaves ~1e-7 |a_pq| behind however small the
+// angle.  (1, 0) when the pair is not rotated.  The skip test runs in FP64 beside the FP32 path.
+__device__ __forceinline__ float2 jacobi_cs32(double app, double aqq, double apq, double inv_s) {
   const double ps = app * inv_s, qs = aqq * inv_s, as = apq * inv_s;
+  const bool need = fabs(as) > 1e-14 && as * as > 1e-24 * fabs(ps * qs);
   const float d = (float)(qs - ps), e = 2.0f * (float)as;
-  const float h = sqrtf(fmaf(d, d, e * e));
-  return (d >= 0.0f ? e : -e) * __frcp_rn(fabsf(d) + h);
+  const float x = fmaf(d, d, e * e);
+  const float h = need ? x * rsqrtf(x) : 1.0f;
+  const float u = h + fabsf(d);
+  const float w = rsqrtf(2.0f * h * u);
+  const float c = u * w, s = (d >= 0.0f ? e : -e) * w;
+  return need ? make_float2(c, s) : make_float2(1.0f, 0.0f);
 }
 
-__device__ __forceinline__ void rot_from_tf(float tf, double& c, double& s) {
-  const double t = (double)tf;
-  const double x = fma(t, t, 1.0);
-  double y = (double)rsqrtf((float)x);
-  y = y * fma(-0.5 * x, y * y, 1.5);
-  y = y * fma(-0.5 * x, y * y, 1.5);
-  c = y;
-  s = t * y;
+// FP64 (c, s) from the FP32 pair: with dl = c32^2 + s32^2 - 1 (the products are exact in FP64),
+// scale both by 1 / sqrt(1 + dl) = 1 - dl/2 + 3 dl^2 / 8 + O(dl^3); |dl| ~ 1e-7, so the applied
+// rotation is orthogonal to FP64 rounding.  (1, 0) stays (1, 0) exactly.  A solver that logs the
+// FP32 pairs and replays them rebuilds bit-identical rotations with this function.
+__device__ __forceinline__ void rot_from_cs32(float2 r, double& c, double& s) {
+  const double c0 = r.x, s0 = r.y;
+  const double dl = fma(c0, c0, fma(s0, s0, -1.0));
+  const double g = fma(dl, fma(dl, 0.375, -0.5), 1.0);
+  c = c0 * g;
+  s = s0 * g;
 }
 
 __device__ __forceinline__ bool jacobi_rotation(double app, double aqq, double apq, double inv_s, double& c,
                                                 double& s) {
-  c = 1.0;
-  s = 0.0;
-  if (!jacobi_needed(app, aqq, apq, inv_s)) return false;
-  rot_from_tf(jacobi_tf(app, aqq, apq, inv_s), c, s);
-  return true;
+  const float2 r = jacobi_cs32(app, aqq, apq, inv_s);
+  rot_from_cs32(r, c, s);
+  return r.y != 0.0f;
 }
 
 }  // namespace ttr

@@ -102,21 +102,56 @@ int launch_gaussian(float* out, long long rows, int cols, long long ld, unsigned
 // ---------------------------------------------------------------------------------------
 // Plain-FP32 sketch  Y = A * W  (split over the long dimension n, FP64 reduction of splits)
 // ---------------------------------------------------------------------------------------
-// 256 rows of A per block (8 per thread) x NT sketch columns (NT / 8 per thread), the long
-// dimension in chunks of 32 columns of A: the next chunk is loaded into registers while the
-// current one is multiplied out of shared memory (two buffers, one barrier per chunk).
+// Asynchronous global -> shared copies (cp.async): 16-byte, and 4-byte with zero fill when
+// `valid` is false (no byte is read then).
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async4(void* dst, const void* src, bool valid) {
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4, %2;" ::"r"((unsigned)__cvta_generic_to_shared(dst)),
+               "l"(src), "r"(valid ? 4 : 0)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int PENDING>
+__device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(PENDING) : "memory");
+}
+
+// 32 x RI rows of A per block (RI per thread) x NT sketch columns (NT / 8 per thread); narrow
+// sketches (NT <= 24) take RI = 16 rows per thread, so that each shared-memory load feeds more
+// FMAs.  The long dimension runs in chunks of JC columns of A (32 KB of A per chunk) streamed
+// through a 3-stage shared-memory ring by cp.async (two chunks in flight while the third is
+// multiplied: the loads need no registers), one barrier per chunk.  Products by paired FP32 FMAs
+// (fma.rn.f32x2, each lane rounded like fmaf), the row pairs straight from 16-byte shared loads;
+// W's rows are padded to NT + 1 words so its copies (JC consecutive rows per warp) hit distinct
+// banks.  Split partials are written in FP64.
+constexpr int kSkStages = 3;
+template <int NT>
+struct SkTile {
+  static constexpr int RI = NT <= 24 ? 16 : 8;  // rows per thread
+  static constexpr int TI = 32 * RI;             // rows per block
+  static constexpr int JC = 8192 / TI;           // columns of A per chunk (TI x JC = 8192 floats)
+  static constexpr int NTP = NT + 1;             // padded row of W in shared memory
+  static constexpr size_t smem = (size_t)kSkStages * (TI * JC + JC * NTP) * sizeof(float);
+};
+template <int NT>
+constexpr size_t sk_smem() { return SkTile<NT>::smem; }
+
 template <int NT>
 __global__ void __launch_bounds__(256, NT >= 40 ? 1 : 2) k_sketch_simt(const float* __restrict__ a, long long m,
                                                                        long long n, const float* __restrict__ w,
                                                                        int N, long long wj, long long wc,
                                                                        long long jchunk, int cblk,
                                                                        double* __restrict__ part) {
-  constexpr int TI = 256, JC = 32, RI = 8, RC = NT / 8;
-  constexpr int AV = (TI * JC / 4) / 256;     // float4 loads of A per thread per chunk
+  using T = SkTile<NT>;
+  constexpr int RI = T::RI, TI = T::TI, JC = T::JC, NTP = T::NTP, RC = NT / 8;
+  constexpr int AV = (TI * JC / 4) / 256;     // 16-byte copies of A per thread per chunk
   constexpr int WV = (JC * NT + 255) / 256;   // W values per thread per chunk
   extern __shared__ __align__(16) float sm_sk[];
-  float* as_base = sm_sk;                // [2][JC][TI]
-  float* ws_base = sm_sk + 2 * JC * TI;  // [2][JC][NT]
+  float* as_base = sm_sk;                            // [ST][JC][TI]
+  float* ws_base = sm_sk + kSkStages * JC * TI;      // [ST][JC][NTP]
   const int tid = threadIdx.x;
   const long long i0 = (long long)blockIdx.x * TI;
   const int split = blockIdx.y;
@@ -124,104 +159,92 @@ __global__ void __launch_bounds__(256, NT >= 40 ? 1 : 2) k_sketch_simt(const flo
   const long long jb = (long long)split * jchunk;
   const long long je = (jb + jchunk < n) ? jb + jchunk : n;
   const int ti = tid >> 3, tc = tid & 7;
-  float acc[RI][RC];
+  // accumulators paired over rows: acc2[p][c] = (acc[2p][c], acc[2p + 1][c])
+  uint64_t acc2[RI / 2][RC];
 #pragma unroll
-  for (int e = 0; e < RI; ++e)
+  for (int e = 0; e < RI / 2; ++e)
 #pragma unroll
-    for (int c = 0; c < RC; ++c) acc[e][c] = 0.f;
+    for (int c = 0; c < RC; ++c) acc2[e][c] = 0ull;
   const bool vec = ((m & 3) == 0) && ((((uintptr_t)a) & 15) == 0);
-  float4 ra[AV];
-  float rw[WV];
-  auto fetch = [&](long long j0) {
+  const int nchunks = je > jb ? (int)((je - jb + JC - 1) / JC) : 0;
+  // Copies of chunk t into ring slot t % ST (one commit group per chunk, empty past the end).
+  auto fill = [&](int t) {
+    if (t < nchunks) {
+      const long long j0 = jb + (long long)t * JC;
+      float* as = as_base + (t % kSkStages) * JC * TI;
+      float* wsm = ws_base + (t % kSkStages) * JC * NTP;
 #pragma unroll
-    for (int q = 0; q < AV; ++q) {
-      const int f = tid + 256 * q;
-      const int jj = f / (TI / 4), i4 = f % (TI / 4);
-      const long long j = j0 + jj, i = i0 + 4 * i4;
-      float4 v = make_float4(0.f, 0.f, 0.f, 0.f);
-      if (j < je) {
-        const float* p = a + j * m + i;
-        if (vec && i + 3 < m) {
-          v = __ldg(reinterpret_cast<const float4*>(p));
+      for (int q = 0; q < AV; ++q) {
+        const int f = tid + 256 * q;
+        const int jj = f / (TI / 4), i4 = f % (TI / 4);
+        const long long j = j0 + jj, i = i0 + 4 * i4;
+        float* dst = &as[jj * TI + 4 * i4];
+        const float* src = a + j * m + i;
+        if (j < je && vec && i + 3 < m) {
+          cp_async16(dst, src);
         } else {
-          if (i < m) v.x = p[0];
-          if (i + 1 < m) v.y = p[1];
-          if (i + 2 < m) v.z = p[2];
-          if (i + 3 < m) v.w = p[3];
+#pragma unroll
+          for (int e = 0; e < 4; ++e) {
+            const bool ok = j < je && i + e < m;
+            cp_async4(dst + e, ok ? src + e : a, ok);
+          }
         }
       }
-      ra[q] = v;
-    }
 #pragma unroll
-    for (int u = 0; u < WV; ++u) {
-      const int f = tid + 256 * u;
-      int jj, c;
-      if (wc == 1) {
-        c = f % NT;
-        jj = f / NT;
-      } else {
-        jj = f % JC;
-        c = f / JC;
-      }
-      const long long j = j0 + jj;
-      rw[u] = (f < JC * NT && j < je && c0 + c < N) ? w[j * wj + (long long)(c0 + c) * wc] : 0.f;
-    }
-  };
-  auto stash = [&](int b) {
-    float* as = as_base + b * JC * TI;
-    float* wsm = ws_base + b * JC * NT;
-#pragma unroll
-    for (int q = 0; q < AV; ++q) {
-      const int f = tid + 256 * q;
-      const int jj = f / (TI / 4), i4 = f % (TI / 4);
-      *reinterpret_cast<float4*>(&as[jj * TI + 4 * i4]) = ra[q];
-    }
-#pragma unroll
-    for (int u = 0; u < WV; ++u) {
-      const int f = tid + 256 * u;
-      if (f < JC * NT) {
-        if (wc == 1)
-          wsm[(f / NT) * NT + f % NT] = rw[u];
-        else
-          wsm[(f % JC) * NT + f / JC] = rw[u];
+      for (int u = 0; u < WV; ++u) {
+        const int f = tid + 256 * u;
+        if (f < JC * NT) {
+          int jj, c;
+          if (wc == 1) {
+            c = f % NT;
+            jj = f / NT;
+          } else {
+            jj = f % JC;
+            c = f / JC;
+          }
+          const long long j = j0 + jj;
+          const bool ok = j < je && c0 + c < N;
+          cp_async4(&wsm[jj * NTP + c], ok ? w + j * wj + (long long)(c0 + c) * wc : w, ok);
+        }
       }
     }
+    cp_async_commit();
   };
-  if (jb < je) {
-    fetch(jb);
-    stash(0);
-  }
-  __syncthreads();
-  int b = 0;
-  for (long long j0 = jb; j0 < je; j0 += JC) {
-    const bool more = j0 + JC < je;
-    if (more) fetch(j0 + JC);
-    const float* as = as_base + b * JC * TI;
-    const float* wsm = ws_base + b * JC * NT;
+  fill(0);
+  fill(1);
+  for (int t = 0; t < nchunks; ++t) {
+    cp_async_wait<kSkStages - 2>();  // this thread's copies of chunk t have landed
+    __syncthreads();                 // everyone's have; slot (t + 2) % ST was last read at t - 1
+    fill(t + 2);
+    const float* as = as_base + (t % kSkStages) * JC * TI;
+    const float* wsm = ws_base + (t % kSkStages) * JC * NTP;
 #pragma unroll
     for (int jj = 0; jj < JC; ++jj) {
-      const float4 x0 = *reinterpret_cast<const float4*>(&as[jj * TI + ti * RI]);
-      const float4 x1 = *reinterpret_cast<const float4*>(&as[jj * TI + ti * RI + 4]);
-      const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-      float wv[RC];
+      uint64_t xp[RI / 2];
 #pragma unroll
-      for (int c = 0; c < RC; ++c) wv[c] = wsm[jj * NT + tc * RC + c];
+      for (int q = 0; q < RI / 4; ++q) {
+        const ulonglong2 x = *reinterpret_cast<const ulonglong2*>(&as[jj * TI + ti * RI + 4 * q]);
+        xp[2 * q] = x.x;
+        xp[2 * q + 1] = x.y;
+      }
 #pragma unroll
-      for (int e = 0; e < RI; ++e)
+      for (int c = 0; c < RC; ++c) {
+        const uint64_t wd = f2_dup(wsm[jj * NTP + tc * RC + c]);
 #pragma unroll
-        for (int c = 0; c < RC; ++c) acc[e][c] = fmaf(xv[e], wv[c], acc[e][c]);
+        for (int e = 0; e < RI / 2; ++e) ffma2(acc2[e][c], xp[e], wd);
+      }
     }
-    if (more) stash(b ^ 1);
-    __syncthreads();
-    b ^= 1;
   }
+  cp_async_wait<0>();
 #pragma unroll
   for (int e = 0; e < RI; ++e) {
     const long long i = i0 + ti * RI + e;
 #pragma unroll
     for (int c = 0; c < RC; ++c) {
       const int col = c0 + tc * RC + c;
-      if (i < m && col < N) part[((long long)split * N + col) * m + i] = (double)acc[e][c];
+      float lo, hi;
+      f2_unpack(acc2[e >> 1][c], lo, hi);
+      if (i < m && col < N) part[((long long)split * N + col) * m + i] = (double)((e & 1) ? hi : lo);
     }
   }
   (void)cblk;
@@ -233,9 +256,11 @@ static void launch_sketch_simt_kernel(const float* a, long long m, long long n, 
                                       long long wc, long long jchunk, int nsplit, double* part, cudaStream_t s) {
   const int NT = N <= 16 ? 16 : N <= 24 ? 24 : N <= 32 ? 32 : N <= 40 ? 40 : N <= 48 ? 48 : 64;
   const int cblk = ceil_div(N, NT);
-  dim3 grid(ceil_div(m, 256), nsplit, cblk);
-  const size_t shm = (size_t)2 * 32 * (256 + NT) * sizeof(float);
-#define SK_ATTR(V) smem_optin_k(k_sketch_simt<V>, (size_t)2 * 32 * (256 + V) * 4)
+  const int TI = NT <= 24 ? SkTile<16>::TI : SkTile<64>::TI;
+  dim3 grid(ceil_div(m, TI), nsplit, cblk);
+  const size_t shm = NT == 16 ? sk_smem<16>() : NT == 24 ? sk_smem<24>() : NT == 32 ? sk_smem<32>()
+                   : NT == 40 ? sk_smem<40>() : NT == 48 ? sk_smem<48>() : sk_smem<64>();
+#define SK_ATTR(V) smem_optin_k(k_sketch_simt<V>, sk_smem<V>())
   SK_ATTR(16); SK_ATTR(24); SK_ATTR(32); SK_ATTR(40); SK_ATTR(48); SK_ATTR(64);
 #undef SK_ATTR
 #define SK_CASE(V) \
@@ -383,11 +408,12 @@ __global__ void __launch_bounds__(256, NT >= 64 ? 1 : 2) k_project_simt(const fl
   const long long j0 = (long long)blockIdx.x * TJ;
   const int c0 = blockIdx.y * NT;
   const int tj = tid >> 3, tc = tid & 7;
-  float acc[RJ][RC];
+  // accumulators paired over output rows (fma.rn.f32x2), as in k_sketch_simt
+  uint64_t acc2[RJ / 2][RC];
 #pragma unroll
-  for (int e = 0; e < RJ; ++e)
+  for (int e = 0; e < RJ / 2; ++e)
 #pragma unroll
-    for (int c = 0; c < RC; ++c) acc[e][c] = 0.f;
+    for (int c = 0; c < RC; ++c) acc2[e][c] = 0ull;
   const bool vec = ((m & 3) == 0) && ((((uintptr_t)a) & 15) == 0);
   // K range of this split (blockIdx.z); the split's output block is out + z * n * ldo.
   const long long kb = (long long)blockIdx.z * kchunk;
@@ -454,16 +480,15 @@ __global__ void __launch_bounds__(256, NT >= 64 ? 1 : 2) k_project_simt(const fl
     const float* qs = qs_base + b * KC * NT;
 #pragma unroll
     for (int kk = 0; kk < KC; ++kk) {
-      const float4 x0 = *reinterpret_cast<const float4*>(&as[kk * TJ + swz(kk, tj * RJ)]);
-      const float4 x1 = *reinterpret_cast<const float4*>(&as[kk * TJ + swz(kk, tj * RJ + 4)]);
-      const float xv[8] = {x0.x, x0.y, x0.z, x0.w, x1.x, x1.y, x1.z, x1.w};
-      float qv[RC];
+      const ulonglong2 x0 = *reinterpret_cast<const ulonglong2*>(&as[kk * TJ + swz(kk, tj * RJ)]);
+      const ulonglong2 x1 = *reinterpret_cast<const ulonglong2*>(&as[kk * TJ + swz(kk, tj * RJ + 4)]);
+      const uint64_t xp[4] = {x0.x, x0.y, x1.x, x1.y};
 #pragma unroll
-      for (int c = 0; c < RC; ++c) qv[c] = qs[kk * NT + tc * RC + c];
+      for (int c = 0; c < RC; ++c) {
+        const uint64_t qd = f2_dup(qs[kk * NT + tc * RC + c]);
 #pragma unroll
-      for (int e = 0; e < RJ; ++e)
-#pragma unroll
-        for (int c = 0; c < RC; ++c) acc[e][c] = fmaf(xv[e], qv[c], acc[e][c]);
+        for (int e = 0; e < RJ / 2; ++e) ffma2(acc2[e][c], xp[e], qd);
+      }
     }
     if (more) stash(b ^ 1);
     __syncthreads();
@@ -477,13 +502,16 @@ __global__ void __launch_bounds__(256, NT >= 64 ? 1 : 2) k_project_simt(const fl
     for (int c = 0; c < RC; ++c) {
       const int col = c0 + tc * RC + c;
       if (col >= N) continue;
+      float lo, hi;
+      f2_unpack(acc2[e >> 1][c], lo, hi);
+      const float v = (e & 1) ? hi : lo;
       if (mode == OUT_ROWMAJOR) {
-        out[j * ldo + col] = acc[e][c];
+        out[j * ldo + col] = v;
       } else if (mode == OUT_COLMAJOR) {
-        out[j + ldo * col] = acc[e][c];
+        out[j + ldo * col] = v;
       } else {
         const int ai = col % r0, bi = col / r0;
-        out[(long long)bi + (long long)r1 * (j + n * (long long)ai)] = acc[e][c];
+        out[(long long)bi + (long long)r1 * (j + n * (long long)ai)] = v;
       }
     }
   }
@@ -902,18 +930,9 @@ static void launch_gram_reduce(const double* part, int nblk, int MP, int M, int 
 // per lane (round-to-nearest FMA, unbiased) and are then added into FP64; ACC64 accumulates
 // every product in FP64 instead.
 // ---------------------------------------------------------------------------------------
-__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
-  const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem) : "memory");
-}
 __device__ __forceinline__ void cp_async4(void* smem, const void* gmem) {
   const unsigned d = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(d), "l"(gmem) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
-template <int N>
-__device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory");
 }
 
 constexpr int GV_VC = 192;  // vectors per stage
@@ -1732,36 +1751,71 @@ __global__ void k_mul_upper(const double* __restrict__ r2, const double* __restr
   r[idx] = (j >= i) ? acc : 0.0;
 }
 
-// Single-CTA CholeskyQR2 for sketches that fit in shared memory (n rows x N <= 64 columns):
-// both passes in one launch.  Y is staged row-major with a padded stride S (S/4 odd, so the
-// float4 row accesses of neighbouring threads fall in distinct banks); per pass:
-//   Gram W = Y^T Y in FP64 (4x4 register tiles over the upper tile triangle, row groups
-//   reduced through W), right-looking Cholesky in FP64 (one barrier per column, dead pivots
-//   below rel_tol * max diag), then Q = Y R^-1 by forward substitution, one row per thread in
-//   FP32 registers against an FP32 copy of R (column-major, diagonal stored as 1/r_cc).
-// Optional R output (column-major) = R2 * R1.
+// Cluster helpers: rank in the cluster, cluster size, cluster-wide barrier (release / acquire),
+// and an FP64 load from the same shared-memory offset in another CTA of the cluster.
+__device__ __forceinline__ unsigned cl_rank() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ unsigned cl_size() {
+  unsigned r;
+  asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(r));
+  return r;
+}
+__device__ __forceinline__ void cl_sync() {
+  asm volatile("barrier.cluster.arrive.release.aligned;\n\tbarrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+__device__ __forceinline__ double ld_peer_f64(const double* p, unsigned rank) {
+  const unsigned a = (unsigned)__cvta_generic_to_shared(p);
+  unsigned ra;
+  double v;
+  asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(ra) : "r"(a), "r"(rank));
+  asm volatile("ld.shared::cluster.f64 %0, [%1];" : "=d"(v) : "r"(ra) : "memory");
+  return v;
+}
+
+// CholeskyQR2 of an n x N sketch (N <= 64) in one launch: a cluster of up to 8 CTAs, each
+// holding `rpc` consecutive rows in shared memory.  Y is staged row-major with a padded
+// stride S (S/4 odd, so the float4 row accesses of neighbouring threads fall in distinct
+// banks); per pass:
+//   each CTA's partial Gram Y_c^T Y_c in FP64 (4x4 register tiles over the upper tile
+//   triangle, row groups reduced through shared memory), summed over the cluster through
+//   distributed shared memory in rank order (every CTA gets the same bits, so the redundant
+//   factorisations agree), right-looking Cholesky in FP64 (one barrier per column, dead
+//   pivots below rel_tol * max diag), then Q = Y R^-1 by forward substitution, one row per
+//   thread in FP32 registers against an FP32 copy of R (column-major, diagonal stored as
+//   1/r_cc).
+// Optional R output (column-major) = R2 * R1, written by rank 0.  Each pass has its own partial
+// buffer, so a CTA that runs ahead never overwrites a partial a peer is still reading; the
+// final cluster barrier keeps every CTA's shared memory alive until the peers are done.
 template <int NP>
 __global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, int n, int N, long long vs,
-                                                       long long es, int S, double* __restrict__ r,
-                                                       double rel_tol) {
+                                                       long long es, int S, int rpc,
+                                                       double* __restrict__ r, double rel_tol) {
   constexpr int NT = 512;
   extern __shared__ __align__(16) unsigned char sm_cq[];
-  float* Ys = reinterpret_cast<float*>(sm_cq);                       // n x S
-  double* W = reinterpret_cast<double*>(Ys + (size_t)n * S);         // N x N row-major
+  const unsigned crank = cl_rank(), csize = cl_size();
+  const int row0 = (int)crank * rpc;
+  const int nl = max(0, min(rpc, n - row0));                         // rows of this CTA
   const int WN = (N * N + 1) & ~1;
+  float* Ys = reinterpret_cast<float*>(sm_cq);                       // rpc x S
+  double* Wp = reinterpret_cast<double*>(Ys + (size_t)rpc * S);      // 2 x N x N partials
+  double* W = Wp + 2 * WN;                                           // N x N row-major
   float* Rf = reinterpret_cast<float*>(W + WN);                      // NP x NP, Rf[c*NP+k] = R[k][c]
   float* invd = Rf + NP * NP;                                        // NP
   double* R1 = reinterpret_cast<double*>(invd + NP);                 // N x N (only with r)
   const int tid = threadIdx.x;
   const int TTa = (N + 3) >> 2;
   const int ngrp = S >> 2;
-  for (int f = tid; f < n * ngrp; f += NT) {
-    const int i = f % n, q4 = f / n;
+  for (int f = tid; f < nl * ngrp; f += NT) {
+    const int i = f % nl, q4 = f / nl;
+    const long long gi = row0 + i;
     float v[4];
 #pragma unroll
     for (int e = 0; e < 4; ++e) {
       const int c = 4 * q4 + e;
-      v[e] = (c < N) ? y[(long long)i * vs + (long long)c * es] : 0.f;
+      v[e] = (c < N) ? y[gi * vs + (long long)c * es] : 0.f;
     }
     *reinterpret_cast<float4*>(&Ys[(size_t)i * S + 4 * q4]) = make_float4(v[0], v[1], v[2], v[3]);
   }
@@ -1777,12 +1831,13 @@ __global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, in
   }
   const int tb = ta + rem;
   for (int pass = 0; pass < 2; ++pass) {
+    double* Wq = Wp + pass * WN;
     __syncthreads();
     double acc[16];
 #pragma unroll
     for (int e = 0; e < 16; ++e) acc[e] = 0.0;
     if (act) {
-      for (int v = g; v < n; v += groups) {
+      for (int v = g; v < nl; v += groups) {
         const float4 xa = *reinterpret_cast<const float4*>(&Ys[(size_t)v * S + 4 * ta]);
         const float4 xb = *reinterpret_cast<const float4*>(&Ys[(size_t)v * S + 4 * tb]);
         const double av[4] = {xa.x, xa.y, xa.z, xa.w};
@@ -1800,23 +1855,51 @@ __global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, in
 #pragma unroll
           for (int q = 0; q < 4; ++q) {
             const int i = 4 * ta + p, j = 4 * tb + q;
-            if (i < N && j < N) W[i * N + j] = (gg == 0 ? 0.0 : W[i * N + j]) + acc[p * 4 + q];
+            if (i < N && j < N) Wq[i * N + j] = (gg == 0 ? 0.0 : Wq[i * N + j]) + acc[p * 4 + q];
           }
       }
       __syncthreads();
     }
+    // Sum the partials over the cluster (upper triangle), in rank order.
+    cl_sync();
+    for (int idx = tid; idx < N * N; idx += NT) {
+      const int i = idx / N, j = idx - (idx / N) * N;
+      if (i > j) continue;
+      double a = Wq[idx];
+      if (csize > 1) {
+        a = 0.0;
+        for (unsigned q = 0; q < csize; ++q) a += ld_peer_f64(Wq + idx, q);
+      }
+      W[idx] = a;
+    }
+    __syncthreads();
     double dmax = 0.0;
     for (int k = 0; k < N; ++k) dmax = fmax(dmax, W[k * N + k]);
     const double tol = rel_tol * dmax;
     for (int k = 0; k < N; ++k) {
       const double d = W[k * N + k];
       if (d > tol && dmax > 0.0) {
-        // trailing update of the upper triangle: thread (row group tid >> 6, column tid & 63)
+        // trailing update of the upper triangle: thread (row group tid >> 6, column tid & 63);
+        // the at most 8 rows of a thread are loaded before any is stored
         const double inv = 1.0 / d;
         const int j = k + 1 + (tid & 63);
         if (j < N) {
           const double wkj = W[k * N + j] * inv;
-          for (int i = k + 1 + (tid >> 6); i <= j; i += NT / 64) W[i * N + j] -= W[k * N + i] * wkj;
+          const int i0 = k + 1 + (tid >> 6);
+          double wk[8], wij[8];
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int i = i0 + 8 * u;
+            if (i <= j) {
+              wk[u] = W[k * N + i];
+              wij[u] = W[i * N + j];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 8; ++u) {
+            const int i = i0 + 8 * u;
+            if (i <= j) W[i * N + j] = fma(-wk[u], wkj, wij[u]);
+          }
         }
       }
       __syncthreads();
@@ -1852,13 +1935,13 @@ __global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, in
             const double sk = 1.0 / sqrt(dk);
             for (int j = k; j <= c; ++j) a += W[k * N + j] * sk * R1[j + N * c];
           }
-          r[idx] = a;
+          if (crank == 0) r[idx] = a;
         }
       }
     }
     __syncthreads();
     // Forward substitution q R = y, one row per thread.
-    for (int i = tid; i < n; i += NT) {
+    for (int i = tid; i < nl; i += NT) {
       float q[NP];
 #pragma unroll
       for (int j4 = 0; j4 < NP / 4; ++j4) {
@@ -1890,28 +1973,38 @@ __global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, in
             *reinterpret_cast<float4*>(&Ys[(size_t)i * S + 4 * j4]) =
                 make_float4(q[4 * j4], q[4 * j4 + 1], q[4 * j4 + 2], q[4 * j4 + 3]);
       } else {
+        const long long gi = row0 + i;
 #pragma unroll
         for (int c = 0; c < NP; ++c)
-          if (c < N) y[(long long)i * vs + (long long)c * es] = q[c];
+          if (c < N) y[gi * vs + (long long)c * es] = q[c];
       }
     }
   }
+  cl_sync();  // peers may still be reading this CTA's second partial
 }
 
 static int max_optin_smem() { return dev_smem_max(); }
 
-// Shared-memory bytes of k_cholqr2_small, or 0 when the sketch does not fit.
-static size_t cholqr2_small_smem(long long n, int N, bool want_r, int* S_out) {
+// Cluster shape and shared-memory bytes of k_cholqr2_small: the fewest CTAs (at most 8) with
+// at least 128 rows each that fit in shared memory; 0 when the sketch does not fit.
+static size_t cholqr2_small_smem(long long n, int N, bool want_r, int* S_out, int* cl_out, int* rpc_out) {
   if (N < 1 || N > 64 || n < 1 || n > (1LL << 20)) return 0;
   const int NP = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : 64;
   int S = 4 * ((N + 3) / 4);
   if (((S / 4) & 1) == 0) S += 4;
   const size_t WN = ((size_t)N * N + 1) & ~(size_t)1;
-  const size_t bytes = (size_t)n * S * 4 + WN * 8 + (size_t)NP * NP * 4 + NP * 4 +
-                       (want_r ? (size_t)N * N * 8 : 0);
-  if (bytes > (size_t)max_optin_smem()) return 0;
-  *S_out = S;
-  return bytes;
+  const size_t fixed = 3 * WN * 8 + (size_t)NP * NP * 4 + NP * 4 + (want_r ? (size_t)N * N * 8 : 0);
+  for (int cl = (int)std::min<long long>(8, std::max<long long>(1, (n + 127) / 128)); cl <= 8; ++cl) {
+    const long long rpc = (n + cl - 1) / cl;
+    const size_t bytes = (size_t)rpc * S * 4 + fixed;
+    if (bytes <= (size_t)max_optin_smem()) {
+      *S_out = S;
+      *cl_out = cl;
+      *rpc_out = (int)rpc;
+      return bytes;
+    }
+  }
+  return 0;
 }
 
 static int cholqr_passes(float* y, long long n, int N, long long vs, long long es, double* r, Arena& ws,
@@ -1940,8 +2033,8 @@ static int cholqr_passes(float* y, long long n, int N, long long vs, long long e
     set_error(TT_ERR_UNSUPPORTED, "cholqr2 width %d > %d", N, TT_MAX_SMALL);
     return TT_ERR_UNSUPPORTED;
   }
-  int S = 0;
-  const size_t sshm = cholqr2_small_smem(n, N, r != nullptr, &S);
+  int S = 0, cl = 1, rpc = 0;
+  const size_t sshm = cholqr2_small_smem(n, N, r != nullptr, &S, &cl, &rpc);
   if (sshm > 0) {
     {
       const int mx = max_optin_smem();
@@ -1950,18 +2043,37 @@ static int cholqr_passes(float* y, long long n, int N, long long vs, long long e
       smem_optin_k(k_cholqr2_small<48>, mx);
       smem_optin_k(k_cholqr2_small<64>, mx);
     }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(cl, 1, 1);
+    cfg.blockDim = dim3(512, 1, 1);
+    cfg.dynamicSmemBytes = sshm;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = cl;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
     const int nn = (int)n;
+    const double tol = 1e-12;
+    cudaError_t e;
     if (N <= 16)
-      k_cholqr2_small<16><<<1, 512, sshm, s>>>(y, nn, N, vs, es, S, r, 1e-12);
+      e = cudaLaunchKernelEx(&cfg, k_cholqr2_small<16>, y, nn, N, vs, es, S, rpc, r, tol);
     else if (N <= 32)
-      k_cholqr2_small<32><<<1, 512, sshm, s>>>(y, nn, N, vs, es, S, r, 1e-12);
+      e = cudaLaunchKernelEx(&cfg, k_cholqr2_small<32>, y, nn, N, vs, es, S, rpc, r, tol);
     else if (N <= 48)
-      k_cholqr2_small<48><<<1, 512, sshm, s>>>(y, nn, N, vs, es, S, r, 1e-12);
+      e = cudaLaunchKernelEx(&cfg, k_cholqr2_small<48>, y, nn, N, vs, es, S, rpc, r, tol);
     else
-      k_cholqr2_small<64><<<1, 512, sshm, s>>>(y, nn, N, vs, es, S, r, 1e-12);
-    count_launch();
-    TT_LAUNCH_CHECK();
-    return TT_OK;
+      e = cudaLaunchKernelEx(&cfg, k_cholqr2_small<64>, y, nn, N, vs, es, S, rpc, r, tol);
+    if (e == cudaSuccess) {
+      count_launch();
+      TT_LAUNCH_CHECK();
+      return TT_OK;
+    }
+    // A cluster that cannot be placed (its CTAs' shared memory on one GPC) falls through to the
+    // multi-launch path below.
+    (void)cudaGetLastError();
   }
   const size_t mk = ws.mark();
   double* w = ws.take<double>((size_t)N * N);
@@ -2012,142 +2124,27 @@ static int cholqr_passes(float* y, long long n, int N, long long vs, long long e
 // ---------------------------------------------------------------------------------------
 // Symmetric eigen-decomposition: parallel cyclic Jacobi (round-robin pairs), FP64
 // ---------------------------------------------------------------------------------------
-// W is held row-major in shared memory, V in shared memory (N <= 64) or global memory.
-template <bool VSMEM>
-__global__ void __launch_bounds__(256) k_syev_jacobi(const double* __restrict__ w_in, int N,
-                                                     double* __restrict__ evals,
-                                                     double* __restrict__ evecs,
-                                                     double* __restrict__ vglob, int max_sweeps,
-                                                     DevStatus* st) {
-  extern __shared__ double sm[];
-  const int Np = N + (N & 1);
-  double* W = sm;                             // Np x Np
-  double* V = VSMEM ? sm + Np * Np : vglob;   // Np x Np
-  double* cs = sm + (VSMEM ? 2 : 1) * Np * Np;
-  double* sn = cs + Np / 2;
-  int* pp = reinterpret_cast<int*>(sn + Np / 2);
-  int* qq = pp + Np / 2;
-  int* order = qq + Np / 2;
-  __shared__ int nrot;
-  __shared__ double floor_abs;
-  const int tid = threadIdx.x, nt = blockDim.x;
-  for (int idx = tid; idx < Np * Np; idx += nt) {
-    const int i = idx / Np, j = idx % Np;
-    // symmetrised: Grams from the tensor cores differ between (i, j) and (j, i) by rounding
-    W[idx] = (i < N && j < N) ? 0.5 * (w_in[i + (long long)N * j] + w_in[j + (long long)N * i]) : 0.0;
-    V[idx] = (i == j) ? 1.0 : 0.0;
-  }
-  __syncthreads();
-  if (tid == 0) {
-    double dm = 0.0;
-    for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(W[i * Np + i]));
-    floor_abs = 1e-15 * dm;
-  }
-  __syncthreads();
-  const double tol = 1e-14;
-  int sweep = 0;
-  bool converged = false;
-  for (; sweep < max_sweeps; ++sweep) {
-    if (tid == 0) nrot = 0;
-    __syncthreads();
-    for (int rnd = 0; rnd < Np - 1; ++rnd) {
-      for (int k = tid; k < Np / 2; k += nt) {
-        const int x = k, y = Np - 1 - k;
-        int p = (x == 0) ? 0 : 1 + (x - 1 + rnd) % (Np - 1);
-        int q = (y == 0) ? 0 : 1 + (y - 1 + rnd) % (Np - 1);
-        if (p > q) {
-          const int t = p;
-          p = q;
-          q = t;
-        }
-        double c = 1.0, s = 0.0;
-        if (q < N) {
-          const double apq = W[p * Np + q], app = W[p * Np + p], aqq = W[q * Np + q];
-          if (fabs(apq) > tol * sqrt(fabs(app * aqq)) && fabs(apq) > floor_abs) {
-            const double theta = (aqq - app) / (2.0 * apq);
-            const double t = (theta >= 0 ? 1.0 : -1.0) / (fabs(theta) + sqrt(1.0 + theta * theta));
-            c = 1.0 / sqrt(1.0 + t * t);
-            s = t * c;
-            atomicAdd(&nrot, 1);
-          }
-        }
-        cs[k] = c;
-        sn[k] = s;
-        pp[k] = p;
-        qq[k] = q;
-      }
-      __syncthreads();
-      // rows: W <- J^T W
-      for (int idx = tid; idx < (Np / 2) * Np; idx += nt) {
-        const int k = idx / Np, j = idx % Np;
-        const double c = cs[k], s = sn[k];
-        if (s == 0.0) continue;
-        const int p = pp[k], q = qq[k];
-        const double wp = W[p * Np + j], wq = W[q * Np + j];
-        W[p * Np + j] = c * wp - s * wq;
-        W[q * Np + j] = s * wp + c * wq;
-      }
-      __syncthreads();
-      // columns: W <- W J, V <- V J
-      for (int idx = tid; idx < (Np / 2) * Np; idx += nt) {
-        const int k = idx / Np, i = idx % Np;
-        const double c = cs[k], s = sn[k];
-        if (s == 0.0) continue;
-        const int p = pp[k], q = qq[k];
-        const double wp = W[i * Np + p], wq = W[i * Np + q];
-        W[i * Np + p] = c * wp - s * wq;
-        W[i * Np + q] = s * wp + c * wq;
-        const double vp = V[i * Np + p], vq = V[i * Np + q];
-        V[i * Np + p] = c * vp - s * vq;
-        V[i * Np + q] = s * vp + c * vq;
-      }
-      __syncthreads();
-    }
-    if (nrot == 0) {
-      converged = true;
-      break;
-    }
-    __syncthreads();
-  }
-  if (tid == 0) {
-    for (int i = 0; i < N; ++i) order[i] = i;
-    for (int i = 0; i < N; ++i) {  // selection sort, descending eigenvalues
-      int best = i;
-      for (int j = i + 1; j < N; ++j)
-        if (W[order[j] * Np + order[j]] > W[order[best] * Np + order[best]]) best = j;
-      const int t = order[i];
-      order[i] = order[best];
-      order[best] = t;
-    }
-    if (st) {
-      atomicMax(&st->sweeps, sweep + 1);
-      if (!converged) dev_fail(st, TT_ERR_NOCONV, sweep);
-    }
-  }
-  __syncthreads();
-  for (int idx = tid; idx < N * N; idx += nt) {
-    const int i = idx % N, a = idx / N;
-    evecs[i + (long long)N * a] = V[i * Np + order[a]];
-  }
-  for (int a = tid; a < N; a += nt) evals[a] = W[order[a] * Np + order[a]];
-}
-
 // Small-N variant (N <= 64): parallel cyclic Jacobi in the Brent-Luk layout.
-// W and V are stored by physical position: the two indices of rotation pair k always sit at
-// positions 2k and 2k+1, so a round is a block-local update W' = J^T W J (each 2 x 2 block of
-// W from itself and the two rotations of its row and column pairs) and V' = V J (each row's
-// 1 x 2 blocks), written straight to the positions the indices take next round (a fixed map
-// `mv`: the round-robin tournament shifts every index but index 0 by one slot per round).
-// W is kept in its upper triangle only (each entry stored once, at its upper position), which
-// halves the scattered stores; a block row is read as one 16-byte load.
-// The last warp computes the next round's rotations meanwhile, from the current blocks and
-// rotations, so a round needs one barrier.  W is symmetrised on input ((W + W^T) / 2), and
-// only the upper blocks are computed (mirrored on store).
-// Rotation angle: t from an FP32 evaluation of theta on the matrix scaled by its largest
-// diagonal entry, then c = 1/sqrt(1 + t^2), s = t c in FP64, so every applied rotation is
-// orthogonal to FP64 precision (an inexact t leaves a tiny a_pq for a later sweep).  Pairs
-// with a_pq^2 <= 1e-24 |a_pp a_qq| or |a_pq| <= 1e-14 max|diag| are not rotated
-// (jacobi_needed); the solve ends after the first sweep that leaves no pair to rotate.  Eigenvalues are ordered by a parallel rank count.
+// W is stored by physical position: the two indices of rotation pair k always sit at positions
+// 2k and 2k+1, so a round is a block-local update W' = J^T W J (each 2 x 2 block of W from itself
+// and the two rotations of its row and column pairs), written straight to the positions the
+// indices take next round.  The round-robin tournament moves every index but index 0 by one slot
+// per round, which in positions is a shear: even positions move down one pair, odd ones up one
+// pair (mv below, with the two ends turning round).  W is kept in its upper triangle only (each
+// entry stored once, at its upper position), which halves the scattered stores; a block row is
+// read as one 16-byte load; W is symmetrised on input ((W + W^T) / 2).
+// The warps split three ways each round, with one barrier per round:
+//   - the W warps update the upper 2 x 2 blocks, one per thread;
+//   - the V warps hold the eigenvectors in registers, transposed: for component i, lane k keeps
+//     the entries at positions 2k and 2k+1, applies pair k's rotation and passes the results on
+//     with two shuffles (the shear: lane k's new even entry comes from lane k+1, its odd entry
+//     from lane k-1);
+//   - the last warp computes the next round's rotations meanwhile, from the current blocks and
+//     rotations (jacobi_cs32: two reciprocal square roots, no division, then an FP64
+//     renormalisation).
+// Pairs with a_pq^2 <= 1e-24 |a_pp a_qq| or |a_pq| <= 1e-14 max|diag| are not rotated
+// (jacobi_needed); the solve ends after the first sweep that leaves no pair to rotate.
+// Eigenvalues are ordered by a parallel rank count.
 // Slot of index i in round-robin round r (slot 0 fixed, slots 1..NR cycle), and its position.
 __device__ __forceinline__ int bl_slot(int i, int r, int NR) {
   if (i == 0) return 0;
@@ -2156,13 +2153,19 @@ __device__ __forceinline__ int bl_slot(int i, int r, int NR) {
   return 1 + v;
 }
 __device__ __forceinline__ int bl_pos(int x, int Np) { return x < Np / 2 ? 2 * x : 2 * (Np - 1 - x) + 1; }
+// Next-round position of the entry at position P (Np >= 4): the Brent-Luk shear.
+__device__ __forceinline__ int bl_move(int P, int Np) {
+  if (P & 1) return P + 2 < Np ? P + 2 : Np - 2;  // odd positions up one pair; the top one turns down
+  return P >= 4 ? P - 2 : (P == 2 ? 1 : 0);       // even positions down one pair; 2 turns up, 0 stays
+}
+
+constexpr int kBlVRows = 5;  // eigenvector components per V warp (N <= 64 with >= 14 V warps)
 
 __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_in, int N,
                                                    double* __restrict__ evals,
                                                    double* __restrict__ evecs, int max_sweeps,
                                                    DevStatus* st) {
-  constexpr int PW = 31;   // warp computing the next round's rotations
-  constexpr int NE = PW * 32;
+  const int PW = (int)(blockDim.x >> 5) - 1;  // the last warp computes the next round's rotations
   extern __shared__ __align__(16) double sm_bl[];
   const int Np = N + (N & 1);
   const int NR = Np - 1;
@@ -2170,81 +2173,65 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
   const int NN = Np * Np;
   double* Wb0 = sm_bl;
   double* Wb1 = Wb0 + NN;
-  double* Vb0 = Wb1 + NN;
-  double* Vb1 = Vb0 + NN;
   __shared__ double2 pcs[2][32];  // (c, s) of each pair, current and next round
-  __shared__ int mv[64], imv[64];
-  __shared__ int2 mv2[32];         // (mv[2k], mv[2k + 1])
+  __shared__ int imv[64];
   __shared__ double dg[64];
-  __shared__ int rk[64];
+  __shared__ int rk[64], pidx[64];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  // position map: slot x -> x - 1 (x >= 2), 1 -> NR, 0 -> 0
-  for (int P = tid; P < Np; P += blockDim.x) {
-    const int x = P % 2 == 0 ? P / 2 : Np - 1 - P / 2;
-    const int xn = x == 0 ? 0 : (x == 1 ? NR : x - 1);
-    const int Pn = bl_pos(xn, Np);
-    mv[P] = Pn;
-    imv[Pn] = P;
-  }
+  const int NWB = H * (H + 1) / 2;       // upper blocks (a <= b), one per W thread
+  const int WU = (NWB + 31) >> 5;        // W warps
+  const int NVW = PW - WU;               // V warps (the launch gives ceil(N / kBlVRows))
+  const int vrows = (N + NVW - 1) / NVW;  // components per V warp (<= kBlVRows)
+  for (int P = tid; P < Np; P += blockDim.x) imv[Np >= 4 ? bl_move(P, Np) : P] = P;
   for (int idx = tid; idx < NN; idx += blockDim.x) {
     const int i = idx / Np, j = idx - (idx / Np) * Np;
     const int Pi = bl_pos(i, Np), Pj = bl_pos(j, Np);  // round 0: index i sits in slot i
     double v = 0.0;
     if (i < N && j < N) v = 0.5 * (w_in[i + (long long)N * j] + w_in[j + (long long)N * i]);
     Wb0[Pi * Np + Pj] = v;
-    Vb0[Pj * Np + i] = (i == j) ? 1.0 : 0.0;  // V by (position, original index): V^T
   }
-  __syncthreads();  // mv complete
-  for (int q = tid; q < Np / 2; q += blockDim.x) mv2[q] = make_int2(mv[2 * q], mv[2 * q + 1]);
   double dm = 0.0;
   for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(w_in[i + (long long)N * i]));
   const double inv_s = dm > 0.0 ? 1.0 / dm : 1.0;
   __syncthreads();
-  // Positions holding real indices in round 0 (the pad index, when N is odd, is N = Np - 1).
   // Rotations of round 0.
-  if (warp == PW) {
-    for (int k = lane; k < H; k += 32) {
-      double c = 1.0, sn = 0.0;
-      const int i0 = k, i1 = Np - 1 - k;  // indices in slots k and Np-1-k at round 0
-      if (i0 < N && i1 < N) jacobi_rotation(Wb0[(2 * k) * Np + 2 * k], Wb0[(2 * k + 1) * Np + 2 * k + 1],
-                                            Wb0[(2 * k) * Np + 2 * k + 1], inv_s, c, sn);
-      pcs[0][k] = make_double2(c, sn);
+  if (warp == PW && lane < H) {
+    const int k = lane;
+    double c = 1.0, sn = 0.0;
+    const int i0 = k, i1 = Np - 1 - k;  // indices in slots k and Np-1-k at round 0
+    if (i0 < N && i1 < N)
+      jacobi_rotation(Wb0[(2 * k) * Np + 2 * k], Wb0[(2 * k + 1) * Np + 2 * k + 1], Wb0[(2 * k) * Np + 2 * k + 1],
+                      inv_s, c, sn);
+    pcs[0][k] = make_double2(c, sn);
+  }
+  // Per-role constants, two registers shared by the roles: a W thread's block (a, b) (a = -1 for
+  // none), or the rotation lane's current positions (P, Q) of the indices that form its pair next
+  // round.
+  int e0 = -1, e1 = 0;
+  if (warp < WU && tid < NWB) {
+    int a = 0, rem = tid;
+    while (rem >= H - a) {
+      rem -= H - a;
+      ++a;
     }
+    e0 = a;
+    e1 = a + rem;
+  }
+  // V warp: components vi0 .. vi0 + vrows - 1, identity at the round-0 positions.
+  const bool vw = warp >= WU && warp < PW;
+  const int vi0 = (warp - WU) * vrows;
+  double v0[kBlVRows], v1[kBlVRows];
+#pragma unroll
+  for (int u = 0; u < kBlVRows; ++u) {
+    const int i = vi0 + u;
+    const int P = (vw && u < vrows && i < N) ? bl_pos(i, Np) : -1;
+    v0[u] = (P == 2 * lane) ? 1.0 : 0.0;
+    v1[u] = (P == 2 * lane + 1) ? 1.0 : 0.0;
   }
   __syncthreads();
-
-  const int NWB = H * (H + 1) / 2;  // upper blocks (a <= b)
-  const int NITEMS = NWB + N * H;   // + V half-rows (rows < N)
-  // This thread's work items, fixed for the whole solve: a | b << 8 (W block) or
-  // i | b << 8 | 1 << 16 (V row i, column pair b); -1 for none.
-  constexpr int MAXIT = (32 * 33 / 2 + 64 * 32 + NE - 1) / NE;
-  int dsc[MAXIT];
-#pragma unroll
-  for (int u = 0; u < MAXIT; ++u) {
-    const int it = tid + u * NE;
-    if (warp == PW || it >= NITEMS) {
-      dsc[u] = -1;
-    } else if (it < NWB) {
-      int a = 0, rem = it;
-      while (rem >= H - a) {
-        rem -= H - a;
-        ++a;
-      }
-      dsc[u] = a | ((a + rem) << 8);
-    } else {
-      const int e = it - NWB;  // V items: index i fastest, so a warp's accesses are contiguous
-      dsc[u] = (e % N) | ((e / N) << 8) | (1 << 16);
-    }
-  }
-  // Param-warp constants: positions (this round) of the indices that form pair `lane` next
-  // round, as (pair, side).
-  int aP = 0, xP = 0, aQ = 0, xQ = 0;
   if (warp == PW && lane < H) {
-    const int P = imv[2 * lane], Q = imv[2 * lane + 1];
-    aP = P >> 1;
-    xP = P & 1;
-    aQ = Q >> 1;
-    xQ = Q & 1;
+    e0 = imv[2 * lane];
+    e1 = imv[2 * lane + 1];
   }
   int R = 0;
   int sweep = 0;
@@ -2255,46 +2242,54 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
       const int cb = R & 1;
       const double* W = cb ? Wb1 : Wb0;
       double* Wn = cb ? Wb0 : Wb1;
-      const double* V = cb ? Vb1 : Vb0;
-      double* Vn = cb ? Vb0 : Vb1;
       const double2* cs_ = pcs[cb];
-      if (warp != PW) {
+      if (warp < WU) {
+        if (e0 >= 0) {
+          const int a = e0, b = e1;
+          // next-round positions of the block's rows and columns
+          const int r0 = Np >= 4 ? bl_move(2 * a, Np) : 0, r1 = Np >= 4 ? bl_move(2 * a + 1, Np) : 1;
+          const int q0 = Np >= 4 ? bl_move(2 * b, Np) : 0, q1 = Np >= 4 ? bl_move(2 * b + 1, Np) : 1;
+          const double2 csa = cs_[a], csb = cs_[b];
+          const double ca = csa.x, sa = csa.y, cbv = csb.x, sb = csb.y;
+          // Only the upper triangle (row <= column) of W is kept.  Block (a, b), a < b, lies
+          // wholly above the diagonal; a diagonal block's lower entry is its upper one.
+          const double2 r0v = *reinterpret_cast<const double2*>(&W[(2 * a) * Np + 2 * b]);
+          const double2 r1v = *reinterpret_cast<const double2*>(&W[(2 * a + 1) * Np + 2 * b]);
+          const double w00 = r0v.x, w01 = r0v.y, w11 = r1v.y;
+          const double w10 = (a == b) ? w01 : r1v.x;
+          // X = J_a^T B: rows (c, -s), (s, c)
+          const double x00 = ca * w00 - sa * w10, x01 = ca * w01 - sa * w11;
+          const double x10 = sa * w00 + ca * w10, x11 = sa * w01 + ca * w11;
+          // X J_b: columns (c, -s)^T, (s, c)^T
+          const double y00 = x00 * cbv - x01 * sb, y01 = x00 * sb + x01 * cbv;
+          const double y10 = x10 * cbv - x11 * sb, y11 = x10 * sb + x11 * cbv;
+          // each entry to its upper position (a diagonal block's two off-diagonal entries
+          // are the same entry)
+          Wn[min(r0, q0) * Np + max(r0, q0)] = y00;
+          Wn[min(r0, q1) * Np + max(r0, q1)] = y01;
+          if (a != b) Wn[min(r1, q0) * Np + max(r1, q0)] = y10;
+          Wn[min(r1, q1) * Np + max(r1, q1)] = y11;
+        }
+      } else if (warp < PW) {
+        double c = 1.0, sn = 0.0;
+        if (lane < H) {
+          const double2 cs = cs_[lane];
+          c = cs.x;
+          sn = cs.y;
+        }
 #pragma unroll
-        for (int u = 0; u < MAXIT; ++u) {
-          const int dd = dsc[u];
-          if (dd < 0) continue;
-          if (!(dd >> 16)) {
-            const int a = dd & 255, b = (dd >> 8) & 255;
-            const double2 csa = cs_[a], csb = cs_[b];
-            const double ca = csa.x, sa = csa.y, cbv = csb.x, sb = csb.y;
-            // Only the upper triangle (row <= column) of W is kept.  Block (a, b), a < b, lies
-            // wholly above the diagonal; a diagonal block's lower entry is its upper one.
-            const double2 r0v = *reinterpret_cast<const double2*>(&W[(2 * a) * Np + 2 * b]);
-            const double2 r1v = *reinterpret_cast<const double2*>(&W[(2 * a + 1) * Np + 2 * b]);
-            const double w00 = r0v.x, w01 = r0v.y, w11 = r1v.y;
-            const double w10 = (a == b) ? w01 : r1v.x;
-            // X = J_a^T B: rows (c, -s), (s, c)
-            const double x00 = ca * w00 - sa * w10, x01 = ca * w01 - sa * w11;
-            const double x10 = sa * w00 + ca * w10, x11 = sa * w01 + ca * w11;
-            // X J_b: columns (c, -s)^T, (s, c)^T
-            const double y00 = x00 * cbv - x01 * sb, y01 = x00 * sb + x01 * cbv;
-            const double y10 = x10 * cbv - x11 * sb, y11 = x10 * sb + x11 * cbv;
-            const int2 ma = mv2[a], mb = mv2[b];
-            const int r0 = ma.x, r1 = ma.y, q0 = mb.x, q1 = mb.y;
-            // each entry to its upper position (a diagonal block's two off-diagonal entries
-            // are the same entry)
-            Wn[min(r0, q0) * Np + max(r0, q0)] = y00;
-            Wn[min(r0, q1) * Np + max(r0, q1)] = y01;
-            if (a != b) Wn[min(r1, q0) * Np + max(r1, q0)] = y10;
-            Wn[min(r1, q1) * Np + max(r1, q1)] = y11;
+        for (int u = 0; u < kBlVRows; ++u) {
+          if (u >= vrows) break;  // uniform across the warp
+          const double n0 = v0[u] * c - v1[u] * sn;
+          const double n1 = v0[u] * sn + v1[u] * c;
+          const double dn = __shfl_down_sync(0xffffffffu, n0, 1);  // lane k+1's even entry
+          const double up = __shfl_up_sync(0xffffffffu, n1, 1);    // lane k-1's odd entry
+          if (H == 1) {
+            v0[u] = n0;
+            v1[u] = n1;
           } else {
-            const int i = dd & 255, b = (dd >> 8) & 255;
-            const double2 csb = cs_[b];
-            const double cbv = csb.x, sb = csb.y;
-            const int2 mb = mv2[b];
-            const double v0 = V[(2 * b) * Np + i], v1 = V[(2 * b + 1) * Np + i];
-            Vn[mb.x * Np + i] = v0 * cbv - v1 * sb;
-            Vn[mb.y * Np + i] = v0 * sb + v1 * cbv;
+            v0[u] = lane == 0 ? n0 : (lane == H - 1 ? n1 : dn);
+            v1[u] = lane == 0 ? dn : up;
           }
         }
       } else if (lane < H) {
@@ -2310,11 +2305,13 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
         }
         double c = 1.0, sn = 0.0;
         if (live) {
+          const int aP = e0 >> 1, xP = e0 & 1, aQ = e1 >> 1, xQ = e1 & 1;
           const double cP = cs_[aP].x, sP = cs_[aP].y, cQ = cs_[aQ].x, sQ = cs_[aQ].y;
           const double tP0 = xP ? sP : cP, tP1 = xP ? cP : -sP;
           const double tQ0 = xQ ? sQ : cQ, tQ1 = xQ ? cQ : -sQ;
-          // entries through the upper triangle (W is kept there only)
-          auto wu = [&](int r, int c2) { return r <= c2 ? W[r * Np + c2] : W[c2 * Np + r]; };
+          // entries through the upper triangle (W is kept there only); the address is selected
+          // arithmetically, so the lanes do not diverge
+          auto wu = [&](int r, int c2) { return W[min(r, c2) * Np + max(r, c2)]; };
           const int P0 = 2 * aP, Q0 = 2 * aQ;
           const double p0 = tP0 * wu(P0, P0) + tP1 * wu(P0, P0 + 1);
           const double p1 = tP0 * wu(P0, P0 + 1) + tP1 * wu(P0 + 1, P0 + 1);
@@ -2349,12 +2346,14 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
       break;
     }
   }
-  // After R rounds the current buffers are (R & 1); index i sits in slot bl_slot(i, R, NR).
+  // After R rounds the current buffer is (R & 1); index i sits in slot bl_slot(i, R, NR).
   const double* Wf = (R & 1) ? Wb1 : Wb0;
-  const double* Vf = (R & 1) ? Vb1 : Vb0;
+  if (tid < Np) pidx[tid] = -1;
+  __syncthreads();
   if (tid < N) {
     const int P = bl_pos(bl_slot(tid, R, NR), Np);
     dg[tid] = Wf[P * Np + P];
+    pidx[P] = tid;
   }
   __syncthreads();
   if (tid < N) {
@@ -2375,17 +2374,22 @@ __global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_i
     if (!converged) dev_fail(st, TT_ERR_NOCONV, sweep);
   }
   __syncthreads();
-  for (int idx = tid; idx < N * N; idx += blockDim.x) {
-    const int i = idx % N, a = idx / N;  // eigenvector of index a, component i
-    const int P = bl_pos(bl_slot(a, R, NR), Np);
-    evecs[i + (long long)N * rk[a]] = Vf[P * Np + i];
+  if (vw && lane < H) {
+    const int a0 = pidx[2 * lane], a1 = pidx[2 * lane + 1];  // indices at this lane's positions
+#pragma unroll
+    for (int u = 0; u < kBlVRows; ++u) {
+      const int i = vi0 + u;
+      if (u >= vrows || i >= N) break;
+      if (a0 >= 0) evecs[i + (long long)N * rk[a0]] = v0[u];
+      if (a1 >= 0) evecs[i + (long long)N * rk[a1]] = v1[u];
+    }
   }
 }
 
 // Large-N variant (64 < N <= 128) of the Brent-Luk solver.  W alone stays in shared memory: its
 // upper triangle packed by rows (row P stored from column P & ~1, so every 2 x 2 block row is a
 // 16-byte load), double-buffered (2 x 66.5 KB for N = 128).  The eigenvectors are not updated
-// round by round: the rotation warps log each round's FP32 tangents to global memory, and
+// round by round: the rotation warps log each round's FP32 (c, s) pairs to global memory, and
 // k_bl_replay applies them afterwards to the rows of V, one CTA per row (rows are independent),
 // with the same moves.  Two warps compute the next round's rotations during the update.
 __device__ __forceinline__ int blp_off(int P, int Np) {
@@ -2395,7 +2399,7 @@ __device__ __forceinline__ int blp_off(int P, int Np) {
 }
 
 __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_in, int N,
-                                                    double* __restrict__ evals, float* __restrict__ tlog,
+                                                    double* __restrict__ evals, float2* __restrict__ tlog,
                                                     int* __restrict__ meta, int max_sweeps, DevStatus* st) {
   constexpr int RW0 = 30;  // warps 30, 31 compute the next round's rotations
   constexpr int NE = RW0 * 32;
@@ -2441,13 +2445,13 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
   if (warp >= RW0 && rl < H) {
     const int k = rl;
     const int i0 = k, i1 = Np - 1 - k;
-    float tf = 0.0f;
-    if (i0 < N && i1 < N) tf = jacobi_tf(Wb0[at(2 * k, 2 * k)], Wb0[at(2 * k + 1, 2 * k + 1)], Wb0[at(2 * k, 2 * k + 1)],
-                                         inv_s);
+    float2 r = make_float2(1.0f, 0.0f);
+    if (i0 < N && i1 < N)
+      r = jacobi_cs32(Wb0[at(2 * k, 2 * k)], Wb0[at(2 * k + 1, 2 * k + 1)], Wb0[at(2 * k, 2 * k + 1)], inv_s);
     double c, sn;
-    rot_from_tf(tf, c, sn);
+    rot_from_cs32(r, c, sn);
     pcs[0][k] = make_double2(c, sn);
-    tlog[k] = tf;
+    tlog[k] = r;
   }
   __syncthreads();
   const int NWB = H * (H + 1) / 2;
@@ -2515,7 +2519,7 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
           const int xs = bl_slot(Np - 1, rn, NR);
           live = (xs != rl) && (xs != Np - 1 - rl);
         }
-        float tf = 0.0f;
+        float2 r = make_float2(1.0f, 0.0f);
         if (live) {
           const double cP = cs_[aP].x, sP = cs_[aP].y, cQ = cs_[aQ].x, sQ = cs_[aQ].y;
           const double tP0 = xP ? sP : cP, tP1 = xP ? cP : -sP;
@@ -2528,12 +2532,12 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
           const double q1 = tQ0 * wu(Q0, Q0 + 1) + tQ1 * wu(Q0 + 1, Q0 + 1);
           const double m0 = tP0 * wu(P0, Q0) + tP1 * wu(P0 + 1, Q0);
           const double m1 = tP0 * wu(P0, Q0 + 1) + tP1 * wu(P0 + 1, Q0 + 1);
-          tf = jacobi_tf(p0 * tP0 + p1 * tP1, q0 * tQ0 + q1 * tQ1, m0 * tQ0 + m1 * tQ1, inv_s);
+          r = jacobi_cs32(p0 * tP0 + p1 * tP1, q0 * tQ0 + q1 * tQ1, m0 * tQ0 + m1 * tQ1, inv_s);
         }
         double c, sn;
-        rot_from_tf(tf, c, sn);
+        rot_from_cs32(r, c, sn);
         pcs[cb ^ 1][rl] = make_double2(c, sn);
-        tlog[(size_t)(R + 1) * H + rl] = tf;  // rotations of round R + 1
+        tlog[(size_t)(R + 1) * H + rl] = r;  // rotations of round R + 1
       }
       __syncthreads();
       if (rnd + 1 == NR) {
@@ -2582,7 +2586,7 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
 
 // Replays the logged rotations on row i of V (one CTA per row, one thread per pair; V starts as
 // the identity with index i at its round-0 position) and writes the eigenvectors by rank.
-__global__ void __launch_bounds__(64) k_bl_replay(const float* __restrict__ tlog, const int* __restrict__ meta,
+__global__ void __launch_bounds__(64) k_bl_replay(const float2* __restrict__ tlog, const int* __restrict__ meta,
                                                   int N, double* __restrict__ evecs) {
   __shared__ double vb[2][128];
   __shared__ int mvs[128];
@@ -2599,16 +2603,17 @@ __global__ void __launch_bounds__(64) k_bl_replay(const float* __restrict__ tlog
   const int m0 = k < H ? mvs[2 * k] : 0, m1 = k < H ? mvs[2 * k + 1] : 0;
   constexpr int U = 8;
   for (int R0 = 0; R0 < rounds; R0 += U) {
-    float tf[U];
+    float2 tf[U];
 #pragma unroll
-    for (int j = 0; j < U; ++j) tf[j] = (k < H && R0 + j < rounds) ? tlog[(size_t)(R0 + j) * H + k] : 0.0f;
+    for (int j = 0; j < U; ++j)
+      tf[j] = (k < H && R0 + j < rounds) ? tlog[(size_t)(R0 + j) * H + k] : make_float2(1.0f, 0.0f);
 #pragma unroll
     for (int j = 0; j < U; ++j) {
       if (R0 + j >= rounds) break;
       const int cb = (R0 + j) & 1;
       if (k < H) {
         double c, sn;
-        rot_from_tf(tf[j], c, sn);
+        rot_from_cs32(tf[j], c, sn);
         const double v0 = vb[cb][2 * k], v1 = vb[cb][2 * k + 1];
         vb[cb ^ 1][m0] = v0 * c - v1 * sn;
         vb[cb ^ 1][m1] = v0 * sn + v1 * c;
@@ -2624,7 +2629,7 @@ size_t syev_ws_bytes(int N, int max_sweeps) {
   if (N <= 64) return 0;
   const int Np = N + (N & 1);
   const int sw = max_sweeps > 0 ? max_sweeps : 40;
-  return ((size_t)sw * (Np - 1) + 2) * (Np / 2) * sizeof(float) + (1 + 2 * 128) * sizeof(int) + 1024;
+  return ((size_t)sw * (Np - 1) + 2) * (Np / 2) * sizeof(float2) + (1 + 2 * 128) * sizeof(int) + 1024;
 }
 
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps, Arena& ws,
@@ -2635,55 +2640,33 @@ int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sw
     return TT_ERR_UNSUPPORTED;
   }
   if (N <= 64) {
-    const int Nps = N + (N & 1);
-    const size_t shm_bl = 4 * (size_t)Nps * Nps * sizeof(double);
-    smem_optin_k(k_syev_bl, 160 * 1024);
-    k_syev_bl<<<1, 1024, shm_bl, s>>>(w, N, evals, evecs, max_sweeps, st);
+    const int Nps = N + (N & 1), H = Nps / 2;
+    const size_t shm_bl = 2 * (size_t)Nps * Nps * sizeof(double);
+    // W warps (one upper 2 x 2 block per thread), V warps (kBlVRows components each), one
+    // rotation warp
+    const int warps = (H * (H + 1) / 2 + 31) / 32 + (N + kBlVRows - 1) / kBlVRows + 1;
+    smem_optin_k(k_syev_bl, shm_bl);
+    k_syev_bl<<<1, 32 * warps, shm_bl, s>>>(w, N, evals, evecs, max_sweeps, st);
     count_launch();
     TT_LAUNCH_CHECK();
     return TT_OK;
   }
-  if (!getenv("TTR_SYEV_JACOBI")) {
-    // 64 < N <= 128: packed Brent-Luk on W, eigenvectors by replaying the logged rotations
-    const int Np = N + (N & 1), H = Np / 2;
-    const int sw = max_sweeps > 0 ? max_sweeps : 40;
-    const size_t mk = ws.mark();
-    float* tlog = ws.take<float>(((size_t)sw * (Np - 1) + 2) * H);
-    int* meta = ws.take<int>(1 + 2 * 128);
-    if (!tlog || !meta) {
-      set_error(TT_ERR_NOMEM, "eigen-solver rotation log");
-      return TT_ERR_NOMEM;
-    }
-    const size_t shm = 2 * (size_t)(2 * (H * Np - H * (H - 1))) * sizeof(double);
-    TT_TRY(smem_optin_k(k_syev_blw, shm));
-    k_syev_blw<<<1, 1024, shm, s>>>(w, N, evals, tlog, meta, sw, st);
-    count_launch();
-    TT_LAUNCH_CHECK();
-    k_bl_replay<<<N, 64, 0, s>>>(tlog, meta, N, evecs);
-    count_launch();
-    TT_LAUNCH_CHECK();
-    ws.reset(mk);
-    return TT_OK;
-  }
-  const int Np = N + (N & 1);
-  const bool vsm = Np <= 64;
-  const size_t shm = (size_t)(vsm ? 2 : 1) * Np * Np * sizeof(double) + Np * sizeof(double) +
-                     (size_t)Np / 2 * 2 * sizeof(int) + Np * sizeof(int) + 64;
+  // 64 < N <= 128: packed Brent-Luk on W, eigenvectors by replaying the logged rotations
+  const int Np = N + (N & 1), H = Np / 2;
+  const int sw = max_sweeps > 0 ? max_sweeps : 40;
   const size_t mk = ws.mark();
-  double* vg = nullptr;
-  if (!vsm) {
-    vg = ws.take<double>((size_t)Np * Np);
-    if (!vg) {
-      set_error(TT_ERR_NOMEM, "jacobi workspace");
-      return TT_ERR_NOMEM;
-    }
+  float2* tlog = ws.take<float2>(((size_t)sw * (Np - 1) + 2) * H);
+  int* meta = ws.take<int>(1 + 2 * 128);
+  if (!tlog || !meta) {
+    set_error(TT_ERR_NOMEM, "eigen-solver rotation log");
+    return TT_ERR_NOMEM;
   }
-  smem_optin_k(k_syev_jacobi<true>, 200 * 1024);
-  smem_optin_k(k_syev_jacobi<false>, 200 * 1024);
-  if (vsm)
-    k_syev_jacobi<true><<<1, 256, shm, s>>>(w, N, evals, evecs, vg, max_sweeps, st);
-  else
-    k_syev_jacobi<false><<<1, 256, shm, s>>>(w, N, evals, evecs, vg, max_sweeps, st);
+  const size_t shm = 2 * (size_t)(2 * (H * Np - H * (H - 1))) * sizeof(double);
+  TT_TRY(smem_optin_k(k_syev_blw, shm));
+  k_syev_blw<<<1, 1024, shm, s>>>(w, N, evals, tlog, meta, sw, st);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  k_bl_replay<<<N, 64, 0, s>>>(tlog, meta, N, evecs);
   count_launch();
   TT_LAUNCH_CHECK();
   ws.reset(mk);

@@ -812,17 +812,6 @@ constexpr size_t G32_RING = (size_t)G32_WARPS * G32_STAGES * G32_STAGE_BYTES;
 constexpr size_t G32_SMEM = 1024 + G32_RING + (size_t)G32_WARPS * G32_STAGES * 8;
 static_assert(G32_RING >= 256 * 65 * sizeof(double), "reduction area fits in the stage ring");
 
-__device__ __forceinline__ uint64_t f2_dup(float a) {
-  uint64_t r;
-  asm("mov.b64 %0, {%1, %1};" : "=l"(r) : "f"(a));
-  return r;
-}
-__device__ __forceinline__ void f2_unpack(uint64_t v, float& lo, float& hi) {
-  asm("mov.b64 {%0, %1}, %2;" : "=f"(lo), "=f"(hi) : "l"(v));
-}
-__device__ __forceinline__ void ffma2(uint64_t& d, uint64_t a, uint64_t b) {
-  asm("fma.rn.f32x2 %0, %1, %2, %0;" : "+l"(d) : "l"(a), "l"(b));
-}
 __device__ __forceinline__ float4 lds_f4(uint32_t addr) {
   float4 v;
   asm volatile("ld.shared.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "r"(addr));
