@@ -18,7 +18,7 @@
 
 #include "kernels.cuh"
 #include "philox.cuh"
-#include "jacobi_rot.cuh"
+#include "bl_solver.cuh"
 
 namespace ttr {
 namespace {
@@ -44,7 +44,7 @@ struct BatchShape {
 constexpr size_t SM_CHUNK = (size_t)BMAXM * BSMALL * sizeof(float);         // U (m x r)
 constexpr size_t SM_YQ = (size_t)BMAXM * (BSMALL + 1) * sizeof(float);        // Y, Q (stride ks|1)
 constexpr size_t SM_W = (size_t)BSMALL * BSMALL * sizeof(double);             // Gram
-constexpr size_t SM_JAC = 4 * (size_t)BSMALL * BSMALL * sizeof(double);       // Jacobi buffers
+constexpr size_t SM_JAC = 2 * (size_t)BSMALL * BSMALL * sizeof(double);       // Jacobi buffers
 constexpr size_t SM_RED = (size_t)BT * 2 * sizeof(double);                    // reductions
 template <int BCH>
 constexpr size_t sm_om() { return (size_t)BCH * BSMALL * sizeof(float); }   // Omega chunk
@@ -55,7 +55,7 @@ struct Smem {
   float* chunk;   // BMAXM x BSMALL
   float* yq;      // BMAXM x (BSMALL+1)
   double* w;      // BSMALL x BSMALL (row-major, stride Np)
-  double* jac;    // 4 x BSMALL^2
+  double* jac;    // 2 x BSMALL^2 (the eigen-solver's double-buffered W)
   float* om;      // BCH x BSMALL
   double* red;    // 2 * BT
 };
@@ -124,165 +124,6 @@ __device__ void cta_gram(const float* __restrict__ base, long long ps, long long
     }
     __syncthreads();
   }
-}
-
-// Eigen-decomposition of the symmetric W (N x N row-major, N <= BSMALL) by cyclic Jacobi with
-// the round-robin pairing, all rotations of a round applied together as W' = J^T W J, V' = V J
-// (double-buffered), the next round's rotations computed meanwhile by the last warp.  Output:
-// evals[N] descending, evecs (N x N column-major, stride N).
-// The solve ends after the first sweep that leaves no pair to rotate.  Returns the sweep count
-// (max_sweeps + 1 when not converged).
-__device__ int cta_jacobi(const double* W, int N, double* jac, double* evals, double* evecs, int max_sweeps,
-                          double* red) {
-  const int tid = threadIdx.x;
-
-  const int Np = N + (N & 1);
-  const int NR = Np - 1;
-  const int NN = Np * Np;
-  double* Wb[2] = {jac, jac + NN};
-  double* Vb[2] = {jac + 2 * NN, jac + 3 * NN};
-  // per round parity b: cosines red[32 b ..], sines red[64 + 32 b ..], and as ints from red + 128:
-  // partner, pair, first flag (3 x Np each parity)
-  int* prb = reinterpret_cast<int*>(red + 128);
-  for (int idx = tid; idx < NN; idx += BT) {
-    const int i = idx / Np, j = idx - (idx / Np) * Np;
-    Wb[0][idx] = (i < N && j < N) ? W[i * N + j] : 0.0;
-    Vb[0][idx] = (i == j) ? 1.0 : 0.0;
-  }
-  double dm = 0.0;
-  for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(W[i * N + i]));
-  const double inv_s = dm > 0.0 ? 1.0 / dm : 1.0;
-  // The last warp computes the rotations of the next round while the others apply the current
-  // one (one barrier per round); it takes the three entries of J^T W J it needs from the
-  // current W and the current rotations.
-  constexpr int PWARP = BT / 32 - 1;
-  const bool pthread = (tid >> 5) == PWARP;
-  const int k = tid & 31;  // pair computed by a lane of the parameter warp
-  auto pair_of = [&](int rnd, int& p, int& q) {
-    const int x = k, y = Np - 1 - k;
-    p = x == 0 ? 0 : 1 + (x - 1 + rnd) % NR;
-    q = y == 0 ? 0 : 1 + (y - 1 + rnd) % NR;
-    if (p > q) {
-      const int tt = p;
-      p = q;
-      q = tt;
-    }
-  };
-  auto publish = [&](int b, int p, int q, double c, double sn) {
-    red[32 * b + k] = c;
-    red[64 + 32 * b + k] = sn;
-    int* pr = prb + 3 * Np * b;
-    pr[p] = q;
-    pr[q] = p;
-    pr[Np + p] = k;
-    pr[Np + q] = k;
-    pr[2 * Np + p] = 1;
-    pr[2 * Np + q] = 0;
-  };
-  __syncthreads();
-  if (pthread && k < Np / 2) {  // rotations of round 0 straight from W
-    int p, q;
-    pair_of(0, p, q);
-    double c = 1.0, sn = 0.0;
-    if (q < N) jacobi_rotation(Wb[0][p * Np + p], Wb[0][q * Np + q], Wb[0][p * Np + q], inv_s, c, sn);
-    publish(0, p, q, c, sn);
-  }
-  // this thread's entries (the parameter warp takes none), fixed for the whole solve
-  constexpr int NU = BT - 32;
-  constexpr int JU = (BSMALL * BSMALL + NU - 1) / NU;
-  int ji[JU], jj[JU];
-#pragma unroll
-  for (int u = 0; u < JU; ++u) {
-    const int idx = tid + u * NU;
-    ji[u] = idx / Np;
-    jj[u] = idx - ji[u] * Np;
-  }
-  __syncthreads();
-  int cur = 0, sweep = 0, R = 0;
-  bool conv = false;
-  for (; sweep < max_sweeps; ++sweep) {
-    for (int rnd = 0; rnd < NR; ++rnd, ++R) {
-      const int b = R & 1;
-      const double* Wc = Wb[cur];
-      const double* cs = red + 32 * b;
-      const double* sn = red + 64 + 32 * b;
-      const int* pr = prb + 3 * Np * b;
-      if (!pthread) {
-        double* Wn = Wb[cur ^ 1];
-        const double* Vc = Vb[cur];
-        double* Vn = Vb[cur ^ 1];
-#pragma unroll
-        for (int u = 0; u < JU; ++u) {
-          const int idx = tid + u * NU;
-          if (idx >= NN) break;
-          const int i = ji[u], j = jj[u];
-          const int pi = pr[i], pj = pr[j];
-          const double ci = cs[pr[Np + i]], si = sn[pr[Np + i]];
-          const double cj = cs[pr[Np + j]], sj = sn[pr[Np + j]];
-          const double jpi = pr[2 * Np + i] ? -si : si, jpj = pr[2 * Np + j] ? -sj : sj;
-          Wn[idx] = ci * (Wc[i * Np + j] * cj + Wc[i * Np + pj] * jpj) +
-                    jpi * (Wc[pi * Np + j] * cj + Wc[pi * Np + pj] * jpj);
-          Vn[idx] = Vc[i * Np + j] * cj + Vc[i * Np + pj] * jpj;
-        }
-      } else if (k < Np / 2) {
-        // next round's pair (p, q) and the entries (p, p), (q, q), (p, q) of J^T W J
-        int p, q;
-        pair_of(rnd + 1 == NR ? 0 : rnd + 1, p, q);
-        double c = 1.0, s2 = 0.0;
-        if (q < N) {
-          auto wj = [&](int a, int bb) {
-            const int pa = pr[a], pb = pr[bb];
-            const double ca = cs[pr[Np + a]], sa = sn[pr[Np + a]];
-            const double cb2 = cs[pr[Np + bb]], sb = sn[pr[Np + bb]];
-            const double ja = pr[2 * Np + a] ? -sa : sa, jb = pr[2 * Np + bb] ? -sb : sb;
-            return ca * (Wc[a * Np + bb] * cb2 + Wc[a * Np + pb] * jb) +
-                   ja * (Wc[pa * Np + bb] * cb2 + Wc[pa * Np + pb] * jb);
-          };
-          jacobi_rotation(wj(p, p), wj(q, q), wj(p, q), inv_s, c, s2);
-        }
-        publish(b ^ 1, p, q, c, s2);
-      }
-      __syncthreads();
-      cur ^= 1;
-    }
-    // stop when no pair of the updated matrix would be rotated (saves the quiet sweep)
-    int need = 0;
-    {
-      const double* Wc = Wb[cur];
-      for (int idx = tid; idx < NN; idx += BT) {
-        const int i = idx / Np, j = idx - (idx / Np) * Np;
-        if (i < j && jacobi_needed(Wc[i * Np + i], Wc[j * Np + j], Wc[i * Np + j], inv_s)) need = 1;
-      }
-    }
-    if (!__syncthreads_or(need)) {
-      conv = true;
-      ++sweep;
-      break;
-    }
-  }
-  int* pr = prb;
-  const double* Wf = Wb[cur];
-  const double* Vf = Vb[cur];
-  int* rk = pr;  // reuse
-  if (tid < N) {
-    double la = Wf[tid * Np + tid];
-    if (la != la) la = -INFINITY;
-    int rank = 0;
-    for (int b = 0; b < N; ++b) {
-      double lb = Wf[b * Np + b];
-      if (lb != lb) lb = -INFINITY;
-      rank += (lb > la || (lb == la && b < tid)) ? 1 : 0;
-    }
-    rk[tid] = rank;
-    evals[rank] = Wf[tid * Np + tid];
-  }
-  __syncthreads();
-  for (int idx = tid; idx < N * N; idx += BT) {
-    const int i = idx % N, a = idx / N;
-    evecs[i + N * rk[a]] = Vf[i * Np + a];
-  }
-  __syncthreads();
-  return conv ? sweep : max_sweeps + 1;
 }
 
 // Largest-|entry| of each of the first r columns of U (rows x r, stride ld) made positive;
@@ -399,7 +240,7 @@ __global__ void __launch_bounds__(BT, 1)
         const int N = (int)small;
         if (m <= cols) cta_gram(src, 1, m, N, cols, S.w);   // W = A A^T, vectors = columns
         else cta_gram(src, m, 1, N, m, S.w);                // W = A^T A, vectors = rows
-        const int sw = cta_jacobi(S.w, N, S.jac, lam, evec, max_sweeps, S.red);
+        const int sw = bl_solve(S.w, N, lam, evec, max_sweeps, S.jac);
         if (tid == 0 && st) {
           atomicMax(&st->sweeps, sw);
           if (sw > max_sweeps) dev_fail(st, TT_ERR_NOCONV, t);
@@ -553,7 +394,7 @@ __global__ void __launch_bounds__(BT, 1)
         }
         __syncthreads();
         cta_gram(Bg, 1, ks, ks, cols, S.w);  // W = B B^T (vectors = columns of B)
-        const int sw = cta_jacobi(S.w, ks, S.jac, lam, evec, max_sweeps, S.red);
+        const int sw = bl_solve(S.w, ks, lam, evec, max_sweeps, S.jac);
         if (tid == 0 && st) {
           atomicMax(&st->sweeps, sw);
           if (sw > max_sweeps) dev_fail(st, TT_ERR_NOCONV, t);
