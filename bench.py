@@ -411,7 +411,7 @@ def measure_batch(args, dev, steps=None, warmup=None):
     import tensor_train_ring_decompositions_hpc_gpu_b200 as ttr
     steps = steps or min(args.steps, 10)
     warmup = max(warmup or args.warmup, 3)
-    xs = batch_tensors_torch(args.seed, dev)
+    xs = batch_tensors_torch(args.seed, dev, count=getattr(args, "batch_count", None))
     b = ttr.Batch(xs, rmax=BATCH["rmax"], device=dev)
     elems = float(b.flat.numel())
     b.make_plan(eps=BATCH["eps"])
@@ -438,7 +438,7 @@ def measure_batch(args, dev, steps=None, warmup=None):
     peak, peak_src = peaks()
     achieved = alg_bytes / (ms * 1e-3) / 1e9
     out = {
-        "metric": "batched TT-SVD of 4096 order-4 tensors (eps 1e-2)", "value": len(xs) / (ms * 1e-3),
+        "metric": f"batched TT-SVD of {len(xs)} order-4 tensors (eps 1e-2)", "value": len(xs) / (ms * 1e-3),
         "unit": "tensors/s", "ms": ms, "steps": steps, "warmup": warmup,
         "config": {"workload": "batch4: 4096 order-4 TT tensors, modes U{8..32}, ranks U{2..16}, 1e-3 noise, "
                                "eps 1e-2", "tensors": len(xs), "elements": elems, "eps": BATCH["eps"],
@@ -961,6 +961,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="tt6", choices=sorted(WORKLOADS) + ["batch4"])
+    ap.add_argument("--batch-count", type=int, default=None,
+                    help="batch4: tensors in the batch (default 4096; smaller for profiling captures)")
     ap.add_argument("--workloads", default="tt3,tr6,batch4,c5",
                     help="other configurations measured in the same run (comma list; '' for none)")
     ap.add_argument("--no-workloads", action="store_true")

@@ -117,8 +117,9 @@ def test_gram_tall_rowmajor(gpu, n, N):
     assert _rel(w, zd.T @ zd) < 1e-12
 
 
-# (1024, 40), (512, 64), (1000, 33), (64, 5), (7, 3), (2048, 16), (1024, 48) fit in one CTA's
-# shared memory (single-launch kernel); the others take the multi-kernel path.
+# (1024, 40), (512, 64), (1000, 33), (64, 5), (7, 3), (2048, 16), (1024, 48), (4096, 16) take the
+# single-launch kernel (a cluster of up to 8 CTAs, >= 128 rows each, in shared memory: 1, 4 and 8
+# CTAs among these); the others take the multi-kernel path.
 @pytest.mark.parametrize("n,N", [(1024, 40), (512, 64), (1000, 33), (64, 5), (7, 3), (2048, 16), (1024, 48),
                                  (100000, 24), (5000, 64), (300, 128), (4096, 16)])
 def test_cholqr2(gpu, n, N):
