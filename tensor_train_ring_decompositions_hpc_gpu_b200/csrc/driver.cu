@@ -734,11 +734,19 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
     // energy outside the eigen-decomposed subspace: 0 for an exact step (its Gram holds the whole
     // unfolding), the carried energy minus every eigenvalue for a plain EDrSVD attempt, and the
     // probe estimate for a learned attempt.
+    // Eigenvalues of the attempt already read back with the probe estimate (learned steps: one
+    // device round trip instead of two), or empty.
+    std::vector<double> lam_pre;
     auto decide = [&](int nev, double outside) -> int {
       if (!adaptive) return TT_OK;
       std::vector<double> lam((size_t)nev);
-      TT_CUDA(cudaMemcpyAsync(lam.data(), B.evals, sizeof(double) * nev, cudaMemcpyDeviceToHost, s));
-      TT_CUDA(cudaStreamSynchronize(s));
+      if (lam_pre.size() == (size_t)nev) {
+        lam.swap(lam_pre);
+      } else {
+        TT_CUDA(cudaMemcpyAsync(lam.data(), B.evals, sizeof(double) * nev, cudaMemcpyDeviceToHost, s));
+        TT_CUDA(cudaStreamSynchronize(s));
+      }
+      lam_pre.clear();
       double inside = 0.0;
       for (double v : lam) inside += std::max(v, 0.0);
       if (norm_from_gram && k == 0) {
@@ -1097,7 +1105,9 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
           // mean over the probe columns is unbiased; two standard errors of the mean are added.
           TT_TRY(launch_probe_resid(B.yf, m, ks, m, B.y0, m, TT_PROBE_COLS, B.resid, s));
           double hr[TT_PROBE_COLS];
+          lam_pre.assign((size_t)ks, 0.0);
           TT_CUDA(cudaMemcpyAsync(hr, B.resid, sizeof(hr), cudaMemcpyDeviceToHost, s));
+          TT_CUDA(cudaMemcpyAsync(lam_pre.data(), B.evals, sizeof(double) * ks, cudaMemcpyDeviceToHost, s));
           TT_CUDA(cudaStreamSynchronize(s));
           double mean = 0.0, var = 0.0;
           for (double v : hr) mean += v;
@@ -1111,6 +1121,7 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
             learned_step = tc_b;
           } else {
             ++nfall;
+            lam_pre.clear();
             ks_next = std::min(ks_cap, std::max(2 * ks, ks_next));
             pw = o.power_iters;
           }

@@ -326,3 +326,17 @@ def test_adaptive_eps_reports_unmet_tolerance(gpu, gemm):
     with pytest.raises(ttr.TTError) as ei:
         ttr.tt_svd(xt, [1, 3, 3, 3, 1], gemm=gemm, eps=1e-3, shape=shape, flags=ttr.TT_FLAG_STRICT_EPS)
     assert ei.value.code == 3  # TT_ERR_RANK
+
+
+def test_unfolding1_all_sigma_full_rank(gpu):
+    """A 32-row first unfolding kept at full rank (the 32^6 bench's step 1, scaled to 32^4 x 16):
+    all 32 singular values within 1e-4 of the oracle's (the exact FP32-product Gram)."""
+    ttr = _ttr()
+    shape, ranks = [32, 32, 32, 32, 16], [1, 32, 32, 32, 16, 1]
+    x = oracle.make_tt_tensor(shape, ranks, 1e-4, seed=71).astype(np.float64)
+    res = ttr.tt_svd(_to_dev(x, gpu), ranks, gemm="auto", flags=ttr.TT_FLAG_KEEP_SIGMA)
+    ref_cores, ref_sig = oracle.tt_svd(x, ranks)
+    s, s_ref = np.asarray(res.sigmas[0], dtype=np.float64), np.asarray(ref_sig[0], dtype=np.float64)
+    assert len(s) >= 32
+    np.testing.assert_allclose(s[:32], s_ref[:32], rtol=1e-4, atol=SIG_FLOOR["auto"] * s_ref[0])
+    _check(x, res, ref_cores, ref_sig, ring=False, ranks=ranks)
