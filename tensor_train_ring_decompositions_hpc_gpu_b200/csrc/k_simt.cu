@@ -1586,6 +1586,10 @@ int launch_gram(const float* x, long long nvec, int M, long long vs, long long e
 // ---------------------------------------------------------------------------------------
 // One block: W (N x N, FP64) -> R (upper, FP64) and R^-1 (FP64).  Pivots below
 // rel_tol * max diag mark a dependent column: its row of R and column of R^-1 are zero.
+// Cholesky right-looking with one barrier per column; in the trailing update thread
+// (row group g, column j) loads all its rows before storing any.  R^-1 is formed column-parallel
+// with no barrier in between: thread j back-substitutes R x = e_j (x_i = -(sum_{k>i} r_ik x_k) / r_ii
+// with the reciprocal diagonal precomputed), four partial sums per dot product.
 __global__ void __launch_bounds__(256) k_chol_inv(const double* __restrict__ w, int N,
                                                   double* __restrict__ r_out,
                                                   double* __restrict__ rinv, double rel_tol,
@@ -1594,77 +1598,100 @@ __global__ void __launch_bounds__(256) k_chol_inv(const double* __restrict__ w, 
   double* A = sm;                                // N x N (row-major), upper part becomes R
   double* Ri = ri_smem ? sm + N * N : rinv;      // N x N (column-major) R^-1, on chip if it fits
   int* dead = reinterpret_cast<int*>(sm + (ri_smem ? 2 : 1) * N * N);
-  __shared__ double piv_s, dmax_s;
-  const int tid = threadIdx.x;
-  for (int idx = tid; idx < N * N; idx += blockDim.x) {
-    const int i = idx / N, j = idx % N;
-    A[idx] = w[i + (long long)N * j];
-  }
-  if (tid == 0) {
-    double dm = 0.0;
-    for (int i = 0; i < N; ++i) dm = fmax(dm, w[i + (long long)N * i]);
-    dmax_s = dm;
+  __shared__ double dinv[128];
+  __shared__ double dmax_s;
+  const int tid = threadIdx.x, NT = blockDim.x;
+  for (int idx = tid; idx < N * N; idx += NT) {
+    const int j = idx / N, i = idx - (idx / N) * N;  // w column-major: coalesced reads
+    A[i * N + j] = w[idx];
   }
   __syncthreads();
-  const double tol = rel_tol * dmax_s;
+  if (tid < 32) {
+    double dm = 0.0;
+    for (int i = tid; i < N; i += 32) dm = fmax(dm, A[i * N + i]);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
+    if (tid == 0) dmax_s = dm;
+  }
+  __syncthreads();
+  const double dmax = dmax_s, tol = rel_tol * dmax;
+  // column j = k + 1 + (tid % CW), rows from k + 1 + tid / CW in steps of RG
+  const int CW = N <= 32 ? 32 : N <= 64 ? 64 : 128;
+  const int RG = NT / CW;
   for (int k = 0; k < N; ++k) {
-    if (tid == 0) {
-      const double d = A[k * N + k];
-      if (!(d > tol) || dmax_s <= 0.0) {
-        dead[k] = 1;
-        piv_s = 0.0;
-      } else {
-        dead[k] = 0;
-        piv_s = sqrt(d);
+    const double d = A[k * N + k];
+    const bool live = d > tol && dmax > 0.0;
+    if (live) {
+      const double inv = 1.0 / d;
+      const int j = k + 1 + (tid % CW);
+      if (j < N) {
+        const double wkj = A[k * N + j] * inv;
+        const int i0 = k + 1 + tid / CW;
+        constexpr int U = 8;
+        for (int ib = i0; ib <= j; ib += U * RG) {
+          double wk[U], wij[U];
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int i = ib + u * RG;
+            if (i <= j) {
+              wk[u] = A[k * N + i];
+              wij[u] = A[i * N + j];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < U; ++u) {
+            const int i = ib + u * RG;
+            if (i <= j) A[i * N + j] = fma(-wk[u], wkj, wij[u]);
+          }
+        }
       }
     }
     __syncthreads();
-    const double pv = piv_s;
-    for (int j = k + tid; j < N; j += blockDim.x) {
-      if (pv == 0.0) {
-        A[k * N + j] = 0.0;
-      } else {
-        A[k * N + j] = (j == k) ? pv : A[k * N + j] / pv;
-      }
+    // row k of R: A[k][c] / sqrt(d) for c >= k (written after the update that read it)
+    if (live) {
+      const double sd = sqrt(d);
+      for (int c = k + tid; c < N; c += NT) A[k * N + c] = (c == k) ? sd : A[k * N + c] / sd;
+    } else {
+      for (int c = k + tid; c < N; c += NT) A[k * N + c] = 0.0;
     }
-    __syncthreads();
-    const int rem = N - k - 1;
-    for (int idx = tid; idx < rem * rem; idx += blockDim.x) {
-      const int i = k + 1 + idx / rem, j = k + 1 + idx % rem;
-      if (j >= i) A[i * N + j] -= A[k * N + i] * A[k * N + j];
-    }
+    if (tid == 0) dead[k] = live ? 0 : 1;
     __syncthreads();
   }
-  // R out (column-major), zero below the diagonal; dead diagonal entries stay 0.
+  for (int i = tid; i < N; i += NT) dinv[i] = dead[i] ? 0.0 : 1.0 / A[i * N + i];
+  // R out (column-major), zero below the diagonal; dead rows are zero.
   if (r_out) {
-    for (int idx = tid; idx < N * N; idx += blockDim.x) {
+    for (int idx = tid; idx < N * N; idx += NT) {
       const int i = idx % N, j = idx / N;
       r_out[idx] = (j >= i) ? A[i * N + j] : 0.0;
     }
   }
-  // R^-1 column by column in shared memory, then one coalesced copy out.
-  for (int idx = tid; idx < N * N; idx += blockDim.x) Ri[idx] = 0.0;
   __syncthreads();
-  for (int j = 0; j < N; ++j) {
-    if (dead[j]) continue;  // uniform across the block
-    const double rjj = A[j * N + j];
-    for (int i = tid; i <= j; i += blockDim.x) {
-      double v;
-      if (i == j) {
-        v = 1.0 / rjj;
-      } else if (dead[i]) {
-        v = 0.0;
-      } else {
-        double acc = 0.0;
-        for (int k = i; k < j; ++k) acc += Ri[i + N * k] * A[k * N + j];
-        v = -acc / rjj;
-      }
-      Ri[i + N * j] = v;
+  // R^-1, column j by thread j: x_j = 1 / r_jj, x_i = -(sum_{k=i+1..j} r_ik x_k) / r_ii.
+  for (int j = tid; j < N; j += NT) {
+    double* x = Ri + (long long)N * j;
+    for (int i = j + 1; i < N; ++i) x[i] = 0.0;
+    if (dead[j]) {
+      for (int i = 0; i <= j; ++i) x[i] = 0.0;
+      continue;
     }
-    __syncthreads();
+    x[j] = dinv[j];
+    for (int i = j - 1; i >= 0; --i) {
+      double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+      int kk = i + 1;
+      for (; kk + 3 <= j; kk += 4) {
+        s0 = fma(A[i * N + kk], x[kk], s0);
+        s1 = fma(A[i * N + kk + 1], x[kk + 1], s1);
+        s2 = fma(A[i * N + kk + 2], x[kk + 2], s2);
+        s3 = fma(A[i * N + kk + 3], x[kk + 3], s3);
+      }
+      for (; kk <= j; ++kk) s0 = fma(A[i * N + kk], x[kk], s0);
+      x[i] = -((s0 + s1) + (s2 + s3)) * dinv[i];
+    }
   }
-  if (ri_smem)
-    for (int idx = tid; idx < N * N; idx += blockDim.x) rinv[idx] = Ri[idx];
+  if (ri_smem) {
+    __syncthreads();
+    for (int idx = tid; idx < N * N; idx += NT) rinv[idx] = Ri[idx];
+  }
   (void)st;
 }
 
