@@ -1587,28 +1587,33 @@ int launch_gram(const float* x, long long nvec, int M, long long vs, long long e
 // One block: W (N x N, FP64) -> R (upper, FP64) and R^-1 (FP64).  Pivots below
 // rel_tol * max diag mark a dependent column: its row of R and column of R^-1 are zero.
 // Cholesky right-looking with one barrier per column; in the trailing update thread
-// (row group g, column j) loads all its rows before storing any.  R^-1 is formed column-parallel
-// with no barrier in between: thread j back-substitutes R x = e_j (x_i = -(sum_{k>i} r_ik x_k) / r_ii
-// with the reciprocal diagonal precomputed), four partial sums per dot product.
+// (row group g, column j) loads all its rows before storing any; the pivot's reciprocal square
+// root is the only special function per column.  R^-1 is formed column-parallel with no barrier
+// in between: thread j back-substitutes R x = e_j (x_i = -(sum_{k>i} r_ik x_k) / r_ii), four
+// partial sums per dot product.  On-chip matrices use an odd row stride (N | 1 doubles), so the
+// threads of a warp, each in a different row or column, read distinct banks.
+constexpr int chol_ld(int N) { return N | 1; }
 __global__ void __launch_bounds__(256) k_chol_inv(const double* __restrict__ w, int N,
                                                   double* __restrict__ r_out,
                                                   double* __restrict__ rinv, double rel_tol,
                                                   int ri_smem, DevStatus* st) {
   extern __shared__ double sm[];
-  double* A = sm;                                // N x N (row-major), upper part becomes R
-  double* Ri = ri_smem ? sm + N * N : rinv;      // N x N (column-major) R^-1, on chip if it fits
-  int* dead = reinterpret_cast<int*>(sm + (ri_smem ? 2 : 1) * N * N);
+  const int L = chol_ld(N);
+  double* A = sm;                                // N x L (row-major), upper part becomes R
+  double* Ri = ri_smem ? sm + N * L : rinv;      // R^-1 column-major: stride L on chip, N in memory
+  const int LR = ri_smem ? L : N;
+  int* dead = reinterpret_cast<int*>(sm + (ri_smem ? 2 : 1) * N * L);
   __shared__ double dinv[128];
   __shared__ double dmax_s;
   const int tid = threadIdx.x, NT = blockDim.x;
   for (int idx = tid; idx < N * N; idx += NT) {
     const int j = idx / N, i = idx - (idx / N) * N;  // w column-major: coalesced reads
-    A[i * N + j] = w[idx];
+    A[i * L + j] = w[idx];
   }
   __syncthreads();
   if (tid < 32) {
     double dm = 0.0;
-    for (int i = tid; i < N; i += 32) dm = fmax(dm, A[i * N + i]);
+    for (int i = tid; i < N; i += 32) dm = fmax(dm, A[i * L + i]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) dm = fmax(dm, __shfl_xor_sync(0xffffffffu, dm, o));
     if (tid == 0) dmax_s = dm;
@@ -1619,13 +1624,14 @@ __global__ void __launch_bounds__(256) k_chol_inv(const double* __restrict__ w, 
   const int CW = N <= 32 ? 32 : N <= 64 ? 64 : 128;
   const int RG = NT / CW;
   for (int k = 0; k < N; ++k) {
-    const double d = A[k * N + k];
+    const double d = A[k * L + k];
     const bool live = d > tol && dmax > 0.0;
+    const double rs = live ? rsqrt(d) : 0.0;  // 1 / r_kk
     if (live) {
-      const double inv = 1.0 / d;
+      const double inv = rs * rs;
       const int j = k + 1 + (tid % CW);
       if (j < N) {
-        const double wkj = A[k * N + j] * inv;
+        const double wkj = A[k * L + j] * inv;
         const int i0 = k + 1 + tid / CW;
         constexpr int U = 8;
         for (int ib = i0; ib <= j; ib += U * RG) {
@@ -1634,41 +1640,37 @@ __global__ void __launch_bounds__(256) k_chol_inv(const double* __restrict__ w, 
           for (int u = 0; u < U; ++u) {
             const int i = ib + u * RG;
             if (i <= j) {
-              wk[u] = A[k * N + i];
-              wij[u] = A[i * N + j];
+              wk[u] = A[k * L + i];
+              wij[u] = A[i * L + j];
             }
           }
 #pragma unroll
           for (int u = 0; u < U; ++u) {
             const int i = ib + u * RG;
-            if (i <= j) A[i * N + j] = fma(-wk[u], wkj, wij[u]);
+            if (i <= j) A[i * L + j] = fma(-wk[u], wkj, wij[u]);
           }
         }
       }
     }
     __syncthreads();
-    // row k of R: A[k][c] / sqrt(d) for c >= k (written after the update that read it)
-    if (live) {
-      const double sd = sqrt(d);
-      for (int c = k + tid; c < N; c += NT) A[k * N + c] = (c == k) ? sd : A[k * N + c] / sd;
-    } else {
-      for (int c = k + tid; c < N; c += NT) A[k * N + c] = 0.0;
+    // row k of R: A[k][c] / r_kk for c > k, r_kk = d / sqrt(d) (after the update that read it)
+    for (int c = k + tid; c < N; c += NT) A[k * L + c] = live ? A[k * L + c] * rs : 0.0;
+    if (tid == 0) {
+      dead[k] = live ? 0 : 1;
+      dinv[k] = rs;
     }
-    if (tid == 0) dead[k] = live ? 0 : 1;
     __syncthreads();
   }
-  for (int i = tid; i < N; i += NT) dinv[i] = dead[i] ? 0.0 : 1.0 / A[i * N + i];
   // R out (column-major), zero below the diagonal; dead rows are zero.
   if (r_out) {
     for (int idx = tid; idx < N * N; idx += NT) {
       const int i = idx % N, j = idx / N;
-      r_out[idx] = (j >= i) ? A[i * N + j] : 0.0;
+      r_out[idx] = (j >= i) ? A[i * L + j] : 0.0;
     }
   }
-  __syncthreads();
   // R^-1, column j by thread j: x_j = 1 / r_jj, x_i = -(sum_{k=i+1..j} r_ik x_k) / r_ii.
   for (int j = tid; j < N; j += NT) {
-    double* x = Ri + (long long)N * j;
+    double* x = Ri + (long long)LR * j;
     for (int i = j + 1; i < N; ++i) x[i] = 0.0;
     if (dead[j]) {
       for (int i = 0; i <= j; ++i) x[i] = 0.0;
@@ -1676,21 +1678,25 @@ __global__ void __launch_bounds__(256) k_chol_inv(const double* __restrict__ w, 
     }
     x[j] = dinv[j];
     for (int i = j - 1; i >= 0; --i) {
+      const double* ar = A + i * L;
       double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
       int kk = i + 1;
       for (; kk + 3 <= j; kk += 4) {
-        s0 = fma(A[i * N + kk], x[kk], s0);
-        s1 = fma(A[i * N + kk + 1], x[kk + 1], s1);
-        s2 = fma(A[i * N + kk + 2], x[kk + 2], s2);
-        s3 = fma(A[i * N + kk + 3], x[kk + 3], s3);
+        s0 = fma(ar[kk], x[kk], s0);
+        s1 = fma(ar[kk + 1], x[kk + 1], s1);
+        s2 = fma(ar[kk + 2], x[kk + 2], s2);
+        s3 = fma(ar[kk + 3], x[kk + 3], s3);
       }
-      for (; kk <= j; ++kk) s0 = fma(A[i * N + kk], x[kk], s0);
+      for (; kk <= j; ++kk) s0 = fma(ar[kk], x[kk], s0);
       x[i] = -((s0 + s1) + (s2 + s3)) * dinv[i];
     }
   }
   if (ri_smem) {
     __syncthreads();
-    for (int idx = tid; idx < N * N; idx += NT) rinv[idx] = Ri[idx];
+    for (int idx = tid; idx < N * N; idx += NT) {
+      const int i = idx % N, j = idx / N;
+      rinv[idx] = Ri[i + L * j];
+    }
   }
   (void)st;
 }
@@ -2147,8 +2153,8 @@ static int cholqr_passes(float* y, long long n, int N, long long vs, long long e
     return TT_ERR_NOMEM;
   }
   const int NP = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : N <= 64 ? 64 : 128;
-  const int ri_smem = 2 * (size_t)N * N * sizeof(double) + N * sizeof(int) + 16 <= 200 * 1024;
-  const size_t shm = (size_t)(ri_smem ? 2 : 1) * N * N * sizeof(double) + N * sizeof(int) + 16;
+  const int ri_smem = 2 * (size_t)N * chol_ld(N) * sizeof(double) + N * sizeof(int) + 16 <= 200 * 1024;
+  const size_t shm = (size_t)(ri_smem ? 2 : 1) * N * chol_ld(N) * sizeof(double) + N * sizeof(int) + 16;
   smem_optin_k(k_chol_inv, 200 * 1024);
   smem_optin_k(k_apply_rinv<16>, 200 * 1024);
   smem_optin_k(k_apply_rinv<32>, 200 * 1024);
@@ -2226,17 +2232,17 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
   __shared__ double2 pcs[2][64];
   __shared__ int mv[128], imv[128];
   __shared__ int2 mv2[64];
-  __shared__ int roff[128];
   __shared__ double dg[128];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  auto at = [&](int P, int Q) { return roff[P] + (Q - (P & ~1)); };  // P <= Q
+  // offset of entry (P, Q), P <= Q: arithmetic (a few integer ops) rather than a table lookup,
+  // which would add a shared-memory load to every access
+  auto at = [&](int P, int Q) { return blp_off(P, Np) + (Q - (P & ~1)); };
   for (int P = tid; P < Np; P += blockDim.x) {
     const int x = P % 2 == 0 ? P / 2 : Np - 1 - P / 2;
     const int xn = x == 0 ? 0 : (x == 1 ? NR : x - 1);
     const int Pn = bl_pos(xn, Np);
     mv[P] = Pn;
     imv[Pn] = P;
-    roff[P] = blp_off(P, Np);
   }
   __syncthreads();
   for (int e = tid; e < 2 * PS; e += blockDim.x) Wb0[e] = 0.0;
@@ -2311,7 +2317,7 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
           const double2 csa = cs_[a], csb = cs_[b];
           const double ca = csa.x, sa = csa.y, cbv = csb.x, sb = csb.y;
           const double2 r0v = *reinterpret_cast<const double2*>(&W[at(2 * a, 2 * b)]);
-          const double2 r1v = *reinterpret_cast<const double2*>(&W[roff[2 * a + 1] + (2 * b - 2 * a)]);
+          const double2 r1v = *reinterpret_cast<const double2*>(&W[blp_off(2 * a + 1, Np) + (2 * b - 2 * a)]);
           const double w00 = r0v.x, w01 = r0v.y, w11 = r1v.y;
           const double w10 = (a == b) ? w01 : r1v.x;
           const double x00 = ca * w00 - sa * w10, x01 = ca * w01 - sa * w11;
@@ -2337,7 +2343,7 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
           const double cP = cs_[aP].x, sP = cs_[aP].y, cQ = cs_[aQ].x, sQ = cs_[aQ].y;
           const double tP0 = xP ? sP : cP, tP1 = xP ? cP : -sP;
           const double tQ0 = xQ ? sQ : cQ, tQ1 = xQ ? cQ : -sQ;
-          auto wu = [&](int r, int c2) { return r <= c2 ? W[at(r, c2)] : W[at(c2, r)]; };
+          auto wu = [&](int r, int c2) { return W[at(min(r, c2), max(r, c2))]; };  // no divergence
           const int P0 = 2 * aP, Q0 = 2 * aQ;
           const double p0 = tP0 * wu(P0, P0) + tP1 * wu(P0, P0 + 1);
           const double p1 = tP0 * wu(P0, P0 + 1) + tP1 * wu(P0 + 1, P0 + 1);
