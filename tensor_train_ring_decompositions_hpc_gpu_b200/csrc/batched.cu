@@ -240,7 +240,7 @@ __global__ void __launch_bounds__(BT, 1)
         const int N = (int)small;
         if (m <= cols) cta_gram(src, 1, m, N, cols, S.w);   // W = A A^T, vectors = columns
         else cta_gram(src, m, 1, N, m, S.w);                // W = A^T A, vectors = rows
-        const int sw = bl_solve(S.w, N, lam, evec, max_sweeps, S.jac);
+        const int sw = bl_solve<0>(S.w, N, lam, evec, max_sweeps, S.jac);
         if (tid == 0 && st) {
           atomicMax(&st->sweeps, sw);
           if (sw > max_sweeps) dev_fail(st, TT_ERR_NOCONV, t);
@@ -394,7 +394,7 @@ __global__ void __launch_bounds__(BT, 1)
         }
         __syncthreads();
         cta_gram(Bg, 1, ks, ks, cols, S.w);  // W = B B^T (vectors = columns of B)
-        const int sw = bl_solve(S.w, ks, lam, evec, max_sweeps, S.jac);
+        const int sw = bl_solve<0>(S.w, ks, lam, evec, max_sweeps, S.jac);
         if (tid == 0 && st) {
           atomicMax(&st->sweeps, sw);
           if (sw > max_sweeps) dev_fail(st, TT_ERR_NOCONV, t);

@@ -2192,13 +2192,17 @@ static int cholqr_passes(float* y, long long n, int N, long long vs, long long e
 // ---------------------------------------------------------------------------------------
 // Symmetric eigen-decomposition: parallel cyclic Jacobi (round-robin pairs), FP64
 // ---------------------------------------------------------------------------------------
-// Single-matrix solver for N <= 64 (bl_solver.cuh): one CTA of bl_shape's warp count.
-__global__ void __launch_bounds__(1024) k_syev_bl(const double* __restrict__ w_in, int N,
+// Single-matrix solver for N <= 64 (bl_solver.cuh): one CTA of bl_shape's warp count, compiled
+// for the smallest thread bound that holds it, so that the compiler may give each thread the
+// registers it needs (at 1024 threads it has 64 and spills): V is row-resident up to N = 46
+// (at most 8 warps for N <= 32, 12 for N <= 46); 46 < N <= 64 splits V and takes 1024 threads.
+template <int MAXT, int VN>
+__global__ void __launch_bounds__(MAXT, 1) k_syev_bl(const double* __restrict__ w_in, int N,
                                                    double* __restrict__ evals,
                                                    double* __restrict__ evecs, int max_sweeps,
                                                    DevStatus* st) {
   extern __shared__ __align__(16) double sm_bl[];
-  const int sw = bl_solve(w_in, N, evals, evecs, max_sweeps, sm_bl);
+  const int sw = bl_solve<VN>(w_in, N, evals, evecs, max_sweeps, sm_bl);
   if (threadIdx.x == 0 && st) {
     atomicMax(&st->sweeps, min(sw, max_sweeps));
     if (sw > max_sweeps) dev_fail(st, TT_ERR_NOCONV, max_sweeps);
@@ -2462,9 +2466,17 @@ int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sw
     const int Nps = N + (N & 1);
     const size_t shm_bl = 2 * (size_t)Nps * Nps * sizeof(double);
     int iso, warps;
-    bl_shape(N, &iso, &warps);
-    smem_optin_k(k_syev_bl, shm_bl);
-    k_syev_bl<<<1, 32 * warps, shm_bl, s>>>(w, N, evals, evecs, max_sweeps, st);
+    bl_shape(N, N <= 46, &iso, &warps);
+    if (N <= 32) {
+      smem_optin_k(k_syev_bl<256, 32>, shm_bl);
+      k_syev_bl<256, 32><<<1, 32 * warps, shm_bl, s>>>(w, N, evals, evecs, max_sweeps, st);
+    } else if (N <= 46) {
+      smem_optin_k(k_syev_bl<384, 48>, shm_bl);
+      k_syev_bl<384, 48><<<1, 32 * warps, shm_bl, s>>>(w, N, evals, evecs, max_sweeps, st);
+    } else {
+      smem_optin_k(k_syev_bl<1024, 0>, shm_bl);
+      k_syev_bl<1024, 0><<<1, 32 * warps, shm_bl, s>>>(w, N, evals, evecs, max_sweeps, st);
+    }
     count_launch();
     TT_LAUNCH_CHECK();
     return TT_OK;
