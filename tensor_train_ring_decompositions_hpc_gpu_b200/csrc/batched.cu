@@ -356,21 +356,29 @@ __global__ void __launch_bounds__(BT, 1)
             }
             __syncthreads();
           }
-          // row i: q R = y (forward substitution, R[k][c] = W[k][c] / sqrt(W[k][k]) on live rows)
+          // R in FP32 once (the eigen-solver's buffer is free here): rf[k ks + c] = W[k][c] /
+          // sqrt(W[k][k]) for live rows k < c (0 on dead ones), rf[ks ks + c] = 1 / sqrt(W[c][c])
+          // (0: dead column), so the substitution below is FMAs only.
+          float* rf = reinterpret_cast<float*>(S.jac);
+          for (int idx = tid; idx < ks * ks + ks; idx += BT) {
+            if (idx < ks * ks) {
+              const int kk = idx / ks, c = idx - kk * ks;
+              const double dk = Wc[kk * ks + kk];
+              rf[idx] = (kk < c && dk > tol && dmax > 0.0) ? (float)(Wc[kk * ks + c] / sqrt(dk)) : 0.f;
+            } else {
+              const double dc = Wc[(idx - ks * ks) * (ks + 1)];
+              rf[idx] = (dc > tol && dmax > 0.0) ? (float)(1.0 / sqrt(dc)) : 0.f;
+            }
+          }
+          __syncthreads();
+          // row i: q R = y (forward substitution; a dead column's entry is 0, so it adds nothing)
           if (tid < mi) {
             float* yr = S.yq + tid * SY;
             for (int c = 0; c < ks; ++c) {
-              const double dc = Wc[c * ks + c];
-              if (!(dc > tol && dmax > 0.0)) {
-                yr[c] = 0.f;
-                continue;
-              }
+              const float dv = rf[ks * ks + c];
               float a = yr[c];
-              for (int kk = 0; kk < c; ++kk) {
-                const double dk = Wc[kk * ks + kk];
-                if (dk > tol && dmax > 0.0) a = fmaf(-yr[kk], (float)(Wc[kk * ks + c] / sqrt(dk)), a);
-              }
-              yr[c] = a * (float)(1.0 / sqrt(dc));
+              for (int kk = 0; kk < c; ++kk) a = fmaf(-yr[kk], rf[kk * ks + c], a);
+              yr[c] = dv == 0.f ? 0.f : a * dv;
             }
           }
           __syncthreads();
