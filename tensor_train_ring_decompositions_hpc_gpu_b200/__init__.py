@@ -298,13 +298,14 @@ def gram_tall(z, rowmajor=False):
     return w
 
 
-def cholqr2(y):
-    """CholeskyQR2 of a tall matrix; returns (Q, R)."""
+def cholqr2(y, want_r=True):
+    """CholeskyQR2 of a tall matrix; returns (Q, R), or (Q, None) with want_r=False (the form the
+    decomposition's sketches use: no R, which lets up to 80 columns run in one launch)."""
     torch = _torch()
     q = y.float().t().contiguous().clone().t()  # private column-major copy
     n, N = q.shape
-    r = _colmajor(N, N, torch.float64, q.device)
-    check(lib().tt_k_cholqr2(_ctx_for(q.device.index), _ptr(q), n, N, n, _ptr(r)))
+    r = _colmajor(N, N, torch.float64, q.device) if want_r else None
+    check(lib().tt_k_cholqr2(_ctx_for(q.device.index), _ptr(q), n, N, n, _ptr(r) if want_r else None))
     return q, r
 
 

@@ -1844,7 +1844,8 @@ __device__ __forceinline__ double ld_peer_f64(const double* p, unsigned rank) {
 }
 
 // CholeskyQR2 of an n x N sketch (N <= 64) in one launch: a cluster of up to 8 CTAs, each
-// holding `rpc` consecutive rows in shared memory.  Y is staged row-major with a padded
+// holding `rpc` consecutive rows in shared memory (64 < N <= 80: one CTA of 256 threads, the
+// Gram summed straight into W, no R output).  Y is staged row-major with a padded
 // stride S (S/4 odd, so the float4 row accesses of neighbouring threads fall in distinct
 // banks); per pass:
 //   each CTA's partial Gram Y_c^T Y_c in FP64 (4x4 register tiles over the upper tile
@@ -1858,10 +1859,11 @@ __device__ __forceinline__ double ld_peer_f64(const double* p, unsigned rank) {
 // buffer, so a CTA that runs ahead never overwrites a partial a peer is still reading; the
 // final cluster barrier keeps every CTA's shared memory alive until the peers are done.
 template <int NP>
-__global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, int n, int N, long long vs,
-                                                       long long es, int S, int rpc,
-                                                       double* __restrict__ r, double rel_tol) {
-  constexpr int NT = 512;
+__global__ void __launch_bounds__(NP > 64 ? 256 : 512) k_cholqr2_small(float* __restrict__ y, int n, int N,
+                                                                      long long vs, long long es, int S,
+                                                                      int rpc, double* __restrict__ r,
+                                                                      double rel_tol) {
+  constexpr int NT = NP > 64 ? 256 : 512;  // the wide rows of the substitution need the registers
   extern __shared__ __align__(16) unsigned char sm_cq[];
   const unsigned crank = cl_rank(), csize = cl_size();
   const int row0 = (int)crank * rpc;
@@ -1869,7 +1871,7 @@ __global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, in
   const int WN = (N * N + 1) & ~1;
   float* Ys = reinterpret_cast<float*>(sm_cq);                       // rpc x S
   double* Wp = reinterpret_cast<double*>(Ys + (size_t)rpc * S);      // 2 x N x N partials
-  double* W = Wp + 2 * WN;                                           // N x N row-major
+  double* W = NP > 64 ? Wp : Wp + 2 * WN;                            // N x N row-major
   float* Rf = reinterpret_cast<float*>(W + WN);                      // NP x NP, Rf[c*NP+k] = R[k][c]
   float* invd = Rf + NP * NP;                                        // NP
   double* R1 = reinterpret_cast<double*>(invd + NP);                 // N x N (only with r)
@@ -1899,7 +1901,7 @@ __global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, in
   }
   const int tb = ta + rem;
   for (int pass = 0; pass < 2; ++pass) {
-    double* Wq = Wp + pass * WN;
+    double* Wq = NP > 64 ? W : Wp + pass * WN;
     __syncthreads();
     double acc[16];
 #pragma unroll
@@ -1947,26 +1949,28 @@ __global__ void __launch_bounds__(512) k_cholqr2_small(float* __restrict__ y, in
     for (int k = 0; k < N; ++k) {
       const double d = W[k * N + k];
       if (d > tol && dmax > 0.0) {
-        // trailing update of the upper triangle: thread (row group tid >> 6, column tid & 63);
-        // the at most 8 rows of a thread are loaded before any is stored
+        // trailing update of the upper triangle: thread (row group tid / CW, column tid % CW);
+        // a thread's rows in chunks of 8, each chunk loaded before any of it is stored
+        constexpr int CW = NP > 64 ? 128 : 64, RG = NT / CW;
         const double inv = 1.0 / d;
-        const int j = k + 1 + (tid & 63);
+        const int j = k + 1 + (tid % CW);
         if (j < N) {
           const double wkj = W[k * N + j] * inv;
-          const int i0 = k + 1 + (tid >> 6);
-          double wk[8], wij[8];
+          for (int i0 = k + 1 + tid / CW; i0 <= j; i0 += 8 * RG) {
+            double wk[8], wij[8];
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const int i = i0 + 8 * u;
-            if (i <= j) {
-              wk[u] = W[k * N + i];
-              wij[u] = W[i * N + j];
+            for (int u = 0; u < 8; ++u) {
+              const int i = i0 + RG * u;
+              if (i <= j) {
+                wk[u] = W[k * N + i];
+                wij[u] = W[i * N + j];
+              }
             }
-          }
 #pragma unroll
-          for (int u = 0; u < 8; ++u) {
-            const int i = i0 + 8 * u;
-            if (i <= j) W[i * N + j] = fma(-wk[u], wkj, wij[u]);
+            for (int u = 0; u < 8; ++u) {
+              const int i = i0 + RG * u;
+              if (i <= j) W[i * N + j] = fma(-wk[u], wkj, wij[u]);
+            }
           }
         }
       }
@@ -2056,13 +2060,15 @@ static int max_optin_smem() { return dev_smem_max(); }
 // Cluster shape and shared-memory bytes of k_cholqr2_small: the fewest CTAs (at most 8) with
 // at least 128 rows each that fit in shared memory; 0 when the sketch does not fit.
 static size_t cholqr2_small_smem(long long n, int N, bool want_r, int* S_out, int* cl_out, int* rpc_out) {
-  if (N < 1 || N > 64 || n < 1 || n > (1LL << 20)) return 0;
-  const int NP = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : 64;
+  if (N < 1 || N > 80 || n < 1 || n > (1LL << 20)) return 0;
+  if (N > 64 && want_r) return 0;  // the one-CTA wide variant forms no R
+  const int NP = N <= 16 ? 16 : N <= 32 ? 32 : N <= 48 ? 48 : N <= 64 ? 64 : 80;
   int S = 4 * ((N + 3) / 4);
   if (((S / 4) & 1) == 0) S += 4;
   const size_t WN = ((size_t)N * N + 1) & ~(size_t)1;
-  const size_t fixed = 3 * WN * 8 + (size_t)NP * NP * 4 + NP * 4 + (want_r ? (size_t)N * N * 8 : 0);
-  for (int cl = (int)std::min<long long>(8, std::max<long long>(1, (n + 127) / 128)); cl <= 8; ++cl) {
+  const size_t fixed = (NP > 64 ? 1 : 3) * WN * 8 + (size_t)NP * NP * 4 + NP * 4 + (want_r ? (size_t)N * N * 8 : 0);
+  const int cl_max = NP > 64 ? 1 : 8;
+  for (int cl = (int)std::min<long long>(cl_max, std::max<long long>(1, (n + 127) / 128)); cl <= cl_max; ++cl) {
     const long long rpc = (n + cl - 1) / cl;
     const size_t bytes = (size_t)rpc * S * 4 + fixed;
     if (bytes <= (size_t)max_optin_smem()) {
@@ -2110,10 +2116,11 @@ static int cholqr_passes(float* y, long long n, int N, long long vs, long long e
       smem_optin_k(k_cholqr2_small<32>, mx);
       smem_optin_k(k_cholqr2_small<48>, mx);
       smem_optin_k(k_cholqr2_small<64>, mx);
+      smem_optin_k(k_cholqr2_small<80>, mx);
     }
     cudaLaunchConfig_t cfg = {};
     cfg.gridDim = dim3(cl, 1, 1);
-    cfg.blockDim = dim3(512, 1, 1);
+    cfg.blockDim = dim3(N > 64 ? 256 : 512, 1, 1);
     cfg.dynamicSmemBytes = sshm;
     cfg.stream = s;
     cudaLaunchAttribute at[1];
@@ -2132,8 +2139,10 @@ static int cholqr_passes(float* y, long long n, int N, long long vs, long long e
       e = cudaLaunchKernelEx(&cfg, k_cholqr2_small<32>, y, nn, N, vs, es, S, rpc, r, tol);
     else if (N <= 48)
       e = cudaLaunchKernelEx(&cfg, k_cholqr2_small<48>, y, nn, N, vs, es, S, rpc, r, tol);
-    else
+    else if (N <= 64)
       e = cudaLaunchKernelEx(&cfg, k_cholqr2_small<64>, y, nn, N, vs, es, S, rpc, r, tol);
+    else
+      e = cudaLaunchKernelEx(&cfg, k_cholqr2_small<80>, y, nn, N, vs, es, S, rpc, r, tol);
     if (e == cudaSuccess) {
       count_launch();
       TT_LAUNCH_CHECK();

@@ -133,6 +133,20 @@ def test_cholqr2(gpu, n, N):
     assert _rel(qd @ rd, y.double().cpu().numpy()) < 1e-5
 
 
+@pytest.mark.parametrize("n,N", [(256, 65), (256, 80), (462, 72), (462, 80), (463, 80), (2000, 80), (5000, 64)])
+def test_cholqr2_without_r(gpu, n, N):
+    """The decomposition's form (no R): up to 80 columns and ~460 rows in one CTA, larger sketches
+    through the cluster or the multi-launch path; Q orthonormal and spanning Y."""
+    ttr = _ttr()
+    y = _randn_cm(n, N, 11, gpu)
+    q, r = ttr.cholqr2(y, want_r=False)
+    assert r is None
+    qd = q.double().cpu().numpy()
+    yd = y.double().cpu().numpy()
+    assert np.linalg.norm(qd.T @ qd - np.eye(N)) < 1e-5
+    assert _rel(qd @ (qd.T @ yd), yd) < 1e-5
+
+
 def test_cholqr2_rank_deficient_zeroes_dependent_columns(gpu):
     import torch
     ttr = _ttr()
@@ -145,7 +159,7 @@ def test_cholqr2_rank_deficient_zeroes_dependent_columns(gpu):
     assert np.all(norms[:6] > 0.99) and np.all(norms[6:] < 1e-3)
 
 
-@pytest.mark.parametrize("N", [1, 2, 5, 24, 32, 33, 40, 63, 64, 65, 96, 128])
+@pytest.mark.parametrize("N", [1, 2, 5, 24, 31, 32, 33, 40, 44, 45, 46, 47, 63, 64, 65, 96, 128])
 def test_syev(gpu, N):
     import torch
     ttr = _ttr()
