@@ -2221,9 +2221,11 @@ __global__ void __launch_bounds__(MAXT, 1) k_syev_bl(const double* __restrict__ 
 // Large-N variant (64 < N <= 128) of the Brent-Luk solver.  W alone stays in shared memory: its
 // upper triangle packed by rows (row P stored from column P & ~1, so every 2 x 2 block row is a
 // 16-byte load), double-buffered (2 x 66.5 KB for N = 128).  The eigenvectors are not updated
-// round by round: the rotation warps log each round's FP32 (c, s) pairs to global memory, and
+// round by round: the rotation warps log each round's renormalised FP64 (c, s) pairs to global
+// memory (so the replay's per-round chain has no conversion or renormalisation), and
 // k_bl_replay applies them afterwards to the rows of V, one CTA per row (rows are independent),
-// with the same moves.  Two warps compute the next round's rotations during the update.
+// with the same moves.  Two warps compute the next round's rotations during the update; every
+// W thread's block addresses and the rotation lanes' entry offsets are computed once.
 __device__ __forceinline__ int blp_off(int P, int Np) {
   // sum over rows p < P of (Np - (p & ~1)): pairs of rows (2a, 2a + 1) hold 2 (Np - 2a) entries
   const int a = P >> 1;
@@ -2231,7 +2233,7 @@ __device__ __forceinline__ int blp_off(int P, int Np) {
 }
 
 __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_in, int N,
-                                                    double* __restrict__ evals, float2* __restrict__ tlog,
+                                                    double* __restrict__ evals, double2* __restrict__ tlog,
                                                     int* __restrict__ meta, int max_sweeps, DevStatus* st) {
   constexpr int RW0 = 30;  // warps 30, 31 compute the next round's rotations
   constexpr int NE = RW0 * 32;
@@ -2244,7 +2246,6 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
   double* Wb1 = Wb0 + PS;
   __shared__ double2 pcs[2][64];
   __shared__ int mv[128], imv[128];
-  __shared__ int2 mv2[64];
   __shared__ double dg[128];
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   // offset of entry (P, Q), P <= Q: arithmetic (a few integer ops) rather than a table lookup,
@@ -2268,7 +2269,6 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
     if (i < N && j < N) v = 0.5 * (w_in[i + (long long)N * j] + w_in[j + (long long)N * i]);
     Wb0[at(Pi, Pj)] = v;
   }
-  for (int q = tid; q < H; q += blockDim.x) mv2[q] = make_int2(mv[2 * q], mv[2 * q + 1]);
   double dm = 0.0;
   for (int i = 0; i < N; ++i) dm = fmax(dm, fabs(w_in[i + (long long)N * i]));
   const double inv_s = dm > 0.0 ? 1.0 / dm : 1.0;
@@ -2283,33 +2283,56 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
     double c, sn;
     rot_from_cs32(r, c, sn);
     pcs[0][k] = make_double2(c, sn);
-    tlog[k] = r;
+    tlog[k] = make_double2(c, sn);
   }
   __syncthreads();
   const int NWB = H * (H + 1) / 2;
   constexpr int MAXIT = (64 * 65 / 2 + NE - 1) / NE;
-  int dsc[MAXIT];
+  // per block of this thread: the pair indices (a | b << 8, -1 for none), the offsets of its two
+  // rows in W and of its four entries' next-round upper positions (fixed over the rounds)
+  int dsc[MAXIT], ldo[MAXIT], sto[MAXIT][4];
 #pragma unroll
   for (int u = 0; u < MAXIT; ++u) {
     const int it = tid + u * NE;
-    if (warp >= RW0 || it >= NWB) {
-      dsc[u] = -1;
-    } else {
+    dsc[u] = -1;
+    ldo[u] = 0;
+    sto[u][0] = sto[u][1] = sto[u][2] = sto[u][3] = 0;
+    if (warp < RW0 && it < NWB) {
       int a = 0, rem = it;
       while (rem >= H - a) {
         rem -= H - a;
         ++a;
       }
-      dsc[u] = a | ((a + rem) << 8);
+      const int b = a + rem;
+      dsc[u] = a | (b << 8);
+      ldo[u] = at(2 * a, 2 * b);
+      const int r0 = mv[2 * a], r1 = mv[2 * a + 1], q0 = mv[2 * b], q1 = mv[2 * b + 1];
+      sto[u][0] = at(min(r0, q0), max(r0, q0));
+      sto[u][1] = at(min(r0, q1), max(r0, q1));
+      sto[u][2] = at(min(r1, q0), max(r1, q0));
+      sto[u][3] = at(min(r1, q1), max(r1, q1));
     }
   }
   int aP = 0, xP = 0, aQ = 0, xQ = 0;
+  int wo[10] = {0, 0, 0, 0, 0, 0, 0, 0, 0, 0};  // offsets of the entries the rotation lane reads
   if (warp >= RW0 && rl < H) {
     const int P = imv[2 * rl], Q = imv[2 * rl + 1];
     aP = P >> 1;
     xP = P & 1;
     aQ = Q >> 1;
     xQ = Q & 1;
+    const int P0 = 2 * aP, Q0 = 2 * aQ;
+    auto ou = [&](int r, int c2) { return at(min(r, c2), max(r, c2)); };
+    wo[0] = ou(P0, P0);
+    wo[1] = ou(P0, P0 + 1);
+    wo[2] = ou(P0 + 1, P0 + 1);
+    wo[3] = ou(Q0, Q0);
+    wo[4] = ou(Q0, Q0 + 1);
+    wo[5] = ou(Q0 + 1, Q0 + 1);
+    wo[6] = ou(P0, Q0);
+    wo[7] = ou(P0 + 1, Q0);
+    wo[8] = ou(P0, Q0 + 1);
+    wo[9] = ou(P0 + 1, Q0 + 1);
   }
   int R = 0;
   int sweep = 0;
@@ -2329,20 +2352,19 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
           const int a = dd & 255, b = (dd >> 8) & 255;
           const double2 csa = cs_[a], csb = cs_[b];
           const double ca = csa.x, sa = csa.y, cbv = csb.x, sb = csb.y;
-          const double2 r0v = *reinterpret_cast<const double2*>(&W[at(2 * a, 2 * b)]);
-          const double2 r1v = *reinterpret_cast<const double2*>(&W[blp_off(2 * a + 1, Np) + (2 * b - 2 * a)]);
+          // row 2a + 1 starts (Np - 2a) entries after row 2a (both stored from column 2a)
+          const double2 r0v = *reinterpret_cast<const double2*>(&W[ldo[u]]);
+          const double2 r1v = *reinterpret_cast<const double2*>(&W[ldo[u] + (Np - 2 * a)]);
           const double w00 = r0v.x, w01 = r0v.y, w11 = r1v.y;
           const double w10 = (a == b) ? w01 : r1v.x;
           const double x00 = ca * w00 - sa * w10, x01 = ca * w01 - sa * w11;
           const double x10 = sa * w00 + ca * w10, x11 = sa * w01 + ca * w11;
           const double y00 = x00 * cbv - x01 * sb, y01 = x00 * sb + x01 * cbv;
           const double y10 = x10 * cbv - x11 * sb, y11 = x10 * sb + x11 * cbv;
-          const int2 ma = mv2[a], mb = mv2[b];
-          const int r0 = ma.x, r1 = ma.y, q0 = mb.x, q1 = mb.y;
-          Wn[at(min(r0, q0), max(r0, q0))] = y00;
-          Wn[at(min(r0, q1), max(r0, q1))] = y01;
-          if (a != b) Wn[at(min(r1, q0), max(r1, q0))] = y10;
-          Wn[at(min(r1, q1), max(r1, q1))] = y11;
+          Wn[sto[u][0]] = y00;
+          Wn[sto[u][1]] = y01;
+          if (a != b) Wn[sto[u][2]] = y10;
+          Wn[sto[u][3]] = y11;
         }
       } else if (rl < H) {
         const int rn = (rnd + 1 == NR) ? 0 : rnd + 1;
@@ -2356,20 +2378,18 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
           const double cP = cs_[aP].x, sP = cs_[aP].y, cQ = cs_[aQ].x, sQ = cs_[aQ].y;
           const double tP0 = xP ? sP : cP, tP1 = xP ? cP : -sP;
           const double tQ0 = xQ ? sQ : cQ, tQ1 = xQ ? cQ : -sQ;
-          auto wu = [&](int r, int c2) { return W[at(min(r, c2), max(r, c2))]; };  // no divergence
-          const int P0 = 2 * aP, Q0 = 2 * aQ;
-          const double p0 = tP0 * wu(P0, P0) + tP1 * wu(P0, P0 + 1);
-          const double p1 = tP0 * wu(P0, P0 + 1) + tP1 * wu(P0 + 1, P0 + 1);
-          const double q0 = tQ0 * wu(Q0, Q0) + tQ1 * wu(Q0, Q0 + 1);
-          const double q1 = tQ0 * wu(Q0, Q0 + 1) + tQ1 * wu(Q0 + 1, Q0 + 1);
-          const double m0 = tP0 * wu(P0, Q0) + tP1 * wu(P0 + 1, Q0);
-          const double m1 = tP0 * wu(P0, Q0 + 1) + tP1 * wu(P0 + 1, Q0 + 1);
+          const double p0 = tP0 * W[wo[0]] + tP1 * W[wo[1]];
+          const double p1 = tP0 * W[wo[1]] + tP1 * W[wo[2]];
+          const double q0 = tQ0 * W[wo[3]] + tQ1 * W[wo[4]];
+          const double q1 = tQ0 * W[wo[4]] + tQ1 * W[wo[5]];
+          const double m0 = tP0 * W[wo[6]] + tP1 * W[wo[7]];
+          const double m1 = tP0 * W[wo[8]] + tP1 * W[wo[9]];
           r = jacobi_cs32(p0 * tP0 + p1 * tP1, q0 * tQ0 + q1 * tQ1, m0 * tQ0 + m1 * tQ1, inv_s);
         }
         double c, sn;
         rot_from_cs32(r, c, sn);
         pcs[cb ^ 1][rl] = make_double2(c, sn);
-        tlog[(size_t)(R + 1) * H + rl] = r;  // rotations of round R + 1
+        tlog[(size_t)(R + 1) * H + rl] = make_double2(c, sn);  // rotations of round R + 1
       }
       __syncthreads();
       if (rnd + 1 == NR) {
@@ -2418,7 +2438,7 @@ __global__ void __launch_bounds__(1024) k_syev_blw(const double* __restrict__ w_
 
 // Replays the logged rotations on row i of V (one CTA per row, one thread per pair; V starts as
 // the identity with index i at its round-0 position) and writes the eigenvectors by rank.
-__global__ void __launch_bounds__(64) k_bl_replay(const float2* __restrict__ tlog, const int* __restrict__ meta,
+__global__ void __launch_bounds__(64) k_bl_replay(const double2* __restrict__ tlog, const int* __restrict__ meta,
                                                   int N, double* __restrict__ evecs) {
   __shared__ double vb[2][128];
   __shared__ int mvs[128];
@@ -2435,17 +2455,16 @@ __global__ void __launch_bounds__(64) k_bl_replay(const float2* __restrict__ tlo
   const int m0 = k < H ? mvs[2 * k] : 0, m1 = k < H ? mvs[2 * k + 1] : 0;
   constexpr int U = 8;
   for (int R0 = 0; R0 < rounds; R0 += U) {
-    float2 tf[U];
+    double2 tf[U];
 #pragma unroll
     for (int j = 0; j < U; ++j)
-      tf[j] = (k < H && R0 + j < rounds) ? tlog[(size_t)(R0 + j) * H + k] : make_float2(1.0f, 0.0f);
+      tf[j] = (k < H && R0 + j < rounds) ? tlog[(size_t)(R0 + j) * H + k] : make_double2(1.0, 0.0);
 #pragma unroll
     for (int j = 0; j < U; ++j) {
       if (R0 + j >= rounds) break;
       const int cb = (R0 + j) & 1;
       if (k < H) {
-        double c, sn;
-        rot_from_cs32(tf[j], c, sn);
+        const double c = tf[j].x, sn = tf[j].y;
         const double v0 = vb[cb][2 * k], v1 = vb[cb][2 * k + 1];
         vb[cb ^ 1][m0] = v0 * c - v1 * sn;
         vb[cb ^ 1][m1] = v0 * sn + v1 * c;
@@ -2461,7 +2480,7 @@ size_t syev_ws_bytes(int N, int max_sweeps) {
   if (N <= 64) return 0;
   const int Np = N + (N & 1);
   const int sw = max_sweeps > 0 ? max_sweeps : 40;
-  return ((size_t)sw * (Np - 1) + 2) * (Np / 2) * sizeof(float2) + (1 + 2 * 128) * sizeof(int) + 1024;
+  return ((size_t)sw * (Np - 1) + 2) * (Np / 2) * sizeof(double2) + (1 + 2 * 128) * sizeof(int) + 1024;
 }
 
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps, Arena& ws,
@@ -2494,7 +2513,7 @@ int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sw
   const int Np = N + (N & 1), H = Np / 2;
   const int sw = max_sweeps > 0 ? max_sweeps : 40;
   const size_t mk = ws.mark();
-  float2* tlog = ws.take<float2>(((size_t)sw * (Np - 1) + 2) * H);
+  double2* tlog = ws.take<double2>(((size_t)sw * (Np - 1) + 2) * H);
   int* meta = ws.take<int>(1 + 2 * 128);
   if (!tlog || !meta) {
     set_error(TT_ERR_NOMEM, "eigen-solver rotation log");
