@@ -126,6 +126,23 @@ __device__ void cta_gram(const float* __restrict__ base, long long ps, long long
   }
 }
 
+template <int W>
+struct Width {
+  static constexpr int value = W;
+};
+
+// Calls f(Width<W>{}) with W = n rounded up to a multiple of 8 (n <= BSMALL).  The per-column
+// register loops of a step (a rank or sketch width of 2..32) then run over W columns rather than
+// all BSMALL with most of them predicated off; columns beyond n are computed on zeros or ignored
+// and never stored, so every kept column's FMA sequence is the same whatever W is.
+template <class F>
+__device__ __forceinline__ void by_width(int n, F&& f) {
+  if (n <= 8) f(Width<8>{});
+  else if (n <= 16) f(Width<16>{});
+  else if (n <= 24) f(Width<24>{});
+  else f(Width<32>{});
+}
+
 // Largest-|entry| of each of the first r columns of U (rows x r, stride ld) made positive;
 // the sign is recorded in sgn[c] (+1/-1) and applied to U.
 __device__ void cta_canon(float* U, int rows, int ld, int r, float* sgn) {
@@ -258,38 +275,67 @@ __global__ void __launch_bounds__(BT, 1)
           __syncthreads();
           cta_canon(U, (int)m, (int)m, r, sgn);
           for (int idx = tid; idx < (int)m * r; idx += BT) cp[idx] = U[idx];
-          for (long long j = tid; j < cols; j += BT) {
-            float acc[BSMALL];
-#pragma unroll
-            for (int c = 0; c < BSMALL; ++c) acc[c] = 0.f;
-            const float* a = src + j * m;
-            for (int i = 0; i < (int)m; ++i) {
-              const float av = a[i];
-#pragma unroll
-              for (int c = 0; c < BSMALL; ++c)
-                if (c < r) acc[c] = fmaf(av, U[i + m * c], acc[c]);
+          by_width(r, [&](auto w) {
+            constexpr int W = decltype(w)::value;
+            float* Ut = S.yq;  // U row-major (m x W, zero beyond r): a row's columns in W/4 float4 loads
+            for (int idx = tid; idx < (int)m * W; idx += BT) {
+              const int i = idx / W, c = idx - i * W;
+              Ut[idx] = c < r ? U[i + m * c] : 0.f;
             }
+            __syncthreads();
+            for (long long j = tid; j < cols; j += BT) {
+              float acc[W];
 #pragma unroll
-            for (int c = 0; c < BSMALL; ++c)
-              if (c < r) dst[j * r + c] = acc[c];
-          }
+              for (int c = 0; c < W; ++c) acc[c] = 0.f;
+              const float* a = src + j * m;
+              for (int i = 0; i < (int)m; ++i) {
+                const float av = a[i];
+                const float4* u4 = reinterpret_cast<const float4*>(Ut + i * W);
+#pragma unroll
+                for (int c4 = 0; c4 < W / 4; ++c4) {
+                  const float4 u = u4[c4];
+                  acc[4 * c4 + 0] = fmaf(av, u.x, acc[4 * c4 + 0]);
+                  acc[4 * c4 + 1] = fmaf(av, u.y, acc[4 * c4 + 1]);
+                  acc[4 * c4 + 2] = fmaf(av, u.z, acc[4 * c4 + 2]);
+                  acc[4 * c4 + 3] = fmaf(av, u.w, acc[4 * c4 + 3]);
+                }
+              }
+#pragma unroll
+              for (int c = 0; c < W; ++c)
+                if (c < r) dst[j * r + c] = acc[c];
+            }
+          });
         } else {
           // cols <= 32 < m: V (cols x cols), U = A V_r / sigma (m x r), next = sigma V_r^T
           for (int c = tid; c < r; c += BT) sig_inv[c] = lam[c] > 0.0 ? (float)(1.0 / sqrt(lam[c])) : 0.f;
-          __syncthreads();
           const int nc = (int)cols;
-          for (long long i = tid; i < m; i += BT) {
-            float arow[BSMALL];
-#pragma unroll
-            for (int q = 0; q < BSMALL; ++q) arow[q] = q < nc ? src[i + m * q] : 0.f;
-            for (int c = 0; c < r; ++c) {
-              float acc = 0.f;
-#pragma unroll
-              for (int q = 0; q < BSMALL; ++q)
-                if (q < nc) acc = fmaf(arow[q], (float)evec[q + nc * c], acc);
-              cp[i + m * c] = acc * sig_inv[c];
+          by_width(nc, [&](auto w) {
+            constexpr int W = decltype(w)::value;
+            float* Vf = S.chunk;  // Vf[c W + q] = V[q][c] in FP32 (zero beyond nc)
+            for (int idx = tid; idx < r * W; idx += BT) {
+              const int c = idx / W, q = idx - c * W;
+              Vf[idx] = q < nc ? (float)evec[q + nc * c] : 0.f;
             }
-          }
+            __syncthreads();
+            for (long long i = tid; i < m; i += BT) {
+              float arow[W];
+#pragma unroll
+              for (int q = 0; q < W; ++q) arow[q] = q < nc ? src[i + m * q] : 0.f;
+              for (int c = 0; c < r; ++c) {
+                const float4* v4 = reinterpret_cast<const float4*>(Vf + c * W);
+                float acc = 0.f;
+#pragma unroll
+                for (int q4 = 0; q4 < W / 4; ++q4) {
+                  const float4 v = v4[q4];
+                  if (4 * q4 + 0 < nc) acc = fmaf(arow[4 * q4 + 0], v.x, acc);
+                  if (4 * q4 + 1 < nc) acc = fmaf(arow[4 * q4 + 1], v.y, acc);
+                  if (4 * q4 + 2 < nc) acc = fmaf(arow[4 * q4 + 2], v.z, acc);
+                  if (4 * q4 + 3 < nc) acc = fmaf(arow[4 * q4 + 3], v.w, acc);
+                }
+                cp[i + m * c] = acc * sig_inv[c];
+              }
+            }
+          });
           __syncthreads();
           // canonical signs on the core columns (global memory), mirrored on the rows of sigma V^T
           cta_canon(cp, (int)m, (int)m, r, sgn);
@@ -307,35 +353,47 @@ __global__ void __launch_bounds__(BT, 1)
         // call (c * cols4 + (j & ~3)) / 4, cols4 = cols rounded up to a multiple of 4.
         const long long cols4 = (cols + 3) & ~3LL;
         const unsigned stream = (unsigned)(t * BMAXD + k);
-        float yacc[BSMALL];
+        by_width(ks, [&](auto w) {
+          constexpr int W = decltype(w)::value;
+          float yacc[W];
 #pragma unroll
-        for (int c = 0; c < BSMALL; ++c) yacc[c] = 0.f;
-        for (long long j0 = 0; j0 < cols; j0 += BCH) {
-          const int nj = (int)min((long long)BCH, cols - j0);
-          __syncthreads();
-          for (int q = tid; q < (BCH / 4) * ks; q += BT) {
-            const int c = q / (BCH / 4), j4 = 4 * (q % (BCH / 4));
-            const float4 g = philox_normal4((unsigned long long)((c * cols4 + j0 + j4) >> 2), stream, seed);
-            S.om[(j4 + 0) * BSMALL + c] = g.x;
-            S.om[(j4 + 1) * BSMALL + c] = g.y;
-            S.om[(j4 + 2) * BSMALL + c] = g.z;
-            S.om[(j4 + 3) * BSMALL + c] = g.w;
-          }
-          __syncthreads();
-          if (tid < mi) {
-            for (int jj = 0; jj < nj; ++jj) {
-              const float av = src[tid + m * (j0 + jj)];
+          for (int c = 0; c < W; ++c) yacc[c] = 0.f;
+          for (long long j0 = 0; j0 < cols; j0 += BCH) {
+            const int nj = (int)min((long long)BCH, cols - j0);
+            __syncthreads();
+            for (int q = tid; q < (BCH / 4) * W; q += BT) {
+              const int c = q / (BCH / 4), j4 = 4 * (q % (BCH / 4));
+              // columns ks..W-1 of the chunk are zero: their accumulators stay finite and unused
+              const float4 g = c < ks
+                                   ? philox_normal4((unsigned long long)((c * cols4 + j0 + j4) >> 2), stream, seed)
+                                   : make_float4(0.f, 0.f, 0.f, 0.f);
+              S.om[(j4 + 0) * BSMALL + c] = g.x;
+              S.om[(j4 + 1) * BSMALL + c] = g.y;
+              S.om[(j4 + 2) * BSMALL + c] = g.z;
+              S.om[(j4 + 3) * BSMALL + c] = g.w;
+            }
+            __syncthreads();
+            if (tid < mi) {
+              for (int jj = 0; jj < nj; ++jj) {
+                const float av = src[tid + m * (j0 + jj)];
+                const float4* o4 = reinterpret_cast<const float4*>(S.om + jj * BSMALL);
 #pragma unroll
-              for (int c = 0; c < BSMALL; ++c)
-                if (c < ks) yacc[c] = fmaf(av, S.om[jj * BSMALL + c], yacc[c]);
+                for (int c4 = 0; c4 < W / 4; ++c4) {
+                  const float4 o = o4[c4];
+                  yacc[4 * c4 + 0] = fmaf(av, o.x, yacc[4 * c4 + 0]);
+                  yacc[4 * c4 + 1] = fmaf(av, o.y, yacc[4 * c4 + 1]);
+                  yacc[4 * c4 + 2] = fmaf(av, o.z, yacc[4 * c4 + 2]);
+                  yacc[4 * c4 + 3] = fmaf(av, o.w, yacc[4 * c4 + 3]);
+                }
+              }
             }
           }
-        }
-        __syncthreads();
-        if (tid < mi)
+          __syncthreads();
+          if (tid < mi)
 #pragma unroll
-          for (int c = 0; c < BSMALL; ++c)
-            if (c < ks) S.yq[tid * SY + c] = yacc[c];
+            for (int c = 0; c < W; ++c)
+              if (c < ks) S.yq[tid * SY + c] = yacc[c];
+        });
         __syncthreads();
         // CholeskyQR2 on Y (rows x ks in shared memory): Gram in FP64, Cholesky, substitution
         for (int pass = 0; pass < 2; ++pass) {
@@ -384,22 +442,36 @@ __global__ void __launch_bounds__(BT, 1)
           __syncthreads();
         }
         // B = Q^T A (ks x cols, column-major in Bg), then W = B B^T in FP64
-        for (long long j = tid; j < cols; j += BT) {
-          float b[BSMALL];
-#pragma unroll
-          for (int c = 0; c < BSMALL; ++c) b[c] = 0.f;
-          const float* a = src + j * m;
-          for (int i = 0; i < mi; ++i) {
-            const float av = a[i];
-            const float* qr = S.yq + i * SY;
-#pragma unroll
-            for (int c = 0; c < BSMALL; ++c)
-              if (c < ks) b[c] = fmaf(av, qr[c], b[c]);
+        by_width(ks, [&](auto w) {
+          constexpr int W = decltype(w)::value;
+          float* Qc = S.chunk;  // Q row-major (mi x W, zero beyond ks): a row in W/4 float4 loads
+          for (int idx = tid; idx < mi * W; idx += BT) {
+            const int i = idx / W, c = idx - i * W;
+            Qc[idx] = c < ks ? S.yq[i * SY + c] : 0.f;
           }
+          __syncthreads();
+          for (long long j = tid; j < cols; j += BT) {
+            float b[W];
 #pragma unroll
-          for (int c = 0; c < BSMALL; ++c)
-            if (c < ks) Bg[j * ks + c] = b[c];
-        }
+            for (int c = 0; c < W; ++c) b[c] = 0.f;
+            const float* a = src + j * m;
+            for (int i = 0; i < mi; ++i) {
+              const float av = a[i];
+              const float4* q4 = reinterpret_cast<const float4*>(Qc + i * W);
+#pragma unroll
+              for (int c4 = 0; c4 < W / 4; ++c4) {
+                const float4 q = q4[c4];
+                b[4 * c4 + 0] = fmaf(av, q.x, b[4 * c4 + 0]);
+                b[4 * c4 + 1] = fmaf(av, q.y, b[4 * c4 + 1]);
+                b[4 * c4 + 2] = fmaf(av, q.z, b[4 * c4 + 2]);
+                b[4 * c4 + 3] = fmaf(av, q.w, b[4 * c4 + 3]);
+              }
+            }
+#pragma unroll
+            for (int c = 0; c < W; ++c)
+              if (c < ks) Bg[j * ks + c] = b[c];
+          }
+        });
         __syncthreads();
         cta_gram(Bg, 1, ks, ks, cols, S.w);  // W = B B^T (vectors = columns of B)
         const int sw = bl_solve<0>(S.w, ks, lam, evec, max_sweeps, S.jac);
@@ -412,28 +484,44 @@ __global__ void __launch_bounds__(BT, 1)
         tails += tail;
         energy = kept;
         // U = Q E_r (m x r) -> canonical signs -> core; next = E_r^T B with the same signs
-        float* U = S.chunk;
-        for (int idx = tid; idx < mi * r; idx += BT) {
-          const int i = idx % mi, c = idx / mi;
-          float acc = 0.f;
-          for (int q = 0; q < ks; ++q) acc = fmaf(S.yq[i * SY + q], (float)evec[q + ks * c], acc);
-          U[idx] = acc;
-        }
-        __syncthreads();
-        cta_canon(U, mi, mi, r, sgn);
-        for (int idx = tid; idx < mi * r; idx += BT) cp[idx] = U[idx];
-        for (long long j = tid; j < cols; j += BT) {
-          float b[BSMALL];
-#pragma unroll
-          for (int q = 0; q < BSMALL; ++q) b[q] = q < ks ? Bg[j * ks + q] : 0.f;
-          for (int c = 0; c < r; ++c) {
-            float acc = 0.f;
-#pragma unroll
-            for (int q = 0; q < BSMALL; ++q)
-              if (q < ks) acc = fmaf(b[q], (float)evec[q + ks * c], acc);
-            dst[j * r + c] = sgn[c] * acc;
+        by_width(ks, [&](auto w) {
+          constexpr int W = decltype(w)::value;
+          // E_r in FP32, Ef[c W + q] = E[q][c] (zero beyond ks), in the eigen-solver's buffer
+          float* Ef = reinterpret_cast<float*>(S.jac);
+          for (int idx = tid; idx < r * W; idx += BT) {
+            const int c = idx / W, q = idx - c * W;
+            Ef[idx] = q < ks ? (float)evec[q + ks * c] : 0.f;
           }
-        }
+          __syncthreads();
+          float* U = S.chunk;
+          for (int idx = tid; idx < mi * r; idx += BT) {
+            const int i = idx % mi, c = idx / mi;
+            float acc = 0.f;
+            for (int q = 0; q < ks; ++q) acc = fmaf(S.yq[i * SY + q], Ef[c * W + q], acc);
+            U[idx] = acc;
+          }
+          __syncthreads();
+          cta_canon(U, mi, mi, r, sgn);
+          for (int idx = tid; idx < mi * r; idx += BT) cp[idx] = U[idx];
+          for (long long j = tid; j < cols; j += BT) {
+            float b[W];
+#pragma unroll
+            for (int q = 0; q < W; ++q) b[q] = q < ks ? Bg[j * ks + q] : 0.f;
+            for (int c = 0; c < r; ++c) {
+              const float4* e4 = reinterpret_cast<const float4*>(Ef + c * W);
+              float acc = 0.f;
+#pragma unroll
+              for (int q4 = 0; q4 < W / 4; ++q4) {
+                const float4 e = e4[q4];
+                if (4 * q4 + 0 < ks) acc = fmaf(b[4 * q4 + 0], e.x, acc);
+                if (4 * q4 + 1 < ks) acc = fmaf(b[4 * q4 + 1], e.y, acc);
+                if (4 * q4 + 2 < ks) acc = fmaf(b[4 * q4 + 2], e.z, acc);
+                if (4 * q4 + 3 < ks) acc = fmaf(b[4 * q4 + 3], e.w, acc);
+              }
+              dst[j * r + c] = sgn[c] * acc;
+            }
+          }
+        });
       } else {
         fail = true;
         if (tid == 0 && st) dev_fail(st, TT_ERR_UNSUPPORTED, t);
