@@ -76,6 +76,11 @@ __device__ double cta_sum(double v, double* red) {
 // W (N x N, row-major, stride N) = sum over `nvec` vectors of v v^T, where component p of
 // vector j is at base[p * ps + j * vs] (N <= BSMALL).  4 x 4 register tiles of the upper
 // triangle, vectors split into groups of threads, groups added in order through W.
+// F32P: products of the FP32 data summed in FP32 over 64 vectors of a thread, then in FP64 (the
+// Grams that feed an eigen-solve: relative errors ~1e-8 of the entries, and no FP64 conversion
+// per product); otherwise FP64 products (CholeskyQR of a sketch, whose condition number the
+// Gram squares).
+template <bool F32P>
 __device__ void cta_gram(const float* __restrict__ base, long long ps, long long vs, int N, long long nvec,
                          double* W) {
   const int tid = threadIdx.x;
@@ -94,6 +99,10 @@ __device__ void cta_gram(const float* __restrict__ base, long long ps, long long
 #pragma unroll
   for (int e = 0; e < 16; ++e) acc[e] = 0.0;
   if (act) {
+    float accf[16];
+#pragma unroll
+    for (int e = 0; e < 16; ++e) accf[e] = 0.f;
+    int cnt = 0;
     for (long long j = g; j < nvec; j += groups) {
       float a[4], b[4];
 #pragma unroll
@@ -102,10 +111,29 @@ __device__ void cta_gram(const float* __restrict__ base, long long ps, long long
         a[p] = ia < N ? base[ia * ps + j * vs] : 0.f;
         b[p] = ib < N ? base[ib * ps + j * vs] : 0.f;
       }
+      if constexpr (F32P) {
 #pragma unroll
-      for (int p = 0; p < 4; ++p)
+        for (int p = 0; p < 4; ++p)
 #pragma unroll
-        for (int q = 0; q < 4; ++q) acc[p * 4 + q] = fma((double)a[p], (double)b[q], acc[p * 4 + q]);
+          for (int q = 0; q < 4; ++q) accf[p * 4 + q] = fmaf(a[p], b[q], accf[p * 4 + q]);
+        if (++cnt == 64) {
+#pragma unroll
+          for (int e = 0; e < 16; ++e) {
+            acc[e] += (double)accf[e];
+            accf[e] = 0.f;
+          }
+          cnt = 0;
+        }
+      } else {
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+          for (int q = 0; q < 4; ++q) acc[p * 4 + q] = fma((double)a[p], (double)b[q], acc[p * 4 + q]);
+      }
+    }
+    if constexpr (F32P) {
+#pragma unroll
+      for (int e = 0; e < 16; ++e) acc[e] += (double)accf[e];
     }
   }
   for (int gg = 0; gg < groups; ++gg) {
@@ -255,8 +283,8 @@ __global__ void __launch_bounds__(BT, 1)
       if (small <= BSMALL) {
         // ---- exact Gram-eigen step ----
         const int N = (int)small;
-        if (m <= cols) cta_gram(src, 1, m, N, cols, S.w);   // W = A A^T, vectors = columns
-        else cta_gram(src, m, 1, N, m, S.w);                // W = A^T A, vectors = rows
+        if (m <= cols) cta_gram<true>(src, 1, m, N, cols, S.w);   // W = A A^T, vectors = columns
+        else cta_gram<true>(src, m, 1, N, m, S.w);                // W = A^T A, vectors = rows
         const int sw = bl_solve<0>(S.w, N, lam, evec, max_sweeps, S.jac);
         if (tid == 0 && st) {
           atomicMax(&st->sweeps, sw);
@@ -284,25 +312,27 @@ __global__ void __launch_bounds__(BT, 1)
             }
             __syncthreads();
             for (long long j = tid; j < cols; j += BT) {
-              float acc[W];
+              uint64_t acc2[W / 2];  // columns (2c, 2c+1) as FP32 pairs (fma.rn.f32x2 per pair)
 #pragma unroll
-              for (int c = 0; c < W; ++c) acc[c] = 0.f;
+              for (int c = 0; c < W / 2; ++c) acc2[c] = 0ull;
               const float* a = src + j * m;
               for (int i = 0; i < (int)m; ++i) {
-                const float av = a[i];
-                const float4* u4 = reinterpret_cast<const float4*>(Ut + i * W);
+                const uint64_t av2 = f2_dup(a[i]);
+                const ulonglong2* u2 = reinterpret_cast<const ulonglong2*>(Ut + i * W);
 #pragma unroll
                 for (int c4 = 0; c4 < W / 4; ++c4) {
-                  const float4 u = u4[c4];
-                  acc[4 * c4 + 0] = fmaf(av, u.x, acc[4 * c4 + 0]);
-                  acc[4 * c4 + 1] = fmaf(av, u.y, acc[4 * c4 + 1]);
-                  acc[4 * c4 + 2] = fmaf(av, u.z, acc[4 * c4 + 2]);
-                  acc[4 * c4 + 3] = fmaf(av, u.w, acc[4 * c4 + 3]);
+                  const ulonglong2 u = u2[c4];
+                  ffma2(acc2[2 * c4 + 0], av2, u.x);
+                  ffma2(acc2[2 * c4 + 1], av2, u.y);
                 }
               }
 #pragma unroll
-              for (int c = 0; c < W; ++c)
-                if (c < r) dst[j * r + c] = acc[c];
+              for (int c2 = 0; c2 < W / 2; ++c2) {
+                float lo, hi;
+                f2_unpack(acc2[c2], lo, hi);
+                if (2 * c2 < r) dst[j * r + 2 * c2] = lo;
+                if (2 * c2 + 1 < r) dst[j * r + 2 * c2 + 1] = hi;
+              }
             }
           });
         } else {
@@ -355,9 +385,9 @@ __global__ void __launch_bounds__(BT, 1)
         const unsigned stream = (unsigned)(t * BMAXD + k);
         by_width(ks, [&](auto w) {
           constexpr int W = decltype(w)::value;
-          float yacc[W];
+          uint64_t yacc2[W / 2];  // sketch columns (2c, 2c+1) as FP32 pairs
 #pragma unroll
-          for (int c = 0; c < W; ++c) yacc[c] = 0.f;
+          for (int c = 0; c < W / 2; ++c) yacc2[c] = 0ull;
           for (long long j0 = 0; j0 < cols; j0 += BCH) {
             const int nj = (int)min((long long)BCH, cols - j0);
             __syncthreads();
@@ -375,15 +405,13 @@ __global__ void __launch_bounds__(BT, 1)
             __syncthreads();
             if (tid < mi) {
               for (int jj = 0; jj < nj; ++jj) {
-                const float av = src[tid + m * (j0 + jj)];
-                const float4* o4 = reinterpret_cast<const float4*>(S.om + jj * BSMALL);
+                const uint64_t av2 = f2_dup(src[tid + m * (j0 + jj)]);
+                const ulonglong2* o2 = reinterpret_cast<const ulonglong2*>(S.om + jj * BSMALL);
 #pragma unroll
                 for (int c4 = 0; c4 < W / 4; ++c4) {
-                  const float4 o = o4[c4];
-                  yacc[4 * c4 + 0] = fmaf(av, o.x, yacc[4 * c4 + 0]);
-                  yacc[4 * c4 + 1] = fmaf(av, o.y, yacc[4 * c4 + 1]);
-                  yacc[4 * c4 + 2] = fmaf(av, o.z, yacc[4 * c4 + 2]);
-                  yacc[4 * c4 + 3] = fmaf(av, o.w, yacc[4 * c4 + 3]);
+                  const ulonglong2 o = o2[c4];
+                  ffma2(yacc2[2 * c4 + 0], av2, o.x);
+                  ffma2(yacc2[2 * c4 + 1], av2, o.y);
                 }
               }
             }
@@ -391,13 +419,17 @@ __global__ void __launch_bounds__(BT, 1)
           __syncthreads();
           if (tid < mi)
 #pragma unroll
-            for (int c = 0; c < W; ++c)
-              if (c < ks) S.yq[tid * SY + c] = yacc[c];
+            for (int c2 = 0; c2 < W / 2; ++c2) {
+              float lo, hi;
+              f2_unpack(yacc2[c2], lo, hi);
+              if (2 * c2 < ks) S.yq[tid * SY + 2 * c2] = lo;
+              if (2 * c2 + 1 < ks) S.yq[tid * SY + 2 * c2 + 1] = hi;
+            }
         });
         __syncthreads();
         // CholeskyQR2 on Y (rows x ks in shared memory): Gram in FP64, Cholesky, substitution
         for (int pass = 0; pass < 2; ++pass) {
-          cta_gram(S.yq, 1, SY, ks, mi, S.w);
+          cta_gram<false>(S.yq, 1, SY, ks, mi, S.w);
           double* Wc = S.w;
           double dmax = 0.0;
           for (int i = 0; i < ks; ++i) dmax = fmax(dmax, Wc[i * ks + i]);
@@ -451,29 +483,31 @@ __global__ void __launch_bounds__(BT, 1)
           }
           __syncthreads();
           for (long long j = tid; j < cols; j += BT) {
-            float b[W];
+            uint64_t b2[W / 2];  // rows (2c, 2c+1) of B as FP32 pairs
 #pragma unroll
-            for (int c = 0; c < W; ++c) b[c] = 0.f;
+            for (int c = 0; c < W / 2; ++c) b2[c] = 0ull;
             const float* a = src + j * m;
             for (int i = 0; i < mi; ++i) {
-              const float av = a[i];
-              const float4* q4 = reinterpret_cast<const float4*>(Qc + i * W);
+              const uint64_t av2 = f2_dup(a[i]);
+              const ulonglong2* q2 = reinterpret_cast<const ulonglong2*>(Qc + i * W);
 #pragma unroll
               for (int c4 = 0; c4 < W / 4; ++c4) {
-                const float4 q = q4[c4];
-                b[4 * c4 + 0] = fmaf(av, q.x, b[4 * c4 + 0]);
-                b[4 * c4 + 1] = fmaf(av, q.y, b[4 * c4 + 1]);
-                b[4 * c4 + 2] = fmaf(av, q.z, b[4 * c4 + 2]);
-                b[4 * c4 + 3] = fmaf(av, q.w, b[4 * c4 + 3]);
+                const ulonglong2 q = q2[c4];
+                ffma2(b2[2 * c4 + 0], av2, q.x);
+                ffma2(b2[2 * c4 + 1], av2, q.y);
               }
             }
 #pragma unroll
-            for (int c = 0; c < W; ++c)
-              if (c < ks) Bg[j * ks + c] = b[c];
+            for (int c2 = 0; c2 < W / 2; ++c2) {
+              float lo, hi;
+              f2_unpack(b2[c2], lo, hi);
+              if (2 * c2 < ks) Bg[j * ks + 2 * c2] = lo;
+              if (2 * c2 + 1 < ks) Bg[j * ks + 2 * c2 + 1] = hi;
+            }
           }
         });
         __syncthreads();
-        cta_gram(Bg, 1, ks, ks, cols, S.w);  // W = B B^T (vectors = columns of B)
+        cta_gram<true>(Bg, 1, ks, ks, cols, S.w);  // W = B B^T (vectors = columns of B)
         const int sw = bl_solve<0>(S.w, ks, lam, evec, max_sweeps, S.jac);
         if (tid == 0 && st) {
           atomicMax(&st->sweeps, sw);
