@@ -91,14 +91,23 @@ def plan_steps(shape, ranks, ring, s=8):
     return steps
 
 
-def chain_flops(shape, ranks, ring, s=8, p=0):
-    """FLOPs the library counts for a fixed-rank chain (same terms as its pass accounting)."""
+def chain_flops(shape, ranks, ring, s=8, p=0, gemm="auto"):
+    """FLOPs the library counts for a fixed-rank chain (same terms as its pass accounting).
+    An exact step over more than 32 rows that truncates (not the TR bond split) and whose Gram
+    runs on the tensor cores (gemm "tc", or "auto" on an unfolding of at least 2^24 elements)
+    replaces the projection by an exact Rayleigh-Ritz refinement on b = r + 16 eigenvectors:
+    Z = A^T U0, the Gram of Z and the next data E_r^T Z^T."""
     fl = 0.0
-    for st in plan_steps(shape, ranks, ring, s):
+    for k, st in enumerate(plan_steps(shape, ranks, ring, s)):
         m, cols, ks, nout = st["m"], st["cols"], st["ks"], st["n_out"]
         if st["path"] == "rows":
             fl += 2.0 * m * m * cols
-            if not st["fold"]:
+            tc = gemm == "tc" or (gemm == "auto" and m * cols >= 1 << 24)
+            refine = tc and m > 32 and st["re"] < m and not (ring and k == 0) and not st["fold"]
+            if refine:
+                b = min(m, st["re"] + 16)
+                fl += 2.0 * m * cols * b + 2.0 * cols * b * b + 2.0 * b * cols * nout
+            elif not st["fold"]:
                 fl += 2.0 * m * cols * nout
         elif st["path"] == "cols":
             fl += 2.0 * m * cols * cols + 2.0 * m * cols * st["rq"]
@@ -629,7 +638,8 @@ def run_reference(args, wl):
         return 0
     xh = host_tensor(wl, args.seed)
     s, p = wl_sp(wl, args)
-    fl = chain_flops(wl["shape"], wl["ranks"], wl["ring"], s, p)
+    gemm = args.gemm if args.gemm is not None else wl.get("gemm", "auto")
+    fl = chain_flops(wl["shape"], wl["ranks"], wl["ring"], s, p, gemm)
     for _ in range(min(args.warmup, 2)):
         cpu_chain(xh, wl, s, p)
     ts = []
@@ -777,7 +787,7 @@ def measure_chain(name, wl, args, dev, local, world, steps, warmup, seed, forms=
         return e.value
 
     err = rel_err_of(list(ranks))
-    fl = chain_flops(shape, ranks, ring, s_ov, p_pw)
+    fl = chain_flops(shape, ranks, ring, s_ov, p_pw, gemm)
     lib_fl = float(stats[-1].flops)
     out = {
         "ms": ms_max, "value": fl * world / (ms_max * 1e-3) / 1e12, "unit": "TFLOP/s", "rel_err": err,

@@ -111,6 +111,7 @@ class Result:
     step_power: list = field(default_factory=list)
     step_attempts: list = field(default_factory=list)
     eps_unmet: int = 0  # eps > 0: unfoldings whose rank bound kept the discarded energy above budget
+    flops: float = 0.0  # arithmetic of the passes the library ran (its own pass accounting)
 
 
 def _opts(gemm, method, oversample, power_iters, seed, flags, max_sweeps):
@@ -186,7 +187,7 @@ def _run(ring: bool, x, ranks, gemm="auto", method="edrsvd", oversample=8, power
                   kernels=st.kernels, jacobi_sweeps=st.jacobi_sweeps, est_rel_err=st.est_rel_err,
                   passes=st.passes, fallbacks=st.fallbacks, step_ks=list(st.step_ks[:ns]),
                   step_power=list(st.step_power[:ns]), step_attempts=list(st.step_attempts[:ns]),
-                  eps_unmet=int(st.eps_unmet))
+                  eps_unmet=int(st.eps_unmet), flops=float(st.flops))
 
 
 def tt_svd(x, ranks, **kw) -> Result:

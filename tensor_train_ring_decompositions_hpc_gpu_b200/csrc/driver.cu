@@ -864,7 +864,13 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
       npasses += st.fold ? 1 : 2;
       TT_TRY(pass.run(TT_PASS_GRAM, 2.0 * m * m * cols, 4.0 * m * cols,
                       [&] { return gram_rows(cur, m, cols, B.w, engine, adaptive); }));
-      TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
+      // A step refined below reads only the span of the top b <= 32 eigenvectors, which the
+      // exact Rayleigh-Ritz then corrects: above 64 rows the subspace solver gives it for a
+      // fraction of the full solve.
+      if (!st.fold && refine_exact(st, engine, adaptive) && m > 64 && refine_width(st) <= 32)
+        TT_TRY(launch_syev_top(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
+      else
+        TT_TRY(launch_syev(B.w, (int)m, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
       k_store_sigma<<<1, 64, 0, s>>>(B.evals, (int)std::min<long long>(m, TT_STATS_MAX_SIGMA), sigdst);
       count_launch();
       TT_TRY(decide((int)m, 0.0));
@@ -1014,7 +1020,12 @@ int run_chain(tt_ctx* c, const float* x_in, Plan P, const tt_opts& o, float* con
           }
           return launch_gram(B.bt, cols, ksa, ksa, 1, B.w, true, ws, s);
         }));
-        TT_TRY(launch_syev(B.w, ksa, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
+        // Fixed ranks keep the first re <= 16 eigenpairs of a wide sketch's Gram: above 64 the
+        // subspace solver's 32 Ritz pairs (the eigenvalues beyond them are reported as 0).
+        if (!adaptive && ksa > 64 && re <= 16)
+          TT_TRY(launch_syev_top(B.w, ksa, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
+        else
+          TT_TRY(launch_syev(B.w, ksa, B.evals, B.evecs, max_sweeps, ws, c->dstat, s));
         k_store_sigma<<<1, 64, 0, s>>>(B.evals, std::min(ksa, TT_STATS_MAX_SIGMA), sigdst);
         count_launch();
         npasses += 2 + 2 * pwa;

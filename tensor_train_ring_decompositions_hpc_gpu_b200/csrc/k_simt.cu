@@ -2532,6 +2532,221 @@ int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sw
 }
 
 // ---------------------------------------------------------------------------------------
+// Leading eigenpairs of a symmetric positive semidefinite W (64 < N <= 128) for steps that use
+// only the first few: orthogonal (subspace) iteration on a block of kSubDim columns, then
+// Rayleigh-Ritz.  One CTA holds W (FP64) and two N x kSubDim blocks in shared memory (column-major,
+// column stride NP = N rounded up to even, the pad row zero).  The start block is Philox
+// Gaussian; every second multiplication by W the block is orthonormalised by one CholeskyQR pass
+// (FP64 Gram by a warp per entry, right-looking Cholesky, forward substitution with each row in
+// registers), and the last basis gets a second pass (CholeskyQR2).  The projected matrix
+// H = Y^T W Y (kSubDim x kSubDim) goes to the N <= 32 Jacobi solver and the Ritz vectors are Y
+// times its eigenvectors.  The span of the first k Ritz vectors converges to W's leading
+// k-dimensional invariant subspace as (lambda_{kSubDim+1} / lambda_k)^kSubMults.
+// ---------------------------------------------------------------------------------------
+constexpr int kSubDim = 32;
+constexpr int kSubMults = 16;
+
+// Y = an orthonormal basis of span(Y), in place.  Columns whose pivot is below 1e-28 of the
+// largest diagonal of Y^T Y (directions W annihilates) come out zero.
+__device__ void sub_cholqr(double* Y, int NP, double* G, double* rf) {
+  constexpr int B = kSubDim;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  for (int e = warp; e < B * (B + 1) / 2; e += nw) {
+    int p = 0, rem = e;
+    while (rem >= B - p) {
+      rem -= B - p;
+      ++p;
+    }
+    const int q = p + rem;
+    double acc = 0.0;
+    for (int i = lane; i < NP; i += 32) acc = fma(Y[p * NP + i], Y[q * NP + i], acc);
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if (lane == 0) {
+      G[p * B + q] = acc;
+      G[q * B + p] = acc;
+    }
+  }
+  __syncthreads();
+  double dmax = 0.0;
+  for (int i = 0; i < B; ++i) dmax = fmax(dmax, G[i * B + i]);
+  const double tol = 1e-28 * dmax;
+  // right-looking Cholesky on the upper triangle (row kk is final after step kk)
+  for (int kk = 0; kk < B; ++kk) {
+    const double dk = G[kk * B + kk];
+    if (dk > tol && dmax > 0.0) {
+      const int j = kk + 1 + lane;
+      if (j < B) {
+        const double wkj = G[kk * B + j] / dk;
+        for (int i = kk + 1 + warp; i <= j; i += nw) G[i * B + j] -= G[kk * B + i] * wkj;
+      }
+    }
+    __syncthreads();
+  }
+  // rf[kk B + c] = R[kk][c] (kk < c, live pivots), rf[B B + c] = 1 / R[c][c] (0: dead column)
+  for (int idx = tid; idx < B * B + B; idx += blockDim.x) {
+    if (idx < B * B) {
+      const int kk = idx / B, c = idx - kk * B;
+      const double dk = G[kk * B + kk];
+      rf[idx] = (kk < c && dk > tol && dmax > 0.0) ? G[kk * B + c] / sqrt(dk) : 0.0;
+    } else {
+      const double dc = G[(idx - B * B) * (B + 1)];
+      rf[idx] = (dc > tol && dmax > 0.0) ? 1.0 / sqrt(dc) : 0.0;
+    }
+  }
+  __syncthreads();
+  for (int i = tid; i < NP; i += blockDim.x) {  // row i: y R = z (forward substitution)
+    double y[B];
+#pragma unroll
+    for (int c = 0; c < B; ++c) {
+      double a0 = Y[c * NP + i], a1 = 0.0;
+#pragma unroll
+      for (int kk = 0; kk < c; ++kk) {
+        if (kk & 1) a1 = fma(-y[kk], rf[kk * B + c], a1);
+        else a0 = fma(-y[kk], rf[kk * B + c], a0);
+      }
+      y[c] = (a0 + a1) * rf[B * B + c];
+    }
+#pragma unroll
+    for (int c = 0; c < B; ++c) Y[c * NP + i] = y[c];
+  }
+  __syncthreads();
+}
+
+// Z = W Y (NP x kSubDim): thread (i, g) computes rows i and i + NP/2 for columns 8g .. 8g + 7,
+// two k at a time (Y's column pairs as 16-byte broadcasts, W's rows read as its columns).
+__device__ void sub_mult(const double* __restrict__ W, const double* __restrict__ Y, double* __restrict__ Z,
+                         int NP) {
+  const int H = NP / 2, tid = threadIdx.x;
+  if (tid < 4 * H) {
+    const int i = tid % H, g = tid / H;
+    double a0[8], a1[8];
+#pragma unroll
+    for (int j = 0; j < 8; ++j) a0[j] = a1[j] = 0.0;
+    const double* y0 = Y + (size_t)(8 * g) * NP;
+    for (int k = 0; k < NP; k += 2) {
+      const double w00 = W[k * NP + i], w01 = W[(k + 1) * NP + i];
+      const double w10 = W[k * NP + i + H], w11 = W[(k + 1) * NP + i + H];
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const double2 y = *reinterpret_cast<const double2*>(y0 + j * NP + k);
+        a0[j] = fma(w01, y.y, fma(w00, y.x, a0[j]));
+        a1[j] = fma(w11, y.y, fma(w10, y.x, a1[j]));
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      Z[(8 * g + j) * NP + i] = a0[j];
+      Z[(8 * g + j) * NP + i + H] = a1[j];
+    }
+  }
+  __syncthreads();
+}
+
+__global__ void __launch_bounds__(512, 1) k_subspace_iter(const double* __restrict__ w_in, int N,
+                                                           unsigned long long seed, double* __restrict__ y_out,
+                                                           double* __restrict__ h_out) {
+  extern __shared__ __align__(16) double sm_sub[];
+  constexpr int B = kSubDim;
+  const int NP = N + (N & 1);
+  double* Ws = sm_sub;           // NP x NP
+  double* Ys = Ws + NP * NP;     // NP x B
+  double* Zs = Ys + NP * B;      // NP x B
+  double* G = Zs + NP * B;       // B x B
+  double* rf = G + B * B;        // B x B + B
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = blockDim.x >> 5;
+  for (int idx = tid; idx < NP * NP; idx += blockDim.x) {
+    const int i = idx % NP, k = idx / NP;
+    Ws[idx] = (i < N && k < N) ? 0.5 * (w_in[i + (long long)N * k] + w_in[k + (long long)N * i]) : 0.0;
+  }
+  for (int q = tid; q < NP * (B / 4); q += blockDim.x) {
+    const int i = q % NP, c4 = 4 * (q / NP);
+    const float4 g = philox_normal4((unsigned long long)q, 0x5ab5u, seed);
+    const bool live = i < N;
+    Ys[(c4 + 0) * NP + i] = live ? g.x : 0.0;
+    Ys[(c4 + 1) * NP + i] = live ? g.y : 0.0;
+    Ys[(c4 + 2) * NP + i] = live ? g.z : 0.0;
+    Ys[(c4 + 3) * NP + i] = live ? g.w : 0.0;
+  }
+  __syncthreads();
+  sub_cholqr(Ys, NP, G, rf);
+  for (int it = 0; it < kSubMults / 2; ++it) {
+    sub_mult(Ws, Ys, Zs, NP);
+    sub_mult(Ws, Zs, Ys, NP);
+    sub_cholqr(Ys, NP, G, rf);
+  }
+  sub_cholqr(Ys, NP, G, rf);
+  sub_mult(Ws, Ys, Zs, NP);
+  // H = Y^T Z symmetrised (a warp per entry), Y out column-major N x B
+  for (int e = warp; e < B * (B + 1) / 2; e += nw) {
+    int p = 0, rem = e;
+    while (rem >= B - p) {
+      rem -= B - p;
+      ++p;
+    }
+    const int q = p + rem;
+    double a = 0.0;
+    for (int i = lane; i < NP; i += 32)
+      a = fma(Ys[p * NP + i], Zs[q * NP + i], fma(Ys[q * NP + i], Zs[p * NP + i], a));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) a += __shfl_xor_sync(0xffffffffu, a, o);
+    if (lane == 0) {
+      h_out[p + B * q] = 0.5 * a;
+      h_out[q + B * p] = 0.5 * a;
+    }
+  }
+  for (int idx = tid; idx < N * B; idx += blockDim.x) {
+    const int i = idx % N, c = idx / N;
+    y_out[idx] = Ys[c * NP + i];
+  }
+}
+
+// evecs (N x N) = [Y E, 0], evals = [lambda(H), 0]: the kSubDim Ritz pairs, zero beyond them.
+__global__ void k_ritz(const double* __restrict__ y, const double* __restrict__ eh, const double* __restrict__ lh,
+                       int N, double* __restrict__ evals, double* __restrict__ evecs) {
+  constexpr int B = kSubDim;
+  for (long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x; idx < (long long)N * N;
+       idx += (long long)gridDim.x * blockDim.x) {
+    const int i = (int)(idx % N), j = (int)(idx / N);
+    double v = 0.0;
+    if (j < B)
+      for (int c = 0; c < B; ++c) v = fma(y[i + (long long)N * c], eh[c + B * j], v);
+    evecs[idx] = v;
+    if (i == 0) evals[j] = j < B ? lh[j] : 0.0;
+  }
+}
+
+size_t syev_top_smem(int N) {
+  const size_t np = (size_t)(N + (N & 1));
+  return (np * np + 2 * np * kSubDim + 2 * (size_t)kSubDim * kSubDim + kSubDim) * sizeof(double);
+}
+
+int launch_syev_top(const double* w, int N, double* evals, double* evecs, int max_sweeps, Arena& ws,
+                    DevStatus* st, cudaStream_t s) {
+  if (N <= 64 || N > TT_MAX_SMALL) return launch_syev(w, N, evals, evecs, max_sweeps, ws, st, s);
+  const size_t mk = ws.mark();
+  double* y = ws.take<double>((size_t)N * kSubDim);
+  double* h = ws.take<double>((size_t)kSubDim * kSubDim);
+  double* eh = ws.take<double>((size_t)kSubDim * kSubDim);
+  double* lh = ws.take<double>(kSubDim);
+  if (!y || !h || !eh || !lh) {
+    set_error(TT_ERR_NOMEM, "subspace eigen-solver workspace");
+    return TT_ERR_NOMEM;
+  }
+  const size_t shm = syev_top_smem(N);
+  TT_TRY(smem_optin_k(k_subspace_iter, shm));
+  k_subspace_iter<<<1, 512, shm, s>>>(w, N, 0x7c3a9e15ull, y, h);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  TT_TRY(launch_syev(h, kSubDim, lh, eh, max_sweeps, ws, st, s));
+  k_ritz<<<ceil_div(N * N, 256), 256, 0, s>>>(y, eh, lh, N, evals, evecs);
+  count_launch();
+  TT_LAUNCH_CHECK();
+  ws.reset(mk);
+  return TT_OK;
+}
+
+// ---------------------------------------------------------------------------------------
 // TR bond permute (r0, r1, n) -> (r1, n, r0), staged through shared memory
 // ---------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_permute231(const float* __restrict__ in,

@@ -70,6 +70,11 @@ size_t syev_ws_bytes(int N, int max_sweeps);
 // Symmetric eigen-decomposition by parallel cyclic Jacobi (FP64, N <= 128), eigenvalues descending.
 int launch_syev(const double* w, int N, double* evals, double* evecs, int max_sweeps,
                 Arena& ws, DevStatus* st, cudaStream_t s);
+// Leading eigenpairs for 64 < N <= 128 when at most the first 16 are used: the kSubDim = 32
+// Ritz pairs of a subspace iteration (columns and eigenvalues beyond them zero); other N take
+// launch_syev.
+int launch_syev_top(const double* w, int N, double* evals, double* evecs, int max_sweeps,
+                    Arena& ws, DevStatus* st, cudaStream_t s);
 
 // out (r0, r1, n) -> (r1, n, r0) column-major.
 int launch_permute231(const float* in, float* out, int r0, int r1, long long n, cudaStream_t s);

@@ -107,6 +107,26 @@ def test_tr_parity(gpu, gemm, shape, ranks):
     _check(x, res, ref_cores, ref_sig, ring=True, ranks=list(ranks), gemm=gemm)
 
 
+@pytest.mark.parametrize("shape,gemm", [
+    # unfoldings 2-4: exact 128-row steps refined by Rayleigh-Ritz on the tensor cores, the span
+    # they refine taken from the subspace eigen-solver
+    ((32, 32, 16, 16, 16, 8), "tc"),
+    # unfolding 3: a 256-row randomized step with an 80-wide sketch (leading eigenpairs of its
+    # B B^T from the subspace eigen-solver); unfolding 4: an exact 128-row refined step
+    ((32, 16, 32, 16, 16, 8), "tc"),
+])
+def test_tr_wide_sketch_leading_eigenpairs(gpu, shape, gemm):
+    """The configuration of the 32^6 ring (bond ranks 8, first split 64, oversampling 72, one
+    power iteration) at smaller sizes: every later unfolding keeps 8 of up to 64 significant
+    components, from eigen-solves of 80- and 128-wide Grams."""
+    ttr = _ttr()
+    x = oracle.make_tr_tensor(list(shape), 8, 1e-4, seed=19).astype(np.float64)
+    ranks = [8] * 7
+    res = ttr.tr_svd(_to_dev(x, gpu), ranks, gemm=gemm, oversample=72, power_iters=1)
+    ref_cores, ref_sig = oracle.tr_svd(x, ranks)
+    _check(x, res, ref_cores, ref_sig, ring=True, ranks=ranks, nsig=8, gemm=gemm)
+
+
 def test_tr_rank_above_first_mode_is_zero_padded(gpu):
     # c3's first split: r0*r1 = 64 > n1 = 32 (scaled down: 4*4 = 16 > n1 = 8)
     ttr = _ttr()
@@ -340,3 +360,29 @@ def test_unfolding1_all_sigma_full_rank(gpu):
     assert len(s) >= 32
     np.testing.assert_allclose(s[:32], s_ref[:32], rtol=1e-4, atol=SIG_FLOOR["auto"] * s_ref[0])
     _check(x, res, ref_cores, ref_sig, ring=False, ranks=ranks)
+
+
+@pytest.mark.parametrize("ring,shape,ranks,s,p,gemm", [
+    # TT: full-rank fold of unfolding 1, tensor-core randomized steps, exact small steps
+    (False, [32, 32, 32, 16, 16, 16], [1, 32, 32, 32, 16, 16, 1], 8, 0, "auto"),
+    # TR: bond split with row compaction; at s = 72 the 128-row unfolding 2 is an exact step
+    # refined by Rayleigh-Ritz on the tensor-core engine, and projected plainly on FP32
+    (True, [32, 32, 16, 16, 16, 16], [8] * 7, 72, 1, "auto"),
+    (True, [32, 32, 16, 16, 16, 16], [8] * 7, 72, 1, "fp32"),
+    (True, [32, 32, 16, 16, 16, 16], [8] * 7, 72, 1, "tc"),
+    # order 3, plain FP32 EDrSVD with a power iteration (the 256^3 workload's form)
+    (False, [128, 128, 128], [1, 16, 16, 1], 8, 1, "fp32"),
+])
+def test_bench_flop_model_matches_library(gpu, ring, shape, ranks, s, p, gemm):
+    """The TFLOP/s numerator of bench.py (chain_flops, a host mirror of the plan) equals the
+    arithmetic the library's pass accounting reports for the same fixed-rank chain."""
+    import torch
+    import bench
+    ttr = _ttr()
+    x = torch.randn(int(np.prod(shape)), device=gpu, dtype=torch.float32)
+    fn = ttr.tr_svd if ring else ttr.tt_svd
+    res = fn(x, ranks, shape=shape, gemm=gemm, oversample=s, power_iters=p)
+    torch.cuda.synchronize()
+    model = bench.chain_flops(shape, ranks, ring, s, p, gemm)
+    assert res.flops > 0
+    assert abs(model - res.flops) <= 1e-9 * res.flops, (model, res.flops)
