@@ -434,6 +434,7 @@ __global__ void __launch_bounds__(BT, 1)
           double dmax = 0.0;
           for (int i = 0; i < ks; ++i) dmax = fmax(dmax, Wc[i * ks + i]);
           const double tol = 1e-12 * dmax;
+          __syncthreads();  // every thread has read the diagonal before the first update changes it
           for (int kk = 0; kk < ks; ++kk) {
             const double dk = Wc[kk * ks + kk];
             if (dk > tol && dmax > 0.0) {

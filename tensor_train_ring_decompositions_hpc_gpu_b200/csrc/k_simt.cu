@@ -1946,6 +1946,7 @@ __global__ void __launch_bounds__(NP > 64 ? 256 : 512) k_cholqr2_small(float* __
     double dmax = 0.0;
     for (int k = 0; k < N; ++k) dmax = fmax(dmax, W[k * N + k]);
     const double tol = rel_tol * dmax;
+    __syncthreads();  // every thread has read the diagonal before the first update changes it
     for (int k = 0; k < N; ++k) {
       const double d = W[k * N + k];
       if (d > tol && dmax > 0.0) {
@@ -2571,6 +2572,7 @@ __device__ void sub_cholqr(double* Y, int NP, double* G, double* rf) {
   double dmax = 0.0;
   for (int i = 0; i < B; ++i) dmax = fmax(dmax, G[i * B + i]);
   const double tol = 1e-28 * dmax;
+  __syncthreads();  // every thread has read the diagonal before the first update changes it
   // right-looking Cholesky on the upper triangle (row kk is final after step kk)
   for (int kk = 0; kk < B; ++kk) {
     const double dk = G[kk * B + kk];
