@@ -839,7 +839,7 @@ def measure_chain(name, wl, args, dev, local, world, steps, warmup, seed, forms=
                       "d2h_bytes_per_step": int(sum(t.numel() * 4 for t in hc)), "steps": e2e_steps}
         del xh, hc
 
-    # The north-star comparison on the same tensor and GPU, every engine at the same (s, p):
+    # The forms of one decomposition on the same tensor and GPU, every engine at the same (s, p):
     # the plain FP32 form (FP32 CUDA-core GEMMs, the reference's EDrSVD defaults s = 8, p = 1),
     # the tensor-core form at p = 0 and 1, and the learned form (eps = 1e-3, the caller's ranks
     # as bounds, the shipped predictor choosing sketch width and power count per randomized step).

@@ -1,7 +1,7 @@
 """NumPy restatement of the reference's TT-SVD / TR-SVD algorithms (FP64 by default).
 
-TEST INFRASTRUCTURE ONLY: the checker for the CUDA path and the timed CPU
-baseline.  The product never imports this file.
+TEST INFRASTRUCTURE ONLY: the FP64 results the CUDA path is compared with, and
+the timed CPU baseline.  The product never imports this file.
 
 Parity status: PINNED.  ``tr_svd(..., convention="python")`` and
 ``tt_svd(..., convention="python")`` are checked bit-for-bit-equivalent
